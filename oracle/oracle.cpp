@@ -1,0 +1,766 @@
+// oracle.cpp -- CPU oracle (TEST INFRASTRUCTURE ONLY; see oracle.h).
+//
+// Compiled with -ffp-contract=off so every float expression rounds exactly as
+// written; the CUDA kernels spell the same intersection arithmetic with
+// explicit round-to-nearest intrinsics, which makes hit ids and t bit-exact.
+#include "oracle.h"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <atomic>
+#include <thread>
+#include <vector>
+
+namespace {
+
+struct V3 { float x, y, z; };
+struct Tri { V3 v0, v1, v2; };
+struct Box { V3 mn, mx; };
+
+// triAABB / mergeAABB / saArea: layer/cuda_bvh_backend.cu:186-197
+Box tri_box(const Tri& t) {
+    return {{fminf(fminf(t.v0.x, t.v1.x), t.v2.x), fminf(fminf(t.v0.y, t.v1.y), t.v2.y),
+             fminf(fminf(t.v0.z, t.v1.z), t.v2.z)},
+            {fmaxf(fmaxf(t.v0.x, t.v1.x), t.v2.x), fmaxf(fmaxf(t.v0.y, t.v1.y), t.v2.y),
+             fmaxf(fmaxf(t.v0.z, t.v1.z), t.v2.z)}};
+}
+Box merge(const Box& a, const Box& b) {
+    return {{fminf(a.mn.x, b.mn.x), fminf(a.mn.y, b.mn.y), fminf(a.mn.z, b.mn.z)},
+            {fmaxf(a.mx.x, b.mx.x), fmaxf(a.mx.y, b.mx.y), fmaxf(a.mx.z, b.mx.z)}};
+}
+float area(const Box& b) {
+    float dx = b.mx.x - b.mn.x, dy = b.mx.y - b.mn.y, dz = b.mx.z - b.mn.z;
+    return 2.f * (dx * dy + dy * dz + dz * dx);
+}
+inline float axis(const V3& v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
+
+struct Node2 { Box box; int left, right, tri_start, tri_count; };
+
+// Binned-SAH BVH2: layer/cuda_bvh_backend.cu:201-251 (NB=16, leaf<=3) and
+// cuda_rt_v40.cu:790-840 (NB=32, maxLeaf).  Same split search, same sort,
+// same fallbacks, so the output is byte-identical to the reference's.
+struct Builder {
+    int nbins = 16, max_leaf = 3;
+    std::vector<Node2> nodes;
+    std::vector<Tri> ordered;
+    std::vector<int> orig;
+    std::vector<Box> pbox;
+    std::vector<V3> cent;
+    const Tri* src = nullptr;
+
+    void build(const Tri* t, int n) {
+        src = t;
+        pbox.resize(n);
+        cent.resize(n);
+        nodes.reserve((size_t)n * 2);
+        for (int i = 0; i < n; i++) {
+            pbox[i] = tri_box(t[i]);
+            cent[i] = {(pbox[i].mn.x + pbox[i].mx.x) * .5f, (pbox[i].mn.y + pbox[i].mx.y) * .5f,
+                       (pbox[i].mn.z + pbox[i].mx.z) * .5f};
+        }
+        std::vector<int> idx(n);
+        for (int i = 0; i < n; i++) idx[i] = i;
+        if (n > 0) rec(idx, 0, n);
+    }
+
+    int rec(std::vector<int>& idx, int s, int e) {
+        Node2 nd;
+        nd.tri_start = nd.tri_count = nd.left = nd.right = 0;
+        nd.box = pbox[idx[s]];
+        for (int i = s + 1; i < e; i++) nd.box = merge(nd.box, pbox[idx[i]]);
+        int cnt = e - s;
+        if (cnt <= max_leaf) {
+            nd.tri_start = (int)ordered.size();
+            nd.tri_count = cnt;
+            for (int i = s; i < e; i++) { ordered.push_back(src[idx[i]]); orig.push_back(idx[i]); }
+            nodes.push_back(nd);
+            return (int)nodes.size() - 1;
+        }
+        const int NB = nbins;
+        float best_cost = 1e30f;
+        int best_axis = 0, best_split = s + cnt / 2;
+        float pA = area(nd.box);
+        std::vector<Box> lb(NB), rb(NB);
+        std::vector<int> lc(NB), rc(NB);
+        for (int ax = 0; ax < 3; ax++) {
+            float cmin = 1e30f, cmax = -1e30f;
+            for (int i = s; i < e; i++) {
+                float c = axis(cent[idx[i]], ax);
+                cmin = fminf(cmin, c);
+                cmax = fmaxf(cmax, c);
+            }
+            if (cmax - cmin < 1e-8f) continue;
+            for (int b = 0; b < NB; b++) {
+                lb[b].mn = {1e30f, 1e30f, 1e30f}; lb[b].mx = {-1e30f, -1e30f, -1e30f}; lc[b] = 0;
+                rb[b].mn = {1e30f, 1e30f, 1e30f}; rb[b].mx = {-1e30f, -1e30f, -1e30f}; rc[b] = 0;
+            }
+            for (int i = s; i < e; i++) {
+                float c = axis(cent[idx[i]], ax);
+                int b = (int)((c - cmin) / (cmax - cmin) * (NB - 1));
+                b = b < 0 ? 0 : (b >= NB ? NB - 1 : b);
+                lb[b] = (lc[b] == 0) ? pbox[idx[i]] : merge(lb[b], pbox[idx[i]]);
+                lc[b]++;
+            }
+            for (int b = 1; b < NB; b++) {
+                if (lc[b] && lc[b - 1]) lb[b] = merge(lb[b], lb[b - 1]);
+                else if (lc[b - 1]) lb[b] = lb[b - 1];
+                lc[b] += lc[b - 1];
+            }
+            for (int i = e - 1; i >= s; i--) {
+                float c = axis(cent[idx[i]], ax);
+                int b = (int)((c - cmin) / (cmax - cmin) * (NB - 1));
+                b = b < 0 ? 0 : (b >= NB ? NB - 1 : b);
+                rb[b] = (rc[b] == 0) ? pbox[idx[i]] : merge(rb[b], pbox[idx[i]]);
+                rc[b]++;
+            }
+            for (int b = NB - 2; b >= 0; b--) {
+                if (rc[b] && rc[b + 1]) rb[b] = merge(rb[b], rb[b + 1]);
+                else if (rc[b + 1]) rb[b] = rb[b + 1];
+                rc[b] += rc[b + 1];
+            }
+            for (int b = 0; b < NB - 1; b++) {
+                if (lc[b] == 0 || rc[b + 1] == 0) continue;
+                float cost = lc[b] * area(lb[b]) / pA + rc[b + 1] * area(rb[b + 1]) / pA + 1.f;
+                if (cost < best_cost) {
+                    best_cost = cost;
+                    best_axis = ax;
+                    float split_c = cmin + (b + 1.f) / NB * (cmax - cmin);
+                    best_split = s;
+                    for (int i = s; i < e; i++)
+                        if (axis(cent[idx[i]], ax) < split_c) best_split++;
+                    best_split = best_split <= s ? s + 1 : (best_split >= e ? e - 1 : best_split);
+                }
+            }
+        }
+        if (best_split <= s) best_split = s + 1;
+        if (best_split >= e) best_split = e - 1;
+        const int ba = best_axis;
+        std::sort(idx.begin() + s, idx.begin() + e,
+                  [&](int a, int b) { return axis(cent[a], ba) < axis(cent[b], ba); });
+        int id = (int)nodes.size();
+        nodes.push_back(nd);
+        int l = rec(idx, s, best_split);
+        int r = rec(idx, best_split, e);
+        nodes[id].left = l;
+        nodes[id].right = r;
+        return id;
+    }
+};
+
+// BVH4 node with fp16 bounds: layer/cuda_bvh_backend.cu:31-34
+struct B4 { uint16_t bx[8], by[8], bz[8]; int child[4]; };
+static_assert(sizeof(B4) == 64, "BVH4 node is 64 bytes");
+
+uint16_t f2h(float f) {
+    _Float16 h = (_Float16)f;  // IEEE binary16, round to nearest even
+    uint16_t u;
+    memcpy(&u, &h, 2);
+    return u;
+}
+
+// collapseToB4: layer/cuda_bvh_backend.cu:391-418
+int collapse_b4(const Builder& b2, int ni, B4* out, int& cnt) {
+    const Node2& n = b2.nodes[ni];
+    if (n.tri_count > 0) return -((n.tri_start << 3) | (n.tri_count - 1)) - 2;
+    int gather[4], ng = 0;
+    int ch[2] = {n.left, n.right};
+    for (int c = 0; c < 2; c++) {
+        const Node2& cn = b2.nodes[ch[c]];
+        if (cn.tri_count > 0 || ng >= 3) { gather[ng++] = ch[c]; continue; }
+        gather[ng++] = cn.left;
+        gather[ng++] = cn.right;
+    }
+    B4 nd;
+    for (int i = 0; i < 4; i++) {
+        if (i < ng) {
+            const Node2& cn = b2.nodes[gather[i]];
+            nd.bx[i] = f2h(cn.box.mn.x); nd.bx[4 + i] = f2h(cn.box.mx.x);
+            nd.by[i] = f2h(cn.box.mn.y); nd.by[4 + i] = f2h(cn.box.mx.y);
+            nd.bz[i] = f2h(cn.box.mn.z); nd.bz[4 + i] = f2h(cn.box.mx.z);
+        } else {
+            nd.bx[i] = f2h(1e30f); nd.bx[4 + i] = f2h(-1e30f);
+            nd.by[i] = f2h(1e30f); nd.by[4 + i] = f2h(-1e30f);
+            nd.bz[i] = f2h(1e30f); nd.bz[4 + i] = f2h(-1e30f);
+        }
+        nd.child[i] = -1;
+    }
+    int me = cnt++;
+    for (int i = 0; i < ng; i++) nd.child[i] = collapse_b4(b2, gather[i], out, cnt);
+    out[me] = nd;
+    return me;
+}
+
+// Preorder numbering + skip pointers: layer/cuda_bvh_backend.cu:462-522 (and
+// the same two-pass scheme at :1632-1687 for the TLAS).  `boxes`, `is_leaf`,
+// `left`, `right`, `leaf_enc` describe any binary tree rooted at node 0.
+template <class NodeVec>
+void dfs_export(const NodeVec& nodes, std::vector<uint32_t>& out) {
+    struct Item { int idx, skip; };
+    std::vector<int> order, skip;
+    std::vector<Item> st;
+    st.push_back({0, -1});
+    while (!st.empty()) {
+        Item it = st.back();
+        st.pop_back();
+        order.push_back(it.idx);
+        skip.push_back(it.skip);
+        const auto& n = nodes[it.idx];
+        if (n.tri_count == 0) {
+            st.push_back({n.right, it.skip});
+            st.push_back({n.left, -2});
+        }
+    }
+    int m = (int)order.size();
+    std::vector<int> size(m, 1);
+    for (int i = m - 1; i >= 0; i--) {
+        const auto& n = nodes[order[i]];
+        if (n.tri_count == 0) {
+            int l = i + 1;
+            size[i] = 1 + size[l];
+            int r = i + 1 + size[l];
+            if (r < m) size[i] += size[r];
+            if (skip[l] == -2) skip[l] = r;
+        }
+    }
+    out.assign((size_t)m * 8, 0u);
+    for (int i = 0; i < m; i++) {
+        const auto& n = nodes[order[i]];
+        uint32_t* p = &out[(size_t)i * 8];
+        memcpy(p + 0, &n.box.mn.x, 4); memcpy(p + 1, &n.box.mn.y, 4); memcpy(p + 2, &n.box.mn.z, 4);
+        memcpy(p + 3, &n.box.mx.x, 4); memcpy(p + 4, &n.box.mx.y, 4); memcpy(p + 5, &n.box.mx.z, 4);
+        int enc = n.tri_count > 0 ? -((n.tri_start << 3) | (n.tri_count - 1)) - 2 : 0;
+        memcpy(p + 6, &enc, 4);
+        memcpy(p + 7, &skip[i], 4);
+    }
+}
+
+struct Handle {
+    Builder b2;
+    std::vector<uint32_t> dfs;
+    std::vector<float> packed;
+    std::vector<B4> b4;
+    float center[3], extent;
+};
+
+// ---------------- Moller-Trumbore (layer/cuda_bvh_backend.cu:143-157) ----------------
+// Returns true and (t,u,v) when the triangle passes all rejection tests; the
+// caller applies the t-interval.  Every product and sum is one IEEE rounding.
+inline bool mt(const float o[3], const float d[3], const float v0[3], const float e1[3],
+               const float e2[3], float& t, float& u, float& v) {
+    float px = d[1] * e2[2] - d[2] * e2[1];
+    float py = d[2] * e2[0] - d[0] * e2[2];
+    float pz = d[0] * e2[1] - d[1] * e2[0];
+    float det = e1[0] * px + e1[1] * py + e1[2] * pz;
+    if (fabsf(det) < 1e-12f) return false;
+    float inv = 1.f / det;
+    float sx = o[0] - v0[0], sy = o[1] - v0[1], sz = o[2] - v0[2];
+    u = inv * (sx * px + sy * py + sz * pz);
+    if (u < 0.f || u > 1.f) return false;
+    float qx = sy * e1[2] - sz * e1[1];
+    float qy = sz * e1[0] - sx * e1[2];
+    float qz = sx * e1[1] - sy * e1[0];
+    v = inv * (d[0] * qx + d[1] * qy + d[2] * qz);
+    if (v < 0.f || u + v > 1.f) return false;
+    t = inv * (e2[0] * qx + e2[1] * qy + e2[2] * qz);
+    return true;
+}
+
+// Packed triangle i (layer/cuda_bvh_backend.cu:716-735): v0, v1, v2, orig id.
+inline void unpack(const float* p, float v0[3], float e1[3], float e2[3], int& prim) {
+    v0[0] = p[0]; v0[1] = p[1]; v0[2] = p[2];
+    e1[0] = p[3] - p[0]; e1[1] = p[4] - p[1]; e1[2] = p[5] - p[2];
+    e2[0] = p[6] - p[0]; e2[1] = p[7] - p[1]; e2[2] = p[8] - p[2];
+    prim = (int)p[9];
+}
+
+// Conservative slab test, evaluated in double with a relative slack, so the
+// oracle never culls a box that holds an accepted fp32 hit.  Culling only
+// affects speed; the hit set is defined by the triangle test alone.
+struct DRay { double o[3], inv[3]; bool zero[3]; };
+inline DRay dray(const float o[3], const float d[3]) {
+    DRay r;
+    for (int a = 0; a < 3; a++) {
+        r.o[a] = o[a];
+        r.zero[a] = (d[a] == 0.f);
+        r.inv[a] = r.zero[a] ? 0.0 : 1.0 / (double)d[a];
+    }
+    return r;
+}
+inline bool box_hit(const DRay& r, const float* bmin, const float* bmax, double tmin, double tmax) {
+    double tn = -INFINITY, tf = INFINITY;
+    for (int a = 0; a < 3; a++) {
+        double lo = bmin[a], hi = bmax[a];
+        if (r.zero[a]) {
+            double sl = 1e-7 * (fabs(lo) + fabs(hi)) + 1e-30;
+            if (r.o[a] < lo - sl || r.o[a] > hi + sl) return false;
+            continue;
+        }
+        double t1 = (lo - r.o[a]) * r.inv[a], t2 = (hi - r.o[a]) * r.inv[a];
+        tn = std::max(tn, std::min(t1, t2));
+        tf = std::min(tf, std::max(t1, t2));
+    }
+    double sl = 1e-5 * std::max(fabs(tn), fabs(tf)) + 1e-9;
+    if (!(tn <= tf + sl)) return false;
+    if (tf < tmin - sl) return false;
+    if (tn > tmax + 1e-5 * fabs(tmax) + sl) return false;
+    return true;
+}
+
+inline bool closer(float t, int prim, float best_t, int best_prim) {
+    return t < best_t || (t == best_t && prim < best_prim);
+}
+
+// Stackless DFS traversal: layer/shaders/bvh2_stackless.comp:37-76.
+// `any` stops at the first accepted triangle.  Returns the best hit.
+template <bool ANY>
+void trace_dfs_one(const uint32_t* dfs, int nnodes, const float* packed, const OrcRay& ray,
+                   OrcHit& hit, uint64_t* st) {
+    const float* o = ray.org;
+    const float* d = ray.dir;
+    DRay dr = dray(o, d);
+    float best_t = ray.tmax;
+    int best_p = -1;
+    float bu = 0.f, bv = 0.f;
+    uint64_t nvis = 0, ntri = 0;
+    int ni = nnodes > 0 ? 0 : -1;
+    while (ni >= 0 && ni < nnodes) {
+        const uint32_t* w = dfs + (size_t)ni * 8;
+        int leaf_enc, skip;
+        memcpy(&leaf_enc, w + 6, 4);
+        memcpy(&skip, w + 7, 4);
+        float bmin[3], bmax[3];
+        memcpy(bmin, w, 12);
+        memcpy(bmax, w + 3, 12);
+        bool hitbox = box_hit(dr, bmin, bmax, ray.tmin, best_t);
+        if (!hitbox) { ni = skip; continue; }
+        if (leaf_enc == 0) { nvis++; ni = ni + 1; continue; }
+        int enc = -(leaf_enc + 2);
+        int ts = enc >> 3, tc = (enc & 7) + 1;
+        for (int k = 0; k < tc; k++) {
+            float v0[3], e1[3], e2[3];
+            int prim;
+            unpack(packed + (size_t)(ts + k) * 12, v0, e1, e2, prim);
+            float t, u, v;
+            ntri++;
+            if (!mt(o, d, v0, e1, e2, t, u, v)) continue;
+            if (!(t > ray.tmin && t < ray.tmax)) continue;
+            if (ANY) { best_p = prim; best_t = t; bu = u; bv = v; break; }
+            if (best_p < 0 ? (t < best_t) : closer(t, prim, best_t, best_p)) {
+                best_t = t; best_p = prim; bu = u; bv = v;
+            }
+        }
+        if (ANY && best_p >= 0) break;
+        ni = skip;
+    }
+    hit.t = best_p >= 0 ? best_t : INFINITY;
+    hit.prim = best_p;
+    hit.u = best_p >= 0 ? bu : 0.f;
+    hit.v = best_p >= 0 ? bv : 0.f;
+    if (st) { st[0] = nvis; st[1] = ntri; }
+}
+
+// Dynamic-chunk parallel loop over [0, n) on `nthreads` host threads
+// (0 = all hardware threads).
+template <class F>
+void parallel_for(int n, int nthreads, int chunk, F fn) {
+    int nt = nthreads > 0 ? nthreads : (int)std::thread::hardware_concurrency();
+    if (nt < 1) nt = 1;
+    if (nt == 1 || n <= chunk) {
+        for (int i = 0; i < n; i++) fn(i);
+        return;
+    }
+    std::atomic<int> next(0);
+    auto work = [&]() {
+        for (;;) {
+            int s = next.fetch_add(chunk);
+            if (s >= n) break;
+            int e = std::min(n, s + chunk);
+            for (int i = s; i < e; i++) fn(i);
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) th.emplace_back(work);
+    work();
+    for (auto& t : th) t.join();
+}
+
+// ---------------- LBVH for TLAS (layer/cuda_bvh_backend.cu:257-389) ----------------
+uint32_t expand_bits(uint32_t v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+uint32_t morton(float x, float y, float z) {
+    x = fminf(fmaxf(x * 1024.0f, 0.0f), 1023.0f);
+    y = fminf(fmaxf(y * 1024.0f, 0.0f), 1023.0f);
+    z = fminf(fmaxf(z * 1024.0f, 0.0f), 1023.0f);
+    return expand_bits((uint32_t)x) * 4 + expand_bits((uint32_t)y) * 2 + expand_bits((uint32_t)z);
+}
+
+struct LNode { Box box; int left, right, tri_start, tri_count; };
+
+struct LBVH {
+    std::vector<LNode> nodes;
+    std::vector<int> ordered;
+    std::vector<float> sorted;
+    void build(const float* a, int n) {
+        float smin[3] = {1e30f, 1e30f, 1e30f}, smax[3] = {-1e30f, -1e30f, -1e30f};
+        for (int i = 0; i < n; i++)
+            for (int k = 0; k < 3; k++) {
+                float c = (a[i * 6 + k] + a[i * 6 + 3 + k]) * 0.5f;
+                smin[k] = fminf(smin[k], c);
+                smax[k] = fmaxf(smax[k], c);
+            }
+        float inv[3];
+        for (int k = 0; k < 3; k++) inv[k] = (smax[k] - smin[k] > 1e-8f) ? 1.0f / (smax[k] - smin[k]) : 0.0f;
+        std::vector<std::pair<uint32_t, int>> mp(n), tmp(n);
+        for (int i = 0; i < n; i++) {
+            float c[3];
+            for (int k = 0; k < 3; k++) c[k] = (a[i * 6 + k] + a[i * 6 + 3 + k]) * 0.5f;
+            mp[i] = {morton((c[0] - smin[0]) * inv[0], (c[1] - smin[1]) * inv[1], (c[2] - smin[2]) * inv[2]), i};
+        }
+        // stable LSD radix sort, 4 x 8 bits (same order as :309-324)
+        for (int pass = 0; pass < 4; pass++) {
+            int sh = pass * 8;
+            int count[256] = {0}, pre[256];
+            for (int i = 0; i < n; i++) count[(mp[i].first >> sh) & 0xFF]++;
+            pre[0] = 0;
+            for (int i = 1; i < 256; i++) pre[i] = pre[i - 1] + count[i - 1];
+            for (int i = 0; i < n; i++) tmp[pre[(mp[i].first >> sh) & 0xFF]++] = mp[i];
+            mp.swap(tmp);
+        }
+        ordered.resize(n);
+        for (int i = 0; i < n; i++) ordered[i] = mp[i].second;
+        sorted.resize((size_t)n * 6);
+        for (int i = 0; i < n; i++)
+            for (int k = 0; k < 6; k++) sorted[(size_t)i * 6 + k] = a[(size_t)ordered[i] * 6 + k];
+        nodes.reserve((size_t)n * 2);
+        rec(0, n);
+    }
+    int rec(int s, int e) {
+        LNode nd;
+        nd.left = nd.right = nd.tri_start = nd.tri_count = 0;
+        nd.box.mn = {1e30f, 1e30f, 1e30f};
+        nd.box.mx = {-1e30f, -1e30f, -1e30f};
+        int cnt = e - s;
+        if (cnt <= 1) {
+            nd.tri_start = s;
+            nd.tri_count = cnt;
+            for (int i = s; i < e; i++) {
+                nd.box.mn.x = fminf(nd.box.mn.x, sorted[i * 6 + 0]);
+                nd.box.mn.y = fminf(nd.box.mn.y, sorted[i * 6 + 1]);
+                nd.box.mn.z = fminf(nd.box.mn.z, sorted[i * 6 + 2]);
+                nd.box.mx.x = fmaxf(nd.box.mx.x, sorted[i * 6 + 3]);
+                nd.box.mx.y = fmaxf(nd.box.mx.y, sorted[i * 6 + 4]);
+                nd.box.mx.z = fmaxf(nd.box.mx.z, sorted[i * 6 + 5]);
+            }
+            nodes.push_back(nd);
+            return (int)nodes.size() - 1;
+        }
+        int mid = s + cnt / 2;
+        int id = (int)nodes.size();
+        nodes.push_back(nd);
+        int l = rec(s, mid), r = rec(mid, e);
+        nodes[id].left = l;
+        nodes[id].right = r;
+        const Box& L = nodes[l].box;
+        const Box& R = nodes[r].box;
+        nodes[id].box = merge(L, R);
+        return id;
+    }
+};
+
+// Instance ray transform: layer/rt_ir_exec.cu:81-91 (inverse 3x4, row major;
+// the direction is not normalised, so t stays in world units).
+inline void xform_ray(const float* inv, const float o[3], const float d[3], float lo[3], float ld[3]) {
+    lo[0] = inv[0] * o[0] + inv[1] * o[1] + inv[2] * o[2] + inv[3];
+    lo[1] = inv[4] * o[0] + inv[5] * o[1] + inv[6] * o[2] + inv[7];
+    lo[2] = inv[8] * o[0] + inv[9] * o[1] + inv[10] * o[2] + inv[11];
+    ld[0] = inv[0] * d[0] + inv[1] * d[1] + inv[2] * d[2];
+    ld[1] = inv[4] * d[0] + inv[5] * d[1] + inv[6] * d[2];
+    ld[2] = inv[8] * d[0] + inv[9] * d[1] + inv[10] * d[2];
+}
+
+// Two-level traversal (layer/rt_ir_exec.cu:93-189): TLAS leaves hold one
+// instance each (layer/cuda_bvh_backend.cu:353-356); each instance's BLAS is
+// walked in object space.  Ties break on (t, instance, prim).
+template <bool ANY>
+void trace_two_level_one(const uint32_t* tlas, int tn, const int* tord, const float* inv12,
+                         const int* iblas, const uint32_t* bdfs, const int* noff, const float* bpk,
+                         const int* toff, const OrcRay& ray, OrcHit& hit, int& inst_out) {
+    DRay dr = dray(ray.org, ray.dir);
+    float best_t = ray.tmax;
+    int best_p = -1, best_i = -1;
+    float bu = 0.f, bv = 0.f;
+    int ni = tn > 0 ? 0 : -1;
+    bool done = false;
+    while (!done && ni >= 0 && ni < tn) {
+        const uint32_t* w = tlas + (size_t)ni * 8;
+        int leaf_enc, skip;
+        memcpy(&leaf_enc, w + 6, 4);
+        memcpy(&skip, w + 7, 4);
+        float bmin[3], bmax[3];
+        memcpy(bmin, w, 12);
+        memcpy(bmax, w + 3, 12);
+        if (!box_hit(dr, bmin, bmax, ray.tmin, best_t)) { ni = skip; continue; }
+        if (leaf_enc == 0) { ni++; continue; }
+        int enc = -(leaf_enc + 2);
+        int ts = enc >> 3, tc = (enc & 7) + 1;
+        for (int k = 0; k < tc && !done; k++) {
+            int inst = tord[ts + k];
+            int b = iblas[inst];
+            float lo[3], ld[3];
+            xform_ray(inv12 + (size_t)inst * 12, ray.org, ray.dir, lo, ld);
+            DRay lr = dray(lo, ld);
+            const uint32_t* nodes = bdfs + (size_t)noff[b] * 8;
+            int nn = noff[b + 1] - noff[b];
+            const float* pk = bpk + (size_t)toff[b] * 12;
+            int bi = nn > 0 ? 0 : -1;
+            while (bi >= 0 && bi < nn) {
+                const uint32_t* bw = nodes + (size_t)bi * 8;
+                int ble, bsk;
+                memcpy(&ble, bw + 6, 4);
+                memcpy(&bsk, bw + 7, 4);
+                float mn[3], mx[3];
+                memcpy(mn, bw, 12);
+                memcpy(mx, bw + 3, 12);
+                if (!box_hit(lr, mn, mx, ray.tmin, best_t)) { bi = bsk; continue; }
+                if (ble == 0) { bi++; continue; }
+                int be = -(ble + 2);
+                int bts = be >> 3, btc = (be & 7) + 1;
+                for (int j = 0; j < btc; j++) {
+                    float v0[3], e1[3], e2[3];
+                    int prim;
+                    unpack(pk + (size_t)(bts + j) * 12, v0, e1, e2, prim);
+                    float t, u, v;
+                    if (!mt(lo, ld, v0, e1, e2, t, u, v)) continue;
+                    if (!(t > ray.tmin && t < ray.tmax)) continue;
+                    if (ANY) { best_p = prim; best_i = inst; best_t = t; done = true; break; }
+                    bool better = best_p < 0 ? (t < best_t)
+                                             : (t < best_t || (t == best_t && (inst < best_i ||
+                                                (inst == best_i && prim < best_p))));
+                    if (better) { best_t = t; best_p = prim; best_i = inst; bu = u; bv = v; }
+                }
+                if (done) break;
+                bi = bsk;
+            }
+        }
+        ni = skip;
+    }
+    hit.t = best_p >= 0 ? best_t : INFINITY;
+    hit.prim = best_p;
+    hit.u = best_p >= 0 ? bu : 0.f;
+    hit.v = best_p >= 0 ? bv : 0.f;
+    inst_out = best_i;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* orc_build(const float* tris9, int n, int nbins, int max_leaf) {
+    if (!tris9 || n <= 0) return nullptr;
+    Handle* h = new Handle();
+    const Tri* t = reinterpret_cast<const Tri*>(tris9);
+    h->b2.nbins = nbins;
+    h->b2.max_leaf = max_leaf;
+    h->b2.build(t, n);
+    dfs_export(h->b2.nodes, h->dfs);
+    int no = (int)h->b2.ordered.size();
+    h->packed.assign((size_t)no * 12, 0.f);
+    for (int i = 0; i < no; i++) {
+        float* p = &h->packed[(size_t)i * 12];
+        const Tri& tr = h->b2.ordered[i];
+        p[0] = tr.v0.x; p[1] = tr.v0.y; p[2] = tr.v0.z; p[3] = tr.v1.x;
+        p[4] = tr.v1.y; p[5] = tr.v1.z; p[6] = tr.v2.x; p[7] = tr.v2.y;
+        p[8] = tr.v2.z; p[9] = (float)h->b2.orig[i]; p[10] = 0.f; p[11] = 0.f;
+    }
+    h->b4.resize(h->b2.nodes.size());
+    int cnt = 0;
+    collapse_b4(h->b2, 0, h->b4.data(), cnt);
+    h->b4.resize(cnt);
+    float bmin[3] = {1e30f, 1e30f, 1e30f}, bmax[3] = {-1e30f, -1e30f, -1e30f};
+    for (int i = 0; i < n; i++)
+        for (int a = 0; a < 3; a++) {
+            const float* tt = tris9 + (size_t)i * 9;
+            bmin[a] = std::min({bmin[a], tt[a], tt[3 + a], tt[6 + a]});
+            bmax[a] = std::max({bmax[a], tt[a], tt[3 + a], tt[6 + a]});
+        }
+    for (int a = 0; a < 3; a++) h->center[a] = (bmin[a] + bmax[a]) * 0.5f;
+    float ex = bmax[0] - bmin[0], ey = bmax[1] - bmin[1], ez = bmax[2] - bmin[2];
+    h->extent = sqrtf(ex * ex + ey * ey + ez * ez);
+    return h;
+}
+void orc_free(void* h) { delete static_cast<Handle*>(h); }
+int orc_num_bvh2(void* h) { return (int)static_cast<Handle*>(h)->b2.nodes.size(); }
+int orc_num_dfs(void* h) { return (int)(static_cast<Handle*>(h)->dfs.size() / 8); }
+const uint32_t* orc_dfs(void* h) { return static_cast<Handle*>(h)->dfs.data(); }
+int orc_num_packed(void* h) { return (int)(static_cast<Handle*>(h)->packed.size() / 4); }
+const float* orc_packed(void* h) { return static_cast<Handle*>(h)->packed.data(); }
+int orc_num_bvh4(void* h) { return (int)static_cast<Handle*>(h)->b4.size(); }
+const void* orc_bvh4(void* h) { return static_cast<Handle*>(h)->b4.data(); }
+const int* orc_orig_idx(void* h) { return static_cast<Handle*>(h)->b2.orig.data(); }
+void orc_bounds(void* hv, float* cx, float* cy, float* cz, float* extent) {
+    Handle* h = static_cast<Handle*>(hv);
+    *cx = h->center[0]; *cy = h->center[1]; *cz = h->center[2]; *extent = h->extent;
+}
+
+int orc_tlas_fast(const float* aabbs, int n, uint32_t** out_nodes, int** out_ordered) {
+    if (!aabbs || n <= 0 || !out_nodes) return 0;
+    LBVH l;
+    l.build(aabbs, n);
+    std::vector<uint32_t> d;
+    dfs_export(l.nodes, d);
+    *out_nodes = (uint32_t*)malloc(d.size() * 4);
+    memcpy(*out_nodes, d.data(), d.size() * 4);
+    if (out_ordered) {
+        *out_ordered = (int*)malloc((size_t)n * 4);
+        memcpy(*out_ordered, l.ordered.data(), (size_t)n * 4);
+    }
+    return (int)(d.size() / 8);
+}
+void orc_free_ptr(void* p) { free(p); }
+
+void orc_trace_closest_dfs(const uint32_t* dfs, int nnodes, const float* packed, const OrcRay* rays,
+                           int nrays, OrcHit* hits, int nthreads, uint64_t* stats) {
+    parallel_for(nrays, nthreads, 256, [&](int i) {
+        trace_dfs_one<false>(dfs, nnodes, packed, rays[i], hits[i], stats ? stats + (size_t)i * 2 : nullptr);
+    });
+}
+
+void orc_trace_any_dfs(const uint32_t* dfs, int nnodes, const float* packed, const OrcRay* rays,
+                       int nrays, uint8_t* occ, int nthreads) {
+    parallel_for(nrays, nthreads, 256, [&](int i) {
+        OrcHit h;
+        trace_dfs_one<true>(dfs, nnodes, packed, rays[i], h, nullptr);
+        occ[i] = h.prim >= 0 ? 1 : 0;
+    });
+}
+
+void orc_brute_closest(const float* tris9, int ntris, const OrcRay* rays, int nrays, OrcHit* hits,
+                       int nthreads) {
+    parallel_for(nrays, nthreads, 16, [&](int i) {
+        const OrcRay& r = rays[i];
+        float bt = r.tmax, bu = 0.f, bv = 0.f;
+        int bp = -1;
+        for (int k = 0; k < ntris; k++) {
+            const float* p = tris9 + (size_t)k * 9;
+            float v0[3] = {p[0], p[1], p[2]};
+            float e1[3] = {p[3] - p[0], p[4] - p[1], p[5] - p[2]};
+            float e2[3] = {p[6] - p[0], p[7] - p[1], p[8] - p[2]};
+            float t, u, v;
+            if (!mt(r.org, r.dir, v0, e1, e2, t, u, v)) continue;
+            if (!(t > r.tmin && t < r.tmax)) continue;
+            if (bp < 0 ? t < bt : closer(t, k, bt, bp)) { bt = t; bp = k; bu = u; bv = v; }
+        }
+        hits[i].t = bp >= 0 ? bt : INFINITY;
+        hits[i].prim = bp;
+        hits[i].u = bp >= 0 ? bu : 0.f;
+        hits[i].v = bp >= 0 ? bv : 0.f;
+    });
+}
+
+void orc_brute_any(const float* tris9, int ntris, const OrcRay* rays, int nrays, uint8_t* occ,
+                   int nthreads) {
+    parallel_for(nrays, nthreads, 16, [&](int i) {
+        const OrcRay& r = rays[i];
+        uint8_t o = 0;
+        for (int k = 0; k < ntris && !o; k++) {
+            const float* p = tris9 + (size_t)k * 9;
+            float v0[3] = {p[0], p[1], p[2]};
+            float e1[3] = {p[3] - p[0], p[4] - p[1], p[5] - p[2]};
+            float e2[3] = {p[6] - p[0], p[7] - p[1], p[8] - p[2]};
+            float t, u, v;
+            if (mt(r.org, r.dir, v0, e1, e2, t, u, v) && t > r.tmin && t < r.tmax) o = 1;
+        }
+        occ[i] = o;
+    });
+}
+
+void orc_trace_closest_two_level(const uint32_t* tlas, int tlas_nodes, const int* tlas_ordered,
+                                 const float* inv12, const int* inst_blas, int ninst,
+                                 const uint32_t* blas_dfs, const int* node_off,
+                                 const float* blas_packed, const int* tri_off, const OrcRay* rays,
+                                 int nrays, OrcHit* hits, int32_t* inst_out, int nthreads) {
+    (void)ninst;
+    parallel_for(nrays, nthreads, 64, [&](int i) {
+        int inst;
+        trace_two_level_one<false>(tlas, tlas_nodes, tlas_ordered, inv12, inst_blas, blas_dfs, node_off,
+                                   blas_packed, tri_off, rays[i], hits[i], inst);
+        if (inst_out) inst_out[i] = inst;
+    });
+}
+
+void orc_trace_any_two_level(const uint32_t* tlas, int tlas_nodes, const int* tlas_ordered,
+                             const float* inv12, const int* inst_blas, int ninst,
+                             const uint32_t* blas_dfs, const int* node_off, const float* blas_packed,
+                             const int* tri_off, const OrcRay* rays, int nrays, uint8_t* occ,
+                             int nthreads) {
+    (void)ninst;
+    parallel_for(nrays, nthreads, 64, [&](int i) {
+        OrcHit h;
+        int inst;
+        trace_two_level_one<true>(tlas, tlas_nodes, tlas_ordered, inv12, inst_blas, blas_dfs, node_off,
+                                  blas_packed, tri_off, rays[i], h, inst);
+        occ[i] = h.prim >= 0 ? 1 : 0;
+    });
+}
+
+// Philox4x32-10, Salmon et al., "Parallel random numbers: as easy as 1, 2, 3" (SC'11).
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; r++) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        c0 = hi1 ^ c1 ^ k0;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ k1;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+uint16_t orc_f2h_rn(float f) { return f2h(f); }
+
+// Recompute every skip pointer of a stackless DFS export from the tree shape
+// (inner node i: left child i+1, right child i+1+size(left)); skip(i) is the
+// first index after i's subtree, -1 past the end.  The reference's two-pass
+// export (layer/cuda_bvh_backend.cu:488-503, :1652-1663) only resolves the
+// placeholder of left children, so the right descendants of a left child keep
+// skip == -2 and a stackless walk stops there.  The byte-identical
+// restatement above keeps that behaviour; traversal parity uses this fix.
+int orc_fix_skips(uint32_t* dfs, int n) {
+    std::vector<int> size(n, 1);
+    for (int i = n - 1; i >= 0; i--) {
+        int le;
+        memcpy(&le, dfs + (size_t)i * 8 + 6, 4);
+        if (le == 0) {
+            int l = i + 1;
+            if (l >= n) return -1;
+            int r = l + size[l];
+            if (r >= n) return -1;
+            size[i] = 1 + size[l] + size[r];
+        }
+    }
+    int changed = 0;
+    for (int i = 0; i < n; i++) {
+        int sk = i + size[i] < n ? i + size[i] : -1;
+        int old;
+        memcpy(&old, dfs + (size_t)i * 8 + 7, 4);
+        if (old != sk) changed++;
+        memcpy(dfs + (size_t)i * 8 + 7, &sk, 4);
+    }
+    return changed;
+}
+
+}  // extern "C"
