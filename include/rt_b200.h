@@ -1,0 +1,141 @@
+/* rt_b200.h -- extension C-ABI of the B200 ray traversal engine.
+ *
+ * The reference's C-ABI (cuda_bvh_backend.h) has no closest-hit call that
+ * returns primitive ids and barycentrics, no any-hit call, no instanced
+ * (TLAS) trace, and no stream or batch parameters (reference
+ * layer/cuda_bvh_backend.h:26-40 traces with hit distance only, on the
+ * default stream).  These entry points fill those gaps with the same
+ * conventions: opaque handles, plain pointers and sizes, int status (0 ok,
+ * negative error; rtGetLastError() explains the last one on this thread).
+ * `stream` is a cudaStream_t passed as void* (NULL = default stream); every
+ * device-pointer call is asynchronous on that stream.
+ */
+#ifndef RT_B200_H
+#define RT_B200_H
+
+#include <stdint.h>
+
+#include "cuda_bvh_backend.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* A ray: origin, tmin, direction (need not be unit length), tmax.  32 bytes,
+ * 16-byte aligned.  Hits are accepted for tmin < t < tmax.  This is the
+ * reference prototypes' Ray {float4 origin_tmin, float4 dir_tmax}
+ * (cuda_rt_v40.cu:30). */
+typedef struct {
+    float org[3];
+    float tmin;
+    float dir[3];
+    float tmax;
+} RtRay;
+
+/* Closest-hit record, 16 bytes: t (+inf on a miss), the input index of the
+ * hit primitive (-1 on a miss), Moller-Trumbore barycentrics.  Equal t is
+ * resolved toward the lower (instance, primitive) id. */
+typedef struct {
+    float t;
+    int32_t prim;
+    float u;
+    float v;
+} RtHit;
+
+/* Status codes. */
+#define RT_OK 0
+#define RT_ERR_INVALID (-1)   /* bad argument */
+#define RT_ERR_CUDA (-2)      /* CUDA runtime error */
+#define RT_ERR_NOMEM (-3)     /* device allocation failed */
+#define RT_ERR_STACK (-4)     /* traversal stack overflow (never silent) */
+#define RT_ERR_TIMEOUT (-5)   /* a bounded wait ran out */
+#define RT_ERR_CAPACITY (-6)  /* admission / size limit */
+
+/* Message of the last failure on the calling thread ("" if none). */
+const char* rtGetLastError(void);
+
+/* Build from triangles already in device memory (9 floats each); the build
+ * runs on `stream` and the call returns once the structure is ready.
+ * NULL on failure. */
+CudaBVH_t cudaBVH_buildDevice(const CudaTri* d_tris, int numTris, void* stream);
+
+/* Closest hit of n rays (device pointers).  Returns RT_OK or an error. */
+int cudaBVH_traceClosest(CudaBVH_t bvh, const RtRay* d_rays, int n, RtHit* d_hits, void* stream);
+
+/* Any hit (occlusion) of n rays: d_occluded[i] = 1 if some primitive is hit
+ * with tmin < t < tmax, else 0. */
+int cudaBVH_traceAny(CudaBVH_t bvh, const RtRay* d_rays, int n, uint8_t* d_occluded, void* stream);
+
+/* The same two calls on host buffers: copies in, traces, copies out and
+ * waits.  Staging buffers are owned by the handle. */
+int cudaBVH_traceClosestHost(CudaBVH_t bvh, const RtRay* h_rays, int n, RtHit* h_hits);
+int cudaBVH_traceAnyHost(CudaBVH_t bvh, const RtRay* h_rays, int n, uint8_t* h_occluded);
+
+/* Host-side structural check of the built acceleration structure (child
+ * indices, triangle ranges, depth within the traversal stack, every
+ * triangle referenced once).  RT_OK or RT_ERR_INVALID.  Setting the
+ * environment variable RTB200_VALIDATE=1 runs it inside every build. */
+int cudaBVH_validate(CudaBVH_t bvh);
+
+/* Build statistics. */
+typedef struct {
+    int num_tris;
+    int num_bvh2_nodes;     /* binary nodes created by the SAH builder */
+    int num_nodes;          /* compressed 8-wide nodes */
+    int depth;              /* 8-wide levels */
+    int max_leaf;
+    int bins;
+    float build_ms;         /* device time of the build kernels */
+    float sah_cost;         /* SAH cost of the binary tree, normalised by root area */
+    uint64_t node_bytes;    /* bytes of the 8-wide nodes */
+    uint64_t tri_bytes;     /* bytes of the triangle records */
+} RtBuildStats;
+int cudaBVH_getBuildStats(CudaBVH_t bvh, RtBuildStats* out);
+
+/* Device arrays of the 8-wide layout (80-byte nodes, 48-byte triangles),
+ * borrowed, valid until destroy. */
+int cudaBVH_getDeviceLayout(CudaBVH_t bvh, const void** d_nodes, int* num_nodes, const void** d_tris,
+                            int* num_tris);
+
+/* Closest hit with per-ray work counters (d_counts: 2 u32 per ray: nodes
+ * fetched, triangles tested).  Same results as cudaBVH_traceClosest; used to
+ * derive the algorithmic bytes per ray.  any != 0 counts the any-hit walk. */
+int cudaBVH_traceCounters(CudaBVH_t bvh, const RtRay* d_rays, int n, int any, uint32_t* d_counts,
+                          void* stream);
+
+/* ---------------- instanced scenes (TLAS over BLASes) ---------------- */
+typedef struct CudaTLASHandle* CudaTLAS_t;
+
+/* One instance: row-major 3x4 object->world transform, the index of its
+ * BLAS in the array given to cudaTLAS_build, and a user id.  64 bytes.
+ * The layer's packing of VkAccelerationStructureInstanceKHR
+ * (layer/VkLayer_CudaRT.cpp:4517-4558) carries the same fields. */
+typedef struct {
+    float xform[12];
+    int32_t blas;
+    uint32_t mask;
+    uint32_t custom;
+    uint32_t pad;
+} RtInstance;
+
+/* Builds the top level over world-space instance boxes on the GPU.  The
+ * BLAS handles must outlive the TLAS.  NULL on failure. */
+CudaTLAS_t cudaTLAS_build(const CudaBVH_t* blas, int numBlas, const RtInstance* instances, int numInstances);
+void cudaTLAS_destroy(CudaTLAS_t tlas);
+
+/* Closest hit over all instances: d_hits[i].prim is the primitive index in
+ * the hit instance's BLAS, d_inst[i] the instance index (-1 on a miss; may
+ * be NULL).  Rays are transformed by the inverse instance transform without
+ * renormalisation, so t is in world units. */
+int cudaTLAS_traceClosest(CudaTLAS_t tlas, const RtRay* d_rays, int n, RtHit* d_hits, int32_t* d_inst,
+                          void* stream);
+int cudaTLAS_traceAny(CudaTLAS_t tlas, const RtRay* d_rays, int n, uint8_t* d_occluded, void* stream);
+
+/* Inverse transforms (12 floats per instance) the TLAS uses, host copy. */
+int cudaTLAS_getInverseTransforms(CudaTLAS_t tlas, float* out, int numInstances);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RT_B200_H */

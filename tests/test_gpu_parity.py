@@ -1,0 +1,313 @@
+"""GPU parity: the CUDA path through the C-ABI against the CPU oracle.
+
+Bar: hit primitive (and instance) ids, t, u, v bit-identical to the oracle
+(both evaluate Moller-Trumbore of layer/cuda_bvh_backend.cu:143-157 in exact
+IEEE single precision, ties toward the lower id); any-hit flags identical.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from rtb200 import lib, scenes
+from rtb200.scenes import HIT_DTYPE, RAY_DTYPE
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(torch, arr):
+    return torch.from_numpy(np.ascontiguousarray(arr).view(np.uint8).copy()).cuda()
+
+
+def gpu_closest(bvh, rays):
+    import torch
+    d_rays = _dev(torch, rays)
+    d_hits = torch.empty(rays.shape[0] * 16, dtype=torch.uint8, device="cuda")
+    bvh.closest(d_rays, rays.shape[0], d_hits)
+    torch.cuda.synchronize()
+    return d_hits.cpu().numpy().view(HIT_DTYPE)
+
+
+def gpu_any(bvh, rays):
+    import torch
+    d_rays = _dev(torch, rays)
+    d_occ = torch.empty(rays.shape[0], dtype=torch.uint8, device="cuda")
+    bvh.any(d_rays, rays.shape[0], d_occ)
+    torch.cuda.synchronize()
+    return d_occ.cpu().numpy()
+
+
+def assert_hits_equal(a, b, what=""):
+    bad = np.nonzero((a["prim"] != b["prim"]) | (a["t"].view(np.uint32) != b["t"].view(np.uint32)) |
+                     (a["u"].view(np.uint32) != b["u"].view(np.uint32)) |
+                     (a["v"].view(np.uint32) != b["v"].view(np.uint32)))[0]
+    assert bad.size == 0, f"{what}: {bad.size} rays differ, first {bad[:5]}: {a[bad[:3]]} vs {b[bad[:3]]}"
+
+
+@pytest.fixture(scope="module")
+def small_scene():
+    return scenes.scene_spheres_100k(0)[:3002]
+
+
+def test_closest_and_any_small_vs_brute_force(cuda, small_scene):
+    bvh = lib.BVH(small_scene)
+    rays = scenes.random_rays(5, 20000)
+    ref = O.brute_closest(small_scene, rays)
+    assert_hits_equal(gpu_closest(bvh, rays), ref, "device")
+    assert_hits_equal(bvh.closest_host(rays), ref, "host")
+    occ = O.brute_any(small_scene, rays)
+    assert np.array_equal(gpu_any(bvh, rays), occ)
+    assert np.array_equal(bvh.any_host(rays), occ)
+    assert (ref["prim"] >= 0).mean() > 0.2
+
+
+def test_primary_1080p_100k_every_ray(cuda):
+    """100,002 triangles, 1920x1080 pinhole rays; every ray checked."""
+    tris = scenes.scene_spheres_100k(0)
+    bvh = lib.BVH(tris)
+    rays = scenes.primary_1080p()
+    ob = O.OracleBVH(tris, nbins=32, max_leaf=4)
+    ref = ob.closest(rays)
+    got = gpu_closest(bvh, rays)
+    assert_hits_equal(got, ref, "primary 1080p")
+    assert 0.2 < (ref["prim"] >= 0).mean() < 0.95
+
+
+def test_incoherent_rays_vs_oracle(cuda):
+    """configs[1] shape on a 400K-triangle scene: cosine diffuse bounces
+    (closest hit) and area-light shadow rays (any hit) from primary hits."""
+    tris = scenes.scene_meshes(1, 400_000)
+    bvh = lib.BVH(tris)
+    prim = scenes.pinhole_rays(480, 270, scenes.CAM_EYE, scenes.CAM_TARGET)
+    ph = gpu_closest(bvh, prim)
+    p, nrm = scenes.hit_frame(tris, prim, ph)
+    dif = scenes.diffuse_rays(p, nrm, 200_000, seed=3)
+    sha = scenes.shadow_rays(p, nrm, 200_000, seed=4)
+    ob = O.OracleBVH(tris, nbins=32, max_leaf=4)
+    assert_hits_equal(ob.closest(prim), ph, "primary")
+    assert_hits_equal(gpu_closest(bvh, dif), ob.closest(dif), "diffuse")
+    assert np.array_equal(gpu_any(bvh, sha), ob.any(sha))
+
+
+def test_edge_cases(cuda):
+    # axis-aligned box faces, a flat grid, zero-area and duplicate triangles
+    box = scenes.box_mesh(3) * 2.0
+    flat = scenes.ground_plane(-3.0, 4.0)
+    degen = np.array([[[0, 0, 0], [0, 0, 0], [0, 0, 0]], [[1, 1, 1], [2, 2, 2], [3, 3, 3]]], np.float64)
+    dup = np.repeat(scenes.ground_plane(5.0, 2.0)[:1], 3, axis=0)
+    tris = np.concatenate([box, flat, degen, dup]).reshape(-1, 9).astype(np.float32)
+    bvh = lib.BVH(tris)
+    rs = np.random.RandomState(0)
+    n = 4000
+    rays = np.zeros(n, RAY_DTYPE)
+    rays["org"] = rs.uniform(-6, 6, (n, 3)).astype(np.float32)
+    d = rs.normal(size=(n, 3))
+    # axis-aligned and zero-component directions
+    d[: n // 4] = np.eye(3)[rs.randint(0, 3, n // 4)] * rs.choice([-1, 1], (n // 4, 1))
+    d[n // 4: n // 2, rs.randint(0, 3)] = 0.0
+    rays["dir"] = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    rays["tmin"] = 0.0
+    rays["tmax"] = rs.choice([1e30, 3.0], n).astype(np.float32)
+    # rays starting exactly on faces
+    rays["org"][-200:, 0] = 2.0
+    # NaN direction: never hits
+    rays["dir"][-1] = np.nan
+    ref = O.brute_closest(tris, rays)
+    assert_hits_equal(gpu_closest(bvh, rays), ref, "edge")
+    assert np.array_equal(gpu_any(bvh, rays), O.brute_any(tris, rays))
+    assert ref["prim"][-1] == -1
+    # a hit exactly at tmax is rejected, just beyond it accepted
+    r1 = np.zeros(2, RAY_DTYPE)
+    r1["org"] = (0.5, 10.0, 0.5)
+    r1["dir"] = (0, -1, 0)
+    r1["tmax"] = (13.0, np.nextafter(np.float32(13.0), np.float32(1e30)))
+    h = bvh.closest_host(r1)
+    assert h["prim"][0] == -1 and h["prim"][1] >= 0 and h["t"][1] == 13.0
+
+
+def test_single_triangle_and_zero_rays(cuda):
+    tri = np.array([[0, 0, 0, 1, 0, 0, 0, 1, 0]], np.float32)
+    bvh = lib.BVH(tri)
+    r = np.zeros(3, RAY_DTYPE)
+    r["org"] = [(0.2, 0.2, 1), (2, 2, 1), (0.2, 0.2, -1)]
+    r["dir"] = [(0, 0, -1), (0, 0, -1), (0, 0, 1)]
+    r["tmax"] = 1e30
+    h = bvh.closest_host(r)
+    assert h["prim"].tolist() == [0, -1, 0]
+    assert np.allclose(h["t"][[0, 2]], 1.0)
+    assert bvh.closest_host(np.zeros(0, RAY_DTYPE)).shape == (0,)
+
+
+def test_reference_shaped_entry_points(cuda, small_scene):
+    bvh = lib.BVH(small_scene)
+    side = 256
+    cam = (0.0, 0.0, -80.0)
+    mrs, t = bvh.trace_primary(side, cam)
+    assert mrs > 0
+    # the same square camera in float32 on the host (layer/cuda_bvh_backend.cu:69-74)
+    px = (np.arange(side * side) % side).astype(np.float32)
+    py = (np.arange(side * side) // side).astype(np.float32)
+    u = (px + np.float32(0.5)) / np.float32(side) * np.float32(2) - np.float32(1)
+    v = (py + np.float32(0.5)) / np.float32(side) * np.float32(2) - np.float32(1)
+    rl = np.float32(1) / np.sqrt(u * u + v * v + np.float32(1))
+    rays = np.zeros(side * side, RAY_DTYPE)
+    rays["org"] = cam
+    rays["dir"] = np.stack([u * rl, v * rl, rl], 1)
+    rays["tmax"] = 1e30
+    ref = O.brute_closest(small_scene, rays)
+    exp_t = np.where(ref["prim"] >= 0, ref["t"], np.float32(1e30))
+    assert np.array_equal(t.view(np.uint32), exp_t.view(np.uint32))
+    # traceDiffuse: host SoA rays in caller order
+    rr = scenes.random_rays(9, 5000)
+    mrs, t2 = bvh.trace_diffuse(rr["org"], rr["dir"])
+    rr["tmin"] = 0.0
+    ref2 = O.brute_closest(small_scene, rr)
+    assert mrs > 0
+    assert np.array_equal(t2.view(np.uint32), np.where(ref2["prim"] >= 0, ref2["t"], np.float32(1e30)).view(np.uint32))
+    # RGBA: sky where the oracle misses, shaded where it hits
+    img = bvh.trace_rgba(64, 48, (0.0, 20.0, -90.0))
+    assert img.shape == (64 * 48,) and np.all((img >> 24) == 255)
+
+
+def test_exports_are_valid_bvhs(cuda, small_scene):
+    bvh = lib.BVH(small_scene)
+    ex = bvh.exports()
+    n = small_scene.shape[0]
+    pk = ex["packed"].reshape(-1, 12)
+    assert pk.shape[0] == n
+    assert sorted(pk[:, 9].astype(np.int64).tolist()) == list(range(n))
+    assert np.array_equal(pk[:, :9], small_scene[pk[:, 9].astype(np.int64)])
+    assert np.array_equal(ex["soa"].T, pk[:, :9])
+    skips = ex["dfs"].reshape(-1, 8)[:, 7].view(np.int32)
+    assert skips[0] == -1 and (skips == -2).sum() == 0
+    assert np.array_equal(O.fix_skips(ex["dfs"]), ex["dfs"])
+    rays = scenes.random_rays(21, 5000)
+    assert_hits_equal(O.trace_closest_dfs(ex["dfs"], ex["packed"], rays), O.brute_closest(small_scene, rays), "dfs")
+    # BVH4 export: every child box (fp16, rounded outward) holds its subtree
+    b4 = ex["bvh4"].reshape(-1, 64)
+    halfs = b4[:, :48].copy().view(np.float16).astype(np.float32).reshape(-1, 3, 8)
+    child = b4[:, 48:].copy().view(np.int32)
+    tri_lo = small_scene.reshape(-1, 3, 3).min(1)
+    tri_hi = small_scene.reshape(-1, 3, 3).max(1)
+    order = pk[:, 9].astype(np.int64)
+
+    def subtree_box(c):
+        if c <= -2:
+            e = -(c + 2)
+            ids = order[(e >> 3):(e >> 3) + (e & 7) + 1]
+            return tri_lo[ids].min(0), tri_hi[ids].max(0)
+        los, his = zip(*[subtree_box(k) for k in child[c] if k != -1])
+        return np.min(los, 0), np.max(his, 0)
+
+    for i in range(0, b4.shape[0], max(1, b4.shape[0] // 200)):
+        for k in range(4):
+            c = child[i, k]
+            if c == -1:
+                continue
+            lo, hi = subtree_box(c)
+            assert np.all(halfs[i, :, k] <= lo) and np.all(halfs[i, :, 4 + k] >= hi)
+    assert ex["num_cwbvh"] == bvh.stats()["num_nodes"]
+
+
+def _d2h(ptr, nbytes):
+    import ctypes as C
+    import torch
+    torch.cuda.synchronize()
+    out = np.zeros(nbytes, np.uint8)
+    rt = C.CDLL("libcudart.so.12")
+    rt.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+    assert rt.cudaMemcpy(out.ctypes.data, ptr, nbytes, 2) == 0
+    return out
+
+
+def test_build_is_deterministic_and_sane(cuda):
+    tris = scenes.scene_meshes(2, 120_000)
+    a, b = lib.BVH(tris), lib.BVH(tris)
+    sa = a.stats()
+    assert sa["num_tris"] == tris.shape[0] and sa["bins"] == 32 and sa["max_leaf"] == 4
+    assert 1 <= sa["depth"] <= 64
+    la, lb = a.layout(), b.layout()
+    assert la[1] == lb[1] and la[3] == lb[3] == tris.shape[0]
+    assert np.array_equal(_d2h(la[0], la[1] * 80), _d2h(lb[0], lb[1] * 80))
+    assert np.array_equal(_d2h(la[2], la[3] * 48), _d2h(lb[2], lb[3] * 48))
+    assert sa["sah_cost"] > 0 and sa["build_ms"] > 0
+
+
+def test_tlas_two_level_vs_oracle(cuda):
+    rs = np.random.RandomState(5)
+    blas_tris = [scenes.scene_meshes(10 + i, 3000 + 1000 * i, box=6.0, lo=200, hi=800, ground=False)
+                 for i in range(4)]
+    blases = [lib.BVH(t) for t in blas_tris]
+    ninst = 24
+    insts = (lib.RtInstance * ninst)()
+    xf = []
+    for k in range(ninst):
+        R = scenes.rotations(rs.uniform(size=(1, 3)))[0] * rs.uniform(0.5, 2.0)
+        t = rs.uniform(-40, 40, 3)
+        M = np.concatenate([R, t[:, None]], 1).astype(np.float32)
+        xf.append(M)
+        insts[k].xform[:] = M.ravel().tolist()
+        insts[k].blas = k % 4
+    L = lib.load()
+    import ctypes as C
+    arr = (C.c_void_p * 4)(*[b.h for b in blases])
+    tl = L.cudaTLAS_build(arr, 4, insts, ninst)
+    assert tl, lib.last_error()
+    try:
+        inv = np.zeros((ninst, 12), np.float32)
+        assert L.cudaTLAS_getInverseTransforms(tl, inv.ctypes.data, ninst) == 0
+        # oracle side: restated builder per BLAS + LBVH over world boxes
+        obs = [O.OracleBVH(t, 32, 4) for t in blas_tris]
+        node_off = np.cumsum([0] + [o.dfs.size // 8 for o in obs]).astype(np.int32)
+        tri_off = np.cumsum([0] + [o.packed.size // 12 for o in obs]).astype(np.int32)
+        bdfs = np.concatenate([o.dfs for o in obs])
+        bpk = np.concatenate([o.packed for o in obs])
+        wb = []
+        for k in range(ninst):
+            v = blas_tris[k % 4].reshape(-1, 3).astype(np.float64) @ xf[k][:, :3].T.astype(np.float64) + xf[k][:, 3]
+            lo, hi = v.min(0), v.max(0)
+            pad = 1e-4 * (np.abs(v).max() + 1)
+            wb.append(np.concatenate([lo - pad, hi + pad]))
+        tnodes, tord = O.tlas_fast(np.array(wb, np.float32))
+        tnodes = O.fix_skips(tnodes)
+        rays = scenes.random_rays(33, 20000)
+        hits = np.zeros(rays.shape[0], HIT_DTYPE)
+        inst_ref = np.zeros(rays.shape[0], np.int32)
+        iblas = np.array([k % 4 for k in range(ninst)], np.int32)
+        Lo = O.lib()
+        Lo.orc_trace_closest_two_level(tnodes.ctypes.data, tnodes.size // 8, tord.ctypes.data, inv.ctypes.data,
+                                       iblas.ctypes.data, ninst, bdfs.ctypes.data, node_off.ctypes.data,
+                                       bpk.ctypes.data, tri_off.ctypes.data, rays.ctypes.data, rays.shape[0],
+                                       hits.ctypes.data, inst_ref.ctypes.data, 0)
+        occ_ref = np.zeros(rays.shape[0], np.uint8)
+        Lo.orc_trace_any_two_level(tnodes.ctypes.data, tnodes.size // 8, tord.ctypes.data, inv.ctypes.data,
+                                   iblas.ctypes.data, ninst, bdfs.ctypes.data, node_off.ctypes.data,
+                                   bpk.ctypes.data, tri_off.ctypes.data, rays.ctypes.data, rays.shape[0],
+                                   occ_ref.ctypes.data, 0)
+        import torch
+        d_rays = _dev(torch, rays)
+        d_hits = torch.empty(rays.shape[0] * 16, dtype=torch.uint8, device="cuda")
+        d_inst = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+        d_occ = torch.empty(rays.shape[0], dtype=torch.uint8, device="cuda")
+        assert L.cudaTLAS_traceClosest(tl, d_rays.data_ptr(), rays.shape[0], d_hits.data_ptr(), d_inst.data_ptr(),
+                                       None) == 0
+        assert L.cudaTLAS_traceAny(tl, d_rays.data_ptr(), rays.shape[0], d_occ.data_ptr(), None) == 0
+        torch.cuda.synchronize()
+        got = d_hits.cpu().numpy().view(HIT_DTYPE)
+        assert_hits_equal(got, hits, "tlas")
+        assert np.array_equal(d_inst.cpu().numpy(), inst_ref)
+        assert np.array_equal(d_occ.cpu().numpy(), occ_ref)
+        assert (hits["prim"] >= 0).mean() > 0.05
+    finally:
+        L.cudaTLAS_destroy(tl)
+
+
+def test_counters_match_closest_results(cuda, small_scene):
+    import torch
+    bvh = lib.BVH(small_scene)
+    rays = scenes.random_rays(44, 10000)
+    d_rays = _dev(torch, rays)
+    d_cnt = torch.zeros(rays.shape[0] * 2, dtype=torch.int32, device="cuda")
+    bvh.counters(d_rays, rays.shape[0], d_cnt)
+    torch.cuda.synchronize()
+    c = d_cnt.cpu().numpy().reshape(-1, 2)
+    assert c[:, 0].min() >= 1 and c[:, 1].mean() > 0

@@ -1,0 +1,901 @@
+// rt_build.cu -- GPU binned-SAH builder (32 bins) and collapse to the
+// compressed 8-wide layout.
+//
+// Builder (replaces the reference's single-threaded CPU BVH2Builder,
+// layer/cuda_bvh_backend.cu:201-251 / cuda_rt_v40.cu:790-840):
+//   * top-down, level-synchronous for tasks larger than `small_task`
+//     primitives: chunked CTA binning into shared-memory bins (3 axes x 32
+//     bins, order-independent min/max/add atomics, so the result does not
+//     depend on scheduling), one warp per task evaluates the 31 split planes
+//     per axis (lane = bin, prefix/suffix by shuffles), a stable partition by
+//     chunk scans;
+//   * tasks of at most `small_task` primitives finish their whole subtree in
+//     one CTA out of shared memory.
+//   Cost model: C = N_L*A(L) + N_R*A(R) (same split search as the reference);
+//   leaves at <= max_leaf primitives; no valid split or depth >= max_sah_depth
+//   -> object-median split.  Every step is deterministic.
+// Collapse: top-down, one thread per 8-wide node: greedily open the child
+// with the largest surface area until 8 children (Ylitie, Karras, Laine,
+// HPG 2017), assign children to octant slots, quantise child boxes outward
+// to 8 bits per plane against a power-of-two grid, emit triangle records
+// in node order.
+#include <cfloat>
+#include <cmath>
+
+#include "rt_internal.h"
+
+namespace rtb {
+
+constexpr unsigned FULL = 0xFFFFFFFFu;
+constexpr int CHUNK = 2048;          // primitives per binning CTA
+constexpr int CHUNK_T = 256;         // threads per binning CTA
+constexpr int SMALL_T = 128;         // threads per small-task CTA
+constexpr int SMALL_STACK = 96;
+
+// ---------------------------------------------------------------- scan --
+template <int T>
+__device__ int block_exclusive_scan(int v, int* ws, int& total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int s = lane < T / 32 ? ws[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(FULL, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < T / 32) ws[lane] = s;
+    }
+    __syncthreads();
+    const int before = w ? ws[w - 1] : 0;
+    total = ws[T / 32 - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+constexpr int SCAN_T = 256, SCAN_IPT = 8, SCAN_TILE = SCAN_T * SCAN_IPT;
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_tiles(const int* __restrict__ in, int* __restrict__ out, int n,
+                                                       int* __restrict__ tile_sums) {
+    __shared__ int ws[SCAN_T / 32];
+    const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_IPT;
+    int v[SCAN_IPT];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_IPT; k++) {
+        v[k] = base + k < n ? in[base + k] : 0;
+        sum += v[k];
+    }
+    int total;
+    int run = block_exclusive_scan<SCAN_T>(sum, ws, total);
+#pragma unroll
+    for (int k = 0; k < SCAN_IPT; k++) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == 0 && tile_sums) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void k_scan_add(int* __restrict__ out, int n, const int* __restrict__ tile_off) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += tile_off[i / SCAN_TILE];
+}
+
+__global__ void k_scan_total(const int* __restrict__ in, const int* __restrict__ out, int n, int* total) {
+    *total = n > 0 ? out[n - 1] + in[n - 1] : 0;
+}
+
+bool scan_exclusive(const int* d_in, int* d_out, int n, int* d_total, cudaStream_t s) {
+    if (n <= 0) {
+        if (d_total) cudaMemsetAsync(d_total, 0, sizeof(int), s);
+        return true;
+    }
+    const int tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (tiles == 1) {
+        k_scan_tiles<<<1, SCAN_T, 0, s>>>(d_in, d_out, n, nullptr);
+    } else {
+        int *sums = nullptr, *offs = nullptr;
+        if (!RT_CUDA(cudaMallocAsync(&sums, sizeof(int) * tiles * 2, s))) return false;
+        offs = sums + tiles;
+        k_scan_tiles<<<tiles, SCAN_T, 0, s>>>(d_in, d_out, n, sums);
+        if (!scan_exclusive(sums, offs, tiles, nullptr, s)) return false;
+        k_scan_add<<<(n + 255) / 256, 256, 0, s>>>(d_out, n, offs);
+        cudaFreeAsync(sums, s);
+    }
+    if (d_total) k_scan_total<<<1, 1, 0, s>>>(d_in, d_out, n, d_total);
+    return RT_CUDA(cudaGetLastError());
+}
+
+// -------------------------------------------------------- prim bounds --
+__global__ void k_tri_bounds(const float* __restrict__ t9, int n, float4* __restrict__ lo,
+                             float4* __restrict__ hi) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* t = t9 + (size_t)i * 9;
+    lo[i] = make_float4(fminf(fminf(t[0], t[3]), t[6]), fminf(fminf(t[1], t[4]), t[7]),
+                        fminf(fminf(t[2], t[5]), t[8]), 0.f);
+    hi[i] = make_float4(fmaxf(fmaxf(t[0], t[3]), t[6]), fmaxf(fmaxf(t[1], t[4]), t[7]),
+                        fmaxf(fmaxf(t[2], t[5]), t[8]), 0.f);
+}
+
+void launch_tri_bounds(const float* d_tris9, int n, float4* d_lo, float4* d_hi, cudaStream_t s) {
+    if (n > 0) k_tri_bounds<<<(n + 255) / 256, 256, 0, s>>>(d_tris9, n, d_lo, d_hi);
+}
+
+__device__ __forceinline__ float centroid(float lo, float hi) { return (lo + hi) * 0.5f; }
+__device__ __forceinline__ float half_area(float lx, float ly, float lz, float hx, float hy, float hz) {
+    const float dx = hx - lx, dy = hy - ly, dz = hz - lz;
+    return dx * dy + dy * dz + dz * dx;
+}
+__device__ __forceinline__ int bin_of(float c, float cmin, float k) {
+    int b = (int)((c - cmin) * k);
+    return b < 0 ? 0 : (b >= kBins ? kBins - 1 : b);
+}
+__device__ __forceinline__ float bin_scale(float cmin, float cmax) {
+    const float ext = cmax - cmin;
+    return ext > 0.f ? (float)kBins / ext : 0.f;
+}
+
+// Global box and centroid box of all primitives (12 ordered uints).
+__global__ void k_root_bounds(const float4* __restrict__ lo, const float4* __restrict__ hi, int n,
+                              uint32_t* __restrict__ acc) {
+    float b[12];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        b[k] = FLT_MAX; b[3 + k] = -FLT_MAX; b[6 + k] = FLT_MAX; b[9 + k] = -FLT_MAX;
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 l = lo[i], h = hi[i];
+        const float L[3] = {l.x, l.y, l.z}, H[3] = {h.x, h.y, h.z};
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            b[k] = fminf(b[k], L[k]);
+            b[3 + k] = fmaxf(b[3 + k], H[k]);
+            const float c = centroid(L[k], H[k]);
+            b[6 + k] = fminf(b[6 + k], c);
+            b[9 + k] = fmaxf(b[9 + k], c);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+        const bool mx = (k >= 3 && k < 6) || k >= 9;
+        float v = b[k];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const float y = __shfl_xor_sync(FULL, v, o);
+            v = mx ? fmaxf(v, y) : fminf(v, y);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            if (mx) atomicMax(&acc[k], f2ord(v));
+            else atomicMin(&acc[k], f2ord(v));
+        }
+    }
+}
+
+// ------------------------------------------------------- large levels --
+struct Task {
+    int node, start, count, depth;
+    float clo[3], chi[3];
+};
+struct Split {
+    int axis, bin, nl, pad;
+};
+struct Chunk {
+    int task, start, count, first;
+};
+
+// bins per task: [axis][bin] x {cnt, lo3, hi3, clo3, chi3} as ordered uints
+constexpr int BIN_WORDS = 13;
+constexpr int TASK_BIN_WORDS = 3 * kBins * BIN_WORDS;
+
+__global__ void k_init_root(Task* tasks, Node2* nodes, const uint32_t* acc, int n, int max_leaf) {
+    Task t;
+    t.node = 0; t.start = 0; t.count = n; t.depth = 0;
+    for (int k = 0; k < 3; k++) { t.clo[k] = ord2f(acc[6 + k]); t.chi[k] = ord2f(acc[9 + k]); }
+    tasks[0] = t;
+    Node2 r;
+    for (int k = 0; k < 3; k++) { r.lo[k] = ord2f(acc[k]); r.hi[k] = ord2f(acc[3 + k]); }
+    r.a = 0; r.b = 0;
+    if (n <= max_leaf) { r.a = 0; r.b = -n; }
+    nodes[0] = r;
+}
+
+__global__ void k_chunk_counts(const Task* __restrict__ tasks, int T, int* __restrict__ cnt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < T) cnt[i] = (tasks[i].count + CHUNK - 1) / CHUNK;
+}
+
+__global__ void k_fill_chunks(const Task* __restrict__ tasks, int T, const int* __restrict__ off,
+                              Chunk* __restrict__ chunks) {
+    const int t = blockIdx.x;
+    if (t >= T) return;
+    const Task tk = tasks[t];
+    const int nc = (tk.count + CHUNK - 1) / CHUNK;
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+        Chunk ch;
+        ch.task = t;
+        ch.start = tk.start + c * CHUNK;
+        ch.count = min(CHUNK, tk.count - c * CHUNK);
+        ch.first = off[t];
+        chunks[off[t] + c] = ch;
+    }
+}
+
+__global__ void k_clear_bins(uint32_t* __restrict__ bins, int T) {
+    const size_t total = (size_t)T * TASK_BIN_WORDS;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int w = (int)(i % BIN_WORDS);
+        // cnt:0, lo: min-acc (init max), hi: max-acc (init 0), clo: min, chi: max
+        bins[i] = (w == 0) ? 0u : ((w >= 1 && w <= 3) || (w >= 7 && w <= 9) ? 0xFFFFFFFFu : 0u);
+    }
+}
+
+__global__ void __launch_bounds__(CHUNK_T) k_bin_large(const Chunk* __restrict__ chunks, const Task* __restrict__ tasks,
+                                                       const int* __restrict__ perm, const float4* __restrict__ plo,
+                                                       const float4* __restrict__ phi, uint32_t* __restrict__ gbins) {
+    __shared__ uint32_t sb[TASK_BIN_WORDS];
+    const Chunk ch = chunks[blockIdx.x];
+    const Task tk = tasks[ch.task];
+    for (int i = threadIdx.x; i < TASK_BIN_WORDS; i += CHUNK_T) {
+        const int w = i % BIN_WORDS;
+        sb[i] = (w == 0) ? 0u : ((w >= 1 && w <= 3) || (w >= 7 && w <= 9) ? 0xFFFFFFFFu : 0u);
+    }
+    float k3[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) k3[a] = bin_scale(tk.clo[a], tk.chi[a]);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ch.count; i += CHUNK_T) {
+        const int p = perm[ch.start + i];
+        const float4 l = plo[p], h = phi[p];
+        const float L[3] = {l.x, l.y, l.z}, H[3] = {h.x, h.y, h.z};
+        float c[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) c[a] = centroid(L[a], H[a]);
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const int b = bin_of(c[a], tk.clo[a], k3[a]);
+            uint32_t* w = sb + (a * kBins + b) * BIN_WORDS;
+            atomicAdd(&w[0], 1u);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                atomicMin(&w[1 + k], f2ord(L[k]));
+                atomicMax(&w[4 + k], f2ord(H[k]));
+                atomicMin(&w[7 + k], f2ord(c[k]));
+                atomicMax(&w[10 + k], f2ord(c[k]));
+            }
+        }
+    }
+    __syncthreads();
+    uint32_t* g = gbins + (size_t)ch.task * TASK_BIN_WORDS;
+    for (int i = threadIdx.x; i < TASK_BIN_WORDS; i += CHUNK_T) {
+        const int w = i % BIN_WORDS;
+        const uint32_t v = sb[i];
+        if (w == 0) { if (v) atomicAdd(&g[i], v); }
+        else if ((w >= 1 && w <= 3) || (w >= 7 && w <= 9)) { if (v != 0xFFFFFFFFu) atomicMin(&g[i], v); }
+        else if (v) atomicMax(&g[i], v);
+    }
+}
+
+struct BinBox {
+    float lo[3], hi[3], clo[3], chi[3];
+    int cnt;
+};
+
+__device__ __forceinline__ void box_merge(BinBox& a, const BinBox& b) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        a.lo[k] = fminf(a.lo[k], b.lo[k]); a.hi[k] = fmaxf(a.hi[k], b.hi[k]);
+        a.clo[k] = fminf(a.clo[k], b.clo[k]); a.chi[k] = fmaxf(a.chi[k], b.chi[k]);
+    }
+    a.cnt += b.cnt;
+}
+__device__ __forceinline__ BinBox shfl_box(const BinBox& v, int src_delta, bool up) {
+    BinBox r;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        r.lo[k] = up ? __shfl_up_sync(FULL, v.lo[k], src_delta) : __shfl_down_sync(FULL, v.lo[k], src_delta);
+        r.hi[k] = up ? __shfl_up_sync(FULL, v.hi[k], src_delta) : __shfl_down_sync(FULL, v.hi[k], src_delta);
+        r.clo[k] = up ? __shfl_up_sync(FULL, v.clo[k], src_delta) : __shfl_down_sync(FULL, v.clo[k], src_delta);
+        r.chi[k] = up ? __shfl_up_sync(FULL, v.chi[k], src_delta) : __shfl_down_sync(FULL, v.chi[k], src_delta);
+    }
+    r.cnt = up ? __shfl_up_sync(FULL, v.cnt, src_delta) : __shfl_down_sync(FULL, v.cnt, src_delta);
+    return r;
+}
+
+// Prefix (bins 0..lane) and suffix (bins lane..31) of one axis.
+__device__ void prefix_suffix(const BinBox& mine, BinBox& pre, BinBox& suf) {
+    const int lane = threadIdx.x & 31;
+    pre = mine;
+    suf = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        BinBox y = shfl_box(pre, o, true);
+        if (lane >= o) box_merge(pre, y);
+        BinBox z = shfl_box(suf, o, false);
+        if (lane + o < 32) box_merge(suf, z);
+    }
+}
+
+__device__ BinBox load_bin(const uint32_t* w) {
+    BinBox b;
+    b.cnt = (int)w[0];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        b.lo[k] = b.cnt ? ord2f(w[1 + k]) : FLT_MAX;
+        b.hi[k] = b.cnt ? ord2f(w[4 + k]) : -FLT_MAX;
+        b.clo[k] = b.cnt ? ord2f(w[7 + k]) : FLT_MAX;
+        b.chi[k] = b.cnt ? ord2f(w[10 + k]) : -FLT_MAX;
+    }
+    return b;
+}
+
+// One warp per task: best (axis, bin) by SAH; writes the split, the two
+// child nodes (ids base + 2t, base + 2t + 1) and their task descriptors.
+__global__ void k_split_large(const Task* __restrict__ tasks, int T, const uint32_t* __restrict__ gbins,
+                              Split* __restrict__ splits, Task* __restrict__ kids, Node2* __restrict__ nodes,
+                              int node_base, int max_leaf, int max_sah_depth) {
+    const int t = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    if (t >= T) return;
+    const int lane = threadIdx.x & 31;
+    const Task tk = tasks[t];
+    const uint32_t* g = gbins + (size_t)t * TASK_BIN_WORDS;
+    float best = FLT_MAX;
+    int best_axis = -1, best_bin = -1;
+    for (int a = 0; a < 3; a++) {
+        BinBox mine = load_bin(g + (a * kBins + lane) * BIN_WORDS), pre, suf;
+        prefix_suffix(mine, pre, suf);
+        BinBox right = shfl_box(suf, 1, false);
+        float cost = FLT_MAX;
+        if (lane < kBins - 1 && pre.cnt > 0 && right.cnt > 0)
+            cost = pre.cnt * half_area(pre.lo[0], pre.lo[1], pre.lo[2], pre.hi[0], pre.hi[1], pre.hi[2]) +
+                   right.cnt * half_area(right.lo[0], right.lo[1], right.lo[2], right.hi[0], right.hi[1], right.hi[2]);
+        // warp argmin, ties toward the lower bin
+        float c = cost;
+        int b = lane;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const float c2 = __shfl_xor_sync(FULL, c, o);
+            const int b2 = __shfl_xor_sync(FULL, b, o);
+            if (c2 < c || (c2 == c && b2 < b)) { c = c2; b = b2; }
+        }
+        if (c < best) { best = c; best_axis = a; best_bin = b; }
+    }
+    const bool median = best_axis < 0 || best == FLT_MAX || tk.depth >= max_sah_depth;
+    BinBox L, R;
+    int nl;
+    const Node2 pn = nodes[tk.node];
+    if (!median) {
+        BinBox mine = load_bin(g + (best_axis * kBins + lane) * BIN_WORDS), pre, suf;
+        prefix_suffix(mine, pre, suf);
+        BinBox right = shfl_box(suf, 1, false);
+        L = pre;
+        R = right;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            L.lo[k] = __shfl_sync(FULL, pre.lo[k], best_bin); L.hi[k] = __shfl_sync(FULL, pre.hi[k], best_bin);
+            L.clo[k] = __shfl_sync(FULL, pre.clo[k], best_bin); L.chi[k] = __shfl_sync(FULL, pre.chi[k], best_bin);
+            R.lo[k] = __shfl_sync(FULL, right.lo[k], best_bin); R.hi[k] = __shfl_sync(FULL, right.hi[k], best_bin);
+            R.clo[k] = __shfl_sync(FULL, right.clo[k], best_bin); R.chi[k] = __shfl_sync(FULL, right.chi[k], best_bin);
+        }
+        nl = __shfl_sync(FULL, pre.cnt, best_bin);
+    } else {
+        nl = tk.count / 2;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            L.lo[k] = R.lo[k] = pn.lo[k];
+            L.hi[k] = R.hi[k] = pn.hi[k];
+            L.clo[k] = R.clo[k] = tk.clo[k];
+            L.chi[k] = R.chi[k] = tk.chi[k];
+        }
+    }
+    if (lane == 0) {
+        Split sp;
+        sp.axis = median ? -1 : best_axis;
+        sp.bin = best_bin;
+        sp.nl = nl;
+        sp.pad = 0;
+        splits[t] = sp;
+        const int lid = node_base + 2 * t, rid = lid + 1;
+        nodes[tk.node].a = lid;
+        nodes[tk.node].b = rid;
+        const int cnt[2] = {nl, tk.count - nl};
+        const int st[2] = {tk.start, tk.start + nl};
+        for (int s = 0; s < 2; s++) {
+            const BinBox& B = s ? R : L;
+            Node2 nd;
+            for (int k = 0; k < 3; k++) { nd.lo[k] = B.lo[k]; nd.hi[k] = B.hi[k]; }
+            nd.a = 0;
+            nd.b = 0;
+            if (cnt[s] <= max_leaf) { nd.a = st[s]; nd.b = -cnt[s]; }
+            nodes[lid + s] = nd;
+            Task kt;
+            kt.node = lid + s;
+            kt.start = st[s];
+            kt.count = cnt[s];
+            kt.depth = tk.depth + 1;
+            for (int k = 0; k < 3; k++) { kt.clo[k] = B.clo[k]; kt.chi[k] = B.chi[k]; }
+            kids[2 * t + s] = kt;
+        }
+    }
+}
+
+__device__ __forceinline__ bool goes_left(const Task& tk, const Split& sp, int pos, const float4& l,
+                                          const float4& h) {
+    if (sp.axis < 0) return pos - tk.start < sp.nl;
+    const float L = sp.axis == 0 ? l.x : (sp.axis == 1 ? l.y : l.z);
+    const float H = sp.axis == 0 ? h.x : (sp.axis == 1 ? h.y : h.z);
+    const float k = bin_scale(tk.clo[sp.axis], tk.chi[sp.axis]);
+    return bin_of(centroid(L, H), tk.clo[sp.axis], k) <= sp.bin;
+}
+
+constexpr int PART_IPT = CHUNK / CHUNK_T;  // 8 consecutive positions per thread
+
+__global__ void __launch_bounds__(CHUNK_T) k_count_left(const Chunk* __restrict__ chunks, const Task* __restrict__ tasks,
+                                                        const Split* __restrict__ splits, const int* __restrict__ perm,
+                                                        const float4* __restrict__ plo, const float4* __restrict__ phi,
+                                                        int* __restrict__ chunk_left) {
+    __shared__ int ws[CHUNK_T / 32];
+    const Chunk ch = chunks[blockIdx.x];
+    const Task tk = tasks[ch.task];
+    const Split sp = splits[ch.task];
+    int c = 0;
+    for (int k = 0; k < PART_IPT; k++) {
+        const int i = threadIdx.x * PART_IPT + k;
+        if (i < ch.count) {
+            const int p = perm[ch.start + i];
+            c += goes_left(tk, sp, ch.start + i, plo[p], phi[p]);
+        }
+    }
+    int total;
+    block_exclusive_scan<CHUNK_T>(c, ws, total);
+    if (threadIdx.x == 0) chunk_left[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(CHUNK_T) k_scatter(const Chunk* __restrict__ chunks, const Task* __restrict__ tasks,
+                                                     const Split* __restrict__ splits, const int* __restrict__ perm,
+                                                     const float4* __restrict__ plo, const float4* __restrict__ phi,
+                                                     const int* __restrict__ left_off, int* __restrict__ out) {
+    __shared__ int ws[CHUNK_T / 32];
+    const Chunk ch = chunks[blockIdx.x];
+    const Task tk = tasks[ch.task];
+    const Split sp = splits[ch.task];
+    bool f[PART_IPT];
+    int pv[PART_IPT];
+    int c = 0;
+    for (int k = 0; k < PART_IPT; k++) {
+        const int i = threadIdx.x * PART_IPT + k;
+        f[k] = false;
+        pv[k] = -1;
+        if (i < ch.count) {
+            pv[k] = perm[ch.start + i];
+            f[k] = goes_left(tk, sp, ch.start + i, plo[pv[k]], phi[pv[k]]);
+            c += f[k];
+        }
+    }
+    int total;
+    int lr = block_exclusive_scan<CHUNK_T>(c, ws, total);  // lefts before my first element
+    const int left_before = left_off[blockIdx.x] - left_off[ch.first];
+    const int right_before = (ch.start - tk.start) - left_before;
+    for (int k = 0; k < PART_IPT; k++) {
+        const int i = threadIdx.x * PART_IPT + k;
+        if (i < ch.count) {
+            const int dst = f[k] ? tk.start + left_before + lr : tk.start + sp.nl + right_before + (i - lr);
+            lr += f[k];
+            out[dst] = pv[k];
+        }
+    }
+}
+
+__global__ void k_copy_back(const Chunk* __restrict__ chunks, const int* __restrict__ src, int* __restrict__ dst) {
+    const Chunk ch = chunks[blockIdx.x];
+    for (int i = threadIdx.x; i < ch.count; i += blockDim.x) dst[ch.start + i] = src[ch.start + i];
+}
+
+__global__ void k_classify_flags(const Task* __restrict__ kids, int K, int max_leaf, int small_task,
+                                 int* __restrict__ is_large, int* __restrict__ is_small) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= K) return;
+    const int c = kids[i].count;
+    is_large[i] = c > small_task;
+    is_small[i] = c > max_leaf && c <= small_task;
+}
+
+__global__ void k_compact_kids(const Task* __restrict__ kids, int K, const int* __restrict__ is_large,
+                               const int* __restrict__ large_off, const int* __restrict__ is_small,
+                               const int* __restrict__ small_off, Task* __restrict__ next, Task* __restrict__ small,
+                               const int* __restrict__ small_base) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= K) return;
+    if (is_large[i]) next[large_off[i]] = kids[i];
+    if (is_small[i]) small[*small_base + small_off[i]] = kids[i];
+}
+
+__global__ void k_add_small(int* small_base, const int* add) { *small_base += *add; }
+
+// ----------------------------------------------------------- small tasks --
+// One CTA finishes the subtree of a task of <= small_task primitives in
+// shared memory.  Node ids come from the task's reserved range, handed out
+// in the CTA's fixed processing order (deterministic).
+struct SubTask {
+    int node, lstart, count, depth;
+};
+
+__global__ void k_reserve(const Task* __restrict__ small, int S, int* __restrict__ need) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < S) need[i] = 2 * small[i].count - 2;
+}
+
+template <int T>
+__device__ void block_minmax6(float (&v)[6], float* sh) {
+    // v[0..2] min-reduced, v[3..5] max-reduced over the block; result in all threads
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const float y = __shfl_xor_sync(FULL, v[k], o);
+            v[k] = k < 3 ? fminf(v[k], y) : fmaxf(v[k], y);
+        }
+    }
+    __syncthreads();
+    if (lane == 0)
+        for (int k = 0; k < 6; k++) sh[w * 6 + k] = v[k];
+    __syncthreads();
+    for (int k = 0; k < 6; k++) {
+        float r = sh[k];
+        for (int j = 1; j < T / 32; j++) r = k < 3 ? fminf(r, sh[j * 6 + k]) : fmaxf(r, sh[j * 6 + k]);
+        v[k] = r;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(SMALL_T) k_build_small(const Task* __restrict__ small, const int* __restrict__ res_off,
+                                                         int res_base, int* __restrict__ perm,
+                                                         const float4* __restrict__ plo, const float4* __restrict__ phi,
+                                                         Node2* __restrict__ nodes, int max_leaf, int max_sah_depth,
+                                                         int small_task, int* __restrict__ status) {
+    extern __shared__ float4 smem4[];
+    float* sm = reinterpret_cast<float*>(smem4);
+    const Task tk = small[blockIdx.x];
+    const int n = tk.count;
+    float* blo = sm;                                  // [3][small_task]
+    float* bhi = blo + 3 * small_task;                // [3][small_task]
+    int* gidx = reinterpret_cast<int*>(bhi + 3 * small_task);  // [small_task]
+    unsigned short* pa = reinterpret_cast<unsigned short*>(gidx + small_task);
+    unsigned short* pb = pa + small_task;
+    uint32_t* bins = reinterpret_cast<uint32_t*>(pb + small_task + (small_task & 1));  // [3][32][7]
+    __shared__ SubTask stack[SMALL_STACK];
+    __shared__ int sp_top, next_node, s_axis, s_bin, s_nl, s_done;
+    __shared__ SubTask cur;
+    __shared__ float red[6 * (SMALL_T / 32)];
+    __shared__ float s_cost[3];
+    __shared__ int s_cbin[3];
+    __shared__ int ws[SMALL_T / 32];
+
+    for (int i = threadIdx.x; i < n; i += SMALL_T) {
+        const int p = perm[tk.start + i];
+        gidx[i] = p;
+        const float4 l = plo[p], h = phi[p];
+        blo[i] = l.x; blo[small_task + i] = l.y; blo[2 * small_task + i] = l.z;
+        bhi[i] = h.x; bhi[small_task + i] = h.y; bhi[2 * small_task + i] = h.z;
+        pa[i] = (unsigned short)i;
+    }
+    if (threadIdx.x == 0) {
+        sp_top = 1;
+        SubTask r;
+        r.node = tk.node; r.lstart = 0; r.count = n; r.depth = tk.depth;
+        stack[0] = r;
+        next_node = res_base + res_off[blockIdx.x];
+    }
+    __syncthreads();
+    while (true) {
+        if (threadIdx.x == 0) {
+            s_done = sp_top == 0;
+            if (!s_done) cur = stack[--sp_top];
+        }
+        __syncthreads();
+        if (s_done) break;
+        const SubTask st = cur;
+        if (st.count <= max_leaf) {
+            if (threadIdx.x == 0) {
+                nodes[st.node].a = tk.start + st.lstart;
+                nodes[st.node].b = -st.count;
+            }
+            __syncthreads();
+            continue;
+        }
+        // centroid bounds of this range
+        float cb[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+        for (int i = threadIdx.x; i < st.count; i += SMALL_T) {
+            const int q = pa[st.lstart + i];
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const float c = centroid(blo[a * small_task + q], bhi[a * small_task + q]);
+                cb[a] = fminf(cb[a], c);
+                cb[3 + a] = fmaxf(cb[3 + a], c);
+            }
+        }
+        block_minmax6<SMALL_T>(cb, red);
+        float k3[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) k3[a] = bin_scale(cb[a], cb[3 + a]);
+        for (int i = threadIdx.x; i < 3 * kBins * 7; i += SMALL_T) {
+            const int w = i % 7;
+            bins[i] = w == 0 ? 0u : (w <= 3 ? 0xFFFFFFFFu : 0u);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < st.count; i += SMALL_T) {
+            const int q = pa[st.lstart + i];
+            float L[3], H[3];
+#pragma unroll
+            for (int a = 0; a < 3; a++) { L[a] = blo[a * small_task + q]; H[a] = bhi[a * small_task + q]; }
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const int b = bin_of(centroid(L[a], H[a]), cb[a], k3[a]);
+                uint32_t* w = bins + (a * kBins + b) * 7;
+                atomicAdd(&w[0], 1u);
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    atomicMin(&w[1 + k], f2ord(L[k]));
+                    atomicMax(&w[4 + k], f2ord(H[k]));
+                }
+            }
+        }
+        __syncthreads();
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (warp < 3) {
+            const uint32_t* w = bins + (warp * kBins + lane) * 7;
+            BinBox mine;
+            mine.cnt = (int)w[0];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                mine.lo[k] = mine.cnt ? ord2f(w[1 + k]) : FLT_MAX;
+                mine.hi[k] = mine.cnt ? ord2f(w[4 + k]) : -FLT_MAX;
+                mine.clo[k] = 0.f; mine.chi[k] = 0.f;
+            }
+            BinBox pre, suf;
+            prefix_suffix(mine, pre, suf);
+            BinBox right = shfl_box(suf, 1, false);
+            float cost = FLT_MAX;
+            if (lane < kBins - 1 && pre.cnt > 0 && right.cnt > 0)
+                cost = pre.cnt * half_area(pre.lo[0], pre.lo[1], pre.lo[2], pre.hi[0], pre.hi[1], pre.hi[2]) +
+                       right.cnt * half_area(right.lo[0], right.lo[1], right.lo[2], right.hi[0], right.hi[1], right.hi[2]);
+            float c = cost;
+            int b = lane;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                const float c2 = __shfl_xor_sync(FULL, c, o);
+                const int b2 = __shfl_xor_sync(FULL, b, o);
+                if (c2 < c || (c2 == c && b2 < b)) { c = c2; b = b2; }
+            }
+            if (lane == 0) { s_cost[warp] = c; s_cbin[warp] = b; }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float best = FLT_MAX;
+            int ba = -1, bb = -1;
+            for (int a = 0; a < 3; a++)
+                if (s_cost[a] < best) { best = s_cost[a]; ba = a; bb = s_cbin[a]; }
+            if (ba < 0 || st.depth >= max_sah_depth) { ba = -1; bb = -1; }
+            s_axis = ba;
+            s_bin = bb;
+        }
+        __syncthreads();
+        const int axis = s_axis, sbin = s_bin;
+        // stable partition of pa[lstart, lstart+count) into pb, then copy back
+        int nl_total = 0;
+        for (int base = 0; base < st.count; base += SMALL_T) {
+            const int i = base + threadIdx.x;
+            int f = 0;
+            int q = 0;
+            if (i < st.count) {
+                q = pa[st.lstart + i];
+                if (axis < 0) f = i < st.count / 2;
+                else f = bin_of(centroid(blo[axis * small_task + q], bhi[axis * small_task + q]), cb[axis], k3[axis]) <= sbin;
+            }
+            int tot;
+            const int r = block_exclusive_scan<SMALL_T>(f, ws, tot);
+            if (i < st.count && f) pb[st.lstart + nl_total + r] = (unsigned short)q;
+            nl_total += tot;
+        }
+        int nr_done = 0;
+        for (int base = 0; base < st.count; base += SMALL_T) {
+            const int i = base + threadIdx.x;
+            int f = 0;
+            int q = 0;
+            if (i < st.count) {
+                q = pa[st.lstart + i];
+                if (axis < 0) f = !(i < st.count / 2);
+                else f = !(bin_of(centroid(blo[axis * small_task + q], bhi[axis * small_task + q]), cb[axis], k3[axis]) <= sbin);
+            }
+            int tot;
+            const int r = block_exclusive_scan<SMALL_T>(f, ws, tot);
+            if (i < st.count && f) pb[st.lstart + nl_total + nr_done + r] = (unsigned short)q;
+            nr_done += tot;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < st.count; i += SMALL_T) pa[st.lstart + i] = pb[st.lstart + i];
+        __syncthreads();
+        const int nl = nl_total;
+        // child boxes by reduction over each side
+        float bl[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+        float br[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+        for (int i = threadIdx.x; i < st.count; i += SMALL_T) {
+            const int q = pa[st.lstart + i];
+            float* B = i < nl ? bl : br;
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                B[a] = fminf(B[a], blo[a * small_task + q]);
+                B[3 + a] = fmaxf(B[3 + a], bhi[a * small_task + q]);
+            }
+        }
+        block_minmax6<SMALL_T>(bl, red);
+        block_minmax6<SMALL_T>(br, red);
+        if (threadIdx.x == 0) {
+            const int lid = next_node, rid = next_node + 1;
+            next_node += 2;
+            nodes[st.node].a = lid;
+            nodes[st.node].b = rid;
+            Node2 L, R;
+            for (int a = 0; a < 3; a++) {
+                L.lo[a] = bl[a]; L.hi[a] = bl[3 + a];
+                R.lo[a] = br[a]; R.hi[a] = br[3 + a];
+            }
+            L.a = tk.start + st.lstart; L.b = -nl;
+            R.a = tk.start + st.lstart + nl; R.b = -(st.count - nl);
+            if (nl > max_leaf) L.b = 0;
+            if (st.count - nl > max_leaf) R.b = 0;
+            nodes[lid] = L;
+            nodes[rid] = R;
+            if (sp_top + 2 > SMALL_STACK) {
+                atomicOr(status, 1);  // cannot happen with the depth bound; reported, never silent
+            } else {
+                SubTask sr, sl;
+                sr.node = rid; sr.lstart = st.lstart + nl; sr.count = st.count - nl; sr.depth = st.depth + 1;
+                sl.node = lid; sl.lstart = st.lstart; sl.count = nl; sl.depth = st.depth + 1;
+                if (sr.count > max_leaf) stack[sp_top++] = sr;
+                if (sl.count > max_leaf) stack[sp_top++] = sl;
+            }
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < n; i += SMALL_T) perm[tk.start + i] = gidx[pa[i]];
+}
+
+__global__ void k_iota(int* __restrict__ p, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = i;
+}
+
+// ----------------------------------------------------------- the driver --
+bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig& cfg, Bvh2Device& out,
+                cudaStream_t s) {
+    if (n <= 0) {
+        set_error("build: empty input");
+        return false;
+    }
+    if (cfg.max_leaf < 1 || cfg.max_leaf > 4) {
+        set_error("build: max_leaf must be 1..4");
+        return false;
+    }
+    out.num_prims = n;
+    if (!out.nodes.alloc((size_t)2 * n + 2) || !out.perm.alloc(n)) return false;
+    cudaMemsetAsync(out.nodes.p, 0, out.nodes.bytes(), s);
+    int* perm = out.perm.p;
+    // temporaries
+    const int maxT = n / (cfg.small_task + 1) + 2;  // large tasks per level
+    DevBuf<int> tmp;
+    DevBuf<uint32_t> acc;
+    DevBuf<Task> tasks_a, tasks_b, kids, small;
+    DevBuf<Split> splits;
+    DevBuf<uint32_t> gbins;
+    DevBuf<int> flags, status;
+    const int maxChunks = n / CHUNK + maxT + 2;
+    DevBuf<Chunk> chunks;
+    DevBuf<int> ccount, coff, cleft, cleftoff;
+    const int maxSmall = n / (cfg.max_leaf + 1) + 2;
+    if (!tmp.alloc(n) || !acc.alloc(12) || !tasks_a.alloc(maxT) || !tasks_b.alloc(maxT) || !kids.alloc(2 * maxT) ||
+        !small.alloc(maxSmall) || !splits.alloc(maxT) || !gbins.alloc((size_t)maxT * TASK_BIN_WORDS) ||
+        !flags.alloc(4 * 2 * maxT + 8) || !chunks.alloc(maxChunks) || !ccount.alloc(maxT) || !coff.alloc(maxT) ||
+        !cleft.alloc(maxChunks) || !cleftoff.alloc(maxChunks) || !status.alloc(1))
+        return false;
+    cudaMemsetAsync(status.p, 0, sizeof(int), s);
+    k_iota<<<(n + 255) / 256, 256, 0, s>>>(perm, n);
+    // root bounds
+    {
+        uint32_t init[12];
+        for (int k = 0; k < 12; k++) init[k] = ((k >= 3 && k < 6) || k >= 9) ? 0u : 0xFFFFFFFFu;
+        cudaMemcpyAsync(acc.p, init, sizeof(init), cudaMemcpyHostToDevice, s);
+        const int blocks = std::min((n + 255) / 256, num_sms() * 8);
+        k_root_bounds<<<blocks, 256, 0, s>>>(d_lo, d_hi, n, acc.p);
+        k_init_root<<<1, 1, 0, s>>>(tasks_a.p, out.nodes.p, acc.p, n, cfg.max_leaf);
+    }
+    int node_count = 1;
+    int num_small = 0;
+    int* d_small_base = flags.p + 8 * maxT;  // running count of small tasks
+    int* d_tot = d_small_base + 1;           // scratch totals [large, small, chunks]
+    cudaMemsetAsync(d_small_base, 0, sizeof(int), s);
+    int T = 0;
+    if (n > cfg.max_leaf) {
+        if (n > cfg.small_task) {
+            T = 1;
+        } else {
+            // the root itself is the only small task
+            cudaMemcpyAsync(small.p, tasks_a.p, sizeof(Task), cudaMemcpyDeviceToDevice, s);
+            num_small = 1;
+        }
+    }
+    Task* cur = tasks_a.p;
+    Task* nxt = tasks_b.p;
+    int* is_large = flags.p;
+    int* is_small = flags.p + 2 * maxT;
+    int* large_off = flags.p + 4 * maxT;
+    int* small_off = flags.p + 6 * maxT;
+    while (T > 0) {
+        // chunks
+        k_chunk_counts<<<(T + 255) / 256, 256, 0, s>>>(cur, T, ccount.p);
+        if (!scan_exclusive(ccount.p, coff.p, T, d_tot + 2, s)) return false;
+        int C = 0;
+        cudaMemcpyAsync(&C, d_tot + 2, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (!RT_CUDA(cudaStreamSynchronize(s))) return false;
+        k_fill_chunks<<<T, 128, 0, s>>>(cur, T, coff.p, chunks.p);
+        k_clear_bins<<<std::min(T * 8, 4096), 256, 0, s>>>(gbins.p, T);
+        k_bin_large<<<C, CHUNK_T, 0, s>>>(chunks.p, cur, perm, d_lo, d_hi, gbins.p);
+        k_split_large<<<(T + 3) / 4, 128, 0, s>>>(cur, T, gbins.p, splits.p, kids.p, out.nodes.p, node_count,
+                                                   cfg.max_leaf, cfg.max_sah_depth);
+        k_count_left<<<C, CHUNK_T, 0, s>>>(chunks.p, cur, splits.p, perm, d_lo, d_hi, cleft.p);
+        if (!scan_exclusive(cleft.p, cleftoff.p, C, nullptr, s)) return false;
+        k_scatter<<<C, CHUNK_T, 0, s>>>(chunks.p, cur, splits.p, perm, d_lo, d_hi, cleftoff.p, tmp.p);
+        k_copy_back<<<C, 256, 0, s>>>(chunks.p, tmp.p, perm);
+        node_count += 2 * T;
+        const int K = 2 * T;
+        k_classify_flags<<<(K + 255) / 256, 256, 0, s>>>(kids.p, K, cfg.max_leaf, cfg.small_task, is_large, is_small);
+        if (!scan_exclusive(is_large, large_off, K, d_tot, s)) return false;
+        if (!scan_exclusive(is_small, small_off, K, d_tot + 1, s)) return false;
+        k_compact_kids<<<(K + 255) / 256, 256, 0, s>>>(kids.p, K, is_large, large_off, is_small, small_off, nxt,
+                                                      small.p, d_small_base);
+        k_add_small<<<1, 1, 0, s>>>(d_small_base, d_tot + 1);
+        int h[2];
+        cudaMemcpyAsync(h, d_tot, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (!RT_CUDA(cudaStreamSynchronize(s))) return false;
+        T = h[0];
+        num_small += h[1];
+        std::swap(cur, nxt);
+        if (num_small > maxSmall) {
+            set_error("build: small-task overflow");
+            return false;
+        }
+    }
+    if (num_small > 0) {
+        DevBuf<int> need, off;
+        if (!need.alloc(num_small) || !off.alloc(num_small)) return false;
+        k_reserve<<<(num_small + 255) / 256, 256, 0, s>>>(small.p, num_small, need.p);
+        if (!scan_exclusive(need.p, off.p, num_small, d_tot, s)) return false;
+        int reserved = 0;
+        cudaMemcpyAsync(&reserved, d_tot, sizeof(int), cudaMemcpyDeviceToHost, s);
+        const size_t smem = (size_t)cfg.small_task * (6 * 4 + 4 + 2 + 2) + 16 + 3 * kBins * 7 * 4;
+        cudaFuncSetAttribute(k_build_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_build_small<<<num_small, SMALL_T, smem, s>>>(small.p, off.p, node_count, perm, d_lo, d_hi, out.nodes.p,
+                                                       cfg.max_leaf, cfg.max_sah_depth, cfg.small_task, status.p);
+        if (!RT_CUDA(cudaStreamSynchronize(s))) return false;
+        node_count += reserved;
+    }
+    int st = 0;
+    cudaMemcpyAsync(&st, status.p, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (!RT_CUDA(cudaStreamSynchronize(s))) return false;
+    if (st) {
+        set_error("build: subtree stack overflow");
+        return false;
+    }
+    out.num_nodes = node_count;
+    return true;
+}
+
+}  // namespace rtb

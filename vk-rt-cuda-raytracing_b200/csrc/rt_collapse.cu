@@ -1,0 +1,280 @@
+// rt_collapse.cu -- BVH2 -> compressed 8-wide nodes (top-down, one thread
+// per output node, one launch pair per level).
+//
+// For every 8-wide node: start from the binary node's two children and
+// repeatedly open the inner child with the largest surface area until there
+// are 8 children or only leaves remain; assign the children to octant slots
+// (slot s takes the child nearest along the direction with sign bits s,
+// greedy on the projected-centroid cost); quantise each child box to 8 bits
+// per plane, rounded outward, on the grid p + q * 2^e; write the triangle
+// records of the leaf children contiguously in slot order.
+#include <cfloat>
+#include <cmath>
+
+#include "rt_internal.h"
+
+namespace rtb {
+
+struct Gather {
+    int kid[8];  // binary node id per slot, -1 = empty
+};
+
+__device__ __forceinline__ float node_area(const Node2& n) {
+    const float dx = n.hi[0] - n.lo[0], dy = n.hi[1] - n.lo[1], dz = n.hi[2] - n.lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+__device__ __forceinline__ bool is_leaf2(const Node2& n) { return n.b < 0; }
+
+__global__ void k_gather(const Node2* __restrict__ nodes, const int* __restrict__ level, int L,
+                         Gather* __restrict__ out, int* __restrict__ n_inner, int* __restrict__ n_items) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L) return;
+    const int b2 = level[i];
+    const Node2 me = nodes[b2];
+    int kid[8];
+    int nk = 0;
+    if (is_leaf2(me)) {
+        kid[nk++] = b2;
+    } else {
+        kid[nk++] = me.a;
+        kid[nk++] = me.b;
+        while (nk < 8) {
+            int best = -1;
+            float ba = -1.f;
+            for (int k = 0; k < nk; k++) {
+                const Node2 c = nodes[kid[k]];
+                if (!is_leaf2(c)) {
+                    const float a = node_area(c);
+                    if (a > ba) { ba = a; best = k; }
+                }
+            }
+            if (best < 0) break;
+            const Node2 c = nodes[kid[best]];
+            kid[best] = c.a;
+            kid[nk++] = c.b;
+        }
+    }
+    // octant slot assignment
+    float pc[3];
+    for (int a = 0; a < 3; a++) pc[a] = (me.lo[a] + me.hi[a]) * 0.5f;
+    float cost[8][8];
+    for (int k = 0; k < nk; k++) {
+        const Node2 c = nodes[kid[k]];
+        float d[3];
+        for (int a = 0; a < 3; a++) d[a] = (c.lo[a] + c.hi[a]) * 0.5f - pc[a];
+        for (int s = 0; s < 8; s++)
+            cost[k][s] = ((s & 1) ? -d[0] : d[0]) + ((s & 2) ? -d[1] : d[1]) + ((s & 4) ? -d[2] : d[2]);
+    }
+    int slot_kid[8];
+    for (int s = 0; s < 8; s++) slot_kid[s] = -1;
+    unsigned used_k = 0, used_s = 0;
+    for (int r = 0; r < nk; r++) {
+        float bc = FLT_MAX;
+        int bk = -1, bs = -1;
+        for (int k = 0; k < nk; k++) {
+            if (used_k & (1u << k)) continue;
+            for (int s = 0; s < 8; s++) {
+                if (used_s & (1u << s)) continue;
+                if (cost[k][s] < bc || bk < 0) { bc = cost[k][s]; bk = k; bs = s; }
+            }
+        }
+        used_k |= 1u << bk;
+        used_s |= 1u << bs;
+        slot_kid[bs] = kid[bk];
+    }
+    Gather g;
+    int ni = 0, nt = 0;
+    for (int s = 0; s < 8; s++) {
+        g.kid[s] = slot_kid[s];
+        if (slot_kid[s] < 0) continue;
+        const Node2 c = nodes[slot_kid[s]];
+        if (is_leaf2(c)) nt += -c.b;
+        else ni++;
+    }
+    out[i] = g;
+    n_inner[i] = ni;
+    n_items[i] = nt;
+}
+
+// smallest e with 255 * 2^e >= ext (ext > 0), from the exact double value
+__device__ __forceinline__ int grid_exponent(double ext) {
+    int k;
+    const double m = frexp(ext / 255.0, &k);  // ext/255 = m * 2^k, m in [0.5, 1)
+    int e = (m == 0.5) ? k - 1 : k;
+    // ext/255 rounding in double can undershoot by one ulp; make sure 255*2^e >= ext
+    if (ldexp(255.0, e) < ext) e++;
+    return e;
+}
+
+__global__ void k_emit(const Node2* __restrict__ nodes, const int* __restrict__ level, int L,
+                       const Gather* __restrict__ gat, const int* __restrict__ inner_off,
+                       const int* __restrict__ item_off, int child_base0, int item_base0,
+                       const int* __restrict__ perm, const float* __restrict__ tris9,
+                       Bvh8Node* __restrict__ out_nodes, int out_base, TriRec* __restrict__ out_tris,
+                       int* __restrict__ out_ids, int* __restrict__ next_level) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L) return;
+    const Gather g = gat[i];
+    const int child_base = child_base0 + inner_off[i];
+    const int tri_base = item_base0 + item_off[i];
+    // node box = union of the children
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int s = 0; s < 8; s++) {
+        if (g.kid[s] < 0) continue;
+        const Node2 c = nodes[g.kid[s]];
+        for (int a = 0; a < 3; a++) {
+            lo[a] = fminf(lo[a], c.lo[a]);
+            hi[a] = fmaxf(hi[a], c.hi[a]);
+        }
+    }
+    uint32_t ebytes[3];
+    double scale[3];
+    for (int a = 0; a < 3; a++) {
+        const double ext = (double)hi[a] - (double)lo[a];
+        if (!(ext > 0.0)) {
+            ebytes[a] = 0;
+            scale[a] = 0.0;
+        } else {
+            int e = grid_exponent(ext);
+            if (e < -126) e = -126;
+            if (e > 127) e = 127;
+            ebytes[a] = (uint32_t)(e + 127);
+            scale[a] = ldexp(1.0, e);
+        }
+    }
+    uint32_t imask = 0;
+    uint32_t meta[2] = {0, 0};
+    uint32_t qlo[3][2] = {{0, 0}, {0, 0}, {0, 0}}, qhi[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+    int inner_seen = 0, offset = 0;
+    for (int s = 0; s < 8; s++) {
+        const int k = g.kid[s];
+        if (k < 0) continue;
+        const Node2 c = nodes[k];
+        for (int a = 0; a < 3; a++) {
+            uint32_t ql = 0, qh = 0;
+            if (scale[a] > 0.0) {
+                double fl = floor(((double)c.lo[a] - (double)lo[a]) / scale[a]);
+                double ch = ceil(((double)c.hi[a] - (double)lo[a]) / scale[a]);
+                fl = fmin(fmax(fl, 0.0), 255.0);
+                ch = fmin(fmax(ch, 0.0), 255.0);
+                ql = (uint32_t)fl;
+                qh = (uint32_t)ch;
+            }
+            qlo[a][s >> 2] |= ql << ((s & 3) * 8);
+            qhi[a][s >> 2] |= qh << ((s & 3) * 8);
+        }
+        uint32_t m;
+        if (is_leaf2(c)) {
+            const int cnt = -c.b;
+            m = ((uint32_t)cnt << 5) | (uint32_t)offset;
+            for (int j = 0; j < cnt; j++) {
+                const int prim = perm[c.a + j];
+                const int dst = tri_base + offset + j;
+                if (tris9) {
+                    const float* t = tris9 + (size_t)prim * 9;
+                    TriRec r;
+                    r.a = make_float4(t[0], t[1], t[2], __int_as_float(prim));
+                    r.b = make_float4(__fsub_rn(t[3], t[0]), __fsub_rn(t[4], t[1]), __fsub_rn(t[5], t[2]), 0.f);
+                    r.c = make_float4(__fsub_rn(t[6], t[0]), __fsub_rn(t[7], t[1]), __fsub_rn(t[8], t[2]), 0.f);
+                    out_tris[dst] = r;
+                } else {
+                    out_ids[dst] = prim;
+                }
+            }
+            offset += cnt;
+        } else {
+            imask |= 1u << s;
+            m = 0xFFu;
+            next_level[inner_off[i] + inner_seen] = k;
+            inner_seen++;
+        }
+        meta[s >> 2] |= m << ((s & 3) * 8);
+    }
+    Bvh8Node nd;
+    nd.w[0] = make_uint4(__float_as_uint(lo[0]), __float_as_uint(lo[1]), __float_as_uint(lo[2]),
+                         ebytes[0] | (ebytes[1] << 8) | (ebytes[2] << 16) | (imask << 24));
+    nd.w[1] = make_uint4((uint32_t)child_base, (uint32_t)tri_base, meta[0], meta[1]);
+    nd.w[2] = make_uint4(qlo[0][0], qlo[0][1], qhi[0][0], qhi[0][1]);
+    nd.w[3] = make_uint4(qlo[1][0], qlo[1][1], qhi[1][0], qhi[1][1]);
+    nd.w[4] = make_uint4(qlo[2][0], qlo[2][1], qhi[2][0], qhi[2][1]);
+    out_nodes[out_base + i] = nd;
+}
+
+bool collapse_bvh8(const Bvh2Device& b2, const float* d_tris9, Bvh8Device& out, cudaStream_t s) {
+    const int n = b2.num_prims;
+    // upper bound on 8-wide nodes: every node has >= 2 children except a
+    // root that is a single leaf, so nodes <= leaves <= n
+    const int max_nodes = n + 1;
+    if (!out.nodes.alloc(max_nodes)) return false;
+    if (d_tris9) {
+        if (!out.tris.alloc(n)) return false;
+    } else {
+        if (!out.leaf_ids.alloc(n)) return false;
+    }
+    DevBuf<int> lvl_a, lvl_b, n_inner, n_items, inner_off, item_off, tot;
+    DevBuf<Gather> gat;
+    if (!lvl_a.alloc(max_nodes) || !lvl_b.alloc(max_nodes) || !n_inner.alloc(max_nodes) ||
+        !n_items.alloc(max_nodes) || !inner_off.alloc(max_nodes) || !item_off.alloc(max_nodes) ||
+        !gat.alloc(max_nodes) || !tot.alloc(2))
+        return false;
+    cudaMemsetAsync(lvl_a.p, 0, sizeof(int), s);  // root binary node 0
+    int L = 1, level_base = 0, items = 0, depth = 0;
+    int* cur = lvl_a.p;
+    int* nxt = lvl_b.p;
+    while (L > 0) {
+        k_gather<<<(L + 127) / 128, 128, 0, s>>>(b2.nodes.p, cur, L, gat.p, n_inner.p, n_items.p);
+        if (!scan_exclusive(n_inner.p, inner_off.p, L, tot.p, s)) return false;
+        if (!scan_exclusive(n_items.p, item_off.p, L, tot.p + 1, s)) return false;
+        int h[2];
+        cudaMemcpyAsync(h, tot.p, sizeof(h), cudaMemcpyDeviceToHost, s);
+        if (!RT_CUDA(cudaStreamSynchronize(s))) return false;
+        const int child_base = level_base + L;
+        if (child_base + h[0] > max_nodes || items + h[1] > n) {
+            set_error("collapse: capacity exceeded");
+            return false;
+        }
+        k_emit<<<(L + 127) / 128, 128, 0, s>>>(b2.nodes.p, cur, L, gat.p, inner_off.p, item_off.p, child_base, items,
+                                               b2.perm.p, d_tris9, out.nodes.p, level_base, out.tris.p,
+                                               out.leaf_ids.p, nxt);
+        level_base = child_base;
+        items += h[1];
+        L = h[0];
+        std::swap(cur, nxt);
+        depth++;
+    }
+    out.num_nodes = level_base;
+    out.num_leaf_items = items;
+    out.depth = depth;
+    return RT_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------- SAH --
+__global__ void k_sah(const Node2* __restrict__ nodes, int m, float* __restrict__ acc) {
+    float s = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const Node2 n = nodes[i];
+        if (n.b == 0 && i != 0) continue;  // unused reserved slot
+        const float dx = n.hi[0] - n.lo[0], dy = n.hi[1] - n.lo[1], dz = n.hi[2] - n.lo[2];
+        const float a = dx * dy + dy * dz + dz * dx;
+        s += n.b < 0 ? a * (float)(-n.b) : a;
+    }
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(acc, s);
+}
+
+float bvh2_sah_cost(const Bvh2Device& b2, cudaStream_t s) {
+    DevBuf<float> acc;
+    if (!acc.alloc(1)) return -1.f;
+    cudaMemsetAsync(acc.p, 0, sizeof(float), s);
+    k_sah<<<std::min((b2.num_nodes + 255) / 256, 1024), 256, 0, s>>>(b2.nodes.p, b2.num_nodes, acc.p);
+    float total = 0.f;
+    Node2 root;
+    cudaMemcpyAsync(&total, acc.p, sizeof(float), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&root, b2.nodes.p, sizeof(Node2), cudaMemcpyDeviceToHost, s);
+    if (!RT_CUDA(cudaStreamSynchronize(s))) return -1.f;
+    const float dx = root.hi[0] - root.lo[0], dy = root.hi[1] - root.lo[1], dz = root.hi[2] - root.lo[2];
+    const float ra = dx * dy + dy * dz + dz * dx;
+    return ra > 0.f ? total / ra : 0.f;
+}
+
+}  // namespace rtb

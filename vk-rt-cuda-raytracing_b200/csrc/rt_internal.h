@@ -1,0 +1,148 @@
+// rt_internal.h -- host-side structures shared by the library's translation
+// units (handles, device buffers, error reporting, launch helpers).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/cuda_bvh_backend.h"
+#include "../../include/rt_b200.h"
+#include "rt_common.cuh"
+
+namespace rtb {
+
+// ---- error reporting (thread-local last error; no entry point aborts) ----
+void set_error(const char* fmt, ...);
+void clear_error();
+bool cuda_ok(cudaError_t e, const char* what);
+#define RT_CUDA(call) ::rtb::cuda_ok((call), #call)
+
+int num_sms();
+
+// ---- a typed device buffer ----
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    bool alloc(size_t count) {
+        release();
+        if (count == 0) return true;
+        if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            set_error("cudaMalloc of %zu bytes failed", count * sizeof(T));
+            return false;
+        }
+        n = count;
+        return true;
+    }
+    bool ensure(size_t count) { return count <= n ? true : alloc(count); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// ---- build configuration ----
+struct BuildConfig {
+    int max_leaf = 4;        // triangles per BVH2 leaf (1..kMaxLeafTris)
+    int small_task = 1024;   // tasks at or below this size finish in one CTA
+    int max_sah_depth = 48;  // deeper tasks fall back to median splits
+};
+
+// Result of the SAH builder on the device.
+struct Bvh2Device {
+    DevBuf<Node2> nodes;     // capacity 2N (reserved slots may stay unused)
+    DevBuf<int> perm;        // leaf order -> primitive index
+    int num_nodes = 0;       // slots used (incl. unused reservations)
+    int num_prims = 0;
+};
+
+// The compressed 8-wide structure the traversal kernels read.
+struct Bvh8Device {
+    DevBuf<Bvh8Node> nodes;
+    DevBuf<TriRec> tris;     // BLAS: triangle records in node order
+    DevBuf<int> leaf_ids;    // TLAS: instance index per leaf slot
+    int num_nodes = 0;
+    int num_leaf_items = 0;
+    int depth = 0;
+};
+
+// Builds the binary SAH BVH over primitive boxes (lo/hi float4 per prim).
+// Returns false on failure (error set).  Stream-ordered; synchronises on
+// small counts between levels.
+bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig& cfg, Bvh2Device& out,
+                cudaStream_t s);
+
+// Collapses a BVH2 into the 8-wide layout.  For a BLAS d_tris9 holds the
+// triangles (9 floats each) and TriRec records are written; for a TLAS
+// d_tris9 is null and leaf_ids receives primitive (instance) indices.
+bool collapse_bvh8(const Bvh2Device& b2, const float* d_tris9, Bvh8Device& out, cudaStream_t s);
+
+// Primitive boxes.
+void launch_tri_bounds(const float* d_tris9, int n, float4* d_lo, float4* d_hi, cudaStream_t s);
+
+// Exclusive scan of n ints (device), total written to *d_total if non-null.
+bool scan_exclusive(const int* d_in, int* d_out, int n, int* d_total, cudaStream_t s);
+
+// Host structural check of an 8-wide structure (error set on failure).
+bool validate_bvh8(const Bvh8Device& b, int num_items, int num_prims);
+
+// SAH cost (root-area normalised) of a BVH2.
+float bvh2_sah_cost(const Bvh2Device& b2, cudaStream_t s);
+
+}  // namespace rtb
+
+// ---- the handle behind CudaBVH_t ----
+struct CudaBVHHandle {
+    int num_tris = 0;
+    float bmin[3], bmax[3], center[3], extent = 0.f;
+    rtb::DevBuf<float> tris9;     // input triangles (device copy)
+    rtb::Bvh2Device bvh2;
+    rtb::Bvh8Device bvh8;
+    RtBuildStats stats{};
+    std::mutex mu;                // guards lazy host exports and staging
+    // lazily built host exports for the layer's Vulkan path
+    std::vector<uint32_t> h_dfs;
+    std::vector<float> h_packed;
+    std::vector<unsigned char> h_bvh4;
+    std::vector<float> h_soa[9];
+    bool exports_ready = false;
+    int num_bvh4 = -1;
+    // per-call scratch: work counters (ring) and host staging
+    rtb::DevBuf<int> counters;
+    unsigned counter_next = 0;
+    rtb::DevBuf<RtRay> stage_rays;
+    rtb::DevBuf<RtHit> stage_hits;
+    rtb::DevBuf<uint8_t> stage_occ;
+    rtb::DevBuf<float> stage_f;
+    rtb::DevBuf<int> status;      // device status word (overflow / errors)
+};
+
+struct CudaTLASHandle {
+    int num_instances = 0;
+    std::vector<CudaBVH_t> blas;
+    rtb::Bvh2Device bvh2;
+    rtb::Bvh8Device bvh8;
+    rtb::DevBuf<float4> inst;     // per instance: inv xform (3 float4) + blas ptrs (1 float4)
+    std::vector<float> h_inv;     // 12 floats per instance
+    rtb::DevBuf<int> counters;
+    unsigned counter_next = 0;
+    rtb::DevBuf<int> status;
+    std::mutex mu;
+};
+
+namespace rtb {
+int* next_counter(rtb::DevBuf<int>& ring, unsigned& next, cudaStream_t s);
+bool ensure_counters(rtb::DevBuf<int>& ring);
+}  // namespace rtb

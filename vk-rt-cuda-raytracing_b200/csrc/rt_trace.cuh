@@ -1,0 +1,113 @@
+// rt_trace.cuh -- traversal building blocks shared by the single-level,
+// two-level and wavefront kernels.
+#pragma once
+#include "rt_common.cuh"
+
+namespace rtb {
+
+constexpr unsigned FULL_MASK = 0xFFFFFFFFu;
+constexpr int TRACE_T = 128;   // threads per persistent CTA
+constexpr int TRACE_MINB = 4;  // CTAs per SM the register budget must allow
+constexpr int SSTACK = 8;      // stack entries per thread in shared memory
+constexpr int LSTACK = 56;     // further entries in local memory (64 total)
+constexpr int SSTACK_TOTAL = SSTACK + LSTACK;
+constexpr int RT_STATUS_STACK = 1;
+constexpr int RT_STATUS_TIMEOUT = 2;
+
+struct Ray {
+    float ox, oy, oz, tmin;
+    float dx, dy, dz, tmax;
+    float ix, iy, iz;  // 1/d, IEEE (+-inf for a zero component)
+    uint32_t oct;      // sign bits of 1/d: x -> 1, y -> 2, z -> 4
+};
+
+__device__ __forceinline__ Ray make_ray(float4 a, float4 b) {
+    Ray r;
+    r.ox = a.x; r.oy = a.y; r.oz = a.z; r.tmin = a.w;
+    r.dx = b.x; r.dy = b.y; r.dz = b.z; r.tmax = b.w;
+    r.ix = __fdiv_rn(1.0f, r.dx);
+    r.iy = __fdiv_rn(1.0f, r.dy);
+    r.iz = __fdiv_rn(1.0f, r.dz);
+    r.oct = (signbit(r.ix) ? 1u : 0u) | (signbit(r.iy) ? 2u : 0u) | (signbit(r.iz) ? 4u : 0u);
+    return r;
+}
+
+__device__ __forceinline__ Ray load_ray(const RtRay* rays, int i) {
+    const float4* p = reinterpret_cast<const float4*>(rays + i);
+    return make_ray(__ldg(p), __ldg(p + 1));
+}
+
+// Stack of node groups: x = child base, y = hit mask (8 bits, near-to-far
+// order) | inner mask << 8 | flags << 16.
+struct Walk {
+    uint2 ng;
+    int sp;
+    __device__ __forceinline__ void start() { sp = 0; }
+    __device__ __forceinline__ bool push(uint2 e, uint2 (*ss)[TRACE_T], uint2* ls) {
+        if (sp < SSTACK) ss[sp][threadIdx.x] = e;
+        else if (sp < SSTACK + LSTACK) ls[sp - SSTACK] = e;
+        else return false;
+        sp++;
+        return true;
+    }
+    __device__ __forceinline__ uint2 pop(uint2 (*ss)[TRACE_T], uint2* ls) {
+        sp--;
+        return sp < SSTACK ? ss[sp][threadIdx.x] : ls[sp - SSTACK];
+    }
+};
+
+// Fetches one 8-wide node and tests its eight child boxes against the ray
+// segment [tmin, thit].  Outputs the node group of hit inner children
+// (`ng`), and the triangle base + 32-bit mask of hit leaf triangles.
+__device__ __forceinline__ void visit_node(const uint4* __restrict__ np, const Ray& r, float thit,
+                                           uint32_t& inner_hits, uint32_t& tri_base, uint32_t& tmask, uint2& ng) {
+    const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+    const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+    const uint32_t e = w0.w;
+    const float sx = __uint_as_float((e & 0xFFu) << 23);
+    const float sy = __uint_as_float(((e >> 8) & 0xFFu) << 23);
+    const float sz = __uint_as_float(((e >> 16) & 0xFFu) << 23);
+    const uint32_t imask = e >> 24;
+    // per axis: S = s/d, O = (p - o)/d, slack E = 2^-22 |O|
+    const float Sx = sx * r.ix, Sy = sy * r.iy, Sz = sz * r.iz;
+    const float Ox = (px - r.ox) * r.ix, Oy = (py - r.oy) * r.iy, Oz = (pz - r.oz) * r.iz;
+    const float Onx = fmaf(-fabsf(Ox), 0x1p-22f, Ox), Ofx = fmaf(fabsf(Ox), 0x1p-22f, Ox);
+    const float Ony = fmaf(-fabsf(Oy), 0x1p-22f, Oy), Ofy = fmaf(fabsf(Oy), 0x1p-22f, Oy);
+    const float Onz = fmaf(-fabsf(Oz), 0x1p-22f, Oz), Ofz = fmaf(fabsf(Oz), 0x1p-22f, Oz);
+    // near plane = lo for a positive 1/d, hi otherwise
+    const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
+    const uint32_t qnx0 = nx ? w2.z : w2.x, qnx1 = nx ? w2.w : w2.y, qfx0 = nx ? w2.x : w2.z, qfx1 = nx ? w2.y : w2.w;
+    const uint32_t qny0 = ny ? w3.z : w3.x, qny1 = ny ? w3.w : w3.y, qfy0 = ny ? w3.x : w3.z, qfy1 = ny ? w3.y : w3.w;
+    const uint32_t qnz0 = nz ? w4.z : w4.x, qnz1 = nz ? w4.w : w4.y, qfz0 = nz ? w4.x : w4.z, qfz1 = nz ? w4.y : w4.w;
+    uint32_t nh = 0, th = 0;
+#pragma unroll
+    for (int s = 0; s < 8; s++) {
+        const int sh = (s & 3) * 8;
+        const uint32_t bx0 = s < 4 ? qnx0 : qnx1, bx1 = s < 4 ? qfx0 : qfx1;
+        const uint32_t by0 = s < 4 ? qny0 : qny1, by1 = s < 4 ? qfy0 : qfy1;
+        const uint32_t bz0 = s < 4 ? qnz0 : qnz1, bz1 = s < 4 ? qfz0 : qfz1;
+        const float tnx = fmaf((float)((bx0 >> sh) & 0xFFu), Sx, Onx);
+        const float tfx = fmaf((float)((bx1 >> sh) & 0xFFu), Sx, Ofx);
+        const float tny = fmaf((float)((by0 >> sh) & 0xFFu), Sy, Ony);
+        const float tfy = fmaf((float)((by1 >> sh) & 0xFFu), Sy, Ofy);
+        const float tnz = fmaf((float)((bz0 >> sh) & 0xFFu), Sz, Onz);
+        const float tfz = fmaf((float)((bz1 >> sh) & 0xFFu), Sz, Ofz);
+        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, r.tmin));
+        const float tf = fminf(fminf(tfx, tfy), fminf(tfz, thit));
+        const bool hit = tn <= fmaf(fabsf(tf), 0x1p-21f, tf);
+        const uint32_t meta = ((s < 4 ? w1.z : w1.w) >> sh) & 0xFFu;
+        if (hit) {
+            if ((imask >> s) & 1u) {
+                nh |= 1u << ((uint32_t)s ^ r.oct);
+            } else if (meta) {
+                th |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
+            }
+        }
+    }
+    inner_hits = nh;
+    tri_base = w1.y;
+    tmask = th;
+    ng = make_uint2(w1.x, nh | (imask << 8));
+}
+
+}  // namespace rtb

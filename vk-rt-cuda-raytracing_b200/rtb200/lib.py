@@ -1,0 +1,271 @@
+"""ctypes binding of libcudabvh_b200.so (the C-ABI in include/*.h).
+
+The library is the product; this module only declares its signatures and
+wraps the handles.  It raises if the shared library is missing: there is no
+fallback path.  Device buffers are torch CUDA tensors (plumbing only); their
+data_ptr() is what crosses the C-ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from pathlib import Path
+
+import numpy as np
+
+from .scenes import HIT_DTYPE, RAY_DTYPE
+
+PKG_ROOT = Path(__file__).resolve().parent.parent
+LIB_PATH = PKG_ROOT / "lib" / "libcudabvh_b200.so"
+INCLUDE_DIR = PKG_ROOT.parent / "include"
+
+_lib = None
+
+
+class RtError(RuntimeError):
+    pass
+
+
+class RtBuildStats(C.Structure):
+    _fields_ = [("num_tris", C.c_int), ("num_bvh2_nodes", C.c_int), ("num_nodes", C.c_int), ("depth", C.c_int),
+                ("max_leaf", C.c_int), ("bins", C.c_int), ("build_ms", C.c_float), ("sah_cost", C.c_float),
+                ("node_bytes", C.c_uint64), ("tri_bytes", C.c_uint64)]
+
+
+class RtInstance(C.Structure):
+    _fields_ = [("xform", C.c_float * 12), ("blas", C.c_int32), ("mask", C.c_uint32), ("custom", C.c_uint32),
+                ("pad", C.c_uint32)]
+
+
+def declared_symbols() -> list[str]:
+    """Function names declared in include/*.h."""
+    names = []
+    for h in sorted(INCLUDE_DIR.glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        for m in re.finditer(r"^\s*[A-Za-z_][\w\s\*]*?\b(\w+)\s*\(", text, flags=re.M):
+            name = m.group(1)
+            if name not in ("if", "defined") and not name.startswith("__"):
+                names.append(name)
+    return sorted(set(names))
+
+
+def load(path: str | os.PathLike | None = None) -> C.CDLL:
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RtError(f"libcudabvh_b200.so not built: {p} (run __graft_entry__.build())")
+    L = C.CDLL(str(p))
+    vp, i32, f32, u64 = C.c_void_p, C.c_int, C.c_float, C.c_uint64
+    sig = {
+        "rtGetLastError": (C.c_char_p, []),
+        "cudaBVH_build": (vp, [vp, i32]),
+        "cudaBVH_buildDevice": (vp, [vp, i32, vp]),
+        "cudaBVH_buildFromAABBs": (vp, [vp, i32]),
+        "cudaBVH_destroy": (None, [vp]),
+        "cudaBVH_traceClosest": (i32, [vp, vp, i32, vp, vp]),
+        "cudaBVH_traceAny": (i32, [vp, vp, i32, vp, vp]),
+        "cudaBVH_traceClosestHost": (i32, [vp, vp, i32, vp]),
+        "cudaBVH_traceAnyHost": (i32, [vp, vp, i32, vp]),
+        "cudaBVH_traceCounters": (i32, [vp, vp, i32, i32, vp, vp]),
+        "cudaBVH_validate": (i32, [vp]),
+        "cudaBVH_getBuildStats": (i32, [vp, C.POINTER(RtBuildStats)]),
+        "cudaBVH_getDeviceLayout": (i32, [vp, C.POINTER(vp), C.POINTER(i32), C.POINTER(vp), C.POINTER(i32)]),
+        "cudaBVH_tracePrimary": (f32, [vp, i32, f32, f32, f32, vp]),
+        "cudaBVH_traceDiffuse": (f32, [vp, i32, vp, vp, vp, vp, vp, vp, vp]),
+        "cudaBVH_traceToRGBA": (i32, [vp, i32, i32, f32, f32, f32, vp]),
+        "cudaBVH_traceToGPUPtr": (i32, [vp, i32, i32, f32, f32, f32, vp, i32]),
+        "cudaBVH_traceToGPUAsync": (None, [vp, i32, i32, f32, f32, f32, vp, i32]),
+        "cudaBVH_traceToHostPtr": (i32, [vp, i32, i32, f32, f32, f32, vp, i32, u64]),
+        "cudaBVH_importBufferFd": (vp, [i32, u64]),
+        "cudaBVH_readGPUMemoryFd": (i32, [i32, u64, u64, u64, vp]),
+        "cudaBVH_getBounds": (None, [vp] + [C.POINTER(f32)] * 4),
+        "cudaBVH_getNumTris": (i32, [vp]),
+        "cudaBVH_getNumBVH4Nodes": (i32, [vp]),
+        "cudaBVH_getNumCWBVHNodes": (i32, [vp]),
+        "cudaBVH_getNodeData": (vp, [vp]),
+        "cudaBVH_getTriData": (None, [vp, vp]),
+        "cudaBVH_getStacklessBVH2": (i32, [vp, C.POINTER(C.POINTER(C.c_uint32))]),
+        "cudaBVH_getPackedTris": (i32, [vp, C.POINTER(C.POINTER(C.c_float))]),
+        "cudaBVH_resetDevice": (None, []),
+        "cudaBVH_buildTLASFast": (i32, [vp, i32, C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.POINTER(C.c_int))]),
+        "cudaTLAS_build": (vp, [vp, i32, vp, i32]),
+        "cudaTLAS_destroy": (None, [vp]),
+        "cudaTLAS_traceClosest": (i32, [vp, vp, i32, vp, vp, vp]),
+        "cudaTLAS_traceAny": (i32, [vp, vp, i32, vp, vp]),
+        "cudaTLAS_getInverseTransforms": (i32, [vp, vp, i32]),
+    }
+    for name, (res, args) in sig.items():
+        if not hasattr(L, name):
+            continue  # test_abi checks completeness against the headers
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    if path is None:
+        _lib = L
+    return L
+
+
+def last_error() -> str:
+    return load().rtGetLastError().decode()
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        raise RtError(f"{what} failed ({rc}): {last_error()}")
+
+
+def _ptr(x) -> int:
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    return int(x)
+
+
+def _stream(stream) -> int | None:
+    if stream is None:
+        return None
+    return stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+
+
+class BVH:
+    """A BLAS: cudaBVH_build (host triangles) or cudaBVH_buildDevice."""
+
+    def __init__(self, tris=None, *, device_tris=None, n: int | None = None, stream=None, handle=None):
+        L = load()
+        if handle is not None:
+            self.h = handle
+        elif device_tris is not None:
+            self.h = L.cudaBVH_buildDevice(_ptr(device_tris), int(n), _stream(stream))
+        else:
+            tris = np.ascontiguousarray(tris, dtype=np.float32).reshape(-1, 9)
+            self.h = L.cudaBVH_build(tris.ctypes.data, tris.shape[0])
+        if not self.h:
+            raise RtError(f"build failed: {last_error()}")
+
+    @classmethod
+    def from_aabbs(cls, aabbs: np.ndarray) -> "BVH":
+        a = np.ascontiguousarray(aabbs, dtype=np.float32).reshape(-1, 6)
+        h = load().cudaBVH_buildFromAABBs(a.ctypes.data, a.shape[0])
+        if not h:
+            raise RtError(f"build failed: {last_error()}")
+        return cls(handle=h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().cudaBVH_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- traversal on device buffers --
+    def closest(self, d_rays, n: int, d_hits, stream=None):
+        _check(load().cudaBVH_traceClosest(self.h, _ptr(d_rays), n, _ptr(d_hits), _stream(stream)),
+               "cudaBVH_traceClosest")
+
+    def any(self, d_rays, n: int, d_occ, stream=None):
+        _check(load().cudaBVH_traceAny(self.h, _ptr(d_rays), n, _ptr(d_occ), _stream(stream)), "cudaBVH_traceAny")
+
+    def counters(self, d_rays, n: int, d_counts, any_hit: bool = False, stream=None):
+        _check(load().cudaBVH_traceCounters(self.h, _ptr(d_rays), n, int(any_hit), _ptr(d_counts), _stream(stream)),
+               "cudaBVH_traceCounters")
+
+    # -- traversal on host buffers --
+    def closest_host(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
+        hits = np.zeros(rays.shape[0], dtype=HIT_DTYPE)
+        _check(load().cudaBVH_traceClosestHost(self.h, rays.ctypes.data, rays.shape[0], hits.ctypes.data),
+               "cudaBVH_traceClosestHost")
+        return hits
+
+    def any_host(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
+        occ = np.zeros(rays.shape[0], dtype=np.uint8)
+        _check(load().cudaBVH_traceAnyHost(self.h, rays.ctypes.data, rays.shape[0], occ.ctypes.data),
+               "cudaBVH_traceAnyHost")
+        return occ
+
+    # -- introspection / exports --
+    def validate(self):
+        _check(load().cudaBVH_validate(self.h), "cudaBVH_validate")
+
+    def stats(self) -> dict:
+        s = RtBuildStats()
+        _check(load().cudaBVH_getBuildStats(self.h, C.byref(s)), "cudaBVH_getBuildStats")
+        return {f: getattr(s, f) for f, _ in RtBuildStats._fields_}
+
+    def layout(self):
+        n_nodes, n_tris = C.c_int(), C.c_int()
+        pn, pt = C.c_void_p(), C.c_void_p()
+        _check(load().cudaBVH_getDeviceLayout(self.h, C.byref(pn), C.byref(n_nodes), C.byref(pt), C.byref(n_tris)),
+               "cudaBVH_getDeviceLayout")
+        return pn.value, n_nodes.value, pt.value, n_tris.value
+
+    def bounds(self):
+        f = [C.c_float() for _ in range(4)]
+        load().cudaBVH_getBounds(self.h, *[C.byref(x) for x in f])
+        return np.array([x.value for x in f], np.float32)
+
+    def exports(self) -> dict:
+        L = load()
+        pd = C.POINTER(C.c_uint32)()
+        nd = L.cudaBVH_getStacklessBVH2(self.h, C.byref(pd))
+        pp = C.POINTER(C.c_float)()
+        npk = L.cudaBVH_getPackedTris(self.h, C.byref(pp))
+        nb4 = L.cudaBVH_getNumBVH4Nodes(self.h)
+        b4p = L.cudaBVH_getNodeData(self.h)
+        ptrs = (C.c_void_p * 9)()
+        L.cudaBVH_getTriData(self.h, C.byref(ptrs))
+        ntri = L.cudaBVH_getNumTris(self.h)
+        return {
+            "dfs": np.ctypeslib.as_array(pd, shape=(nd * 8,)).copy() if nd else np.zeros(0, np.uint32),
+            "packed": np.ctypeslib.as_array(pp, shape=(npk * 4,)).copy() if npk else np.zeros(0, np.float32),
+            "bvh4": np.frombuffer(C.string_at(b4p, nb4 * 64), np.uint8).copy() if nb4 else np.zeros(0, np.uint8),
+            "soa": np.stack([np.ctypeslib.as_array(C.cast(ptrs[i], C.POINTER(C.c_float)), shape=(ntri,)).copy()
+                             for i in range(9)]),
+            "num_cwbvh": L.cudaBVH_getNumCWBVHNodes(self.h),
+        }
+
+    # -- reference-shaped traces --
+    def trace_primary(self, side: int, cam, want_t: bool = True):
+        t = np.zeros(side * side, np.float32) if want_t else None
+        mrs = load().cudaBVH_tracePrimary(self.h, side, float(cam[0]), float(cam[1]), float(cam[2]),
+                                          t.ctypes.data if want_t else None)
+        return mrs, t
+
+    def trace_diffuse(self, org: np.ndarray, dirs: np.ndarray):
+        n = org.shape[0]
+        cols = [np.ascontiguousarray(org[:, k], np.float32) for k in range(3)] + \
+               [np.ascontiguousarray(dirs[:, k], np.float32) for k in range(3)]
+        t = np.zeros(n, np.float32)
+        mrs = load().cudaBVH_traceDiffuse(self.h, n, *[c.ctypes.data for c in cols], t.ctypes.data)
+        return mrs, t
+
+    def trace_rgba(self, w: int, h: int, cam) -> np.ndarray:
+        out = np.zeros(w * h, np.uint32)
+        _check(load().cudaBVH_traceToRGBA(self.h, w, h, float(cam[0]), float(cam[1]), float(cam[2]),
+                                          out.ctypes.data), "cudaBVH_traceToRGBA")
+        return out
+
+
+def tlas_fast(aabbs: np.ndarray):
+    a = np.ascontiguousarray(aabbs, dtype=np.float32).reshape(-1, 6)
+    L = load()
+    pn = C.POINTER(C.c_uint32)()
+    po = C.POINTER(C.c_int)()
+    m = L.cudaBVH_buildTLASFast(a.ctypes.data, a.shape[0], C.byref(pn), C.byref(po))
+    if m <= 0:
+        return np.zeros(0, np.uint32), np.zeros(0, np.int32)
+    nodes = np.ctypeslib.as_array(pn, shape=(m * 8,)).copy()
+    ordered = np.ctypeslib.as_array(po, shape=(a.shape[0],)).copy()
+    libc = C.CDLL("libc.so.6")
+    libc.free(C.cast(pn, C.c_void_p))
+    libc.free(C.cast(po, C.c_void_p))
+    return nodes, ordered
