@@ -1,0 +1,385 @@
+#!/usr/bin/env python3
+"""Benchmark: incoherent closest-hit Mrays/s on one B200 (the configs[1]
+workload: 2M cosine-weighted diffuse bounce rays, closest hit, from the hit
+points of a 1920x1080 pinhole camera, against a seeded 2,000,000-triangle
+scene of random sphere and box meshes; plus 2M area-light shadow rays, any
+hit, reported beside it).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one closest-hit pass over the 2M-ray batch.  `value` is device
+time (CUDA events on the launching stream, L2 flushed between steps) of the
+traversal kernel; `e2e` goes through the C-ABI entry point a user calls with
+pinned host buffers (host->device rays, trace, device->host hits, every
+step).  Multi-GPU: one process per GPU, each holds a replica of the scene and
+traces its own ray batch (weak scaling, no collective on the data path);
+time = max over ranks.  `--impl reference` times the reference's CPU path
+(its own builder, compiled from its sources, plus the restated traversal)
+on the host cores.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "vk-rt-cuda-raytracing_b200"))
+
+METRIC = "Mrays/s incoherent closest-hit; p99 trace latency served vs plain, 1 B200"
+UNIT = "Mrays/s"
+N_TRIS = 2_000_000
+N_RAYS = 2_000_000
+L2_FLUSH_BYTES = 256 << 20
+TRI_BYTES_MIN = 36  # minimal fp32 triangle charged per test (3 x float3)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(seed_scene=1):
+    from rtb200 import scenes
+    t0 = time.time()
+    tris = scenes.scene_meshes(seed_scene, N_TRIS)
+    log(f"scene: {tris.shape[0]} tris in {time.time() - t0:.1f}s")
+    return tris
+
+
+def derive_rays(tris, bvh, torch):
+    """Primary 1080p hits (traced by the GPU) -> diffuse + shadow batches."""
+    from rtb200 import scenes
+    prim = scenes.primary_1080p()
+    d_prim = torch.from_numpy(prim.view(np.uint8).copy()).cuda()
+    d_hits = torch.empty(prim.shape[0] * 16, dtype=torch.uint8, device="cuda")
+    bvh.closest(d_prim, prim.shape[0], d_hits)
+    torch.cuda.synchronize()
+    ph = d_hits.cpu().numpy().view(scenes.HIT_DTYPE)
+    p, n = scenes.hit_frame(tris, prim, ph)
+    dif = scenes.diffuse_rays(p, n, N_RAYS, seed=3)
+    sha = scenes.shadow_rays(p, n, N_RAYS, seed=4)
+    return prim, dif, sha, float((ph["prim"] >= 0).mean())
+
+
+def time_steps(torch, fn, steps, warmup, flush):
+    """Per-step device time with CUDA events on the current stream, L2
+    flushed (256 MiB memset) between steps outside the events."""
+    s = torch.cuda.current_stream()
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for e0, e1 in evs:
+        flush.zero_()
+        e0.record(s)
+        fn()
+        e1.record(s)
+    torch.cuda.synchronize()
+    return [e0.elapsed_time(e1) for e0, e1 in evs]
+
+
+def reference_gpu_kernel(tris, d_rays, n, torch, steps, flush):
+    """The reference's traceBVH4Diffuse (cuda_rt_v40.cu:505) rebuilt for
+    sm_100a, on its own CPU-built BVH4 of the same scene, same rays."""
+    import ctypes as C
+    path = ROOT / "oracle" / "_ref" / "libref_v40.so"
+    if not path.exists():
+        return {"unavailable": "oracle/_ref/libref_v40.so not built"}
+    R = C.CDLL(str(path))
+    R.refv40_build.restype = C.c_void_p
+    R.refv40_build.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    R.refv40_trace_bvh4.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
+    R.refv40_destroy.argtypes = [C.c_void_p]
+    best = None
+    out = {"kernel": "traceBVH4Diffuse (cuda_rt_v40.cu:505), rebuilt sm_100a, -O3 --use_fast_math"}
+    d_h = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    for leaf in (3, 4):
+        t0 = time.time()
+        h = R.refv40_build(tris.ctypes.data, tris.shape[0], leaf)
+        out[f"cpu_build_s_leaf{leaf}"] = round(time.time() - t0, 2)
+        for blocks, thr in ((640, 256), (960, 256), (1280, 128)):
+            ms = time_steps(torch, lambda: R.refv40_trace_bvh4(h, d_rays.data_ptr(), d_h.data_ptr(), n, blocks, thr,
+                                                                st), steps, 2, flush)
+            v = n / (sum(ms) / len(ms)) / 1e3
+            if best is None or v > best[0]:
+                best = (v, leaf, blocks, thr)
+        R.refv40_destroy(h)
+    out.update({"value": round(best[0], 1), "unit": UNIT, "leaf": best[1], "grid": f"{best[2]}x{best[3]}"})
+    return out
+
+
+def cpu_baseline(tris, dif, budget_s=20.0):
+    """The restated scalar traversal (oracle) on the host cores over the
+    restated reference builder's BVH (32 bins, leaf 4), bounded sample."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    t0 = time.time()
+    ob = O.OracleBVH(tris, nbins=32, max_leaf=4)
+    build_s = time.time() - t0
+    n = 200_000
+    t0 = time.time()
+    ob.closest(dif[:n], nthreads=threads)
+    dt = time.time() - t0
+    # grow the sample to roughly budget_s of CPU work
+    m = int(min(dif.shape[0], max(n, n * budget_s / max(dt, 1e-3))))
+    t0 = time.time()
+    ob.closest(dif[:m], nthreads=threads)
+    dt = time.time() - t0
+    return {"value": round(m / dt / 1e6, 3), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {m} of the 2M diffuse rays, closest hit, restated traversal "
+                      f"(layer/shaders/bvh2_stackless.comp:37-76) over the restated reference SAH builder "
+                      f"(32 bins, leaf 4; build {build_s:.1f}s not timed)"}
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    from rtb200 import scenes
+    tris = make_workload()
+    # hit points from the reference's own builder + the restated traversal
+    threads = os.cpu_count() or 1
+    if O.ref_available():
+        ex = O.RefBackend().build_exports(tris)
+        dfs, packed, bvh_src = O.fix_skips(ex["dfs"]), ex["packed"], "reference builder (oracle/_ref, 16 bins, leaf 3)"
+    else:
+        ob = O.OracleBVH(tris, 16, 3)
+        dfs, packed, bvh_src = ob.dfs, ob.packed, "restated reference builder (16 bins, leaf 3)"
+    prim = scenes.primary_1080p()
+    ph = O.trace_closest_dfs(dfs, packed, prim, threads)
+    p, n = scenes.hit_frame(tris, prim, ph)
+    dif = scenes.diffuse_rays(p, n, N_RAYS, seed=3)
+    sample = 250_000
+    for _ in range(args.warmup):
+        O.trace_closest_dfs(dfs, packed, dif[:20_000], threads)
+    times = []
+    for k in range(args.steps):
+        t0 = time.time()
+        O.trace_closest_dfs(dfs, packed, dif[k * 1000: k * 1000 + sample], threads)
+        times.append(time.time() - t0)
+    v = sample / (sum(times) / len(times)) / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sum(times) / len(times), 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "incoherent_2m: 2M diffuse closest-hit rays vs 2M-triangle mesh scene",
+                       "sample_rays_per_step": sample},
+            "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{sample} diffuse rays per step; BVH from the {bvh_src}; "
+                                       "restated stackless traversal, one thread per core"},
+            "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from rtb200 import lib
+    lib.load()
+    tris = make_workload()
+    t0 = time.time()
+    bvh = lib.BVH(tris)
+    torch.cuda.synchronize()
+    stats = bvh.stats()
+    log(f"build: {stats['build_ms']:.1f} ms device, {time.time() - t0:.2f}s wall, {stats['num_nodes']} nodes, "
+        f"depth {stats['depth']}, SAH {stats['sah_cost']:.2f}")
+    prim, dif, sha, prim_hit = derive_rays(tris, bvh, torch)
+    d_dif = torch.from_numpy(dif.view(np.uint8).copy()).cuda()
+    d_sha = torch.from_numpy(sha.view(np.uint8).copy()).cuda()
+    d_hits = torch.empty(N_RAYS * 16, dtype=torch.uint8, device="cuda")
+    d_occ = torch.empty(N_RAYS, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    # algorithmic bytes per ray from the per-ray work counters (outside timing)
+    d_cnt = torch.zeros(N_RAYS * 2, dtype=torch.int32, device="cuda")
+    bvh.counters(d_dif, N_RAYS, d_cnt, stream=stream)
+    torch.cuda.synchronize()
+    cnt = d_cnt.cpu().numpy().reshape(-1, 2).astype(np.float64)
+    n_node, n_tri = float(cnt[:, 0].mean()), float(cnt[:, 1].mean())
+    bytes_per_ray = 32 + 16 + n_node * 80 + n_tri * TRI_BYTES_MIN
+
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ms = time_steps(torch, lambda: bvh.closest(d_dif, N_RAYS, d_hits, stream=stream), args.steps, args.warmup,
+                        flush)
+    t_step = sum(ms) / len(ms)
+    if ws > 1:
+        tt = torch.tensor([t_step], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_step = float(tt.item())
+    value = ws * N_RAYS / t_step / 1e3
+    ms_any = time_steps(torch, lambda: bvh.any(d_sha, N_RAYS, d_occ, stream=stream), args.steps, args.warmup, flush)
+    any_mrays = N_RAYS / (sum(ms_any) / len(ms_any)) / 1e3
+    hits = d_hits.cpu().numpy().view([("t", "<f4"), ("prim", "<i4"), ("u", "<f4"), ("v", "<f4")])
+
+    # end to end through the C-ABI with pinned host buffers
+    h_rays = torch.empty(N_RAYS * 32, dtype=torch.uint8, pin_memory=True)
+    h_rays.numpy()[:] = dif.view(np.uint8)
+    h_hits = torch.empty(N_RAYS * 16, dtype=torch.uint8, pin_memory=True)
+    L = lib.load()
+
+    def e2e_step():
+        rc = L.cudaBVH_traceClosestHost(bvh.h, h_rays.data_ptr(), N_RAYS, h_hits.data_ptr())
+        if rc != 0:
+            raise RuntimeError(lib.last_error())
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    e2e_val = ws * N_RAYS / (sum(e2e_ms) / len(e2e_ms)) / 1e3
+    assert np.array_equal(h_hits.numpy().view(hits.dtype)["prim"], hits["prim"]), "e2e hits differ"
+
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_per_ray * N_RAYS / (t_step * 1e-3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "trace_closest_incoherent_2m.json"
+    if prof.exists():
+        traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "incoherent_2m: 2M cosine-weighted diffuse closest-hit rays from 1920x1080 primary "
+                               "hits vs a seeded 2,000,000-triangle scene (sphere/box meshes 1K-20K tris)",
+                   "rays_per_step_per_gpu": N_RAYS, "triangles": N_TRIS, "bvh": "8-wide compressed, GPU SAH 32 bins",
+                   "l2": "flushed between timed steps (256 MiB memset outside the events)",
+                   "parallelism": f"replicas x{ws} (rays sharded per GPU, no collective)"},
+        "e2e": {"value": round(e2e_val, 1), "unit": UNIT, "h2d_bytes_per_step": N_RAYS * 32,
+                "d2h_bytes_per_step": N_RAYS * 16,
+                "path": "cudaBVH_traceClosestHost (C-ABI), pinned host rays in, hits out, every step"},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "peak_kind": f"{peak_kind} hbm_gbs (burst)",
+                     "bytes_per_ray": round(bytes_per_ray, 1), "nodes_per_ray": round(n_node, 2),
+                     "tris_per_ray": round(n_tri, 2),
+                     "formula": "32 ray + 16 hit + nodes*80 + tris*36"},
+        "anyhit_shadow_mrays": round(any_mrays, 1),
+        "build": {"device_ms": round(stats["build_ms"], 2), "nodes": stats["num_nodes"], "depth": stats["depth"],
+                  "sah_cost": round(stats["sah_cost"], 3)},
+        "hit_fraction": {"primary": round(prim_hit, 4), "diffuse": round(float((hits["prim"] >= 0).mean()), 4)},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_baselines:
+        out["reference_gpu_kernel"] = reference_gpu_kernel(tris, d_dif, N_RAYS, torch, max(3, args.steps // 2), flush)
+        if "value" in out["reference_gpu_kernel"]:
+            out["speedup_vs_reference_gpu_kernel"] = round(value / ws / out["reference_gpu_kernel"]["value"], 3)
+        out["cpu_baseline"] = cpu_baseline(tris, dif)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-baselines", action="store_true", help="skip the reference-kernel and CPU legs")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -117,7 +117,7 @@ def test_edge_cases(cuda):
     assert ref["prim"][-1] == -1
     # a hit exactly at tmax is rejected, just beyond it accepted
     r1 = np.zeros(2, RAY_DTYPE)
-    r1["org"] = (0.5, 10.0, 0.5)
+    r1["org"] = (3.5, 10.0, 3.5)  # above the y = -3 plane, clear of the box and the y = 5 plane
     r1["dir"] = (0, -1, 0)
     r1["tmax"] = (13.0, np.nextafter(np.float32(13.0), np.float32(1e30)))
     h = bvh.closest_host(r1)
@@ -269,7 +269,11 @@ def test_tlas_two_level_vs_oracle(cuda):
             wb.append(np.concatenate([lo - pad, hi + pad]))
         tnodes, tord = O.tlas_fast(np.array(wb, np.float32))
         tnodes = O.fix_skips(tnodes)
+        # half the rays aimed at instance centres, half random
         rays = scenes.random_rays(33, 20000)
+        tgt = np.array([m[:, 3] for m in xf])[rs.randint(0, ninst, 10000)] + rs.normal(0, 1.5, (10000, 3))
+        d = tgt - rays["org"][:10000]
+        rays["dir"][:10000] = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
         hits = np.zeros(rays.shape[0], HIT_DTYPE)
         inst_ref = np.zeros(rays.shape[0], np.int32)
         iblas = np.array([k % 4 for k in range(ninst)], np.int32)

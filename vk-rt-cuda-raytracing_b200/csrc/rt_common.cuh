@@ -84,7 +84,7 @@ __device__ __forceinline__ bool intersect_tri(float ox, float oy, float oz, floa
     const float pz = sub(mul(dx, e2y), mul(dy, e2x));
     const float det = add(add(mul(e1x, px), mul(e1y, py)), mul(e1z, pz));
     if (fabsf(det) < 1e-12f) return false;
-    const float inv = __fdiv_rn(1.0f, det);
+    const float inv = __frcp_rn(det);  // correctly rounded 1/det, as 1.f/det
     const float sx = sub(ox, A.x), sy = sub(oy, A.y), sz = sub(oz, A.z);
     u = mul(inv, add(add(mul(sx, px), mul(sy, py)), mul(sz, pz)));
     if (u < 0.f || u > 1.f) return false;

@@ -17,17 +17,28 @@ constexpr int RT_STATUS_TIMEOUT = 2;
 struct Ray {
     float ox, oy, oz, tmin;
     float dx, dy, dz, tmax;
-    float ix, iy, iz;  // 1/d, IEEE (+-inf for a zero component)
-    uint32_t oct;      // sign bits of 1/d: x -> 1, y -> 2, z -> 4
+    float ix, iy, iz;  // box-test reciprocal direction (see guard_rcp)
+    uint32_t oct;      // sign bits of ix, iy, iz: x -> 1, y -> 2, z -> 4
 };
+
+// Reciprocal direction for the box test only.  A component with |d| <= 2^-64
+// (an exact zero included) is replaced by +-2^-64 keeping its sign, so the
+// slab arithmetic stays finite (1/0 = inf would turn q*S + O into NaN and
+// silently disable culling on that axis).  The box offsets carry an absolute
+// slack of 2^-22 |(p - o)/d|, which for such an axis is |p - o| * 2^42 and
+// covers the drift of the guarded direction over any finite scene, so the
+// test stays conservative.  The triangle test uses the true direction.
+__device__ __forceinline__ float guard_rcp(float d) {
+    return __frcp_rn(fabsf(d) > 0x1p-64f ? d : copysignf(0x1p-64f, d));
+}
 
 __device__ __forceinline__ Ray make_ray(float4 a, float4 b) {
     Ray r;
     r.ox = a.x; r.oy = a.y; r.oz = a.z; r.tmin = a.w;
     r.dx = b.x; r.dy = b.y; r.dz = b.z; r.tmax = b.w;
-    r.ix = __fdiv_rn(1.0f, r.dx);
-    r.iy = __fdiv_rn(1.0f, r.dy);
-    r.iz = __fdiv_rn(1.0f, r.dz);
+    r.ix = guard_rcp(r.dx);
+    r.iy = guard_rcp(r.dy);
+    r.iz = guard_rcp(r.dz);
     r.oct = (signbit(r.ix) ? 1u : 0u) | (signbit(r.iy) ? 2u : 0u) | (signbit(r.iz) ? 4u : 0u);
     return r;
 }
@@ -55,6 +66,12 @@ struct Walk {
         return sp < SSTACK ? ss[sp][threadIdx.x] : ls[sp - SSTACK];
     }
 };
+
+// Byte k of w as an exact float: PRMT builds the float 2^23 + byte
+// (0x4B0000bb) and one subtraction removes 2^23.
+__device__ __forceinline__ float qbyte(uint32_t w, int k) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, (uint32_t)k | 0x7540u)) - 8388608.0f;
+}
 
 // Fetches one 8-wide node and tests its eight child boxes against the ray
 // segment [tmin, thit].  Outputs the node group of hit inner children
@@ -86,12 +103,12 @@ __device__ __forceinline__ void visit_node(const uint4* __restrict__ np, const R
         const uint32_t bx0 = s < 4 ? qnx0 : qnx1, bx1 = s < 4 ? qfx0 : qfx1;
         const uint32_t by0 = s < 4 ? qny0 : qny1, by1 = s < 4 ? qfy0 : qfy1;
         const uint32_t bz0 = s < 4 ? qnz0 : qnz1, bz1 = s < 4 ? qfz0 : qfz1;
-        const float tnx = fmaf((float)((bx0 >> sh) & 0xFFu), Sx, Onx);
-        const float tfx = fmaf((float)((bx1 >> sh) & 0xFFu), Sx, Ofx);
-        const float tny = fmaf((float)((by0 >> sh) & 0xFFu), Sy, Ony);
-        const float tfy = fmaf((float)((by1 >> sh) & 0xFFu), Sy, Ofy);
-        const float tnz = fmaf((float)((bz0 >> sh) & 0xFFu), Sz, Onz);
-        const float tfz = fmaf((float)((bz1 >> sh) & 0xFFu), Sz, Ofz);
+        const float tnx = fmaf(qbyte(bx0, s & 3), Sx, Onx);
+        const float tfx = fmaf(qbyte(bx1, s & 3), Sx, Ofx);
+        const float tny = fmaf(qbyte(by0, s & 3), Sy, Ony);
+        const float tfy = fmaf(qbyte(by1, s & 3), Sy, Ofy);
+        const float tnz = fmaf(qbyte(bz0, s & 3), Sz, Onz);
+        const float tfz = fmaf(qbyte(bz1, s & 3), Sz, Ofz);
         const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, r.tmin));
         const float tf = fminf(fminf(tfx, tfy), fminf(tfz, thit));
         const bool hit = tn <= fmaf(fabsf(tf), 0x1p-21f, tf);
