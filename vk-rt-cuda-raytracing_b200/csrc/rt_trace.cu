@@ -6,21 +6,28 @@
 // Execution model (B200, 148 SMs): persistent warps sized to fill every SM;
 // each lane owns one ray; idle lanes refill from a global ray counter with
 // one warp-aggregated atomic (dynamic fetch), so warps stay full while ray
-// lengths diverge.  Per node: one 80-byte node = five 16-byte loads; the
-// eight child boxes are decoded from 8-bit planes with one FMA per plane
-// and tested against the ray; hit inner children become an 8-bit mask in
-// near-to-far order (slot ^ octant), hit leaves a 32-bit triangle mask.  The
-// traversal stack holds (child base, hit mask, inner mask) groups: the top
-// SSTACK entries live in shared memory, the rest in local memory; overflow
-// is reported through the status word, never dropped.
+// lengths diverge.  One loop iteration = two warp-wide phases:
+//   node phase      every lane with pending inner nodes visits one 8-wide
+//                   node: five 16-byte loads, eight child boxes decoded from
+//                   8-bit planes with one FMA per plane;
+//   triangle phase  the triangles of all lanes' hit leaves are pooled and
+//                   spread over the 32 lanes (prefix sum + shuffle owner
+//                   search), so a lane with 20 triangles does not idle the
+//                   other 31.  Each result is folded into its owner's
+//                   shared-memory key (ordered t << 32 | primitive) with a
+//                   64-bit atomicMin, which is exactly the tie rule "lower t,
+//                   then lower primitive"; the owner re-evaluates the winning
+//                   triangle once for its barycentrics.
+// The traversal stack holds (child base, hit mask, inner mask) groups: the
+// top SSTACK entries live in shared memory, the rest in local memory;
+// overflow is reported through the status word, never dropped.
 //
 // Box test robustness: t = q * (s/d) + (p - o)/d is evaluated with an
 // absolute slack of 2^-22 |(p - o)/d| folded into the near/far offsets and
 // a relative slack of 2^-21 on the far distance, which bounds every
 // rounding of the decode, so a box that contains an accepted triangle hit
 // is never culled.  Hit results are therefore defined by the triangle test
-// alone: Moller-Trumbore in exact IEEE single precision (rt_common.cuh),
-// ties on t resolved toward the lower primitive id.
+// alone: Moller-Trumbore in exact IEEE single precision (rt_common.cuh).
 #include <cfloat>
 
 #include "rt_internal.h"
@@ -34,8 +41,12 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
                  int n, RtHit* __restrict__ hits, uint8_t* __restrict__ occ, uint32_t* __restrict__ counts,
                  int* __restrict__ work, int* __restrict__ status) {
     __shared__ uint2 sstack[SSTACK][TRACE_T];
+    __shared__ unsigned long long s_key[TRACE_T];  // owner's best (ordered t, prim)
+    __shared__ int s_rec[TRACE_T];                 // set when a worker improved it (any hit: found)
+    __shared__ float2 s_uv[TRACE_T];               // barycentrics of the improved best
     uint2 lstack[LSTACK];
     const int lane = threadIdx.x & 31;
+    const int wbase = threadIdx.x & ~31;
     int ray = -1;
     bool exhausted = false;
     Ray r;
@@ -44,6 +55,7 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
     int hprim = -1;
     uint32_t cn = 0, ct = 0;
     for (;;) {
+        // ---- refill idle lanes ----
         const bool need = ray < 0 && !exhausted;
         const unsigned want = __ballot_sync(FULL_MASK, need);
         if (want) {
@@ -68,69 +80,130 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
             }
         }
         if (__all_sync(FULL_MASK, ray < 0)) break;
-        if (ray < 0) continue;
-        // ---- one node visit ----
+        // ---- node phase ----
         uint32_t tri_base = 0, tmask = 0;
-        if (w.ng.y & 0xFFu) {
-            uint32_t hitsm = w.ng.y & 0xFFu;
-            const uint32_t imask = (w.ng.y >> 8) & 0xFFu;
-            const int k = __ffs(hitsm) - 1;
-            hitsm &= hitsm - 1;
-            const uint32_t slot = (uint32_t)k ^ r.oct;
-            const uint32_t ni = w.ng.x + __popc(imask & ((1u << slot) - 1));
-            if (hitsm) {
-                if (!w.push(make_uint2(w.ng.x, hitsm | (imask << 8)), sstack, lstack)) {
-                    atomicOr(status, RT_STATUS_STACK);
-                    hprim = -2;
-                    goto finish;
+        bool overflow = false;
+#pragma unroll 1
+        for (int it = 0; it < RTB_NODE_ITERS; it++) {
+            if (ray >= 0 && tmask == 0 && !overflow && (w.ng.y & 0xFFu)) {
+                uint32_t hitsm = w.ng.y & 0xFFu;
+                const uint32_t imask = (w.ng.y >> 8) & 0xFFu;
+                const int k = __ffs(hitsm) - 1;
+                hitsm &= hitsm - 1;
+                const uint32_t slot = (uint32_t)k ^ r.oct;
+                const uint32_t ni = w.ng.x + __popc(imask & ((1u << slot) - 1));
+                if (hitsm && !w.push(make_uint2(w.ng.x, hitsm | (imask << 8)), sstack, lstack)) overflow = true;
+                if (COUNT) cn++;
+                uint32_t nmask;
+                visit_node(nodes + (size_t)ni * 5, r, thit, nmask, tri_base, tmask, w.ng);
+                prefetch_next(nodes, w.ng, r.oct);
+                if (RTB_NODE_ITERS > 1 && tmask == 0 && (w.ng.y & 0xFFu) == 0 && w.sp > 0) {
+                    w.ng = w.pop(sstack, lstack);
                 }
             }
-            if (COUNT) cn++;
-            uint32_t nmask;
-            visit_node(nodes + (size_t)ni * 5, r, thit, nmask, tri_base, tmask, w.ng);
-            (void)nmask;
         }
-        // ---- triangles of the node just visited ----
-        while (tmask) {
-            const int j = __ffs(tmask) - 1;
-            tmask &= tmask - 1;
-            const float4* tp = tris + (size_t)(tri_base + j) * 3;
-            const float4 A = __ldg(tp), B = __ldg(tp + 1), Cc = __ldg(tp + 2);
-            if (COUNT) ct++;
-            float t, u, v;
-            if (intersect_tri(r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, A, B, Cc, t, u, v)) {
-                const int prim = __float_as_int(A.w);
-                if (ANY) {
-                    if (t > r.tmin && t < r.tmax) {
-                        hprim = prim;
-                        goto finish;
+        // ---- triangle phase: pooled over the warp ----
+        const int cnt = __popc(tmask);
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL_MASK, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int total = __shfl_sync(FULL_MASK, incl, 31);
+        bool found_any = false;
+        if (total) {
+            const int excl = incl - cnt;
+            if (COUNT) ct += cnt;
+            if (!ANY) {
+                s_key[threadIdx.x] = ((unsigned long long)f2ord(thit) << 32) | (uint32_t)(hprim >= 0 ? hprim : -1);
+                s_rec[threadIdx.x] = -1;
+            } else {
+                s_rec[threadIdx.x] = 0;
+            }
+            __syncwarp();
+            for (int base = 0; base < total; base += 32) {
+                const int g = base + lane;
+                // owner = first lane whose inclusive count exceeds g
+                int o = 0;
+#pragma unroll
+                for (int s = 16; s; s >>= 1) {
+                    const int v = __shfl_sync(FULL_MASK, incl, o + s - 1);
+                    if (v <= g) o += s;
+                }
+                o = min(o, 31);
+                const int k = g - __shfl_sync(FULL_MASK, excl, o);
+                const uint32_t om = __shfl_sync(FULL_MASK, tmask, o);
+                const uint32_t ob = __shfl_sync(FULL_MASK, tri_base, o);
+                const float ox = __shfl_sync(FULL_MASK, r.ox, o), oy = __shfl_sync(FULL_MASK, r.oy, o),
+                            oz = __shfl_sync(FULL_MASK, r.oz, o);
+                const float dx = __shfl_sync(FULL_MASK, r.dx, o), dy = __shfl_sync(FULL_MASK, r.dy, o),
+                            dz = __shfl_sync(FULL_MASK, r.dz, o);
+                const float tmn = __shfl_sync(FULL_MASK, r.tmin, o), tmx = __shfl_sync(FULL_MASK, r.tmax, o);
+                unsigned long long key = ~0ull;
+                float u = 0.f, v = 0.f;
+                if (g < total) {
+                    const int rec = (int)ob + (int)__fns(om, 0, k + 1);
+                    const float4* tp = tris + (size_t)rec * 3;
+                    const float4 A = __ldg(tp), B = __ldg(tp + 1), Cc = __ldg(tp + 2);
+                    float t;
+                    if (intersect_tri(ox, oy, oz, dx, dy, dz, A, B, Cc, t, u, v) && t > tmn && t < tmx) {
+                        if (ANY) s_rec[wbase + o] = 1;
+                        else key = ((unsigned long long)f2ord(t) << 32) | (uint32_t)__float_as_int(A.w);
                     }
-                } else if (t > r.tmin && (t < thit || (t == thit && hprim >= 0 && prim < hprim))) {
-                    thit = t;
-                    hprim = prim;
-                    hu = u;
-                    hv = v;
+                }
+                if (!ANY) {
+                    if (key != ~0ull) atomicMin(&s_key[wbase + o], key);
+                    __syncwarp();
+                    // the unique winner (keys are distinct per ray) publishes its barycentrics
+                    if (key != ~0ull && s_key[wbase + o] == key) {
+                        s_rec[wbase + o] = 1;
+                        s_uv[wbase + o] = make_float2(u, v);
+                    }
+                    __syncwarp();
                 }
             }
+            __syncwarp();
+            if (ANY) {
+                found_any = s_rec[threadIdx.x] != 0;
+            } else if (s_rec[threadIdx.x] >= 0) {
+                // a new closest hit for this lane
+                const unsigned long long key = s_key[threadIdx.x];
+                const float2 uv = s_uv[threadIdx.x];
+                thit = ord2f((uint32_t)(key >> 32));
+                hprim = (int)(uint32_t)key;
+                hu = uv.x;
+                hv = uv.y;
+            }
         }
-        if ((w.ng.y & 0xFFu) == 0) {
-            if (w.sp == 0) goto finish;
-            w.ng = w.pop(sstack, lstack);
+        // ---- advance / finish ----
+        if (ray >= 0) {
+            bool done = overflow || (ANY && found_any);
+            if (!done && (w.ng.y & 0xFFu) == 0) {
+                if (w.sp == 0) {
+                    done = true;
+                } else {
+                    w.ng = w.pop(sstack, lstack);
+                    prefetch_next(nodes, w.ng, r.oct);
+                }
+            }
+            if (done) {
+                if (overflow) {
+                    atomicOr(status, RT_STATUS_STACK);
+                    hprim = -1;
+                    found_any = false;
+                }
+                if (ANY) {
+                    occ[ray] = found_any ? 1 : 0;
+                } else {
+                    reinterpret_cast<float4*>(hits)[ray] =
+                        make_float4(hprim >= 0 ? thit : __int_as_float(0x7f800000), __int_as_float(hprim),
+                                    hprim >= 0 ? hu : 0.f, hprim >= 0 ? hv : 0.f);
+                }
+                if (COUNT) reinterpret_cast<uint2*>(counts)[ray] = make_uint2(cn, ct);
+                ray = -1;
+            }
         }
-        continue;
-    finish:
-        if (ANY) {
-            occ[ray] = hprim >= 0 ? 1 : 0;
-        } else {
-            RtHit h;
-            h.t = hprim >= 0 ? thit : __int_as_float(0x7f800000);
-            h.prim = hprim >= 0 ? hprim : -1;
-            h.u = hprim >= 0 ? hu : 0.f;
-            h.v = hprim >= 0 ? hv : 0.f;
-            reinterpret_cast<float4*>(hits)[ray] = make_float4(h.t, __int_as_float(h.prim), h.u, h.v);
-        }
-        if (COUNT) reinterpret_cast<uint2*>(counts)[ray] = make_uint2(cn, ct);
-        ray = -1;
     }
 }
 
