@@ -71,6 +71,21 @@ int cudaBVH_traceAny(CudaBVH_t bvh, const RtRay* d_rays, int n, uint8_t* d_occlu
 int cudaBVH_traceClosestHost(CudaBVH_t bvh, const RtRay* h_rays, int n, RtHit* h_hits);
 int cudaBVH_traceAnyHost(CudaBVH_t bvh, const RtRay* h_rays, int n, uint8_t* h_occluded);
 
+/* Closest hit of up to 65,536 host rays without allocating any memory.
+ * No counterpart in the reference.  For callers that must not allocate while
+ * they trace: a Vulkan layer tracing on the application's render thread (a
+ * cudaMalloc there can synchronise the device and stall the frame, and the
+ * application owns the memory budget), real-time callers that cannot afford
+ * the implicit synchronisation of cudaMalloc/cudaFree, and code running under
+ * a fixed memory cap.  Rays and hits are staged in one fixed device array
+ * compiled into the library (about 3 MiB, held by every GPU that loads the
+ * library until exit); more than 65,536 rays -> RT_ERR_CAPACITY.  The first
+ * call on each device looks up that array's device address (make it before
+ * any stream capture).  All calls share the array: calls whose GPU work
+ * overlaps corrupt each other's rays and hits, so serialise them.  Waits
+ * for the result on `stream`.  Same results as cudaBVH_traceClosestHost. */
+int cudaBVH_traceClosestHostNoAlloc(CudaBVH_t bvh, const RtRay* h_rays, int n, RtHit* h_hits, void* stream);
+
 /* Host-side structural check of the built acceleration structure (child
  * indices, triangle ranges, depth within the traversal stack, every
  * triangle referenced once).  RT_OK or RT_ERR_INVALID.  Setting the

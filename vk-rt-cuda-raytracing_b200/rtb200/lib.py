@@ -70,6 +70,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "cudaBVH_traceClosestHost": (i32, [vp, vp, i32, vp]),
         "cudaBVH_traceAnyHost": (i32, [vp, vp, i32, vp]),
         "cudaBVH_traceCounters": (i32, [vp, vp, i32, i32, vp, vp]),
+        "cudaBVH_traceClosestHostNoAlloc": (i32, [vp, vp, i32, vp, vp]),
         "cudaBVH_validate": (i32, [vp]),
         "cudaBVH_getBuildStats": (i32, [vp, C.POINTER(RtBuildStats)]),
         "cudaBVH_getDeviceLayout": (i32, [vp, C.POINTER(vp), C.POINTER(i32), C.POINTER(vp), C.POINTER(i32)]),
