@@ -366,6 +366,61 @@ def run_ours(args):
     return 0
 
 
+def run_pathtrace(args):
+    """wavefront path tracer, 1920x1080, 8 spp, <= 4 bounces,
+    RR from bounce 2, TLAS of 64 instances over 16 BLASes (5M triangles).
+    value = (extension + shadow rays) / frame time; radiance checked against
+    the FP64 oracle on a random pixel subset."""
+    import torch
+    from rtb200 import lib, scenes
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    t0 = time.time()
+    blases, xf, bidx, alb, emi = scenes.instanced_scene(2, 5_000_000, nblas=16, ninst=64, world=100.0,
+                                                        emissive_frac=0.05)
+    log(f"scene: 5M tris / 16 BLAS / 64 instances in {time.time() - t0:.1f}s, emissive {(emi.max(1) > 0).sum()}")
+    bvhs = [lib.BVH(t) for t in blases]
+    tl = lib.TLAS(bvhs, xf, bidx)
+    pt = lib.PathTracer(tl, alb, emi)
+    W, H, spp = 1920, 1080, 8
+    cam = lib.make_camera(scenes.PT_CAM_EYE, scenes.PT_CAM_TARGET, vfov=50.0)
+    d_rgb = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    ms = time_steps(torch, lambda: pt.render(cam, W, H, spp, 4, 2, 1, d_rgb, stream=stream), args.steps, args.warmup,
+                    flush)
+    st = pt.stats()
+    rays = st["extension_rays"] + st["shadow_rays"]
+    t_frame = sum(ms) / len(ms)
+    img = d_rgb.cpu().numpy().reshape(-1, 3).astype(np.float64)
+    out = {"metric": "Mrays/s wavefront path tracer (extension + shadow rays)", "value": round(rays / t_frame / 1e3, 1),
+           "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_frame, 3),
+           "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "pathtrace_tlas_5m: 1920x1080, 8 spp, <=4 bounces, RR from bounce 2, 64 instances "
+                                  "over 16 BLASes (5,000,000 triangles), Lambertian, 5% emissive",
+                      "l2": "flushed between timed frames"},
+           "rays_per_frame": {"extension": st["extension_rays"], "shadow": st["shadow_rays"]},
+           "light_triangles": st["light_tris"], "mean_radiance": float(img.mean())}
+    if not args.no_baselines:
+        from oracle import oracle as O
+        t0 = time.time()
+        orc = O.OraclePT(blases, xf, bidx, tl.inverse(), alb, emi)
+        build_s = time.time() - t0
+        rs = np.random.RandomState(0)
+        px = np.sort(rs.choice(W * H, 4096, replace=False)).astype(np.int32)
+        t0 = time.time()
+        ref, counts = orc.pixels(lib.camera_basis(cam, W, H), W, H, spp, px, 4, 2, 1, nthreads=os.cpu_count() or 1)
+        cpu_s = time.time() - t0
+        g = img[px]
+        out["fp64_oracle"] = {"pixels": int(px.size), "mean_rel_err": float(np.abs(g - ref).sum() / max(np.abs(ref).sum(), 1e-30)),
+                              "max_abs_err": float(np.abs(g - ref).max()), "oracle_build_s": round(build_s, 1)}
+        out["cpu_baseline"] = {"value": round(float(counts.sum()) / cpu_s / 1e6, 3), "unit": UNIT,
+                               "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": f"{px.size} pixels x {spp} spp through the FP64 oracle path tracer"}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -373,11 +428,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-baselines", action="store_true", help="skip the reference-kernel and CPU legs")
+    ap.add_argument("--workload", choices=["incoherent", "pathtrace"], default="incoherent",
+                    help="incoherent = configs[1] headline; pathtrace = configs[2]")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "pathtrace":
+        return run_pathtrace(args)
     return run_ours(args)
 
 

@@ -149,6 +149,56 @@ int cudaTLAS_traceAny(CudaTLAS_t tlas, const RtRay* d_rays, int n, uint8_t* d_oc
 /* Inverse transforms (12 floats per instance) the TLAS uses, host copy. */
 int cudaTLAS_getInverseTransforms(CudaTLAS_t tlas, float* out, int numInstances);
 
+/* ---------------- wavefront path tracer ----------------
+ * Lambertian scene over a TLAS: per-instance albedo and emission; emission
+ * counted on camera hits; next-event estimation toward one emissive triangle
+ * (area-proportional choice, exact integer CDF; two-sided emitters);
+ * cosine-weighted bounces; Russian roulette from bounce rr_start with
+ * p = max(max throughput component, 0.05); black environment.  Philox4x32-10
+ * keyed by (seed, pixel, sample, bounce), so a pixel's value does not depend
+ * on how paths are scheduled.  Output: W*H*3 floats (RGB), row-major. */
+typedef struct {
+    float albedo[3];
+    float emission[3];
+} RtMaterial;
+
+typedef struct {
+    float eye[3];
+    float target[3];
+    float up[3];
+    float vfov_deg;
+} RtCamera;
+
+typedef struct {
+    int width, height, spp;
+    int max_bounces;  /* path vertices, 1..16 */
+    int rr_start;     /* first bounce with Russian roulette */
+    uint32_t seed;
+} RtPTParams;
+
+typedef struct {
+    uint64_t extension_rays;  /* closest-hit rays traced by the last render */
+    uint64_t shadow_rays;     /* any-hit rays traced by the last render */
+    int light_tris;
+    double light_area;
+} RtPTStats;
+
+typedef struct RtPathTracerHandle* RtPathTracer_t;
+
+/* materials[i] and instances[i] describe TLAS instance i (the same records
+ * given to cudaTLAS_build).  The TLAS and its BLASes must outlive the path
+ * tracer.  NULL on failure. */
+RtPathTracer_t rtPT_create(CudaTLAS_t tlas, const RtMaterial* materials, int numMaterials,
+                           const RtInstance* instances);
+/* Renders into d_rgb (device, W*H*3 floats) on `stream`; path state buffers
+ * are owned by the handle and grow to W*H*spp paths. */
+int rtPT_render(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* params, float* d_rgb, void* stream);
+int rtPT_getStats(RtPathTracer_t pt, RtPTStats* out);
+void rtPT_destroy(RtPathTracer_t pt);
+/* The fp32 camera basis the renderer uses: eye[3], forward[3], right[3],
+ * up[3], tan(vfov/2), aspect (14 floats). */
+int rtPT_cameraBasis(const RtCamera* cam, int width, int height, float* out14);
+
 #ifdef __cplusplus
 }
 #endif

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -761,6 +762,227 @@ int orc_fix_skips(uint32_t* dfs, int n) {
         memcpy(dfs + (size_t)i * 8 + 7, &sk, 4);
     }
     return changed;
+}
+
+}  // extern "C"
+
+// ===================== FP64 path-tracing oracle =====================
+// Mirrors the wavefront path tracer's model step by step (camera, hit
+// frame, next-event estimation with an exact integer light CDF, Malley
+// bounce, Russian roulette).  Every geometric quantity and every decision
+// uses the same fp32 operations as the GPU (this file is compiled with
+// -ffp-contract=off), so the paths are the same; radiance is accumulated
+// in double.
+namespace {
+
+const uint32_t kPtKey = 0x50545201u;
+
+inline void pt_rand(uint32_t pixel, uint32_t s, uint32_t b, uint32_t purpose, uint32_t seed, uint32_t out[4]) {
+    const uint32_t ctr[4] = {pixel, s, (b << 8) | purpose, 0u};
+    const uint32_t key[2] = {seed, kPtKey};
+    orc_philox4x32_10(ctr, key, out);
+}
+inline float u01f(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+inline float dot3f(float ax, float ay, float az, float bx, float by, float bz) { return ax * bx + ay * by + az * bz; }
+inline void xpoint(const float* m, float x, float y, float z, float& ox, float& oy, float& oz) {
+    ox = m[0] * x + m[1] * y + m[2] * z + m[3];
+    oy = m[4] * x + m[5] * y + m[6] * z + m[7];
+    oz = m[8] * x + m[9] * y + m[10] * z + m[11];
+}
+
+double tri_area_world_d(const float* m, const float* v) {
+    double p[3][3];
+    for (int k = 0; k < 3; k++)
+        for (int r = 0; r < 3; r++)
+            p[k][r] = (double)m[r * 4] * v[k * 3] + (double)m[r * 4 + 1] * v[k * 3 + 1] +
+                      (double)m[r * 4 + 2] * v[k * 3 + 2] + (double)m[r * 4 + 3];
+    const double a[3] = {p[1][0] - p[0][0], p[1][1] - p[0][1], p[1][2] - p[0][2]};
+    const double b[3] = {p[2][0] - p[0][0], p[2][1] - p[0][1], p[2][2] - p[0][2]};
+    const double c[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+    return 0.5 * sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+}
+
+}  // namespace
+
+extern "C" {
+
+
+
+void orc_pt_pixels(const OrcPTScene* S, const float* cam, const OrcPTParams* P, const int* pixels, int npix,
+                   double* out_rgb, int nthreads, uint64_t* ray_counts) {
+    // light table: emissive instances in order, their primitives in order
+    std::vector<double> areas;
+    std::vector<std::pair<int, int>> lights;
+    for (int k = 0; k < S->ninst; k++) {
+        const float* e = S->emission3 + 3 * k;
+        if (!(e[0] > 0.f || e[1] > 0.f || e[2] > 0.f)) continue;
+        const int b = S->inst_blas[k];
+        for (int p = 0; p < S->blas_tri_count[b]; p++) {
+            areas.push_back(tri_area_world_d(S->fwd12 + 12 * k, S->blas_tris9 + (size_t)(S->blas_tri_base[b] + p) * 9));
+            lights.push_back({k, p});
+        }
+    }
+    std::vector<unsigned long long> cdf(areas.size());
+    unsigned long long total_q = 0;
+    double light_area = 0.0;
+    if (!areas.empty()) {
+        double amax = 0.0;
+        for (double a : areas) amax = std::max(amax, a);
+        const int K = (int)floor(61.0 - log2((double)areas.size() * std::max(amax, 1e-300)));
+        for (size_t i = 0; i < areas.size(); i++) {
+            total_q += (unsigned long long)floor(ldexp(areas[i], K));
+            cdf[i] = total_q;
+        }
+        light_area = ldexp((double)total_q, -K);
+    }
+    const float* eye = cam; const float* F = cam + 3; const float* R = cam + 6; const float* U = cam + 9;
+    const float th = cam[12], aspect = cam[13];
+    const int W = P->width, H = P->height, spp = P->spp;
+    std::atomic<uint64_t> n_ext(0), n_sha(0);
+    parallel_for(npix, nthreads, 1, [&](int ip) {
+        const uint32_t pixel = (uint32_t)pixels[ip];
+        const uint32_t px = pixel % W, py = pixel / W;
+        double acc[3] = {0, 0, 0};
+        uint64_t ne = 0, ns = 0;
+        for (int s = 0; s < spp; s++) {
+            uint32_t rr[4];
+            pt_rand(pixel, s, 0, 0, P->seed, rr);
+            const float j1 = u01f(rr[0]), j2 = u01f(rr[1]);
+            const float x = (((float)px + j1) / (float)W * 2.f - 1.f) * th * aspect;
+            const float y = (1.f - ((float)py + j2) / (float)H * 2.f) * th;
+            float dx = F[0] + x * R[0] + y * U[0];
+            float dy = F[1] + x * R[1] + y * U[1];
+            float dz = F[2] + x * R[2] + y * U[2];
+            const float len = sqrtf(dot3f(dx, dy, dz, dx, dy, dz));
+            OrcRay ray;
+            ray.org[0] = eye[0]; ray.org[1] = eye[1]; ray.org[2] = eye[2]; ray.tmin = 0.f;
+            ray.dir[0] = dx / len; ray.dir[1] = dy / len; ray.dir[2] = dz / len; ray.tmax = 1e30f;
+            float tpf[3] = {1.f, 1.f, 1.f};
+            double tpd[3] = {1.0, 1.0, 1.0};
+            double L[3] = {0, 0, 0};
+            for (int b = 0; b < P->max_bounces; b++) {
+                OrcHit h;
+                int inst = -1;
+                ne++;
+                trace_two_level_one<false>(S->tlas, S->tlas_nodes, S->tlas_ordered, S->inv12, S->inst_blas,
+                                           S->blas_dfs, S->node_off, S->blas_packed, S->tri_off, ray, h, inst);
+                if (h.prim < 0) break;
+                const float* alb = S->albedo3 + 3 * inst;
+                const float* emi = S->emission3 + 3 * inst;
+                if (b == 0 && (emi[0] > 0.f || emi[1] > 0.f || emi[2] > 0.f))
+                    for (int c = 0; c < 3; c++) L[c] += tpd[c] * (double)emi[c];
+                const float hx = ray.org[0] + h.t * ray.dir[0];
+                const float hy = ray.org[1] + h.t * ray.dir[1];
+                const float hz = ray.org[2] + h.t * ray.dir[2];
+                const int bl = S->inst_blas[inst];
+                const float* tv = S->blas_tris9 + (size_t)(S->blas_tri_base[bl] + h.prim) * 9;
+                const float e1x = tv[3] - tv[0], e1y = tv[4] - tv[1], e1z = tv[5] - tv[2];
+                const float e2x = tv[6] - tv[0], e2y = tv[7] - tv[1], e2z = tv[8] - tv[2];
+                const float nox = e1y * e2z - e1z * e2y, noy = e1z * e2x - e1x * e2z, noz = e1x * e2y - e1y * e2x;
+                const float* iv = S->inv12 + 12 * inst;
+                float nx = iv[0] * nox + iv[4] * noy + iv[8] * noz;
+                float ny = iv[1] * nox + iv[5] * noy + iv[9] * noz;
+                float nz = iv[2] * nox + iv[6] * noy + iv[10] * noz;
+                const float nl = sqrtf(dot3f(nx, ny, nz, nx, ny, nz));
+                nx = nx / nl; ny = ny / nl; nz = nz / nl;
+                if (dot3f(nx, ny, nz, ray.dir[0], ray.dir[1], ray.dir[2]) > 0.f) { nx = -nx; ny = -ny; nz = -nz; }
+                const float ox = hx + 1e-3f * nx, oy = hy + 1e-3f * ny, oz = hz + 1e-3f * nz;
+                if (!lights.empty()) {
+                    uint32_t rl[4];
+                    pt_rand(pixel, s, b, 1, P->seed, rl);
+                    const unsigned long long r64 = ((unsigned long long)rl[0] << 32) | rl[1];
+                    const unsigned long long target = (unsigned long long)(((unsigned __int128)r64 * total_q) >> 64);
+                    const size_t li = std::upper_bound(cdf.begin(), cdf.end(), target) - cdf.begin();
+                    const int linst = lights[li].first, lprim = lights[li].second;
+                    const int lb = S->inst_blas[linst];
+                    const float* lv = S->blas_tris9 + (size_t)(S->blas_tri_base[lb] + lprim) * 9;
+                    const float* fw = S->fwd12 + 12 * linst;
+                    float ax, ay, az, bx, by, bz, cx, cy, cz;
+                    xpoint(fw, lv[0], lv[1], lv[2], ax, ay, az);
+                    xpoint(fw, lv[3], lv[4], lv[5], bx, by, bz);
+                    xpoint(fw, lv[6], lv[7], lv[8], cx, cy, cz);
+                    const float su = sqrtf(u01f(rl[2])), xb = u01f(rl[3]);
+                    const float wa = 1.f - su, wb = su * (1.f - xb), wc = su * xb;
+                    const float lx = wa * ax + wb * bx + wc * cx;
+                    const float ly = wa * ay + wb * by + wc * cy;
+                    const float lz = wa * az + wb * bz + wc * cz;
+                    const float f1x = bx - ax, f1y = by - ay, f1z = bz - az;
+                    const float f2x = cx - ax, f2y = cy - ay, f2z = cz - az;
+                    const float gx = f1y * f2z - f1z * f2y, gy = f1z * f2x - f1x * f2z, gz = f1x * f2y - f1y * f2x;
+                    const float gl = sqrtf(dot3f(gx, gy, gz, gx, gy, gz));
+                    const float tx = lx - ox, ty = ly - oy, tz = lz - oz;
+                    const float d2 = dot3f(tx, ty, tz, tx, ty, tz);
+                    const float dist = sqrtf(d2);
+                    if (dist > 0.f && gl > 0.f) {
+                        const float sdx = tx / dist, sdy = ty / dist, sdz = tz / dist;
+                        const float cxf = dot3f(nx, ny, nz, sdx, sdy, sdz);
+                        const float clf = fabsf(dot3f(gx, gy, gz, sdx, sdy, sdz)) / gl;
+                        if (cxf > 0.f && clf > 0.f) {
+                            OrcRay sr;
+                            sr.org[0] = ox; sr.org[1] = oy; sr.org[2] = oz; sr.tmin = 1e-4f;
+                            sr.dir[0] = sdx; sr.dir[1] = sdy; sr.dir[2] = sdz; sr.tmax = dist * 0.9999f;
+                            OrcHit sh;
+                            int sinst;
+                            ns++;
+                            trace_two_level_one<true>(S->tlas, S->tlas_nodes, S->tlas_ordered, S->inv12, S->inst_blas,
+                                                      S->blas_dfs, S->node_off, S->blas_packed, S->tri_off, sr, sh,
+                                                      sinst);
+                            if (sh.prim < 0) {
+                                const float* le = S->emission3 + 3 * linst;
+                                const double g = (double)cxf * (double)clf / (double)d2 * light_area / M_PI;
+                                for (int c = 0; c < 3; c++) L[c] += tpd[c] * (double)alb[c] * (double)le[c] * g;
+                            }
+                        }
+                    }
+                }
+                if (b + 1 >= P->max_bounces) break;
+                float tfx, tfy, tfz;
+                if (fabsf(nx) > fabsf(ny)) {
+                    const float il = 1.f / sqrtf(nx * nx + nz * nz);
+                    tfx = -(nz * il); tfy = 0.f; tfz = nx * il;
+                } else {
+                    const float il = 1.f / sqrtf(ny * ny + nz * nz);
+                    tfx = 0.f; tfy = nz * il; tfz = -(ny * il);
+                }
+                const float bfx = ny * tfz - nz * tfy, bfy = nz * tfx - nx * tfz, bfz = nx * tfy - ny * tfx;
+                float X = 0.f, Y = 0.f;
+                bool got = false;
+                for (int q = 0; q < 4 && !got; q++) {
+                    uint32_t rd[4];
+                    pt_rand(pixel, s, b, 3 + q, P->seed, rd);
+                    for (int k = 0; k < 2 && !got; k++) {
+                        const float a = u01f(rd[2 * k]) * 2.f - 1.f, c = u01f(rd[2 * k + 1]) * 2.f - 1.f;
+                        if (a * a + c * c < 1.f) { X = a; Y = c; got = true; }
+                    }
+                }
+                const float Z = sqrtf(std::max(0.f, 1.f - X * X - Y * Y));
+                float ndx = X * tfx + Y * bfx + Z * nx;
+                float ndy = X * tfy + Y * bfy + Z * ny;
+                float ndz = X * tfz + Y * bfz + Z * nz;
+                const float dl = sqrtf(dot3f(ndx, ndy, ndz, ndx, ndy, ndz));
+                ndx = ndx / dl; ndy = ndy / dl; ndz = ndz / dl;
+                float t0 = tpf[0] * alb[0], t1 = tpf[1] * alb[1], t2 = tpf[2] * alb[2];
+                double d0 = tpd[0] * alb[0], d1 = tpd[1] * alb[1], d2d = tpd[2] * alb[2];
+                if (b >= P->rr_start) {
+                    const float p = std::max(std::max(std::max(t0, t1), t2), 0.05f);
+                    uint32_t rq[4];
+                    pt_rand(pixel, s, b, 2, P->seed, rq);
+                    if (u01f(rq[0]) >= p) break;
+                    t0 = t0 / p; t1 = t1 / p; t2 = t2 / p;
+                    d0 /= (double)p; d1 /= (double)p; d2d /= (double)p;
+                }
+                tpf[0] = t0; tpf[1] = t1; tpf[2] = t2;
+                tpd[0] = d0; tpd[1] = d1; tpd[2] = d2d;
+                ray.org[0] = ox; ray.org[1] = oy; ray.org[2] = oz; ray.tmin = 1e-4f;
+                ray.dir[0] = ndx; ray.dir[1] = ndy; ray.dir[2] = ndz; ray.tmax = 1e30f;
+            }
+            for (int c = 0; c < 3; c++) acc[c] += L[c];
+        }
+        for (int c = 0; c < 3; c++) out_rgb[(size_t)ip * 3 + c] = acc[c] / spp;
+        n_ext += ne;
+        n_sha += ns;
+    });
+    if (ray_counts) { ray_counts[0] = n_ext.load(); ray_counts[1] = n_sha.load(); }
 }
 
 }  // extern "C"

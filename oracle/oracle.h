@@ -87,6 +87,20 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
  * changed, -1 if the array is not a well-formed preorder binary tree). */
 int    orc_fix_skips(uint32_t* dfs, int n);
 
+/* ---- FP64 path-tracing oracle (mirrors the wavefront path tracer) ---- */
+typedef struct {
+    const uint32_t* tlas; int tlas_nodes; const int* tlas_ordered;
+    const float* inv12; const float* fwd12; const int* inst_blas; int ninst;
+    const uint32_t* blas_dfs; const int* node_off; const float* blas_packed; const int* tri_off;
+    const float* blas_tris9; const int* blas_tri_base; const int* blas_tri_count;
+    const float* albedo3; const float* emission3;
+} OrcPTScene;
+typedef struct { int width, height, spp, max_bounces, rr_start; uint32_t seed; } OrcPTParams;
+/* Radiance (double RGB) of the listed pixels; cam = the renderer's 14-float
+ * camera basis; ray_counts (optional): extension and shadow rays traced. */
+void orc_pt_pixels(const OrcPTScene* scene, const float* cam, const OrcPTParams* params, const int* pixels,
+                   int npix, double* out_rgb, int nthreads, uint64_t* ray_counts);
+
 /* ---- fp16 helpers (round to nearest even, as __float2half) ---- */
 uint16_t orc_f2h_rn(float f);
 

@@ -59,8 +59,7 @@ def lib() -> C.CDLL:
         L.orc_fix_skips.argtypes = [vp, i32]
         L.orc_f2h_rn.restype = C.c_uint16
         L.orc_f2h_rn.argtypes = [C.c_float]
-        if hasattr(L, "orc_pt_pixels"):
-            L.orc_pt_pixels.argtypes = [vp, vp, i32, vp, i32]
+        L.orc_pt_pixels.argtypes = [vp, vp, vp, vp, i32, vp, i32, vp]
         _lib = L
     return _lib
 
@@ -264,3 +263,63 @@ def ref_available(name: str = "libref_backend.so") -> bool:
 
 def default_threads() -> int:
     return os.cpu_count() or 1
+
+
+# --------------------------------------------------------------------------
+# FP64 path-tracing oracle over an instanced scene.
+# --------------------------------------------------------------------------
+class _PTScene(C.Structure):
+    _fields_ = [("tlas", C.c_void_p), ("tlas_nodes", C.c_int), ("tlas_ordered", C.c_void_p),
+                ("inv12", C.c_void_p), ("fwd12", C.c_void_p), ("inst_blas", C.c_void_p), ("ninst", C.c_int),
+                ("blas_dfs", C.c_void_p), ("node_off", C.c_void_p), ("blas_packed", C.c_void_p),
+                ("tri_off", C.c_void_p), ("blas_tris9", C.c_void_p), ("blas_tri_base", C.c_void_p),
+                ("blas_tri_count", C.c_void_p), ("albedo3", C.c_void_p), ("emission3", C.c_void_p)]
+
+
+class _PTParams(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("spp", C.c_int), ("max_bounces", C.c_int),
+                ("rr_start", C.c_int), ("seed", C.c_uint32)]
+
+
+class OraclePT:
+    """Two-level oracle scene (restated builder per BLAS, LBVH over padded
+    world boxes) plus the FP64 path tracer."""
+
+    def __init__(self, blases, xforms, blas_index, inv12, albedo, emission):
+        self.obs = [OracleBVH(t, 32, 4) for t in blases]
+        self.node_off = np.cumsum([0] + [o.dfs.size // 8 for o in self.obs]).astype(np.int32)
+        self.tri_off = np.cumsum([0] + [o.packed.size // 12 for o in self.obs]).astype(np.int32)
+        self.bdfs = np.concatenate([o.dfs for o in self.obs])
+        self.bpk = np.concatenate([o.packed for o in self.obs])
+        self.tris9 = np.concatenate([np.asarray(t, np.float32).reshape(-1, 9) for t in blases])
+        self.tri_base = np.cumsum([0] + [len(t) for t in blases])[:-1].astype(np.int32)
+        self.tri_count = np.array([len(t) for t in blases], np.int32)
+        self.xf = np.ascontiguousarray(np.asarray(xforms, np.float32).reshape(-1, 12))
+        self.inv = np.ascontiguousarray(np.asarray(inv12, np.float32).reshape(-1, 12))
+        self.iblas = np.ascontiguousarray(blas_index, np.int32)
+        self.albedo = np.ascontiguousarray(albedo, np.float32)
+        self.emission = np.ascontiguousarray(emission, np.float32)
+        wb = []
+        for k in range(len(self.iblas)):
+            v = np.asarray(blases[self.iblas[k]], np.float64).reshape(-1, 3)
+            M = self.xf[k].reshape(3, 4).astype(np.float64)
+            w = v @ M[:, :3].T + M[:, 3]
+            pad = 1e-4 * (np.abs(w).max() + 1)
+            wb.append(np.concatenate([w.min(0) - pad, w.max(0) + pad]))
+        tn, self.tord = tlas_fast(np.array(wb, np.float32))
+        self.tnodes = fix_skips(tn)
+        self.scene = _PTScene(self.tnodes.ctypes.data, self.tnodes.size // 8, self.tord.ctypes.data,
+                              self.inv.ctypes.data, self.xf.ctypes.data, self.iblas.ctypes.data, len(self.iblas),
+                              self.bdfs.ctypes.data, self.node_off.ctypes.data, self.bpk.ctypes.data,
+                              self.tri_off.ctypes.data, self.tris9.ctypes.data, self.tri_base.ctypes.data,
+                              self.tri_count.ctypes.data, self.albedo.ctypes.data, self.emission.ctypes.data)
+
+    def pixels(self, cam14, w, h, spp, pixels, max_bounces=4, rr_start=2, seed=1, nthreads=0):
+        cam14 = np.ascontiguousarray(cam14, np.float32)
+        px = np.ascontiguousarray(pixels, np.int32)
+        out = np.zeros((px.size, 3), np.float64)
+        counts = np.zeros(2, np.uint64)
+        p = _PTParams(w, h, spp, max_bounces, rr_start, seed)
+        lib().orc_pt_pixels(C.byref(self.scene), cam14.ctypes.data, C.byref(p), px.ctypes.data, px.size,
+                            out.ctypes.data, nthreads, counts.ctypes.data)
+        return out, counts

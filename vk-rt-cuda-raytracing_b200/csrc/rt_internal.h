@@ -134,7 +134,7 @@ struct CudaTLASHandle {
     std::vector<CudaBVH_t> blas;
     rtb::Bvh2Device bvh2;
     rtb::Bvh8Device bvh8;
-    rtb::DevBuf<float4> inst;     // per instance: inv xform (3 float4) + blas ptrs (1 float4)
+    rtb::DevBuf<float4> inst;     // per instance: inv xform (3 float4), BLAS ptrs, id base
     std::vector<float> h_inv;     // 12 floats per instance
     rtb::DevBuf<int> counters;
     unsigned counter_next = 0;
@@ -143,6 +143,9 @@ struct CudaTLASHandle {
 };
 
 namespace rtb {
+// Two-level trace; n_dev (optional) supplies the ray count from device memory.
+int launch_trace_tlas(const CudaTLASHandle* t, const RtRay* rays, int n, const int* n_dev, RtHit* hits,
+                      int32_t* inst_out, uint8_t* occ, int* work, int* status, cudaStream_t s);
 int* next_counter(rtb::DevBuf<int>& ring, unsigned& next, cudaStream_t s);
 bool ensure_counters(rtb::DevBuf<int>& ring);
 }  // namespace rtb

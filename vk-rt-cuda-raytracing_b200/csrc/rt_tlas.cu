@@ -23,15 +23,51 @@ namespace rtb {
 
 constexpr uint32_t G_TOP = 1u << 16;   // group belongs to the top level
 constexpr uint32_t G_INST = 1u << 17;  // group is a mask of instance leaves
+constexpr int INST_F4 = 5;             // float4 words per instance record
 
+// Instance record (5 x float4): inverse 3x4 rows, BLAS node and triangle
+// pointers, and the instance's base in the global (instance, primitive)
+// numbering used for tie breaks.
+struct InstView {
+    float m[12];
+    const uint4* nodes;
+    const float4* tris;
+    uint32_t base;
+};
+
+__device__ __forceinline__ InstView load_inst(const float4* __restrict__ inst, int i) {
+    const float4* ip = inst + (size_t)i * INST_F4;
+    const float4 r0 = __ldg(ip), r1 = __ldg(ip + 1), r2 = __ldg(ip + 2), pp = __ldg(ip + 3), bb = __ldg(ip + 4);
+    InstView v;
+    v.m[0] = r0.x; v.m[1] = r0.y; v.m[2] = r0.z; v.m[3] = r0.w;
+    v.m[4] = r1.x; v.m[5] = r1.y; v.m[6] = r1.z; v.m[7] = r1.w;
+    v.m[8] = r2.x; v.m[9] = r2.y; v.m[10] = r2.z; v.m[11] = r2.w;
+    v.nodes = reinterpret_cast<const uint4*>(((unsigned long long)__float_as_uint(pp.y) << 32) | __float_as_uint(pp.x));
+    v.tris = reinterpret_cast<const float4*>(((unsigned long long)__float_as_uint(pp.w) << 32) | __float_as_uint(pp.z));
+    v.base = __float_as_uint(bb.x);
+    return v;
+}
+
+// Two-level closest/any hit.  Same iteration structure as the single-level
+// kernel (rt_trace.cu): up to RTB_NODE_ITERS steps per lane (a step visits a
+// top or bottom node, or enters the next instance of an instance group),
+// then the warp-pooled triangle phase over the lanes walking a BLAS; the
+// shared key's low word is the global id base(instance) + primitive, so one
+// 64-bit atomicMin resolves ties by (t, instance, primitive).
 template <bool ANY>
 __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
     k_trace_tlas(const uint4* __restrict__ tnodes, const int* __restrict__ leaf_ids, const float4* __restrict__ inst,
-                 const RtRay* __restrict__ rays, int n, RtHit* __restrict__ hits, int32_t* __restrict__ inst_out,
-                 uint8_t* __restrict__ occ, int* __restrict__ work, int* __restrict__ status) {
+                 const RtRay* __restrict__ rays, int n, const int* __restrict__ n_dev, RtHit* __restrict__ hits,
+                 int32_t* __restrict__ inst_out, uint8_t* __restrict__ occ, int* __restrict__ work,
+                 int* __restrict__ status) {
     __shared__ uint2 sstack[SSTACK][TRACE_T];
+    __shared__ unsigned long long s_key[TRACE_T];
+    __shared__ int s_rec[TRACE_T];
+    __shared__ int4 s_res[TRACE_T];  // u, v bits, instance, primitive of the improved best
+    if (n_dev) n = *n_dev;  // ray count produced on the device by an earlier stage
     uint2 lstack[LSTACK];
     const int lane = threadIdx.x & 31;
+    const int wbase = threadIdx.x & ~31;
     int ray = -1;
     bool exhausted = false;
     Ray wr, cr;
@@ -40,8 +76,10 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
     const uint4* bnodes = nullptr;
     const float4* btris = nullptr;
     int cur_inst = -1;
+    uint32_t cur_base = 0;
     float thit = 0.f, hu = 0.f, hv = 0.f;
     int hprim = -1, hinst = -1;
+    uint32_t hid = 0xFFFFFFFFu;
     for (;;) {
         const bool need = ray < 0 && !exhausted;
         const unsigned want = __ballot_sync(FULL_MASK, need);
@@ -59,6 +97,7 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
                     in_blas = false;
                     thit = wr.tmax;
                     hprim = hinst = -1;
+                    hid = 0xFFFFFFFFu;
                     hu = hv = 0.f;
                     w.start();
                     w.ng = make_uint2(0u, (1u << wr.oct) | (1u << 8) | G_TOP);
@@ -68,97 +107,63 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
             }
         }
         if (__all_sync(FULL_MASK, ray < 0)) break;
-        if (ray < 0) continue;
-        if (w.ng.y & G_INST) {
-            // enter the next instance of an instance group
-            uint32_t m = w.ng.y & 0xFFu;
-            const int j = __ffs(m) - 1;
-            m &= m - 1;
-            const uint32_t base = w.ng.x;
-            if (m) {
-                if (!w.push(make_uint2(base, m | G_INST | G_TOP), sstack, lstack)) {
-                    atomicOr(status, RT_STATUS_STACK);
-                    hprim = -2;
-                    goto finish;
+        // ---- node phase ----
+        uint32_t tri_base = 0, tmask = 0;
+        bool overflow = false;
+#pragma unroll 1
+        for (int it = 0; it < RTB_NODE_ITERS; it++) {
+            if (ray < 0 || tmask || overflow) break;
+            if (w.ng.y & G_INST) {
+                // enter the next instance of an instance group
+                uint32_t m = w.ng.y & 0xFFu;
+                const int j = __ffs(m) - 1;
+                m &= m - 1;
+                if (m && !w.push(make_uint2(w.ng.x, m | G_INST | G_TOP), sstack, lstack)) {
+                    overflow = true;
+                    break;
                 }
+                cur_inst = leaf_ids[w.ng.x + j];
+                const InstView iv = load_inst(inst, cur_inst);
+                float ox, oy, oz, dx, dy, dz;
+                xform_point(iv.m, wr.ox, wr.oy, wr.oz, ox, oy, oz);
+                xform_dir(iv.m, wr.dx, wr.dy, wr.dz, dx, dy, dz);
+                cr = make_ray(make_float4(ox, oy, oz, wr.tmin), make_float4(dx, dy, dz, wr.tmax));
+                bnodes = iv.nodes;
+                btris = iv.tris;
+                cur_base = iv.base;
+                in_blas = true;
+                w.ng = make_uint2(0u, (1u << cr.oct) | (1u << 8));
+                continue;
             }
-            cur_inst = leaf_ids[base + j];
-            const float4* ip = inst + (size_t)cur_inst * 4;
-            const float4 r0 = __ldg(ip), r1 = __ldg(ip + 1), r2 = __ldg(ip + 2), pp = __ldg(ip + 3);
-            const float m12[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w};
-            float ox, oy, oz, dx, dy, dz;
-            xform_point(m12, wr.ox, wr.oy, wr.oz, ox, oy, oz);
-            xform_dir(m12, wr.dx, wr.dy, wr.dz, dx, dy, dz);
-            cr = make_ray(make_float4(ox, oy, oz, wr.tmin), make_float4(dx, dy, dz, wr.tmax));
-            bnodes = reinterpret_cast<const uint4*>(((unsigned long long)__float_as_uint(pp.y) << 32) | __float_as_uint(pp.x));
-            btris = reinterpret_cast<const float4*>(((unsigned long long)__float_as_uint(pp.w) << 32) | __float_as_uint(pp.z));
-            in_blas = true;
-            w.ng = make_uint2(0u, (1u << cr.oct) | (1u << 8));
-            continue;
-        }
-        {
-            uint32_t tri_base = 0, tmask = 0;
-            if (w.ng.y & 0xFFu) {
-                uint32_t hitsm = w.ng.y & 0xFFu;
-                const uint32_t imask = (w.ng.y >> 8) & 0xFFu;
-                const uint32_t top = w.ng.y & G_TOP;
-                const int k = __ffs(hitsm) - 1;
-                hitsm &= hitsm - 1;
-                const uint32_t slot = (uint32_t)k ^ cr.oct;
-                const uint32_t ni = w.ng.x + __popc(imask & ((1u << slot) - 1));
-                if (hitsm) {
-                    if (!w.push(make_uint2(w.ng.x, hitsm | (imask << 8) | top), sstack, lstack)) {
-                        atomicOr(status, RT_STATUS_STACK);
-                        hprim = -2;
-                        goto finish;
-                    }
-                }
-                uint32_t nh;
-                visit_node((top ? tnodes : bnodes) + (size_t)ni * 5, cr, thit, nh, tri_base, tmask, w.ng);
-                if (top) {
-                    w.ng.y |= G_TOP;
-                    if (tmask) {
-                        // instance leaves of this top node: keep the node group, walk the instances
-                        if (w.ng.y & 0xFFu) {
-                            if (!w.push(w.ng, sstack, lstack)) {
-                                atomicOr(status, RT_STATUS_STACK);
-                                hprim = -2;
-                                goto finish;
-                            }
-                        }
-                        w.ng = make_uint2(tri_base, (tmask & 0xFFu) | G_INST | G_TOP);
-                        tmask = 0;
-                        continue;
-                    }
-                }
+            if ((w.ng.y & 0xFFu) == 0) break;
+            uint32_t hitsm = w.ng.y & 0xFFu;
+            const uint32_t imask = (w.ng.y >> 8) & 0xFFu;
+            const uint32_t top = w.ng.y & G_TOP;
+            const int k = __ffs(hitsm) - 1;
+            hitsm &= hitsm - 1;
+            const uint32_t slot = (uint32_t)k ^ cr.oct;
+            const uint32_t ni = w.ng.x + __popc(imask & ((1u << slot) - 1));
+            if (hitsm && !w.push(make_uint2(w.ng.x, hitsm | (imask << 8) | top), sstack, lstack)) {
+                overflow = true;
+                break;
             }
-            while (tmask) {
-                const int j = __ffs(tmask) - 1;
-                tmask &= tmask - 1;
-                const float4* tp = btris + (size_t)(tri_base + j) * 3;
-                const float4 A = __ldg(tp), B = __ldg(tp + 1), Cc = __ldg(tp + 2);
-                float t, u, v;
-                if (intersect_tri(cr.ox, cr.oy, cr.oz, cr.dx, cr.dy, cr.dz, A, B, Cc, t, u, v)) {
-                    const int prim = __float_as_int(A.w);
-                    if (ANY) {
-                        if (t > wr.tmin && t < wr.tmax) {
-                            hprim = prim;
-                            hinst = cur_inst;
-                            goto finish;
-                        }
-                    } else if (t > wr.tmin &&
-                               (t < thit || (t == thit && hprim >= 0 &&
-                                             (cur_inst < hinst || (cur_inst == hinst && prim < hprim))))) {
-                        thit = t;
-                        hprim = prim;
-                        hinst = cur_inst;
-                        hu = u;
-                        hv = v;
+            uint32_t nh, tb, tm;
+            visit_node((top ? tnodes : bnodes) + (size_t)ni * 5, cr, thit, nh, tb, tm, w.ng);
+            if (top) {
+                w.ng.y |= G_TOP;
+                if (tm) {
+                    // instance leaves: keep the node group, walk the instances next
+                    if ((w.ng.y & 0xFFu) && !w.push(w.ng, sstack, lstack)) {
+                        overflow = true;
+                        break;
                     }
+                    w.ng = make_uint2(tb, (tm & 0xFFu) | G_INST | G_TOP);
                 }
+            } else {
+                tri_base = tb;
+                tmask = tm;
             }
-            if ((w.ng.y & 0xFFu) == 0) {
-                if (w.sp == 0) goto finish;
+            if ((w.ng.y & 0xFFu) == 0 && !(w.ng.y & G_INST) && !tmask && w.sp > 0) {
                 w.ng = w.pop(sstack, lstack);
                 if (in_blas && (w.ng.y & G_TOP)) {
                     in_blas = false;
@@ -166,17 +171,111 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
                 }
             }
         }
-        continue;
-    finish:
-        if (ANY) {
-            occ[ray] = hprim >= 0 ? 1 : 0;
-        } else {
-            reinterpret_cast<float4*>(hits)[ray] =
-                make_float4(hprim >= 0 ? thit : __int_as_float(0x7f800000), __int_as_float(hprim >= 0 ? hprim : -1),
-                            hprim >= 0 ? hu : 0.f, hprim >= 0 ? hv : 0.f);
-            if (inst_out) inst_out[ray] = hprim >= 0 ? hinst : -1;
+        // ---- triangle phase: pooled over the warp ----
+        const int cnt = __popc(tmask);
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL_MASK, incl, o);
+            if (lane >= o) incl += y;
         }
-        ray = -1;
+        const int total = __shfl_sync(FULL_MASK, incl, 31);
+        bool found_any = false;
+        if (total) {
+            const int excl = incl - cnt;
+            if (!ANY) s_key[threadIdx.x] = ((unsigned long long)f2ord(thit) << 32) | hid;
+            s_rec[threadIdx.x] = ANY ? 0 : -1;
+            __syncwarp();
+            const unsigned long long tp64 = (unsigned long long)btris;
+            for (int b = 0; b < total; b += 32) {
+                const int g = b + lane;
+                int o = 0;
+#pragma unroll
+                for (int s = 16; s; s >>= 1) {
+                    const int v = __shfl_sync(FULL_MASK, incl, o + s - 1);
+                    if (v <= g) o += s;
+                }
+                o = min(o, 31);
+                const int k = g - __shfl_sync(FULL_MASK, excl, o);
+                const uint32_t om = __shfl_sync(FULL_MASK, tmask, o);
+                const uint32_t ob = __shfl_sync(FULL_MASK, tri_base, o);
+                const unsigned long long optr = __shfl_sync(FULL_MASK, tp64, o);
+                const uint32_t obase = __shfl_sync(FULL_MASK, cur_base, o);
+                const int oinst = __shfl_sync(FULL_MASK, cur_inst, o);
+                const float ox = __shfl_sync(FULL_MASK, cr.ox, o), oy = __shfl_sync(FULL_MASK, cr.oy, o),
+                            oz = __shfl_sync(FULL_MASK, cr.oz, o);
+                const float dx = __shfl_sync(FULL_MASK, cr.dx, o), dy = __shfl_sync(FULL_MASK, cr.dy, o),
+                            dz = __shfl_sync(FULL_MASK, cr.dz, o);
+                const float tmn = __shfl_sync(FULL_MASK, wr.tmin, o), tmx = __shfl_sync(FULL_MASK, wr.tmax, o);
+                unsigned long long key = ~0ull;
+                float u = 0.f, v = 0.f;
+                int prim = 0;
+                if (g < total) {
+                    const int rec = (int)ob + (int)__fns(om, 0, k + 1);
+                    const float4* tp = reinterpret_cast<const float4*>(optr) + (size_t)rec * 3;
+                    const float4 A = __ldg(tp), B = __ldg(tp + 1), Cc = __ldg(tp + 2);
+                    float t;
+                    if (intersect_tri(ox, oy, oz, dx, dy, dz, A, B, Cc, t, u, v) && t > tmn && t < tmx) {
+                        prim = __float_as_int(A.w);
+                        if (ANY) s_rec[wbase + o] = 1;
+                        else key = ((unsigned long long)f2ord(t) << 32) | (obase + (uint32_t)prim);
+                    }
+                }
+                if (!ANY) {
+                    if (key != ~0ull) atomicMin(&s_key[wbase + o], key);
+                    __syncwarp();
+                    if (key != ~0ull && s_key[wbase + o] == key) {
+                        s_rec[wbase + o] = 1;
+                        s_res[wbase + o] = make_int4(__float_as_int(u), __float_as_int(v), oinst, prim);
+                    }
+                    __syncwarp();
+                }
+            }
+            __syncwarp();
+            if (ANY) {
+                found_any = s_rec[threadIdx.x] != 0;
+            } else if (s_rec[threadIdx.x] >= 0) {
+                const unsigned long long key = s_key[threadIdx.x];
+                const int4 res = s_res[threadIdx.x];
+                thit = ord2f((uint32_t)(key >> 32));
+                hid = (uint32_t)key;
+                hu = __int_as_float(res.x);
+                hv = __int_as_float(res.y);
+                hinst = res.z;
+                hprim = res.w;
+            }
+        }
+        // ---- advance / finish ----
+        if (ray >= 0) {
+            bool done = overflow || (ANY && found_any);
+            if (!done && (w.ng.y & 0xFFu) == 0 && !(w.ng.y & G_INST)) {
+                if (w.sp == 0) {
+                    done = true;
+                } else {
+                    w.ng = w.pop(sstack, lstack);
+                    if (in_blas && (w.ng.y & G_TOP)) {
+                        in_blas = false;
+                        cr = wr;
+                    }
+                }
+            }
+            if (done) {
+                if (overflow) {
+                    atomicOr(status, RT_STATUS_STACK);
+                    hprim = -1;
+                    found_any = false;
+                }
+                if (ANY) {
+                    occ[ray] = found_any ? 1 : 0;
+                } else {
+                    reinterpret_cast<float4*>(hits)[ray] =
+                        make_float4(hprim >= 0 ? thit : __int_as_float(0x7f800000), __int_as_float(hprim),
+                                    hprim >= 0 ? hu : 0.f, hprim >= 0 ? hv : 0.f);
+                    if (inst_out) inst_out[ray] = hprim >= 0 ? hinst : -1;
+                }
+                ray = -1;
+            }
+        }
     }
 }
 
@@ -190,17 +289,17 @@ static int grid_for(K kernel) {
     return per_sm * num_sms();
 }
 
-int launch_trace_tlas(const CudaTLASHandle* t, const RtRay* rays, int n, RtHit* hits, int32_t* inst_out,
-                      uint8_t* occ, int* work, int* status, cudaStream_t s) {
+int launch_trace_tlas(const CudaTLASHandle* t, const RtRay* rays, int n, const int* n_dev, RtHit* hits,
+                      int32_t* inst_out, uint8_t* occ, int* work, int* status, cudaStream_t s) {
     const uint4* nodes = reinterpret_cast<const uint4*>(t->bvh8.nodes.p);
     if (occ) {
         static const int g = grid_for(k_trace_tlas<true>);
-        k_trace_tlas<true><<<g, TRACE_T, 0, s>>>(nodes, t->bvh8.leaf_ids.p, t->inst.p, rays, n, hits, inst_out, occ,
-                                                 work, status);
+        k_trace_tlas<true><<<g, TRACE_T, 0, s>>>(nodes, t->bvh8.leaf_ids.p, t->inst.p, rays, n, n_dev, hits,
+                                                 inst_out, occ, work, status);
     } else {
         static const int g = grid_for(k_trace_tlas<false>);
-        k_trace_tlas<false><<<g, TRACE_T, 0, s>>>(nodes, t->bvh8.leaf_ids.p, t->inst.p, rays, n, hits, inst_out,
-                                                  occ, work, status);
+        k_trace_tlas<false><<<g, TRACE_T, 0, s>>>(nodes, t->bvh8.leaf_ids.p, t->inst.p, rays, n, n_dev, hits,
+                                                  inst_out, occ, work, status);
     }
     return cudaGetLastError() == cudaSuccess ? RT_OK : RT_ERR_CUDA;
 }
@@ -253,7 +352,8 @@ CudaTLAS_t cudaTLAS_build(const CudaBVH_t* blas, int nb, const RtInstance* inst,
     t->num_instances = ni;
     t->blas.assign(blas, blas + nb);
     t->h_inv.resize((size_t)ni * 12);
-    std::vector<float4> rec((size_t)ni * 4), lo(ni), hi(ni);
+    std::vector<float4> rec((size_t)ni * INST_F4), lo(ni), hi(ni);
+    unsigned long long id_base = 0;
     for (int k = 0; k < ni; k++) {
         const RtInstance& I = inst[k];
         if (I.blas < 0 || I.blas >= nb) {
@@ -288,11 +388,18 @@ CudaTLAS_t cudaTLAS_build(const CudaBVH_t* blas, int nb, const RtInstance* inst,
         hi[k] = make_float4(nextafterf((float)(wh[0] + pad), INFINITY), nextafterf((float)(wh[1] + pad), INFINITY),
                             nextafterf((float)(wh[2] + pad), INFINITY), 0.f);
         const unsigned long long np = (unsigned long long)b->bvh8.nodes.p, tp = (unsigned long long)b->bvh8.tris.p;
-        rec[(size_t)k * 4 + 0] = make_float4(fi[0], fi[1], fi[2], fi[3]);
-        rec[(size_t)k * 4 + 1] = make_float4(fi[4], fi[5], fi[6], fi[7]);
-        rec[(size_t)k * 4 + 2] = make_float4(fi[8], fi[9], fi[10], fi[11]);
-        rec[(size_t)k * 4 + 3] = make_float4(bits_f((uint32_t)np), bits_f((uint32_t)(np >> 32)), bits_f((uint32_t)tp),
+        rec[(size_t)k * INST_F4 + 0] = make_float4(fi[0], fi[1], fi[2], fi[3]);
+        rec[(size_t)k * INST_F4 + 1] = make_float4(fi[4], fi[5], fi[6], fi[7]);
+        rec[(size_t)k * INST_F4 + 2] = make_float4(fi[8], fi[9], fi[10], fi[11]);
+        rec[(size_t)k * INST_F4 + 4] = make_float4(bits_f((uint32_t)id_base), 0.f, 0.f, 0.f);
+        id_base += (unsigned long long)b->num_tris;
+        rec[(size_t)k * INST_F4 + 3] = make_float4(bits_f((uint32_t)np), bits_f((uint32_t)(np >> 32)), bits_f((uint32_t)tp),
                                              bits_f((uint32_t)(tp >> 32)));
+    }
+    if (id_base >= 0xFFFFFFFFull) {
+        set_error("cudaTLAS_build: %llu instance primitives exceed the 32-bit tie-break id", id_base);
+        delete t;
+        return nullptr;
     }
     DevBuf<float4> dlo, dhi;
     BuildConfig cfg;
@@ -327,7 +434,7 @@ int cudaTLAS_traceClosest(CudaTLAS_t t, const RtRay* d_rays, int n, RtHit* d_hit
     if (n == 0) return RT_OK;
     cudaStream_t s = (cudaStream_t)stream;
     int* work = next_counter(t->counters, t->counter_next, s);
-    const int rc = launch_trace_tlas(t, d_rays, n, d_hits, d_inst, nullptr, work, t->status.p, s);
+    const int rc = launch_trace_tlas(t, d_rays, n, nullptr, d_hits, d_inst, nullptr, work, t->status.p, s);
     if (rc != RT_OK) RT_CUDA(cudaGetLastError());
     return rc;
 }
@@ -340,7 +447,7 @@ int cudaTLAS_traceAny(CudaTLAS_t t, const RtRay* d_rays, int n, uint8_t* d_occ, 
     if (n == 0) return RT_OK;
     cudaStream_t s = (cudaStream_t)stream;
     int* work = next_counter(t->counters, t->counter_next, s);
-    const int rc = launch_trace_tlas(t, d_rays, n, nullptr, nullptr, d_occ, work, t->status.p, s);
+    const int rc = launch_trace_tlas(t, d_rays, n, nullptr, nullptr, nullptr, d_occ, work, t->status.p, s);
     if (rc != RT_OK) RT_CUDA(cudaGetLastError());
     return rc;
 }

@@ -38,6 +38,24 @@ class RtInstance(C.Structure):
                 ("pad", C.c_uint32)]
 
 
+class RtMaterial(C.Structure):
+    _fields_ = [("albedo", C.c_float * 3), ("emission", C.c_float * 3)]
+
+
+class RtCamera(C.Structure):
+    _fields_ = [("eye", C.c_float * 3), ("target", C.c_float * 3), ("up", C.c_float * 3), ("vfov_deg", C.c_float)]
+
+
+class RtPTParams(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("spp", C.c_int), ("max_bounces", C.c_int),
+                ("rr_start", C.c_int), ("seed", C.c_uint32)]
+
+
+class RtPTStats(C.Structure):
+    _fields_ = [("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("light_tris", C.c_int),
+                ("light_area", C.c_double)]
+
+
 def declared_symbols() -> list[str]:
     """Function names declared in include/*.h."""
     names = []
@@ -97,6 +115,11 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "cudaTLAS_traceClosest": (i32, [vp, vp, i32, vp, vp, vp]),
         "cudaTLAS_traceAny": (i32, [vp, vp, i32, vp, vp]),
         "cudaTLAS_getInverseTransforms": (i32, [vp, vp, i32]),
+        "rtPT_create": (vp, [vp, vp, i32, vp]),
+        "rtPT_render": (i32, [vp, C.POINTER(RtCamera), C.POINTER(RtPTParams), vp, vp]),
+        "rtPT_getStats": (i32, [vp, C.POINTER(RtPTStats)]),
+        "rtPT_destroy": (None, [vp]),
+        "rtPT_cameraBasis": (i32, [C.POINTER(RtCamera), i32, i32, vp]),
     }
     for name, (res, args) in sig.items():
         if not hasattr(L, name):
@@ -270,3 +293,96 @@ def tlas_fast(aabbs: np.ndarray):
     libc.free(C.cast(pn, C.c_void_p))
     libc.free(C.cast(po, C.c_void_p))
     return nodes, ordered
+
+
+class TLAS:
+    """cudaTLAS_build over BVH handles and 3x4 instance transforms."""
+
+    def __init__(self, blases, xforms: np.ndarray, blas_index: np.ndarray):
+        L = load()
+        self.blases = list(blases)
+        n = len(blas_index)
+        self.instances = (RtInstance * n)()
+        for k in range(n):
+            self.instances[k].xform[:] = np.asarray(xforms[k], np.float32).ravel().tolist()
+            self.instances[k].blas = int(blas_index[k])
+        arr = (C.c_void_p * len(self.blases))(*[b.h for b in self.blases])
+        self.h = L.cudaTLAS_build(arr, len(self.blases), self.instances, n)
+        if not self.h:
+            raise RtError(f"cudaTLAS_build failed: {last_error()}")
+        self.n = n
+
+    def inverse(self) -> np.ndarray:
+        out = np.zeros((self.n, 12), np.float32)
+        _check(load().cudaTLAS_getInverseTransforms(self.h, out.ctypes.data, self.n), "getInverseTransforms")
+        return out
+
+    def closest(self, d_rays, n, d_hits, d_inst=None, stream=None):
+        _check(load().cudaTLAS_traceClosest(self.h, _ptr(d_rays), n, _ptr(d_hits),
+                                            _ptr(d_inst) if d_inst is not None else None, _stream(stream)),
+               "cudaTLAS_traceClosest")
+
+    def any(self, d_rays, n, d_occ, stream=None):
+        _check(load().cudaTLAS_traceAny(self.h, _ptr(d_rays), n, _ptr(d_occ), _stream(stream)), "cudaTLAS_traceAny")
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().cudaTLAS_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def make_camera(eye, target, up=(0.0, 1.0, 0.0), vfov=45.0) -> RtCamera:
+    c = RtCamera()
+    c.eye[:] = list(map(float, eye))
+    c.target[:] = list(map(float, target))
+    c.up[:] = list(map(float, up))
+    c.vfov_deg = float(vfov)
+    return c
+
+
+def camera_basis(cam: RtCamera, w: int, h: int) -> np.ndarray:
+    out = np.zeros(14, np.float32)
+    _check(load().rtPT_cameraBasis(C.byref(cam), w, h, out.ctypes.data), "rtPT_cameraBasis")
+    return out
+
+
+class PathTracer:
+    """rtPT_create / rtPT_render over a TLAS."""
+
+    def __init__(self, tlas: TLAS, albedo: np.ndarray, emission: np.ndarray):
+        n = tlas.n
+        self.mats = (RtMaterial * n)()
+        for k in range(n):
+            self.mats[k].albedo[:] = np.asarray(albedo[k], np.float32).tolist()
+            self.mats[k].emission[:] = np.asarray(emission[k], np.float32).tolist()
+        self.tlas = tlas
+        self.h = load().rtPT_create(tlas.h, self.mats, n, tlas.instances)
+        if not self.h:
+            raise RtError(f"rtPT_create failed: {last_error()}")
+
+    def render(self, cam: RtCamera, w: int, h: int, spp: int, max_bounces: int = 4, rr_start: int = 2,
+               seed: int = 1, d_rgb=None, stream=None):
+        p = RtPTParams(w, h, spp, max_bounces, rr_start, seed)
+        _check(load().rtPT_render(self.h, C.byref(cam), C.byref(p), _ptr(d_rgb), _stream(stream)), "rtPT_render")
+
+    def stats(self) -> dict:
+        s = RtPTStats()
+        _check(load().rtPT_getStats(self.h, C.byref(s)), "rtPT_getStats")
+        return {f: getattr(s, f) for f, _ in RtPTStats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().rtPT_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -291,3 +291,41 @@ def random_rays(seed: int, count: int, box: float = 100.0) -> np.ndarray:
     rays["tmin"] = 0.0
     rays["tmax"] = 1e30
     return rays
+
+
+# ------------------------------------------------------- instanced scenes --
+def instanced_scene(seed: int, total_tris: int, nblas: int = 16, ninst: int = 64, world: float = 100.0,
+                    emissive_frac: float = 0.05):
+    """configs[2] scene: `nblas` BLASes (clusters of sphere/box meshes in a
+    local 12^3 box over a 36 x 36 two-triangle floor) totalling `total_tris` triangles, `ninst` instances with
+    random rotation, log-uniform scale [1.5, 5] and uniform translation in
+    the world box, Lambertian albedo U[0.1, 0.9] per instance and emission
+    U[1, 20] (grey) on ~emissive_frac of the instances (at least one).
+    Returns (blas list of (n,9) float32, xforms (ninst,3,4) float32,
+    blas index per instance, albedo (ninst,3), emission (ninst,3))."""
+    per = total_tris // nblas
+    blases = []
+    for b in range(nblas):
+        n = per if b < nblas - 1 else total_tris - per * (nblas - 1)
+        blases.append(scene_meshes(seed * 1000 + b, n, box=12.0, lo=min(1000, n), hi=max(min(20000, n), 1000),
+                                   ground=True))
+    u = uniforms(seed, S_INST, ninst, 12).astype(np.float64)
+    R = rotations(u[:, 0:3])
+    sc = log_uniform(u[:, 3], 1.5, 5.0)
+    t = (u[:, 4:7] - 0.5) * world
+    xf = np.zeros((ninst, 3, 4), np.float32)
+    xf[:, :, :3] = (R * sc[:, None, None]).astype(np.float32)
+    xf[:, :, 3] = t.astype(np.float32)
+    bidx = (np.arange(ninst) % nblas).astype(np.int32)
+    m = uniforms(seed, S_MAT, ninst, 8).astype(np.float64)
+    albedo = (0.1 + 0.8 * m[:, 0:3]).astype(np.float32)
+    emissive = m[:, 3] < emissive_frac
+    if not emissive.any():
+        emissive[int(np.argmin(m[:, 3]))] = True
+    emission = np.zeros((ninst, 3), np.float32)
+    emission[emissive] = (1.0 + 19.0 * m[emissive, 4:5]).astype(np.float32)
+    return blases, xf, bidx, albedo, emission
+
+
+PT_CAM_EYE = (0.0, 20.0, -120.0)
+PT_CAM_TARGET = (0.0, 0.0, 0.0)
