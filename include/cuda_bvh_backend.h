@@ -4,7 +4,7 @@
  * reference project's layer/cuda_bvh_backend.h:1-147, so VkLayer_CudaRT and
  * the OptiX shim link against libcudabvh_b200.so unchanged.  Each entry point
  * names the reference declaration it replaces.  Behavioural differences (all
- * deliberate, listed in DESIGN.md) are noted inline.
+ * deliberate) are noted inline.
  *
  * Ownership: the handle owns every buffer until cudaBVH_destroy; getters
  * return borrowed host pointers that stay valid until destroy;

@@ -149,6 +149,33 @@ int cudaTLAS_traceAny(CudaTLAS_t tlas, const RtRay* d_rays, int n, uint8_t* d_oc
 /* Inverse transforms (12 floats per instance) the TLAS uses, host copy. */
 int cudaTLAS_getInverseTransforms(CudaTLAS_t tlas, float* out, int numInstances);
 
+/* ---------------- batched scenes ----------------
+ * Many independent scenes built in one multi-scene SAH build (every build
+ * stage is one launch for all scenes) and traced by one persistent
+ * work-stealing launch.  Triangles of scene i are tri_offsets[i] ..
+ * tri_offsets[i+1]-1 of h_tris; rays of scene i are d_ray_offsets[i] ..
+ * d_ray_offsets[i+1]-1 (device array, num_scenes+1 entries).  Reported
+ * primitive ids are relative to their scene. */
+typedef struct RtBatchHandle* RtBatch_t;
+RtBatch_t rtBatch_build(const CudaTri* h_tris, const int* tri_offsets, int num_scenes, void* stream);
+void rtBatch_destroy(RtBatch_t batch);
+int rtBatch_traceClosest(RtBatch_t batch, const RtRay* d_rays, const int* d_ray_offsets, int n, RtHit* d_hits,
+                         void* stream);
+int rtBatch_traceAny(RtBatch_t batch, const RtRay* d_rays, const int* d_ray_offsets, int n, uint8_t* d_occluded,
+                     void* stream);
+/* Same trace, replayed from a CUDA graph captured on the first call with
+ * these arguments (re-captured when the arguments or the tuning change).
+ * any != 0: d_out is uint8_t occlusion, else RtHit. */
+int rtBatch_traceGraph(RtBatch_t batch, const RtRay* d_rays, const int* d_ray_offsets, int n, void* d_out, int any,
+                       void* stream);
+/* Autotuner: times persistent CTAs per SM {2,4,6,8} x node visits per
+ * iteration {1,2} on this batch and keeps the fastest.  With the environment
+ * variable RTB200_TUNE_CACHE=<file> the choice is stored and reused. */
+int rtBatch_autotune(RtBatch_t batch, const RtRay* d_rays, const int* d_ray_offsets, int n, RtHit* d_hits,
+                     void* stream, int* out_ctas_per_sm, int* out_node_iters);
+int rtBatch_setTuning(RtBatch_t batch, int ctas_per_sm, int node_iters);
+int rtBatch_getInfo(RtBatch_t batch, int* num_scenes, int* num_nodes, float* build_ms);
+
 /* ---------------- wavefront path tracer ----------------
  * Lambertian scene over a TLAS: per-instance albedo and emission; emission
  * counted on camera hits; next-event estimation toward one emissive triangle

@@ -1,5 +1,5 @@
 // ref_v40_harness.cu -- drives the reference's own cuda_rt_v40.cu kernels
-// (traceBVH4Diffuse, traceCWBVH) rebuilt for sm_100a.  BASELINE ONLY: this is
+// (traceBVH4Diffuse, traceCWBVH) rebuilt for sm_100a.  Comparison arm only: this is
 // how the in-run "rebuilt reference kernel" is timed.  The reference source is
 // #included from where it lies (REF_V40_SOURCE, set by oracle/Makefile); its
 // main() is renamed with -Dmain=ref_v40_main.  Nothing here changes the

@@ -61,7 +61,7 @@ def test_closest_and_any_small_vs_brute_force(cuda, small_scene):
 
 
 def test_primary_1080p_100k_every_ray(cuda):
-    """100,002 triangles, 1920x1080 pinhole rays; every ray checked."""
+    """Primary-ray workload: 100,002 triangles, 1920x1080 pinhole rays; every ray checked."""
     tris = scenes.scene_spheres_100k(0)
     bvh = lib.BVH(tris)
     rays = scenes.primary_1080p()
@@ -73,7 +73,7 @@ def test_primary_1080p_100k_every_ray(cuda):
 
 
 def test_incoherent_rays_vs_oracle(cuda):
-    """configs[1] shape on a 400K-triangle scene: cosine diffuse bounces
+    """Incoherent-ray workload shape on a 400K-triangle scene: cosine diffuse bounces
     (closest hit) and area-light shadow rays (any hit) from primary hits."""
     tris = scenes.scene_meshes(1, 400_000)
     bvh = lib.BVH(tris)
@@ -318,7 +318,7 @@ def test_counters_match_closest_results(cuda, small_scene):
 
 
 def test_path_tracer_vs_fp64_oracle(cuda):
-    """Wavefront path tracer (configs[2] model, reduced size) against the FP64
+    """Wavefront path tracer (the 1080p TLAS workload, reduced size) against the FP64
     oracle on every pixel: the same paths (identical extension and shadow ray
     counts) and radiance within 1e-4 mean relative error."""
     import torch
@@ -344,3 +344,44 @@ def test_path_tracer_vs_fp64_oracle(cuda):
     pt.render(cam, W, H, spp, 4, 2, 7, d2)
     torch.cuda.synchronize()
     assert torch.equal(d_rgb, d2)
+
+
+def test_batched_scenes_equal_per_scene_calls(cuda):
+    """rtBatch_*: one multi-scene build and one persistent launch (plain and
+    replayed from a CUDA graph) give exactly the per-scene results,
+    including a 1-triangle scene and scenes without rays."""
+    import torch
+    sizes = [1, 3, 250, 5000, 20000, 777, 40000, 12]
+    tris = [scenes.scene_meshes(100 + i, n, box=30.0, lo=min(n, 100), hi=max(min(n, 2000), 100), ground=False)
+            if n > 2 else np.array([[0, 0, 0, 1, 0, 0, 0, 1, 0]] * n, np.float32) + np.float32(i)
+            for i, n in enumerate(sizes)]
+    nr = [3000, 0, 2000, 8000, 10000, 0, 12000, 500]
+    rays = [scenes.random_rays(200 + i, k, box=40.0) for i, k in enumerate(nr)]
+    off = np.concatenate([[0], np.cumsum(nr)]).astype(np.int32)
+    allr = np.concatenate(rays)
+    b = lib.Batch(tris)
+    d_rays = _dev(torch, allr)
+    d_off = torch.from_numpy(off).cuda()
+    n = allr.shape[0]
+    d_h = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
+    d_g = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
+    d_o = torch.empty(n, dtype=torch.uint8, device="cuda")
+    b.closest(d_rays, d_off, n, d_h)
+    b.graph(d_rays, d_off, n, d_g)
+    b.graph(d_rays, d_off, n, d_g)  # replay
+    b.any(d_rays, d_off, n, d_o)
+    torch.cuda.synchronize()
+    got = d_h.cpu().numpy().view(HIT_DTYPE)
+    assert np.array_equal(d_g.cpu().numpy(), d_h.cpu().numpy())
+    occ = d_o.cpu().numpy()
+    for i, t in enumerate(tris):
+        if nr[i] == 0:
+            continue
+        ref = O.brute_closest(t, rays[i])
+        assert_hits_equal(got[off[i]:off[i + 1]], ref, f"scene {i}")
+        assert np.array_equal(occ[off[i]:off[i + 1]], O.brute_any(t, rays[i]))
+    ctas, iters = b.autotune(d_rays, d_off, n, d_h)
+    assert 1 <= ctas <= 8 and iters in (1, 2)
+    b.graph(d_rays, d_off, n, d_g)
+    torch.cuda.synchronize()
+    assert np.array_equal(d_g.cpu().numpy(), d_h.cpu().numpy())

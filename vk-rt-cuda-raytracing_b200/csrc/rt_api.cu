@@ -398,7 +398,7 @@ namespace rtb {
 // Host check of an 8-wide structure: every child index, triangle range and
 // grid exponent in bounds, nodes numbered after their parents (acyclic),
 // every leaf item referenced exactly once, depth within the stack bound.
-bool validate_bvh8(const Bvh8Device& b, int num_items, int num_prims) {
+bool validate_bvh8(const Bvh8Device& b, int num_items, int num_prims, int num_roots) {
     std::vector<Bvh8Node> nd(b.num_nodes);
     if (!RT_CUDA(cudaMemcpy(nd.data(), b.nodes.p, nd.size() * sizeof(Bvh8Node), cudaMemcpyDeviceToHost))) return false;
     std::vector<int> items(num_items, -1);
@@ -414,7 +414,7 @@ bool validate_bvh8(const Bvh8Device& b, int num_items, int num_prims) {
         set_error("validate: no nodes");
         return false;
     }
-    depth[0] = 1;
+    for (int r = 0; r < num_roots && r < b.num_nodes; r++) depth[r] = 1;
     for (int i = 0; i < b.num_nodes; i++) {
         if (depth[i] == 0) {
             set_error("validate: node %d unreachable", i);

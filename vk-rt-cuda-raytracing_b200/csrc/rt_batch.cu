@@ -1,0 +1,277 @@
+// rt_batch.cu -- many independent scenes built and traced together (the
+// batched form): every scene's root task enters the same level-synchronous
+// SAH pipeline (scene i's root is node i), so all builds share each builder
+// stage's launches; all ray batches are traced by one persistent,
+// work-stealing launch in which every lane starts at its own scene's root;
+// that launch can be captured once into a CUDA graph and replayed.  The
+// autotuner times the persistent worker count and the node visits per
+// iteration on the caller's batch and keeps the fastest.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "rt_internal.h"
+#include "rt_legacy.h"
+#include "rt_trace.cuh"
+
+using namespace rtb;
+
+struct RtBatchHandle {
+    int num_scenes = 0;
+    int num_tris = 0;
+    std::vector<int> tri_off;
+    DevBuf<int> d_tri_off;
+    DevBuf<float> tris9;
+    Bvh2Device bvh2;
+    Bvh8Device bvh8;
+    DevBuf<int> work, status;  // work[0]: plain launches, work[1]: graph launches
+    int ctas_per_sm = TRACE_MINB;
+    int node_iters = 2;
+    float build_ms = 0.f;
+    // captured graph and the arguments it was captured with
+    cudaGraphExec_t gexec = nullptr;
+    cudaStream_t cap_stream = nullptr;
+    const void* g_rays = nullptr;
+    const void* g_off = nullptr;
+    void* g_out = nullptr;
+    int g_n = -1, g_any = -1, g_ctas = -1, g_iters = -1;
+    ~RtBatchHandle() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (cap_stream) cudaStreamDestroy(cap_stream);
+    }
+};
+
+namespace {
+
+bool tune_from_cache(RtBatchHandle* b, int n) {
+    const char* path = getenv("RTB200_TUNE_CACHE");
+    if (!path) return false;
+    FILE* f = fopen(path, "r");
+    if (!f) return false;
+    char key[128];
+    snprintf(key, sizeof(key), "\"batch:%d:%d:%d\"", b->num_scenes, b->num_tris, n);
+    char line[512];
+    bool found = false;
+    while (fgets(line, sizeof(line), f)) {
+        const char* k = strstr(line, key);
+        if (!k) continue;
+        int c = 0, it = 0;
+        if (sscanf(k + strlen(key), " : [%d, %d]", &c, &it) == 2 && c >= 1 && c <= TRACE_MINB &&
+            (it == 1 || it == 2)) {
+            b->ctas_per_sm = c;
+            b->node_iters = it;
+            found = true;
+        }
+    }
+    fclose(f);
+    return found;
+}
+
+void tune_to_cache(const RtBatchHandle* b, int n) {
+    const char* path = getenv("RTB200_TUNE_CACHE");
+    if (!path) return;
+    FILE* f = fopen(path, "a");
+    if (!f) return;
+    fprintf(f, "{\"batch:%d:%d:%d\" : [%d, %d]}\n", b->num_scenes, b->num_tris, n, b->ctas_per_sm, b->node_iters);
+    fclose(f);
+}
+
+int check_trace_args(RtBatchHandle* b, const RtRay* rays, const int* off, int n, const void* out, const char* who) {
+    if (!b || n < 0 || (n > 0 && (!rays || !off || !out))) {
+        set_error("%s: invalid argument", who);
+        return RT_ERR_INVALID;
+    }
+    return RT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+RtBatch_t rtBatch_build(const CudaTri* h_tris, const int* tri_offsets, int num_scenes, void* stream) {
+    clear_error();
+    if (!h_tris || !tri_offsets || num_scenes <= 0 || tri_offsets[0] != 0) {
+        set_error("rtBatch_build: invalid argument");
+        return nullptr;
+    }
+    for (int i = 0; i < num_scenes; i++)
+        if (tri_offsets[i + 1] <= tri_offsets[i]) {
+            set_error("rtBatch_build: scene %d has no triangles", i);
+            return nullptr;
+        }
+    cudaStream_t s = (cudaStream_t)stream;
+    RtBatchHandle* b = new (std::nothrow) RtBatchHandle();
+    if (!b) return nullptr;
+    b->num_scenes = num_scenes;
+    b->num_tris = tri_offsets[num_scenes];
+    b->tri_off.assign(tri_offsets, tri_offsets + num_scenes + 1);
+    const int n = b->num_tris;
+    DevBuf<float4> lo, hi;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    bool ok = b->tris9.alloc((size_t)n * 9) && b->d_tri_off.alloc(num_scenes + 1) && lo.alloc(n) && hi.alloc(n) &&
+              b->work.alloc(2) && b->status.alloc(1) &&
+              RT_CUDA(cudaMemcpyAsync(b->tris9.p, h_tris, sizeof(CudaTri) * (size_t)n, cudaMemcpyHostToDevice, s)) &&
+              RT_CUDA(cudaMemcpyAsync(b->d_tri_off.p, tri_offsets, sizeof(int) * (num_scenes + 1),
+                                      cudaMemcpyHostToDevice, s)) &&
+              RT_CUDA(cudaMemsetAsync(b->status.p, 0, sizeof(int), s));
+    if (ok) {
+        cudaEventRecord(e0, s);
+        launch_tri_bounds(b->tris9.p, n, lo.p, hi.p, s);
+        BuildConfig cfg;
+        ok = build_bvh2(lo.p, hi.p, n, cfg, b->bvh2, s, &b->tri_off) && collapse_bvh8(b->bvh2, b->tris9.p, b->bvh8, s);
+        cudaEventRecord(e1, s);
+        ok = ok && RT_CUDA(cudaEventSynchronize(e1));
+        if (ok) cudaEventElapsedTime(&b->build_ms, e0, e1);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (ok && getenv("RTB200_VALIDATE") && atoi(getenv("RTB200_VALIDATE")))
+        ok = validate_bvh8(b->bvh8, b->bvh8.num_leaf_items, n, num_scenes);
+    if (!ok) {
+        delete b;
+        return nullptr;
+    }
+    return b;
+}
+
+void rtBatch_destroy(RtBatch_t b) {
+    if (!b) return;
+    cudaDeviceSynchronize();
+    delete b;
+}
+
+int rtBatch_traceClosest(RtBatch_t b, const RtRay* d_rays, const int* d_ray_offsets, int n, RtHit* d_hits,
+                         void* stream) {
+    int rc = check_trace_args(b, d_rays, d_ray_offsets, n, d_hits, "rtBatch_traceClosest");
+    if (rc != RT_OK || n == 0) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaMemsetAsync(b->work.p, 0, sizeof(int), s);
+    rc = launch_trace_multi(b->bvh8, d_rays, n, d_ray_offsets, b->d_tri_off.p, b->num_scenes, d_hits, nullptr,
+                            b->work.p, b->status.p, b->ctas_per_sm, b->node_iters, s);
+    if (rc != RT_OK) RT_CUDA(cudaGetLastError());
+    return rc;
+}
+
+int rtBatch_traceAny(RtBatch_t b, const RtRay* d_rays, const int* d_ray_offsets, int n, uint8_t* d_occ,
+                     void* stream) {
+    int rc = check_trace_args(b, d_rays, d_ray_offsets, n, d_occ, "rtBatch_traceAny");
+    if (rc != RT_OK || n == 0) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaMemsetAsync(b->work.p, 0, sizeof(int), s);
+    rc = launch_trace_multi(b->bvh8, d_rays, n, d_ray_offsets, b->d_tri_off.p, b->num_scenes, nullptr, d_occ,
+                            b->work.p, b->status.p, b->ctas_per_sm, b->node_iters, s);
+    if (rc != RT_OK) RT_CUDA(cudaGetLastError());
+    return rc;
+}
+
+int rtBatch_traceGraph(RtBatch_t b, const RtRay* d_rays, const int* d_ray_offsets, int n, void* d_out, int any,
+                       void* stream) {
+    int rc = check_trace_args(b, d_rays, d_ray_offsets, n, d_out, "rtBatch_traceGraph");
+    if (rc != RT_OK || n == 0) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool same = b->gexec && b->g_rays == d_rays && b->g_off == d_ray_offsets && b->g_out == d_out &&
+                      b->g_n == n && b->g_any == any && b->g_ctas == b->ctas_per_sm && b->g_iters == b->node_iters;
+    if (!same) {
+        if (b->gexec) {
+            cudaGraphExecDestroy(b->gexec);
+            b->gexec = nullptr;
+        }
+        if (!b->cap_stream && !RT_CUDA(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking)))
+            return RT_ERR_CUDA;
+        cudaGraph_t g = nullptr;
+        if (!RT_CUDA(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal))) return RT_ERR_CUDA;
+        cudaMemsetAsync(b->work.p + 1, 0, sizeof(int), b->cap_stream);
+        const int lrc = launch_trace_multi(b->bvh8, d_rays, n, d_ray_offsets, b->d_tri_off.p, b->num_scenes,
+                                           any ? nullptr : (RtHit*)d_out, any ? (uint8_t*)d_out : nullptr,
+                                           b->work.p + 1, b->status.p, b->ctas_per_sm, b->node_iters, b->cap_stream);
+        const bool ended = RT_CUDA(cudaStreamEndCapture(b->cap_stream, &g));
+        if (lrc != RT_OK || !ended) {
+            if (g) cudaGraphDestroy(g);
+            return RT_ERR_CUDA;
+        }
+        const bool inst = RT_CUDA(cudaGraphInstantiate(&b->gexec, g, 0));
+        cudaGraphDestroy(g);
+        if (!inst) return RT_ERR_CUDA;
+        b->g_rays = d_rays;
+        b->g_off = d_ray_offsets;
+        b->g_out = d_out;
+        b->g_n = n;
+        b->g_any = any;
+        b->g_ctas = b->ctas_per_sm;
+        b->g_iters = b->node_iters;
+    }
+    return RT_CUDA(cudaGraphLaunch(b->gexec, s)) ? RT_OK : RT_ERR_CUDA;
+}
+
+int rtBatch_autotune(RtBatch_t b, const RtRay* d_rays, const int* d_ray_offsets, int n, RtHit* d_hits,
+                     void* stream, int* out_ctas_per_sm, int* out_node_iters) {
+    int rc = check_trace_args(b, d_rays, d_ray_offsets, n, d_hits, "rtBatch_autotune");
+    if (rc != RT_OK) return rc;
+    if (n > 0 && !tune_from_cache(b, n)) {
+        cudaStream_t s = (cudaStream_t)stream;
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        float best = 1e30f;
+        int bc = b->ctas_per_sm, bi = b->node_iters;
+        const int cands[] = {2, 4, 6, TRACE_MINB};
+        for (int c : cands) {
+            for (int it = 1; it <= 2; it++) {
+                b->ctas_per_sm = c;
+                b->node_iters = it;
+                rtBatch_traceClosest(b, d_rays, d_ray_offsets, n, d_hits, stream);  // warm
+                cudaEventRecord(e0, s);
+                for (int k = 0; k < 3; k++) rtBatch_traceClosest(b, d_rays, d_ray_offsets, n, d_hits, stream);
+                cudaEventRecord(e1, s);
+                if (!RT_CUDA(cudaEventSynchronize(e1))) {
+                    cudaEventDestroy(e0);
+                    cudaEventDestroy(e1);
+                    return RT_ERR_CUDA;
+                }
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms < best) {
+                    best = ms;
+                    bc = c;
+                    bi = it;
+                }
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        b->ctas_per_sm = bc;
+        b->node_iters = bi;
+        tune_to_cache(b, n);
+    }
+    if (out_ctas_per_sm) *out_ctas_per_sm = b->ctas_per_sm;
+    if (out_node_iters) *out_node_iters = b->node_iters;
+    return RT_OK;
+}
+
+int rtBatch_setTuning(RtBatch_t b, int ctas_per_sm, int node_iters) {
+    if (!b || ctas_per_sm < 1 || ctas_per_sm > TRACE_MINB || node_iters < 1 || node_iters > 2) {
+        set_error("rtBatch_setTuning: invalid argument");
+        return RT_ERR_INVALID;
+    }
+    b->ctas_per_sm = ctas_per_sm;
+    b->node_iters = node_iters;
+    return RT_OK;
+}
+
+int rtBatch_getInfo(RtBatch_t b, int* num_scenes, int* num_nodes, float* build_ms) {
+    if (!b) {
+        set_error("rtBatch_getInfo: invalid argument");
+        return RT_ERR_INVALID;
+    }
+    if (num_scenes) *num_scenes = b->num_scenes;
+    if (num_nodes) *num_nodes = b->bvh8.num_nodes;
+    if (build_ms) *build_ms = b->build_ms;
+    return RT_OK;
+}
+
+}  // extern "C"

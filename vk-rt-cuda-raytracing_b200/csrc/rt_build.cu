@@ -19,8 +19,10 @@
 // HPG 2017), assign children to octant slots, quantise child boxes outward
 // to 8 bits per plane against a power-of-two grid, emit triangle records
 // in node order.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstring>
 
 #include "rt_internal.h"
 
@@ -143,15 +145,18 @@ __device__ __forceinline__ float bin_scale(float cmin, float cmax) {
     return ext > 0.f ? (float)kBins / ext : 0.f;
 }
 
-// Global box and centroid box of all primitives (12 ordered uints).
-__global__ void k_root_bounds(const float4* __restrict__ lo, const float4* __restrict__ hi, int n,
-                              uint32_t* __restrict__ acc) {
+// Per-segment box and centroid box (12 ordered uints per segment); grid.y
+// is the segment, grid.x strides over its primitives.
+__global__ void k_seg_bounds(const float4* __restrict__ lo, const float4* __restrict__ hi,
+                             const int* __restrict__ seg_off, uint32_t* __restrict__ acc) {
+    const int sgi = blockIdx.y;
+    const int beg = seg_off[sgi], end = seg_off[sgi + 1];
     float b[12];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         b[k] = FLT_MAX; b[3 + k] = -FLT_MAX; b[6 + k] = FLT_MAX; b[9 + k] = -FLT_MAX;
     }
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (int i = beg + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
         const float4 l = lo[i], h = hi[i];
         const float L[3] = {l.x, l.y, l.z}, H[3] = {h.x, h.y, h.z};
 #pragma unroll
@@ -163,6 +168,7 @@ __global__ void k_root_bounds(const float4* __restrict__ lo, const float4* __res
             b[9 + k] = fmaxf(b[9 + k], c);
         }
     }
+    uint32_t* a = acc + (size_t)sgi * 12;
 #pragma unroll
     for (int k = 0; k < 12; k++) {
         const bool mx = (k >= 3 && k < 6) || k >= 9;
@@ -173,8 +179,8 @@ __global__ void k_root_bounds(const float4* __restrict__ lo, const float4* __res
             v = mx ? fmaxf(v, y) : fminf(v, y);
         }
         if ((threadIdx.x & 31) == 0) {
-            if (mx) atomicMax(&acc[k], f2ord(v));
-            else atomicMin(&acc[k], f2ord(v));
+            if (mx) atomicMax(&a[k], f2ord(v));
+            else atomicMin(&a[k], f2ord(v));
         }
     }
 }
@@ -194,18 +200,6 @@ struct Chunk {
 // bins per task: [axis][bin] x {cnt, lo3, hi3, clo3, chi3} as ordered uints
 constexpr int BIN_WORDS = 13;
 constexpr int TASK_BIN_WORDS = 3 * kBins * BIN_WORDS;
-
-__global__ void k_init_root(Task* tasks, Node2* nodes, const uint32_t* acc, int n, int max_leaf) {
-    Task t;
-    t.node = 0; t.start = 0; t.count = n; t.depth = 0;
-    for (int k = 0; k < 3; k++) { t.clo[k] = ord2f(acc[6 + k]); t.chi[k] = ord2f(acc[9 + k]); }
-    tasks[0] = t;
-    Node2 r;
-    for (int k = 0; k < 3; k++) { r.lo[k] = ord2f(acc[k]); r.hi[k] = ord2f(acc[3 + k]); }
-    r.a = 0; r.b = 0;
-    if (n <= max_leaf) { r.a = 0; r.b = -n; }
-    nodes[0] = r;
-}
 
 __global__ void k_chunk_counts(const Task* __restrict__ tasks, int T, int* __restrict__ cnt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -776,7 +770,7 @@ __global__ void k_iota(int* __restrict__ p, int n) {
 
 // ----------------------------------------------------------- the driver --
 bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig& cfg, Bvh2Device& out,
-                cudaStream_t s) {
+                cudaStream_t s, const std::vector<int>* segments) {
     if (n <= 0) {
         set_error("build: empty input");
         return false;
@@ -785,13 +779,25 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
         set_error("build: max_leaf must be 1..4");
         return false;
     }
+    std::vector<int> seg = segments ? *segments : std::vector<int>{0, n};
+    const int S = (int)seg.size() - 1;
+    if (S < 1 || seg.front() != 0 || seg.back() != n) {
+        set_error("build: bad segment table");
+        return false;
+    }
+    for (int i = 0; i < S; i++)
+        if (seg[i + 1] <= seg[i]) {
+            set_error("build: segment %d is empty", i);
+            return false;
+        }
     out.num_prims = n;
+    out.num_roots = S;
     if (!out.nodes.alloc((size_t)2 * n + 2) || !out.perm.alloc(n)) return false;
     cudaMemsetAsync(out.nodes.p, 0, out.nodes.bytes(), s);
     int* perm = out.perm.p;
     // temporaries
     const int maxT = n / (cfg.small_task + 1) + 2;  // large tasks per level
-    DevBuf<int> tmp;
+    DevBuf<int> tmp, dseg;
     DevBuf<uint32_t> acc;
     DevBuf<Task> tasks_a, tasks_b, kids, small;
     DevBuf<Split> splits;
@@ -801,37 +807,76 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
     DevBuf<Chunk> chunks;
     DevBuf<int> ccount, coff, cleft, cleftoff;
     const int maxSmall = n / (cfg.max_leaf + 1) + 2;
-    if (!tmp.alloc(n) || !acc.alloc(12) || !tasks_a.alloc(maxT) || !tasks_b.alloc(maxT) || !kids.alloc(2 * maxT) ||
-        !small.alloc(maxSmall) || !splits.alloc(maxT) || !gbins.alloc((size_t)maxT * TASK_BIN_WORDS) ||
-        !flags.alloc(4 * 2 * maxT + 8) || !chunks.alloc(maxChunks) || !ccount.alloc(maxT) || !coff.alloc(maxT) ||
-        !cleft.alloc(maxChunks) || !cleftoff.alloc(maxChunks) || !status.alloc(1))
+    if (!tmp.alloc(n) || !acc.alloc((size_t)12 * S) || !dseg.alloc(S + 1) || !tasks_a.alloc(maxT) ||
+        !tasks_b.alloc(maxT) || !kids.alloc(2 * maxT) || !small.alloc(maxSmall) || !splits.alloc(maxT) ||
+        !gbins.alloc((size_t)maxT * TASK_BIN_WORDS) || !flags.alloc(4 * 2 * maxT + 8) || !chunks.alloc(maxChunks) ||
+        !ccount.alloc(maxT) || !coff.alloc(maxT) || !cleft.alloc(maxChunks) || !cleftoff.alloc(maxChunks) ||
+        !status.alloc(1))
         return false;
     cudaMemsetAsync(status.p, 0, sizeof(int), s);
     k_iota<<<(n + 255) / 256, 256, 0, s>>>(perm, n);
-    // root bounds
-    {
-        uint32_t init[12];
-        for (int k = 0; k < 12; k++) init[k] = ((k >= 3 && k < 6) || k >= 9) ? 0u : 0xFFFFFFFFu;
-        cudaMemcpyAsync(acc.p, init, sizeof(init), cudaMemcpyHostToDevice, s);
-        const int blocks = std::min((n + 255) / 256, num_sms() * 8);
-        k_root_bounds<<<blocks, 256, 0, s>>>(d_lo, d_hi, n, acc.p);
-        k_init_root<<<1, 1, 0, s>>>(tasks_a.p, out.nodes.p, acc.p, n, cfg.max_leaf);
-    }
-    int node_count = 1;
-    int num_small = 0;
-    int* d_small_base = flags.p + 8 * maxT;  // running count of small tasks
-    int* d_tot = d_small_base + 1;           // scratch totals [large, small, chunks]
-    cudaMemsetAsync(d_small_base, 0, sizeof(int), s);
-    int T = 0;
-    if (n > cfg.max_leaf) {
-        if (n > cfg.small_task) {
-            T = 1;
+    // per-segment root bounds, then the initial task lists (on the host, in
+    // segment order, so node ids and task order are deterministic)
+    std::vector<uint32_t> hacc((size_t)12 * S);
+    for (int i = 0; i < S; i++)
+        for (int k = 0; k < 12; k++) hacc[(size_t)i * 12 + k] = ((k >= 3 && k < 6) || k >= 9) ? 0u : 0xFFFFFFFFu;
+    int maxcnt = 0;
+    for (int i = 0; i < S; i++) maxcnt = std::max(maxcnt, seg[i + 1] - seg[i]);
+    if (!RT_CUDA(cudaMemcpyAsync(acc.p, hacc.data(), hacc.size() * 4, cudaMemcpyHostToDevice, s)) ||
+        !RT_CUDA(cudaMemcpyAsync(dseg.p, seg.data(), seg.size() * 4, cudaMemcpyHostToDevice, s)))
+        return false;
+    k_seg_bounds<<<dim3(std::min((maxcnt + 2047) / 2048, 64), S), 256, 0, s>>>(d_lo, d_hi, dseg.p, acc.p);
+    if (!RT_CUDA(cudaMemcpyAsync(hacc.data(), acc.p, hacc.size() * 4, cudaMemcpyDeviceToHost, s)) ||
+        !RT_CUDA(cudaStreamSynchronize(s)))
+        return false;
+    auto ordf = [](uint32_t u) {
+        const uint32_t v = (u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u;
+        float f;
+        memcpy(&f, &v, 4);
+        return f;
+    };
+    std::vector<Node2> roots(S);
+    std::vector<Task> large0, small0;
+    for (int i = 0; i < S; i++) {
+        const uint32_t* a = &hacc[(size_t)i * 12];
+        Node2& r = roots[i];
+        Task t;
+        t.node = i;
+        t.start = seg[i];
+        t.count = seg[i + 1] - seg[i];
+        t.depth = 0;
+        for (int k = 0; k < 3; k++) {
+            r.lo[k] = ordf(a[k]);
+            r.hi[k] = ordf(a[3 + k]);
+            t.clo[k] = ordf(a[6 + k]);
+            t.chi[k] = ordf(a[9 + k]);
+        }
+        r.a = 0;
+        r.b = 0;
+        if (t.count <= cfg.max_leaf) {
+            r.a = t.start;
+            r.b = -t.count;
+        } else if (t.count <= cfg.small_task) {
+            small0.push_back(t);
         } else {
-            // the root itself is the only small task
-            cudaMemcpyAsync(small.p, tasks_a.p, sizeof(Task), cudaMemcpyDeviceToDevice, s);
-            num_small = 1;
+            large0.push_back(t);
         }
     }
+    if (!RT_CUDA(cudaMemcpyAsync(out.nodes.p, roots.data(), roots.size() * sizeof(Node2), cudaMemcpyHostToDevice, s)))
+        return false;
+    if (!large0.empty() &&
+        !RT_CUDA(cudaMemcpyAsync(tasks_a.p, large0.data(), large0.size() * sizeof(Task), cudaMemcpyHostToDevice, s)))
+        return false;
+    if (!small0.empty() &&
+        !RT_CUDA(cudaMemcpyAsync(small.p, small0.data(), small0.size() * sizeof(Task), cudaMemcpyHostToDevice, s)))
+        return false;
+    int node_count = S;
+    int num_small = (int)small0.size();
+    int* d_small_base = flags.p + 8 * maxT;  // running count of small tasks
+    int* d_tot = d_small_base + 1;           // scratch totals [large, small, chunks]
+    cudaMemcpyAsync(d_small_base, &num_small, sizeof(int), cudaMemcpyHostToDevice, s);
+    int T = (int)large0.size();
+    if (!RT_CUDA(cudaStreamSynchronize(s))) return false;
     Task* cur = tasks_a.p;
     Task* nxt = tasks_b.p;
     int* is_large = flags.p;

@@ -10,6 +10,7 @@
 // records of the leaf children contiguously in slot order.
 #include <cfloat>
 #include <cmath>
+#include <vector>
 
 #include "rt_internal.h"
 
@@ -202,9 +203,10 @@ __global__ void k_emit(const Node2* __restrict__ nodes, const int* __restrict__ 
 
 bool collapse_bvh8(const Bvh2Device& b2, const float* d_tris9, Bvh8Device& out, cudaStream_t s) {
     const int n = b2.num_prims;
+    const int R = b2.num_roots;
     // upper bound on 8-wide nodes: every node has >= 2 children except a
-    // root that is a single leaf, so nodes <= leaves <= n
-    const int max_nodes = n + 1;
+    // root that is a single leaf, so nodes <= leaves + roots <= n + R
+    const int max_nodes = n + R;
     if (!out.nodes.alloc(max_nodes)) return false;
     if (d_tris9) {
         if (!out.tris.alloc(n)) return false;
@@ -217,8 +219,15 @@ bool collapse_bvh8(const Bvh2Device& b2, const float* d_tris9, Bvh8Device& out, 
         !n_items.alloc(max_nodes) || !inner_off.alloc(max_nodes) || !item_off.alloc(max_nodes) ||
         !gat.alloc(max_nodes) || !tot.alloc(2))
         return false;
-    cudaMemsetAsync(lvl_a.p, 0, sizeof(int), s);  // root binary node 0
-    int L = 1, level_base = 0, items = 0, depth = 0;
+    {
+        // level 0: the roots, binary nodes 0 .. R-1 -> 8-wide nodes 0 .. R-1
+        std::vector<int> roots(R);
+        for (int i = 0; i < R; i++) roots[i] = i;
+        if (!RT_CUDA(cudaMemcpyAsync(lvl_a.p, roots.data(), R * sizeof(int), cudaMemcpyHostToDevice, s)) ||
+            !RT_CUDA(cudaStreamSynchronize(s)))
+            return false;
+    }
+    int L = R, level_base = 0, items = 0, depth = 0;
     int* cur = lvl_a.p;
     int* nxt = lvl_b.p;
     while (L > 0) {

@@ -66,6 +66,7 @@ struct Bvh2Device {
     DevBuf<int> perm;        // leaf order -> primitive index
     int num_nodes = 0;       // slots used (incl. unused reservations)
     int num_prims = 0;
+    int num_roots = 1;       // one root per segment, nodes 0 .. num_roots-1
 };
 
 // The compressed 8-wide structure the traversal kernels read.
@@ -81,8 +82,10 @@ struct Bvh8Device {
 // Builds the binary SAH BVH over primitive boxes (lo/hi float4 per prim).
 // Returns false on failure (error set).  Stream-ordered; synchronises on
 // small counts between levels.
+// `segments` (optional, host) splits the primitives into independent scenes
+// [seg[i], seg[i+1]) built together; scene i's root is node i.
 bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig& cfg, Bvh2Device& out,
-                cudaStream_t s);
+                cudaStream_t s, const std::vector<int>* segments = nullptr);
 
 // Collapses a BVH2 into the 8-wide layout.  For a BLAS d_tris9 holds the
 // triangles (9 floats each) and TriRec records are written; for a TLAS
@@ -95,8 +98,9 @@ void launch_tri_bounds(const float* d_tris9, int n, float4* d_lo, float4* d_hi, 
 // Exclusive scan of n ints (device), total written to *d_total if non-null.
 bool scan_exclusive(const int* d_in, int* d_out, int n, int* d_total, cudaStream_t s);
 
-// Host structural check of an 8-wide structure (error set on failure).
-bool validate_bvh8(const Bvh8Device& b, int num_items, int num_prims);
+// Host structural check of an 8-wide structure with roots 0 .. num_roots-1
+// (error set on failure).
+bool validate_bvh8(const Bvh8Device& b, int num_items, int num_prims, int num_roots = 1);
 
 // SAH cost (root-area normalised) of a BVH2.
 float bvh2_sah_cost(const Bvh2Device& b2, cudaStream_t s);

@@ -21,5 +21,8 @@ void launch_shade(const RtRay* rays, const RtHit* hits, const float* tris9, int 
 struct Bvh8Device;
 int launch_trace_blas(const Bvh8Device& b, const RtRay* rays, int n, RtHit* hits, uint8_t* occ,
                       uint32_t* counts, int* work, int* status, cudaStream_t s);
+int launch_trace_multi(const Bvh8Device& b, const RtRay* rays, int n, const int* ray_off, const int* tri_off,
+                       int nscenes, RtHit* hits, uint8_t* occ, int* work, int* status, int ctas_per_sm,
+                       int node_iters, cudaStream_t s);
 
 }  // namespace rtb

@@ -28,6 +28,7 @@
 // rounding of the decode, so a box that contains an accepted triangle hit
 // is never culled.  Hit results are therefore defined by the triangle test
 // alone: Moller-Trumbore in exact IEEE single precision (rt_common.cuh).
+#include <algorithm>
 #include <cfloat>
 
 #include "rt_internal.h"
@@ -35,11 +36,15 @@
 
 namespace rtb {
 
-template <bool ANY, bool COUNT>
+// MULTI: the structure holds several scenes (roots 0 .. nscenes-1); ray i
+// belongs to the scene s with ray_off[s] <= i < ray_off[s+1], starts at root
+// s, and reports primitives relative to tri_off[s].
+template <bool ANY, bool COUNT, bool MULTI, int NITERS>
 __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
     k_trace_blas(const uint4* __restrict__ nodes, const float4* __restrict__ tris, const RtRay* __restrict__ rays,
                  int n, RtHit* __restrict__ hits, uint8_t* __restrict__ occ, uint32_t* __restrict__ counts,
-                 int* __restrict__ work, int* __restrict__ status) {
+                 int* __restrict__ work, int* __restrict__ status, const int* __restrict__ ray_off,
+                 const int* __restrict__ tri_off, int nscenes) {
     __shared__ uint2 sstack[SSTACK][TRACE_T];
     __shared__ unsigned long long s_key[TRACE_T];  // owner's best (ordered t, prim)
     __shared__ int s_rec[TRACE_T];                 // set when a worker improved it (any hit: found)
@@ -53,6 +58,7 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
     Walk w;
     float thit = 0.f, hu = 0.f, hv = 0.f;
     int hprim = -1;
+    int prim_base = 0;
     uint32_t cn = 0, ct = 0;
     for (;;) {
         // ---- refill idle lanes ----
@@ -72,7 +78,18 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
                     hprim = -1;
                     hu = hv = 0.f;
                     w.start();
-                    w.ng = make_uint2(0u, (1u << r.oct) | (1u << 8));
+                    uint32_t root = 0;
+                    if (MULTI) {
+                        int lo = 0, hi = nscenes - 1;  // last scene whose first ray <= ri
+                        while (lo < hi) {
+                            const int mid = (lo + hi + 1) >> 1;
+                            if (__ldg(ray_off + mid) <= ri) lo = mid;
+                            else hi = mid - 1;
+                        }
+                        root = (uint32_t)lo;
+                        prim_base = __ldg(tri_off + lo);
+                    }
+                    w.ng = make_uint2(root, (1u << r.oct) | (1u << 8));
                     cn = ct = 0;
                 } else {
                     exhausted = true;
@@ -84,7 +101,7 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
         uint32_t tri_base = 0, tmask = 0;
         bool overflow = false;
 #pragma unroll 1
-        for (int it = 0; it < RTB_NODE_ITERS; it++) {
+        for (int it = 0; it < NITERS; it++) {
             if (ray >= 0 && tmask == 0 && !overflow && (w.ng.y & 0xFFu)) {
                 uint32_t hitsm = w.ng.y & 0xFFu;
                 const uint32_t imask = (w.ng.y >> 8) & 0xFFu;
@@ -97,7 +114,7 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
                 uint32_t nmask;
                 visit_node(nodes + (size_t)ni * 5, r, thit, nmask, tri_base, tmask, w.ng);
                 prefetch_next(nodes, w.ng, r.oct);
-                if (RTB_NODE_ITERS > 1 && tmask == 0 && (w.ng.y & 0xFFu) == 0 && w.sp > 0) {
+                if (NITERS > 1 && tmask == 0 && (w.ng.y & 0xFFu) == 0 && w.sp > 0) {
                     w.ng = w.pop(sstack, lstack);
                 }
             }
@@ -197,7 +214,8 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
                     occ[ray] = found_any ? 1 : 0;
                 } else {
                     reinterpret_cast<float4*>(hits)[ray] =
-                        make_float4(hprim >= 0 ? thit : __int_as_float(0x7f800000), __int_as_float(hprim),
+                        make_float4(hprim >= 0 ? thit : __int_as_float(0x7f800000),
+                                    __int_as_float(hprim >= 0 ? hprim - prim_base : -1),
                                     hprim >= 0 ? hu : 0.f, hprim >= 0 ? hv : 0.f);
                 }
                 if (COUNT) reinterpret_cast<uint2*>(counts)[ray] = make_uint2(cn, ct);
@@ -221,20 +239,51 @@ int launch_trace_blas(const Bvh8Device& b, const RtRay* rays, int n, RtHit* hits
                       uint32_t* counts, int* work, int* status, cudaStream_t s) {
     const uint4* nodes = reinterpret_cast<const uint4*>(b.nodes.p);
     const float4* tris = reinterpret_cast<const float4*>(b.tris.p);
+    constexpr int NI = RTB_NODE_ITERS;
     if (counts) {
         if (occ) {
-            static const int g = persistent_grid(k_trace_blas<true, true>, TRACE_T);
-            k_trace_blas<true, true><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work, status);
+            static const int g = persistent_grid(k_trace_blas<true, true, false, NI>, TRACE_T);
+            k_trace_blas<true, true, false, NI><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work,
+                                                                     status, nullptr, nullptr, 1);
         } else {
-            static const int g = persistent_grid(k_trace_blas<false, true>, TRACE_T);
-            k_trace_blas<false, true><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work, status);
+            static const int g = persistent_grid(k_trace_blas<false, true, false, NI>, TRACE_T);
+            k_trace_blas<false, true, false, NI><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work,
+                                                                      status, nullptr, nullptr, 1);
         }
     } else if (occ) {
-        static const int g = persistent_grid(k_trace_blas<true, false>, TRACE_T);
-        k_trace_blas<true, false><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work, status);
+        static const int g = persistent_grid(k_trace_blas<true, false, false, NI>, TRACE_T);
+        k_trace_blas<true, false, false, NI><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work,
+                                                                  status, nullptr, nullptr, 1);
     } else {
-        static const int g = persistent_grid(k_trace_blas<false, false>, TRACE_T);
-        k_trace_blas<false, false><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work, status);
+        static const int g = persistent_grid(k_trace_blas<false, false, false, NI>, TRACE_T);
+        k_trace_blas<false, false, false, NI><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work,
+                                                                   status, nullptr, nullptr, 1);
+    }
+    return cudaGetLastError() == cudaSuccess ? RT_OK : RT_ERR_CUDA;
+}
+
+// Many scenes in one persistent launch: ctas_per_sm (1..TRACE_MINB) sets the
+// worker count, node_iters (1 or 2) the node visits per iteration.
+int launch_trace_multi(const Bvh8Device& b, const RtRay* rays, int n, const int* ray_off, const int* tri_off,
+                       int nscenes, RtHit* hits, uint8_t* occ, int* work, int* status, int ctas_per_sm,
+                       int node_iters, cudaStream_t s) {
+    const uint4* nodes = reinterpret_cast<const uint4*>(b.nodes.p);
+    const float4* tris = reinterpret_cast<const float4*>(b.tris.p);
+    const int g = std::max(1, std::min(ctas_per_sm, TRACE_MINB)) * num_sms();
+    if (occ) {
+        if (node_iters == 1)
+            k_trace_blas<true, false, true, 1><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
+                                                                    status, ray_off, tri_off, nscenes);
+        else
+            k_trace_blas<true, false, true, 2><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
+                                                                    status, ray_off, tri_off, nscenes);
+    } else {
+        if (node_iters == 1)
+            k_trace_blas<false, false, true, 1><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
+                                                                     status, ray_off, tri_off, nscenes);
+        else
+            k_trace_blas<false, false, true, 2><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
+                                                                     status, ray_off, tri_off, nscenes);
     }
     return cudaGetLastError() == cudaSuccess ? RT_OK : RT_ERR_CUDA;
 }

@@ -115,6 +115,14 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "cudaTLAS_traceClosest": (i32, [vp, vp, i32, vp, vp, vp]),
         "cudaTLAS_traceAny": (i32, [vp, vp, i32, vp, vp]),
         "cudaTLAS_getInverseTransforms": (i32, [vp, vp, i32]),
+        "rtBatch_build": (vp, [vp, vp, i32, vp]),
+        "rtBatch_destroy": (None, [vp]),
+        "rtBatch_traceClosest": (i32, [vp, vp, vp, i32, vp, vp]),
+        "rtBatch_traceAny": (i32, [vp, vp, vp, i32, vp, vp]),
+        "rtBatch_traceGraph": (i32, [vp, vp, vp, i32, vp, i32, vp]),
+        "rtBatch_autotune": (i32, [vp, vp, vp, i32, vp, vp, C.POINTER(i32), C.POINTER(i32)]),
+        "rtBatch_setTuning": (i32, [vp, i32, i32]),
+        "rtBatch_getInfo": (i32, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(f32)]),
         "rtPT_create": (vp, [vp, vp, i32, vp]),
         "rtPT_render": (i32, [vp, C.POINTER(RtCamera), C.POINTER(RtPTParams), vp, vp]),
         "rtPT_getStats": (i32, [vp, C.POINTER(RtPTStats)]),
@@ -379,6 +387,57 @@ class PathTracer:
     def close(self):
         if getattr(self, "h", None):
             load().rtPT_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """rtBatch_*: many scenes built and traced together."""
+
+    def __init__(self, scenes_tris, stream=None):
+        L = load()
+        tris = [np.ascontiguousarray(t, np.float32).reshape(-1, 9) for t in scenes_tris]
+        self.tri_off = np.concatenate([[0], np.cumsum([t.shape[0] for t in tris])]).astype(np.int32)
+        allt = np.ascontiguousarray(np.concatenate(tris))
+        self.h = L.rtBatch_build(allt.ctypes.data, self.tri_off.ctypes.data, len(tris), _stream(stream))
+        if not self.h:
+            raise RtError(f"rtBatch_build failed: {last_error()}")
+        self.num_scenes = len(tris)
+
+    def info(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_float()
+        _check(load().rtBatch_getInfo(self.h, C.byref(a), C.byref(b), C.byref(c)), "rtBatch_getInfo")
+        return {"num_scenes": a.value, "num_nodes": b.value, "build_ms": c.value}
+
+    def closest(self, d_rays, d_off, n, d_hits, stream=None):
+        _check(load().rtBatch_traceClosest(self.h, _ptr(d_rays), _ptr(d_off), n, _ptr(d_hits), _stream(stream)),
+               "rtBatch_traceClosest")
+
+    def any(self, d_rays, d_off, n, d_occ, stream=None):
+        _check(load().rtBatch_traceAny(self.h, _ptr(d_rays), _ptr(d_off), n, _ptr(d_occ), _stream(stream)),
+               "rtBatch_traceAny")
+
+    def graph(self, d_rays, d_off, n, d_out, any_hit=False, stream=None):
+        _check(load().rtBatch_traceGraph(self.h, _ptr(d_rays), _ptr(d_off), n, _ptr(d_out), int(any_hit),
+                                         _stream(stream)), "rtBatch_traceGraph")
+
+    def autotune(self, d_rays, d_off, n, d_hits, stream=None):
+        c, it = C.c_int(), C.c_int()
+        _check(load().rtBatch_autotune(self.h, _ptr(d_rays), _ptr(d_off), n, _ptr(d_hits), _stream(stream),
+                                       C.byref(c), C.byref(it)), "rtBatch_autotune")
+        return c.value, it.value
+
+    def set_tuning(self, ctas, iters):
+        _check(load().rtBatch_setTuning(self.h, ctas, iters), "rtBatch_setTuning")
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().rtBatch_destroy(self.h)
             self.h = None
 
     def __del__(self):

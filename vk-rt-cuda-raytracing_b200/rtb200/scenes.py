@@ -19,7 +19,10 @@ Workloads (sizes as stated for them):
 """
 from __future__ import annotations
 
+import concurrent.futures
+import functools
 import math
+import os
 
 import numpy as np
 
@@ -36,47 +39,59 @@ F32 = np.float32
 
 # ------------------------------------------------------------------ meshes --
 def uv_sphere(segs: int, rings: int) -> np.ndarray:
-    """Unit UV sphere: 2*segs*(rings-1) triangles (caps are fans)."""
+    """Unit UV sphere: 2*segs*(rings-1) triangles (caps are fans).  Quad
+    (r, s) spans rings r..r+1 and segments s..s+1 and gives triangles
+    (a, b, c) except on the top ring and (a, c, d) except on the bottom."""
     th = np.linspace(0.0, math.pi, rings + 1)
     ph = np.linspace(0.0, 2.0 * math.pi, segs + 1)
     T, P = np.meshgrid(th, ph, indexing="ij")
     V = np.stack([np.sin(T) * np.cos(P), np.cos(T), np.sin(T) * np.sin(P)], axis=-1)
-    tris = []
-    for r in range(rings):
-        for s in range(segs):
-            a, b, c, d = V[r, s], V[r, s + 1], V[r + 1, s + 1], V[r + 1, s]
-            if r != 0:
-                tris.append((a, b, c))
-            if r != rings - 1:
-                tris.append((a, c, d))
-    return np.asarray(tris, dtype=np.float64)
+    a, b, c, d = V[:-1, :-1], V[:-1, 1:], V[1:, 1:], V[1:, :-1]
+    t = np.empty((rings, segs, 2, 3, 3))
+    t[:, :, 0] = np.stack([a, b, c], axis=2)
+    t[:, :, 1] = np.stack([a, c, d], axis=2)
+    keep = np.ones((rings, segs, 2), bool)
+    keep[0, :, 0] = False
+    keep[rings - 1, :, 1] = False
+    return t[keep].reshape(-1, 3, 3)
 
 
 def box_mesh(m: int) -> np.ndarray:
-    """Unit cube [-1,1]^3, each face an m x m grid of quads: 12*m*m triangles."""
+    """Unit cube [-1,1]^3, each face an m x m grid of quads: 12*m*m triangles,
+    faces in (axis, sign) order, quads (i, j) row-major, two triangles per
+    quad, winding reversed on the negative faces."""
     g = np.linspace(-1.0, 1.0, m + 1)
-    tris = []
+    i, j = np.meshgrid(np.arange(m), np.arange(m), indexing="ij")
+    corners = [(i, j), (i + 1, j), (i + 1, j + 1), (i, j + 1)]
+    out = []
     for axis in range(3):
         for sign in (-1.0, 1.0):
-            for i in range(m):
-                for j in range(m):
-                    quad = []
-                    for (a, b) in ((i, j), (i + 1, j), (i + 1, j + 1), (i, j + 1)):
-                        p = [0.0, 0.0, 0.0]
-                        p[axis] = sign
-                        p[(axis + 1) % 3] = g[a]
-                        p[(axis + 2) % 3] = g[b]
-                        quad.append(p)
-                    q = np.asarray(quad)
-                    if sign < 0:
-                        q = q[::-1]
-                    tris.append((q[0], q[1], q[2]))
-                    tris.append((q[0], q[2], q[3]))
-    return np.asarray(tris, dtype=np.float64)
+            q = np.zeros((m, m, 4, 3))
+            for k, (ca, cb) in enumerate(corners):
+                q[:, :, k, axis] = sign
+                q[:, :, k, (axis + 1) % 3] = g[ca]
+                q[:, :, k, (axis + 2) % 3] = g[cb]
+            if sign < 0:
+                q = q[:, :, ::-1]
+            t = np.stack([q[:, :, [0, 1, 2]], q[:, :, [0, 2, 3]]], axis=2)
+            out.append(t.reshape(-1, 3, 3))
+    return np.concatenate(out)
+
+
+@functools.lru_cache(maxsize=None)
+def _template(kind: int, ntris: int) -> np.ndarray:
+    t = _mesh_of_size(kind, ntris)
+    t.setflags(write=False)
+    return t
 
 
 def mesh_of_size(kind: int, ntris: int) -> np.ndarray:
-    """Sphere (kind 0) or box (kind 1) template with about `ntris` triangles."""
+    """Sphere (kind 0) or box (kind 1) template with about `ntris` triangles
+    (templates are cached; the result is read-only)."""
+    return _template(kind, ntris)
+
+
+def _mesh_of_size(kind: int, ntris: int) -> np.ndarray:
     if kind == 0:
         segs = max(3, int(round(math.sqrt(ntris))))
         rings = max(2, int(round(ntris / (2 * segs))) + 1)
@@ -141,14 +156,18 @@ def scene_meshes(seed: int, ntris: int, box: float = 100.0, lo: int = 1000, hi: 
         total = 2
     i = 0
     scale = box / 100.0
+    cap = 0
     while total < ntris:
-        u = uniforms(seed, S_MESH, i + 1, 8)[i]
+        if i >= cap:  # item i of a Philox stream does not depend on how many are drawn
+            cap = max(64, 2 * cap)
+            um, up = uniforms(seed, S_MESH, cap, 8), uniforms(seed, S_PLACE, cap, 4)
+        u = um[i]
         k = int(u[0] < 0.5)
         want = int(round(log_uniform(float(u[1]), lo, hi)))
         m = mesh_of_size(k, want)
         R = rotations(u[None, 2:5])[0]
         c = (u[5:8].astype(np.float64) - 0.5) * box
-        r = log_uniform(float(uniforms(seed, S_PLACE, i + 1, 4)[i, 0]), 2.0, 10.0) * scale
+        r = log_uniform(float(up[i, 0]), 2.0, 10.0) * scale
         m = _place(m, R, r, c)
         if total + m.shape[0] > ntris:
             m = m[: ntris - total]
@@ -296,7 +315,7 @@ def random_rays(seed: int, count: int, box: float = 100.0) -> np.ndarray:
 # ------------------------------------------------------- instanced scenes --
 def instanced_scene(seed: int, total_tris: int, nblas: int = 16, ninst: int = 64, world: float = 100.0,
                     emissive_frac: float = 0.05):
-    """configs[2] scene: `nblas` BLASes (clusters of sphere/box meshes in a
+    """Instanced path-tracing scene: `nblas` BLASes (clusters of sphere/box meshes in a
     local 12^3 box over a 36 x 36 two-triangle floor) totalling `total_tris` triangles, `ninst` instances with
     random rotation, log-uniform scale [1.5, 5] and uniform translation in
     the world box, Lambertian albedo U[0.1, 0.9] per instance and emission
@@ -329,3 +348,62 @@ def instanced_scene(seed: int, total_tris: int, nblas: int = 16, ninst: int = 64
 
 PT_CAM_EYE = (0.0, 20.0, -120.0)
 PT_CAM_TARGET = (0.0, 0.0, 0.0)
+
+
+# ---------------------------------------------------------- batched scenes --
+def batched_workload(nscenes: int = 256, tri_lo: int = 1000, tri_hi: int = 500_000, ray_lo: int = 4096,
+                     ray_hi: int = 2_000_000, seed: int = 7):
+    """Batched workload of 256 scenes: scene i = scene_meshes(seed=i, n_i) with
+    n_i log-uniform in [tri_lo, tri_hi]; its ray batch has r_i log-uniform in
+    [ray_lo, ray_hi] rays, half primary and half diffuse (scene_rays).
+    Returns (list of (n_i, 9) float32, rays concatenated, ray offsets)."""
+    u = uniforms(seed, S_BATCH, nscenes, 4).astype(np.float64)
+    ntris = np.round(log_uniform(u[:, 0], tri_lo, tri_hi)).astype(int)
+    nrays = np.round(log_uniform(u[:, 1], ray_lo, ray_hi)).astype(int)
+    def one(i):
+        t = scene_meshes(i, int(ntris[i]))
+        return t, scene_rays(t, int(nrays[i]), seed=i)
+
+    with concurrent.futures.ThreadPoolExecutor(min(16, os.cpu_count() or 1)) as ex:
+        res = list(ex.map(one, range(nscenes)))
+    tris, rays = [r[0] for r in res], [r[1] for r in res]
+    off = np.concatenate([[0], np.cumsum([r.shape[0] for r in rays])]).astype(np.int32)
+    return tris, np.concatenate(rays), off
+
+
+def scene_rays(tris: np.ndarray, n: int, seed: int) -> np.ndarray:
+    """n rays for one scene: n//2 coherent primary rays (row-major pixels of
+    a 16:9 pinhole camera in front of the scene's bounds) then n - n//2
+    diffuse rays (uniform point on a uniformly chosen triangle, cosine-
+    weighted about its face normal by the polar disk map).  Drawn with
+    numpy's PCG64 seeded by (seed, 3): cheap enough for tens of millions."""
+    v = tris.reshape(-1, 3, 3)
+    flat = v.reshape(-1, 3)
+    lo, hi = flat.min(0).astype(np.float64), flat.max(0).astype(np.float64)
+    c, ext = (lo + hi) / 2, float(np.linalg.norm(hi - lo))
+    npri = n // 2
+    w = max(16, int(math.ceil(math.sqrt(npri * 16 / 9))))
+    h = max(9, int(math.ceil(npri / w)))
+    pri = pinhole_rays(w, h, c + np.array([0.0, 0.3, -1.2]) * ext, c, 50.0)[:npri]
+    nd = n - npri
+    rng = np.random.default_rng([seed, 3])
+    k = rng.integers(0, v.shape[0], nd)
+    u = rng.random((nd, 4), dtype=np.float32)
+    su = np.sqrt(u[:, 0])
+    w0, w1 = 1 - su, su * (1 - u[:, 1])
+    w2 = su * u[:, 1]
+    a, b, cc = v[k, 0], v[k, 1], v[k, 2]
+    p = w0[:, None] * a + w1[:, None] * b + w2[:, None] * cc
+    nrm = np.cross(b - a, cc - a)
+    nrm /= np.maximum(np.linalg.norm(nrm, axis=1, keepdims=True), F32(1e-30))
+    t, bt = _onb(nrm)
+    r, ph = np.sqrt(u[:, 2]), F32(2 * math.pi) * u[:, 3]
+    x, y, z = r * np.cos(ph), r * np.sin(ph), np.sqrt(np.maximum(F32(0), 1 - u[:, 2]))
+    d = x[:, None] * t + y[:, None] * bt + z[:, None] * nrm
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    dif = np.zeros(nd, dtype=RAY_DTYPE)
+    dif["org"] = p + F32(1e-3) * ext * nrm
+    dif["dir"] = d
+    dif["tmin"] = 0.0
+    dif["tmax"] = 1e30
+    return np.concatenate([pri, dif])
