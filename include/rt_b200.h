@@ -226,6 +226,62 @@ void rtPT_destroy(RtPathTracer_t pt);
  * up[3], tan(vfov/2), aspect (14 floats). */
 int rtPT_cameraBasis(const RtCamera* cam, int width, int height, float* out14);
 
+/* ---- Served form: a request loop over scenes resident in HBM ------------
+ * No counterpart in the reference (its layer calls one synchronous trace per
+ * ray batch, layer/cuda_bvh_backend.cu:526-598).  Scenes are copied into one
+ * device arena; clients submit requests from any thread; a scheduler thread
+ * admits host-buffer requests by footprint (rays + results) under the HBM
+ * budget, packs the rays of admitted requests (oldest first, in chunks) into
+ * shared wavefronts traced by one persistent launch per hit kind, keeps up
+ * to max_waves wavefronts in flight, and copies each chunk's results back
+ * as soon as it is traced.  A request's results are bit-identical to
+ * cudaBVH_traceClosest / cudaBVH_traceAny of the same rays on the scene's
+ * BVH, whatever else is in flight.  Host buffers should be pinned (page-
+ * locked) for the copies to overlap; they must stay valid until the request
+ * is waited for.  Every ticket must be waited for once (that frees it). */
+typedef struct RtServerHandle* RtServer_t;
+typedef struct {
+    uint64_t hbm_budget_bytes; /* resident scenes + admitted request buffers; 0 = 120 GiB */
+    uint64_t pool_bytes;       /* device staging pool for host-buffer requests; 0 = 4 GiB */
+    int max_inflight;          /* requests admitted at once; 0 = 256 */
+    int wave_rays;             /* rays per shared wavefront; 0 = 4 Mi */
+    int chunk_rays;            /* rays per chunk of a request; 0 = 1 Mi */
+    int max_waves;             /* wavefronts in flight, each on its own stream (1..8); 0 = 2 */
+} RtServerConfig;
+typedef struct {
+    double submit_us, admit_us, done_us; /* steady clock, microseconds since rtServer_create */
+    int status;                          /* RT_OK, RT_ERR_STACK or RT_ERR_CUDA */
+    int waves;                           /* wavefronts the request's chunks were traced in */
+} RtRequestInfo;
+typedef struct {
+    uint64_t requests_done, rays_done, waves;
+    uint64_t resident_bytes, pool_bytes, peak_pool_used;
+    int num_scenes;
+} RtServerStats;
+
+/* cfg may be NULL (all defaults).  The server runs on the current device. */
+RtServer_t rtServer_create(const RtServerConfig* cfg);
+/* Copies the BVH into the resident arena (the handle may be destroyed
+ * afterwards).  Returns the scene id (>= 0) or RT_ERR_CAPACITY when the
+ * budget would be exceeded, another error code otherwise.  Waits until no
+ * wavefront is in flight. */
+int rtServer_addScene(RtServer_t s, CudaBVH_t bvh);
+/* Host-buffer request: n rays in h_rays, results (RtHit, or one byte per ray
+ * for any_hit) to h_out.  RT_ERR_CAPACITY if the request can never fit the
+ * staging pool.  *ticket identifies it for rtServer_wait. */
+int rtServer_submit(RtServer_t s, int scene, int any_hit, const RtRay* h_rays, int n, void* h_out,
+                    uint64_t* ticket);
+/* Device-buffer request (no staging, no footprint): rays and results stay in
+ * the caller's device memory. */
+int rtServer_submitDevice(RtServer_t s, int scene, int any_hit, const RtRay* d_rays, int n, void* d_out,
+                          uint64_t* ticket);
+/* Waits up to timeout_ms (< 0: no limit) for a request; RT_ERR_TIMEOUT if it
+ * is not done (the ticket stays valid), else its status; info optional. */
+int rtServer_wait(RtServer_t s, uint64_t ticket, int timeout_ms, RtRequestInfo* info);
+int rtServer_getStats(RtServer_t s, RtServerStats* st);
+/* Finishes every submitted request, then frees the server. */
+void rtServer_destroy(RtServer_t s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,4 +25,19 @@ int launch_trace_multi(const Bvh8Device& b, const RtRay* rays, int n, const int*
                        int nscenes, RtHit* hits, uint8_t* occ, int* work, int* status, int ctas_per_sm,
                        int node_iters, cudaStream_t s);
 
+// A shared-wavefront segment: rays [first, next.first) of the launch are
+// rays[0 ..] of this segment, traced from arena node `root`, results to out.
+struct alignas(16) WaveSeg {
+    const RtRay* rays;
+    void* out;
+    uint32_t first;
+    uint32_t root;
+    uint32_t pad[2];
+};
+enum { MODE_SINGLE = 0, MODE_BATCH = 1, MODE_WAVE = 2 };
+int launch_trace_wave(const uint4* nodes, const float4* tris, const WaveSeg* segs, int nseg, int n, bool any,
+                      int* work, int* status, int ctas_per_sm, cudaStream_t s);
+void launch_rebase_nodes(const void* src, void* dst, int count, uint32_t node_off, uint32_t tri_off,
+                         cudaStream_t s);
+
 }  // namespace rtb

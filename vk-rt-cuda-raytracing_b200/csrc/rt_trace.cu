@@ -32,19 +32,29 @@
 #include <cfloat>
 
 #include "rt_internal.h"
+#include "rt_legacy.h"
 #include "rt_trace.cuh"
 
 namespace rtb {
 
-// MULTI: the structure holds several scenes (roots 0 .. nscenes-1); ray i
-// belongs to the scene s with ray_off[s] <= i < ray_off[s+1], starts at root
-// s, and reports primitives relative to tri_off[s].
-template <bool ANY, bool COUNT, bool MULTI, int NITERS>
+__device__ __forceinline__ void* ldg_ptr(const void* p) {
+    return reinterpret_cast<void*>(__ldg(reinterpret_cast<const unsigned long long*>(p)));
+}
+
+// MODE_SINGLE: one scene, root 0, ray i -> rays[i], result i.
+// MODE_BATCH: the structure holds several scenes (roots 0 .. nscenes-1); ray
+//   i belongs to the scene s with ray_off[s] <= i < ray_off[s+1], starts at
+//   root s, and reports primitives relative to tri_off[s].
+// MODE_WAVE: a shared wavefront of `nscenes` segments (chunks of requests
+//   against scenes resident in one arena); ray i belongs to the last segment
+//   g with segs[g].first <= i, is read from segs[g].rays[i - first], starts
+//   at node segs[g].root and is written to segs[g].out[i - first].
+template <bool ANY, bool COUNT, int MODE, int NITERS>
 __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
     k_trace_blas(const uint4* __restrict__ nodes, const float4* __restrict__ tris, const RtRay* __restrict__ rays,
                  int n, RtHit* __restrict__ hits, uint8_t* __restrict__ occ, uint32_t* __restrict__ counts,
                  int* __restrict__ work, int* __restrict__ status, const int* __restrict__ ray_off,
-                 const int* __restrict__ tri_off, int nscenes) {
+                 const int* __restrict__ tri_off, int nscenes, const WaveSeg* __restrict__ segs) {
     __shared__ uint2 sstack[SSTACK][TRACE_T];
     __shared__ unsigned long long s_key[TRACE_T];  // owner's best (ordered t, prim)
     __shared__ int s_rec[TRACE_T];                 // set when a worker improved it (any hit: found)
@@ -59,6 +69,7 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
     float thit = 0.f, hu = 0.f, hv = 0.f;
     int hprim = -1;
     int prim_base = 0;
+    int wseg = 0;
     uint32_t cn = 0, ct = 0;
     for (;;) {
         // ---- refill idle lanes ----
@@ -72,14 +83,8 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
             if (need) {
                 const int ri = base + __popc(want & ((1u << lane) - 1));
                 if (ri < n) {
-                    ray = ri;
-                    r = load_ray(rays, ri);
-                    thit = r.tmax;
-                    hprim = -1;
-                    hu = hv = 0.f;
-                    w.start();
                     uint32_t root = 0;
-                    if (MULTI) {
+                    if (MODE == MODE_BATCH) {
                         int lo = 0, hi = nscenes - 1;  // last scene whose first ray <= ri
                         while (lo < hi) {
                             const int mid = (lo + hi + 1) >> 1;
@@ -89,6 +94,25 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
                         root = (uint32_t)lo;
                         prim_base = __ldg(tri_off + lo);
                     }
+                    if (MODE == MODE_WAVE) {
+                        int lo = 0, hi = nscenes - 1;  // last segment whose first ray <= ri
+                        while (lo < hi) {
+                            const int mid = (lo + hi + 1) >> 1;
+                            if ((int)__ldg(&segs[mid].first) <= ri) lo = mid;
+                            else hi = mid - 1;
+                        }
+                        wseg = lo;
+                        root = __ldg(&segs[lo].root);
+                        ray = ri - (int)__ldg(&segs[lo].first);
+                        r = load_ray(reinterpret_cast<const RtRay*>(ldg_ptr(&segs[lo].rays)), ray);
+                    } else {
+                        ray = ri;
+                        r = load_ray(rays, ri);
+                    }
+                    thit = r.tmax;
+                    hprim = -1;
+                    hu = hv = 0.f;
+                    w.start();
                     w.ng = make_uint2(root, (1u << r.oct) | (1u << 8));
                     cn = ct = 0;
                 } else {
@@ -210,6 +234,10 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
                     hprim = -1;
                     found_any = false;
                 }
+                if (MODE == MODE_WAVE) {
+                    if (ANY) occ = reinterpret_cast<uint8_t*>(ldg_ptr(&segs[wseg].out));
+                    else hits = reinterpret_cast<RtHit*>(ldg_ptr(&segs[wseg].out));
+                }
                 if (ANY) {
                     occ[ray] = found_any ? 1 : 0;
                 } else {
@@ -242,22 +270,22 @@ int launch_trace_blas(const Bvh8Device& b, const RtRay* rays, int n, RtHit* hits
     constexpr int NI = RTB_NODE_ITERS;
     if (counts) {
         if (occ) {
-            static const int g = persistent_grid(k_trace_blas<true, true, false, NI>, TRACE_T);
-            k_trace_blas<true, true, false, NI><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work,
-                                                                     status, nullptr, nullptr, 1);
+            static const int g = persistent_grid(k_trace_blas<true, true, MODE_SINGLE, NI>, TRACE_T);
+            k_trace_blas<true, true, MODE_SINGLE, NI><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work,
+                                                                     status, nullptr, nullptr, 1, nullptr);
         } else {
-            static const int g = persistent_grid(k_trace_blas<false, true, false, NI>, TRACE_T);
-            k_trace_blas<false, true, false, NI><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work,
-                                                                      status, nullptr, nullptr, 1);
+            static const int g = persistent_grid(k_trace_blas<false, true, MODE_SINGLE, NI>, TRACE_T);
+            k_trace_blas<false, true, MODE_SINGLE, NI><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work,
+                                                                      status, nullptr, nullptr, 1, nullptr);
         }
     } else if (occ) {
-        static const int g = persistent_grid(k_trace_blas<true, false, false, NI>, TRACE_T);
-        k_trace_blas<true, false, false, NI><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work,
-                                                                  status, nullptr, nullptr, 1);
+        static const int g = persistent_grid(k_trace_blas<true, false, MODE_SINGLE, NI>, TRACE_T);
+        k_trace_blas<true, false, MODE_SINGLE, NI><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work,
+                                                                  status, nullptr, nullptr, 1, nullptr);
     } else {
-        static const int g = persistent_grid(k_trace_blas<false, false, false, NI>, TRACE_T);
-        k_trace_blas<false, false, false, NI><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work,
-                                                                   status, nullptr, nullptr, 1);
+        static const int g = persistent_grid(k_trace_blas<false, false, MODE_SINGLE, NI>, TRACE_T);
+        k_trace_blas<false, false, MODE_SINGLE, NI><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work,
+                                                                   status, nullptr, nullptr, 1, nullptr);
     }
     return cudaGetLastError() == cudaSuccess ? RT_OK : RT_ERR_CUDA;
 }
@@ -272,20 +300,60 @@ int launch_trace_multi(const Bvh8Device& b, const RtRay* rays, int n, const int*
     const int g = std::max(1, std::min(ctas_per_sm, TRACE_MINB)) * num_sms();
     if (occ) {
         if (node_iters == 1)
-            k_trace_blas<true, false, true, 1><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
-                                                                    status, ray_off, tri_off, nscenes);
+            k_trace_blas<true, false, MODE_BATCH, 1><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
+                                                                    status, ray_off, tri_off, nscenes, nullptr);
         else
-            k_trace_blas<true, false, true, 2><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
-                                                                    status, ray_off, tri_off, nscenes);
+            k_trace_blas<true, false, MODE_BATCH, 2><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
+                                                                    status, ray_off, tri_off, nscenes, nullptr);
     } else {
         if (node_iters == 1)
-            k_trace_blas<false, false, true, 1><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
-                                                                     status, ray_off, tri_off, nscenes);
+            k_trace_blas<false, false, MODE_BATCH, 1><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
+                                                                     status, ray_off, tri_off, nscenes, nullptr);
         else
-            k_trace_blas<false, false, true, 2><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
-                                                                     status, ray_off, tri_off, nscenes);
+            k_trace_blas<false, false, MODE_BATCH, 2><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
+                                                                     status, ray_off, tri_off, nscenes, nullptr);
     }
     return cudaGetLastError() == cudaSuccess ? RT_OK : RT_ERR_CUDA;
+}
+
+// One shared wavefront: `n` rays over `nseg` segments, all of one kind.
+int launch_trace_wave(const uint4* nodes, const float4* tris, const WaveSeg* segs, int nseg, int n, bool any,
+                      int* work, int* status, int ctas_per_sm, cudaStream_t s) {
+    const int g = std::max(1, std::min(ctas_per_sm, TRACE_MINB)) * num_sms();
+    if (any)
+        k_trace_blas<true, false, MODE_WAVE, 2><<<g, TRACE_T, 0, s>>>(nodes, tris, nullptr, n, nullptr, nullptr,
+                                                                     nullptr, work, status, nullptr, nullptr, nseg,
+                                                                     segs);
+    else
+        k_trace_blas<false, false, MODE_WAVE, 2><<<g, TRACE_T, 0, s>>>(nodes, tris, nullptr, n, nullptr, nullptr,
+                                                                      nullptr, work, status, nullptr, nullptr, nseg,
+                                                                      segs);
+    return cudaGetLastError() == cudaSuccess ? RT_OK : RT_ERR_CUDA;
+}
+
+// Copies one scene's 8-wide nodes into an arena at node offset `node_off`,
+// rebasing child and triangle bases by node_off and tri_off.
+__global__ void k_rebase_nodes(const uint4* __restrict__ src, uint4* __restrict__ dst, int count, uint32_t node_off,
+                               uint32_t tri_off) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const uint4* a = src + (size_t)i * 5;
+    uint4* b = dst + (size_t)i * 5;
+    uint4 w1 = a[1];
+    w1.x += node_off;
+    w1.y += tri_off;
+    b[0] = a[0];
+    b[1] = w1;
+    b[2] = a[2];
+    b[3] = a[3];
+    b[4] = a[4];
+}
+
+void launch_rebase_nodes(const void* src, void* dst, int count, uint32_t node_off, uint32_t tri_off,
+                         cudaStream_t s) {
+    if (count <= 0) return;
+    k_rebase_nodes<<<(count + 255) / 256, 256, 0, s>>>(reinterpret_cast<const uint4*>(src),
+                                                         reinterpret_cast<uint4*>(dst), count, node_off, tri_off);
 }
 
 }  // namespace rtb

@@ -56,6 +56,22 @@ class RtPTStats(C.Structure):
                 ("light_area", C.c_double)]
 
 
+class RtServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("pool_bytes", C.c_uint64), ("max_inflight", C.c_int),
+                ("wave_rays", C.c_int), ("chunk_rays", C.c_int), ("max_waves", C.c_int)]
+
+
+class RtRequestInfo(C.Structure):
+    _fields_ = [("submit_us", C.c_double), ("admit_us", C.c_double), ("done_us", C.c_double), ("status", C.c_int),
+                ("waves", C.c_int)]
+
+
+class RtServerStats(C.Structure):
+    _fields_ = [("requests_done", C.c_uint64), ("rays_done", C.c_uint64), ("waves", C.c_uint64),
+                ("resident_bytes", C.c_uint64), ("pool_bytes", C.c_uint64), ("peak_pool_used", C.c_uint64),
+                ("num_scenes", C.c_int)]
+
+
 def declared_symbols() -> list[str]:
     """Function names declared in include/*.h."""
     names = []
@@ -123,6 +139,13 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "rtBatch_autotune": (i32, [vp, vp, vp, i32, vp, vp, C.POINTER(i32), C.POINTER(i32)]),
         "rtBatch_setTuning": (i32, [vp, i32, i32]),
         "rtBatch_getInfo": (i32, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(f32)]),
+        "rtServer_create": (vp, [C.POINTER(RtServerConfig)]),
+        "rtServer_addScene": (i32, [vp, vp]),
+        "rtServer_submit": (i32, [vp, i32, i32, vp, i32, vp, C.POINTER(C.c_uint64)]),
+        "rtServer_submitDevice": (i32, [vp, i32, i32, vp, i32, vp, C.POINTER(C.c_uint64)]),
+        "rtServer_wait": (i32, [vp, C.c_uint64, i32, C.POINTER(RtRequestInfo)]),
+        "rtServer_getStats": (i32, [vp, C.POINTER(RtServerStats)]),
+        "rtServer_destroy": (None, [vp]),
         "rtPT_create": (vp, [vp, vp, i32, vp]),
         "rtPT_render": (i32, [vp, C.POINTER(RtCamera), C.POINTER(RtPTParams), vp, vp]),
         "rtPT_getStats": (i32, [vp, C.POINTER(RtPTStats)]),
@@ -438,6 +461,54 @@ class Batch:
     def close(self):
         if getattr(self, "h", None):
             load().rtBatch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """rtServer_*: resident scenes, requests admitted by footprint and traced
+    in shared wavefronts by the library's scheduler thread."""
+
+    def __init__(self, hbm_budget_bytes=0, pool_bytes=0, max_inflight=0, wave_rays=0, chunk_rays=0, max_waves=0):
+        cfg = RtServerConfig(hbm_budget_bytes, pool_bytes, max_inflight, wave_rays, chunk_rays, max_waves)
+        self.h = load().rtServer_create(C.byref(cfg))
+        if not self.h:
+            raise RtError(f"rtServer_create failed: {last_error()}")
+
+    def add_scene(self, bvh: "BVH") -> int:
+        rc = load().rtServer_addScene(self.h, bvh.h)
+        if rc < 0:
+            raise RtError(f"rtServer_addScene failed ({rc}): {last_error()}")
+        return rc
+
+    def submit(self, scene: int, any_hit: bool, rays_ptr: int, n: int, out_ptr: int, device: bool = False) -> int:
+        """Pointers are raw addresses (host for device=False, device otherwise)."""
+        t = C.c_uint64()
+        f = load().rtServer_submitDevice if device else load().rtServer_submit
+        _check(f(self.h, scene, int(any_hit), rays_ptr, n, out_ptr, C.byref(t)), "rtServer_submit")
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> dict:
+        info = RtRequestInfo()
+        rc = load().rtServer_wait(self.h, ticket, timeout_ms, C.byref(info))
+        if rc != 0:
+            raise RtError(f"rtServer_wait: {rc}: {last_error()}")
+        return {"submit_us": info.submit_us, "admit_us": info.admit_us, "done_us": info.done_us,
+                "status": info.status, "waves": info.waves}
+
+    def stats(self) -> dict:
+        st = RtServerStats()
+        _check(load().rtServer_getStats(self.h, C.byref(st)), "rtServer_getStats")
+        return {k: getattr(st, k) for k, _ in RtServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().rtServer_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -32,7 +32,7 @@ RAY_DTYPE = np.dtype([("org", "<f4", 3), ("tmin", "<f4"), ("dir", "<f4", 3), ("t
 HIT_DTYPE = np.dtype([("t", "<f4"), ("prim", "<i4"), ("u", "<f4"), ("v", "<f4")])
 
 # Philox stream ids (second key word) for the different draws.
-S_PLACE, S_MESH, S_DIFFUSE, S_SHADOW, S_INST, S_MAT, S_BATCH = 1, 2, 3, 4, 5, 6, 7
+S_PLACE, S_MESH, S_DIFFUSE, S_SHADOW, S_INST, S_MAT, S_BATCH, S_SERVE = 1, 2, 3, 4, 5, 6, 7, 8
 
 F32 = np.float32
 
@@ -407,3 +407,54 @@ def scene_rays(tris: np.ndarray, n: int, seed: int) -> np.ndarray:
     dif["tmin"] = 0.0
     dif["tmax"] = 1e30
     return np.concatenate([pri, dif])
+
+
+# ----------------------------------------------------------- served trace --
+def served_scenes(nscenes: int = 16, total: int = 30_000_000, lo: int = 200_000, hi: int = 5_000_000,
+                  seed: int = 11):
+    """Resident scenes of the served workload: sizes log-uniform in [lo, hi],
+    rescaled so they sum to `total` (each kept within [lo, hi]); scene i =
+    scene_meshes(seed=1000 + i, n_i), all in the same 100^3 box."""
+    u = uniforms(seed, S_SERVE, nscenes, 4)[:, 0].astype(np.float64)
+    w = log_uniform(u, lo, hi)
+    n = np.clip(np.round(w * total / w.sum()), lo, hi).astype(int)
+    n[-1] += total - n.sum()
+    n = np.clip(n, lo, hi)
+    with concurrent.futures.ThreadPoolExecutor(min(16, os.cpu_count() or 1)) as ex:
+        return list(ex.map(lambda i: scene_meshes(1000 + i, int(n[i])), range(nscenes)))
+
+
+def served_trace(nreq: int, rate: float = 2000.0, nscenes: int = 16, ray_lo: int = 1000, ray_hi: int = 8_000_000,
+                 any_frac: float = 0.3, pool: int = 8_000_000, seed: int = 12):
+    """Poisson request trace: arrival times (s, exponential gaps at `rate`),
+    scene uniform, ray count log-uniform [ray_lo, ray_hi], any hit with
+    probability any_frac, and the start of the request's window in a shared
+    ray pool of `pool` rays."""
+    u = uniforms(seed, S_SERVE + 1, nreq, 8).astype(np.float64)
+    arrival = np.cumsum(-np.log1p(-u[:, 0]) / rate)
+    arrival -= arrival[0]
+    scene = np.minimum((u[:, 1] * nscenes).astype(int), nscenes - 1)
+    n = np.round(log_uniform(u[:, 2], ray_lo, ray_hi)).astype(int)
+    any_hit = u[:, 3] < any_frac
+    start = np.floor(u[:, 4] * (pool - n + 1)).astype(int)
+    return arrival, scene, n, any_hit, start
+
+
+def served_ray_pools(n: int = 8_000_000, box: float = 100.0, seed: int = 13):
+    """Shared pools for the served workload, drawn with numpy's PCG64 seeded
+    by (seed, kind): incoherent closest-hit rays (uniform origins in the
+    box, uniform directions) and any-hit segments of the same kind with
+    length uniform in [10, 100]."""
+    def pool(kind):
+        rng = np.random.default_rng([seed, kind])
+        u = rng.random((n, 6), dtype=np.float32)
+        z = 2 * u[:, 3] - 1
+        ph = F32(2 * math.pi) * u[:, 4]
+        sr = np.sqrt(np.maximum(F32(0), 1 - z * z))
+        r = np.zeros(n, dtype=RAY_DTYPE)
+        r["org"] = (u[:, 0:3] - F32(0.5)) * F32(box)
+        r["dir"] = np.stack([sr * np.cos(ph), sr * np.sin(ph), z], 1)
+        r["tmin"] = 0.0
+        r["tmax"] = 1e30 if kind == 0 else F32(10) + F32(90) * u[:, 5]
+        return r
+    return pool(0), pool(1)
