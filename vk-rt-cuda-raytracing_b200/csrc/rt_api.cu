@@ -573,23 +573,85 @@ static int check_status(CudaBVHHandle* h) {
     return RT_OK;
 }
 
+namespace rtb {
+
+bool HostPipe::init() {
+    if (ready) return true;
+    bool ok = RT_CUDA(cudaStreamCreateWithFlags(&in, cudaStreamNonBlocking)) &&
+              RT_CUDA(cudaStreamCreateWithFlags(&comp, cudaStreamNonBlocking)) &&
+              RT_CUDA(cudaStreamCreateWithFlags(&out, cudaStreamNonBlocking)) &&
+              RT_CUDA(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+    for (int i = 0; ok && i < kMaxPieces; i++)
+        ok = RT_CUDA(cudaEventCreateWithFlags(&ev_in[i], cudaEventDisableTiming)) &&
+             RT_CUDA(cudaEventCreateWithFlags(&ev_tr[i], cudaEventDisableTiming));
+    ready = ok;
+    return ok;
+}
+
+HostPipe::~HostPipe() {
+    for (cudaStream_t s : {in, comp, out})
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    if (start) cudaEventDestroy(start);
+    for (int i = 0; i < kMaxPieces; i++) {
+        if (ev_in[i]) cudaEventDestroy(ev_in[i]);
+        if (ev_tr[i]) cudaEventDestroy(ev_tr[i]);
+    }
+}
+
+}  // namespace rtb
+
+namespace {
+
+// Host-buffer trace: the batch is cut into pieces (at least 512K rays, at
+// most HostPipe::kMaxPieces of them); piece k's copy in, trace and copy out
+// run on three streams chained by events, so the copy of piece k+1 and the
+// results of piece k-1 cross PCIe while piece k is traced.  Ordered after
+// earlier work on the legacy default stream; returns when the results are
+// in host memory.
+int trace_host(CudaBVHHandle* h, const RtRay* rays, int n, void* out, bool any) {
+    std::lock_guard<std::mutex> g(h->mu);
+    HostPipe& p = h->pipe;
+    if (!p.init()) return RT_ERR_CUDA;
+    if (!h->stage_rays.ensure(n) || (any ? !h->stage_occ.ensure(n) : !h->stage_hits.ensure(n))) return RT_ERR_NOMEM;
+    constexpr int kMinPiece = 1 << 19;
+    int piece = std::max(kMinPiece, (n + HostPipe::kMaxPieces - 1) / HostPipe::kMaxPieces);
+    piece = (piece + 31) & ~31;
+    const size_t es = any ? 1 : sizeof(RtHit);
+    char* dev_out = any ? (char*)h->stage_occ.p : (char*)h->stage_hits.p;
+    if (!RT_CUDA(cudaEventRecord(p.start, 0)) || !RT_CUDA(cudaStreamWaitEvent(p.in, p.start, 0)))
+        return RT_ERR_CUDA;
+    int k = 0;
+    for (int b = 0; b < n; b += piece, k++) {
+        const int c = std::min(piece, n - b);
+        if (!RT_CUDA(cudaMemcpyAsync(h->stage_rays.p + b, rays + b, sizeof(RtRay) * (size_t)c, cudaMemcpyHostToDevice,
+                                     p.in)) ||
+            !RT_CUDA(cudaEventRecord(p.ev_in[k], p.in)) || !RT_CUDA(cudaStreamWaitEvent(p.comp, p.ev_in[k], 0)))
+            return RT_ERR_CUDA;
+        int* work = next_counter(h->counters, h->counter_next, p.comp);
+        const int rc = launch_trace_blas(h->bvh8, h->stage_rays.p + b, c, any ? nullptr : h->stage_hits.p + b,
+                                         any ? h->stage_occ.p + b : nullptr, nullptr, work, h->status.p, p.comp);
+        if (rc != RT_OK) return RT_CUDA(cudaGetLastError()) ? rc : RT_ERR_CUDA;
+        if (!RT_CUDA(cudaEventRecord(p.ev_tr[k], p.comp)) || !RT_CUDA(cudaStreamWaitEvent(p.out, p.ev_tr[k], 0)) ||
+            !RT_CUDA(cudaMemcpyAsync((char*)out + (size_t)b * es, dev_out + (size_t)b * es, (size_t)c * es,
+                                     cudaMemcpyDeviceToHost, p.out)))
+            return RT_ERR_CUDA;
+    }
+    if (!RT_CUDA(cudaStreamSynchronize(p.out))) return RT_ERR_CUDA;
+    return check_status(h);
+}
+
+}  // namespace
+
 int cudaBVH_traceClosestHost(CudaBVH_t h, const RtRay* rays, int n, RtHit* hits) {
     if (!h || n < 0 || (n > 0 && (!rays || !hits))) {
         set_error("cudaBVH_traceClosestHost: invalid argument");
         return RT_ERR_INVALID;
     }
     if (n == 0) return RT_OK;
-    std::lock_guard<std::mutex> g(h->mu);
-    if (!h->stage_rays.ensure(n) || !h->stage_hits.ensure(n)) return RT_ERR_NOMEM;
-    if (!RT_CUDA(cudaMemcpyAsync(h->stage_rays.p, rays, sizeof(RtRay) * (size_t)n, cudaMemcpyHostToDevice, 0)))
-        return RT_ERR_CUDA;
-    int* work = next_counter(h->counters, h->counter_next, 0);
-    int rc = launch_trace_blas(h->bvh8, h->stage_rays.p, n, h->stage_hits.p, nullptr, nullptr, work, h->status.p, 0);
-    if (rc != RT_OK) return RT_CUDA(cudaGetLastError()) ? rc : RT_ERR_CUDA;
-    if (!RT_CUDA(cudaMemcpyAsync(hits, h->stage_hits.p, sizeof(RtHit) * (size_t)n, cudaMemcpyDeviceToHost, 0)) ||
-        !RT_CUDA(cudaStreamSynchronize(0)))
-        return RT_ERR_CUDA;
-    return check_status(h);
+    return trace_host(h, rays, n, hits, false);
 }
 
 int cudaBVH_traceAnyHost(CudaBVH_t h, const RtRay* rays, int n, uint8_t* occ) {
@@ -598,17 +660,7 @@ int cudaBVH_traceAnyHost(CudaBVH_t h, const RtRay* rays, int n, uint8_t* occ) {
         return RT_ERR_INVALID;
     }
     if (n == 0) return RT_OK;
-    std::lock_guard<std::mutex> g(h->mu);
-    if (!h->stage_rays.ensure(n) || !h->stage_occ.ensure(n)) return RT_ERR_NOMEM;
-    if (!RT_CUDA(cudaMemcpyAsync(h->stage_rays.p, rays, sizeof(RtRay) * (size_t)n, cudaMemcpyHostToDevice, 0)))
-        return RT_ERR_CUDA;
-    int* work = next_counter(h->counters, h->counter_next, 0);
-    int rc = launch_trace_blas(h->bvh8, h->stage_rays.p, n, nullptr, h->stage_occ.p, nullptr, work, h->status.p, 0);
-    if (rc != RT_OK) return RT_CUDA(cudaGetLastError()) ? rc : RT_ERR_CUDA;
-    if (!RT_CUDA(cudaMemcpyAsync(occ, h->stage_occ.p, (size_t)n, cudaMemcpyDeviceToHost, 0)) ||
-        !RT_CUDA(cudaStreamSynchronize(0)))
-        return RT_ERR_CUDA;
-    return check_status(h);
+    return trace_host(h, rays, n, occ, true);
 }
 
 int cudaBVH_getBuildStats(CudaBVH_t h, RtBuildStats* out) {

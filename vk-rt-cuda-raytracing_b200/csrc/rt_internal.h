@@ -107,6 +107,19 @@ float bvh2_sah_cost(const Bvh2Device& b2, cudaStream_t s);
 
 }  // namespace rtb
 
+namespace rtb {
+// Copy-in / trace / copy-out pipeline of the host-buffer entry points: one
+// non-blocking stream per stage and an event per piece and stage.
+struct HostPipe {
+    static constexpr int kMaxPieces = 16;
+    cudaStream_t in = nullptr, comp = nullptr, out = nullptr;
+    cudaEvent_t start = nullptr, ev_in[kMaxPieces] = {}, ev_tr[kMaxPieces] = {};
+    bool ready = false;
+    bool init();
+    ~HostPipe();
+};
+}  // namespace rtb
+
 // ---- the handle behind CudaBVH_t ----
 struct CudaBVHHandle {
     int num_tris = 0;
@@ -131,6 +144,7 @@ struct CudaBVHHandle {
     rtb::DevBuf<uint8_t> stage_occ;
     rtb::DevBuf<float> stage_f;
     rtb::DevBuf<int> status;      // device status word (overflow / errors)
+    rtb::HostPipe pipe;           // host-buffer entry points
 };
 
 struct CudaTLASHandle {
