@@ -154,34 +154,73 @@ def time_steps(torch, fn, steps, warmup, flush):
     return [e0.elapsed_time(e1) for e0, e1 in evs]
 
 
-def reference_gpu_kernel(tris, d_rays, n, torch, steps, flush):
-    """The reference's traceBVH4Diffuse (cuda_rt_v40.cu:505) rebuilt for
-    sm_100a, on its own CPU-built BVH4 of the same scene, same rays."""
+def morton_order(rays):
+    """Ray order of the reference's regrouping step (cuda_rt_v40.cu:94-124,
+    1226-1239): 10-bit-per-axis Morton code of the origin normalised to the
+    scene cube, stable sort."""
+    o = rays["org"].astype(np.float64)
+    lo, size = o.min(), max(o.max() - o.min(), 1e-30)
+    q = np.clip(((o - lo) / size * 1024.0).astype(np.int64), 0, 1023).astype(np.uint64)
+
+    def spread(v):
+        v = (v | (v << np.uint64(16))) & np.uint64(0x030000FF)
+        v = (v | (v << np.uint64(8))) & np.uint64(0x0300F00F)
+        v = (v | (v << np.uint64(4))) & np.uint64(0x030C30C3)
+        return (v | (v << np.uint64(2))) & np.uint64(0x09249249)
+
+    key = (spread(q[:, 0]) << np.uint64(2)) | (spread(q[:, 1]) << np.uint64(1)) | spread(q[:, 2])
+    return np.argsort(key, kind="stable")
+
+
+def reference_gpu_kernel(tris, rays, d_rays, n, torch, steps, flush):
+    """The reference's closest-hit kernels rebuilt for sm_100a on its own
+    CPU-built structures of the same scene: traceBVH4Diffuse
+    (cuda_rt_v40.cu:505, fp16 BVH4) and traceCWBVH (cuda_rt_v40.cu:142,
+    8-wide compressed BVH, Woop triangles), each at leaf 3 and 4, three
+    launch shapes, on the rays as given and regrouped in Morton order as the
+    reference's own benchmark does (sort not timed).  The bar is the
+    fastest."""
     import ctypes as C
     path = ROOT / "oracle" / "_ref" / "libref_v40.so"
     if not path.exists():
         return {"unavailable": "oracle/_ref/libref_v40.so not built"}
     R = C.CDLL(str(path))
+    if not hasattr(R, "refv40_abi") or R.refv40_abi() != 2:
+        return {"unavailable": "oracle/_ref/libref_v40.so is stale (harness ABI 2 expected); rebuild: make -C oracle ref"}
     R.refv40_build.restype = C.c_void_p
     R.refv40_build.argtypes = [C.c_void_p, C.c_int, C.c_int]
     R.refv40_trace_bvh4.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
+    R.refv40_build_cwbvh.argtypes = [C.c_void_p]
+    R.refv40_trace_cwbvh.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
     R.refv40_destroy.argtypes = [C.c_void_p]
-    best = None
-    out = {"kernel": "traceBVH4Diffuse (cuda_rt_v40.cu:505), rebuilt sm_100a, -O3 --use_fast_math"}
+    order = morton_order(rays)
+    d_sorted = torch.from_numpy(np.ascontiguousarray(rays[order]).view(np.uint8)).cuda()
     d_h = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
     st = torch.cuda.current_stream().cuda_stream
+    out = {"flags": "-O3 --use_fast_math (reference Makefile)", "variants": {}}
+    best = None
     for leaf in (3, 4):
         t0 = time.time()
         h = R.refv40_build(tris.ctypes.data, tris.shape[0], leaf)
         out[f"cpu_build_s_leaf{leaf}"] = round(time.time() - t0, 2)
-        for blocks, thr in ((640, 256), (960, 256), (1280, 128)):
-            ms = time_steps(torch, lambda: R.refv40_trace_bvh4(h, d_rays.data_ptr(), d_h.data_ptr(), n, blocks, thr,
-                                                                st), steps, 2, flush)
-            v = n / (sum(ms) / len(ms)) / 1e3
-            if best is None or v > best[0]:
-                best = (v, leaf, blocks, thr)
+        R.refv40_build_cwbvh(h)
+        for ray_kind, dr in (("as_given", d_rays), ("morton", d_sorted)):
+            launches = [("traceBVH4Diffuse", f"{b}x{t}",
+                         lambda b=b, t=t: R.refv40_trace_bvh4(h, dr.data_ptr(), d_h.data_ptr(), n, b, t, st))
+                        for b, t in ((640, 256), (960, 256), (1280, 128))]
+            launches += [("traceCWBVH", f"({gx},{gy})x64",
+                          lambda gx=gx, gy=gy: R.refv40_trace_cwbvh(h, dr.data_ptr(), d_h.data_ptr(), n, gx, gy, st))
+                         for gx, gy in ((32, 32), (74, 32), (148, 32))]
+            for kern, shape, fn in launches:
+                ms = time_steps(torch, fn, steps, 2, flush)
+                v = n / (sum(ms) / len(ms)) / 1e3
+                hitfrac = float((d_h.view(torch.int32).view(-1, 4)[:, 1] != -1).float().mean().item())
+                name = f"{kern} leaf{leaf} {ray_kind} {shape}"
+                out["variants"][name] = {"mrays_s": round(v, 1), "hit_fraction": round(hitfrac, 4)}
+                if best is None or v > best[0]:
+                    best = (v, name)
         R.refv40_destroy(h)
-    out.update({"value": round(best[0], 1), "unit": UNIT, "leaf": best[1], "grid": f"{best[2]}x{best[3]}"})
+    out.update({"value": round(best[0], 1), "unit": UNIT, "kernel": best[1]})
     return out
 
 
@@ -359,7 +398,8 @@ def run_ours(args):
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.no_baselines:
-        out["reference_gpu_kernel"] = reference_gpu_kernel(tris, d_dif, N_RAYS, torch, max(3, args.steps // 2), flush)
+        out["reference_gpu_kernel"] = reference_gpu_kernel(tris, dif, d_dif, N_RAYS, torch, max(3, args.steps // 2),
+                                                           flush)
         if "value" in out["reference_gpu_kernel"]:
             out["speedup_vs_reference_gpu_kernel"] = round(value / ws / out["reference_gpu_kernel"]["value"], 3)
         out["cpu_baseline"] = cpu_baseline(tris, dif)
@@ -529,13 +569,16 @@ def run_batched(args):
 def run_served(args):
     """Served form: 16 resident scenes (30M triangles, 200K-5M each), a
     Poisson trace of 256 requests at 2,000 requests/s (scene uniform, rays
-    log-uniform 1K-8M, 70% closest / 30% any hit) with pinned host buffers.
+    log-uniform 1K-8M, 70% closest / 30% any hit), replayed twice per arm:
+    with pinned host buffers (rays in, results out across PCIe) and with
+    device buffers (rays produced and results consumed on the GPU).
     Served: every request submitted to one rtServer at its arrival time
     (admission under a 120 GB HBM budget, shared wavefronts).  Plain: the
     same trace through the per-call C-ABI (cudaBVH_traceClosestHost /
-    cudaBVH_traceAnyHost), one call at a time in arrival order.  Latency =
-    results back in host memory - scheduled arrival; aggregate = all rays /
-    (last completion - first arrival)."""
+    cudaBVH_traceAnyHost, or cudaBVH_traceClosest / cudaBVH_traceAny and a
+    synchronize), one call at a time in arrival order.  Latency = results
+    ready - scheduled arrival; aggregate = all rays / (last completion -
+    first arrival)."""
     import threading
     import zlib
     import torch
@@ -553,98 +596,130 @@ def run_served(args):
     bvhs = [lib.BVH(t) for t in tris]
     torch.cuda.synchronize()
     log(f"16 BVH builds: {time.time() - t0:.2f}s")
-    h_c = torch.empty(pool_c.nbytes, dtype=torch.uint8, pin_memory=True)
-    h_a = torch.empty(pool_a.nbytes, dtype=torch.uint8, pin_memory=True)
-    h_c.numpy()[:] = pool_c.view(np.uint8)
-    h_a.numpy()[:] = pool_a.view(np.uint8)
     esz = np.where(anyh, 1, 16)
-    out_off = np.concatenate([[0], np.cumsum(nray * esz)]).astype(np.int64)
-    h_out = torch.empty(int(out_off[-1]), dtype=torch.uint8, pin_memory=True)
-    base_out = h_out.data_ptr()
-
-    def rays_ptr(i):
-        return (h_a if anyh[i] else h_c).data_ptr() + int(start[i]) * 32
-
-    def crcs():
-        o = h_out.numpy()
-        return [zlib.crc32(o[out_off[i]:out_off[i + 1]]) for i in range(NREQ)]
-
-    # ---- served arm
+    # each request's result slot starts on a 16-byte boundary (hit records
+    # are written as 16-byte vectors by the device paths)
+    out_off = np.concatenate([[0], np.cumsum((nray * esz + 15) // 16 * 16)]).astype(np.int64)
+    total = int(nray.sum())
+    L = lib.load()
+    bufs = {}
+    for mode in ("host", "device"):
+        if mode == "host":
+            ic = torch.empty(pool_c.nbytes, dtype=torch.uint8, pin_memory=True)
+            ia = torch.empty(pool_a.nbytes, dtype=torch.uint8, pin_memory=True)
+            ic.numpy()[:] = pool_c.view(np.uint8)
+            ia.numpy()[:] = pool_a.view(np.uint8)
+            out = torch.empty(int(out_off[-1]), dtype=torch.uint8, pin_memory=True)
+        else:
+            ic, ia = bufs["host"][0].cuda(), bufs["host"][1].cuda()
+            out = torch.empty(int(out_off[-1]), dtype=torch.uint8, device="cuda")
+        bufs[mode] = (ic, ia, out)
     srv = lib.Server(hbm_budget_bytes=120 << 30, pool_bytes=16 << 30)
     for b in bvhs:
         srv.add_scene(b)
-    for i in range(4):  # warm-up: largest requests of each kind
-        k = int(np.argmax(nray * (anyh == bool(i & 1))))
-        srv.wait(srv.submit(int(scene[k]), bool(anyh[k]), rays_ptr(k), int(nray[k]), base_out + int(out_off[k])))
-    tickets, lag = [0] * NREQ, np.zeros(NREQ)
+    res = {}
+    for mode in ("host", "device"):
+        ic, ia, outb = bufs[mode]
+        dev = mode == "device"
+        base_out = outb.data_ptr()
 
-    def submitter():
+        def rays_ptr(i):
+            return (ia if anyh[i] else ic).data_ptr() + int(start[i]) * 32
+
+        def out_ptr(i):
+            return base_out + int(out_off[i])
+
+        def crcs():
+            o = outb.cpu().numpy() if dev else outb.numpy()
+            return [zlib.crc32(o[out_off[i]:out_off[i] + nray[i] * esz[i]]) for i in range(NREQ)]
+
+        # ---- served arm
+        for i in range(4):  # warm-up: largest requests of each kind
+            k = int(np.argmax(nray * (anyh == bool(i & 1))))
+            srv.wait(srv.submit(int(scene[k]), bool(anyh[k]), rays_ptr(k), int(nray[k]), out_ptr(k), device=dev))
+        w0 = srv.stats()["waves"]
+        tickets, lag = [0] * NREQ, np.zeros(NREQ)
+
+        def submitter():
+            T0 = time.perf_counter()
+            for i in range(NREQ):
+                ta = T0 + arrival[i]
+                while time.perf_counter() < ta:
+                    pass
+                tickets[i] = srv.submit(int(scene[i]), bool(anyh[i]), rays_ptr(i), int(nray[i]), out_ptr(i),
+                                        device=dev)
+                lag[i] = time.perf_counter() - ta
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        infos = [srv.wait(t, timeout_ms=600_000) for t in tickets]
+        st = srv.stats()
+        lat_s = np.array([(f["done_us"] - f["submit_us"]) / 1e3 for f in infos]) + lag * 1e3
+        first = infos[0]["submit_us"] - lag[0] * 1e6
+        span_s = (max(f["done_us"] for f in infos) - first) / 1e3
+        crc_srv = crcs()
+        # ---- plain arm: the per-call path, one call at a time
+        if dev:
+            fc, fa = L.cudaBVH_traceClosest, L.cudaBVH_traceAny
+        else:
+            fc, fa = L.cudaBVH_traceClosestHost, L.cudaBVH_traceAnyHost
+
+        def call(i):
+            f = fa if anyh[i] else fc
+            args_ = (bvhs[scene[i]].h, rays_ptr(i), int(nray[i]), out_ptr(i)) + ((None,) if dev else ())
+            rc = f(*args_)
+            if dev:
+                torch.cuda.synchronize()
+            if rc != 0:
+                raise RuntimeError(lib.last_error())
+
+        for sc in range(len(bvhs)):  # warm-up: each scene's staging sized by its largest request
+            for kind in (False, True):
+                m = np.nonzero((scene == sc) & (anyh == kind))[0]
+                if m.size:
+                    call(int(m[np.argmax(nray[m])]))
+        outb.zero_()
+        torch.cuda.synchronize()
+        lat_p = np.zeros(NREQ)
         T0 = time.perf_counter()
         for i in range(NREQ):
             ta = T0 + arrival[i]
             while time.perf_counter() < ta:
                 pass
-            tickets[i] = srv.submit(int(scene[i]), bool(anyh[i]), rays_ptr(i), int(nray[i]),
-                                    base_out + int(out_off[i]))
-            lag[i] = time.perf_counter() - ta
-
-    th = threading.Thread(target=submitter)
-    th.start()
-    th.join()
-    infos = [srv.wait(t, timeout_ms=600_000) for t in tickets]
-    st = srv.stats()
+            call(i)
+            lat_p[i] = (time.perf_counter() - ta) * 1e3
+        span_p = (time.perf_counter() - T0) * 1e3
+        same = crcs() == crc_srv
+        srv_m, pl_m = total / span_s / 1e3, total / span_p / 1e3
+        pc = lambda a, q: round(float(np.percentile(a, q)), 3)
+        res[mode] = {
+            "served": {"p50_ms": pc(lat_s, 50), "p99_ms": pc(lat_s, 99), "mrays_s": round(srv_m, 1),
+                       "span_ms": round(span_s, 2), "waves": st["waves"] - w0,
+                       "peak_pool_gb": round(st["peak_pool_used"] / 2 ** 30, 3),
+                       "max_submit_lag_ms": round(float(lag.max() * 1e3), 3)},
+            "plain": {"p50_ms": pc(lat_p, 50), "p99_ms": pc(lat_p, 99), "mrays_s": round(pl_m, 1),
+                      "span_ms": round(span_p, 2)},
+            "p99_served_over_plain": round(float(np.percentile(lat_s, 99) / np.percentile(lat_p, 99)), 3),
+            "mrays_served_over_plain": round(srv_m / pl_m, 3),
+            "results_equal_plain": same}
+        log(f"{mode}: {json.dumps(res[mode])}")
+    resident = srv.stats()["resident_bytes"]
     srv.close()
-    lat_s = np.array([(f["done_us"] - f["submit_us"]) / 1e3 for f in infos]) + lag * 1e3
-    first = infos[0]["submit_us"] - lag[0] * 1e6
-    span_s = (max(f["done_us"] for f in infos) - first) / 1e3
-    crc_srv = crcs()
-    # ---- plain arm: the per-call path, one call at a time
-    L = lib.load()
-    for sc in range(len(bvhs)):  # warm-up: each scene's staging sized by its largest request
-        for kind in (False, True):
-            m = np.nonzero((scene == sc) & (anyh == kind))[0]
-            if m.size:
-                k = int(m[np.argmax(nray[m])])
-                f = L.cudaBVH_traceAnyHost if kind else L.cudaBVH_traceClosestHost
-                f(bvhs[sc].h, rays_ptr(k), int(nray[k]), base_out + int(out_off[k]))
-    h_out.zero_()
-    lat_p = np.zeros(NREQ)
-    T0 = time.perf_counter()
-    for i in range(NREQ):
-        ta = T0 + arrival[i]
-        while time.perf_counter() < ta:
-            pass
-        f = L.cudaBVH_traceAnyHost if anyh[i] else L.cudaBVH_traceClosestHost
-        rc = f(bvhs[scene[i]].h, rays_ptr(i), int(nray[i]), base_out + int(out_off[i]))
-        if rc != 0:
-            raise RuntimeError(lib.last_error())
-        lat_p[i] = (time.perf_counter() - ta) * 1e3
-    span_p = (time.perf_counter() - T0) * 1e3
-    same = crcs() == crc_srv
-    total = int(nray.sum())
-    srv_m, pl_m = total / span_s / 1e3, total / span_p / 1e3
-    p = lambda a, q: round(float(np.percentile(a, q)), 3)
-    out = {"metric": "p99 trace latency served vs plain (ms), 256-request Poisson trace", "value": p(lat_s, 99),
-           "unit": "ms", "n_gpus": 1, "steps": 1, "warmup": 4, "higher_is_better": False, "dtype": "f32",
-           "data": "synthetic",
+    ok = all(r["results_equal_plain"] for r in res.values())
+    out = {"metric": "p99 trace latency served vs plain (ms), 256-request Poisson trace, host buffers",
+           "value": res["host"]["served"]["p99_ms"], "unit": "ms", "n_gpus": 1, "steps": 1, "warmup": 4,
+           "higher_is_better": False, "dtype": "f32", "data": "synthetic",
            "config": {"workload": "served_16x30m: 16 resident scenes (30,000,000 triangles, 200K-5M each), "
                                   f"{NREQ} requests Poisson at {RATE:.0f}/s, rays log-uniform 1K-8M "
-                                  "(random incoherent rays), 70% closest / 30% any hit, pinned host buffers",
-                      "hbm_budget_gb": 120, "staging_pool_gb": 16},
-           "served": {"p50_ms": p(lat_s, 50), "p99_ms": p(lat_s, 99), "mrays_s": round(srv_m, 1),
-                      "span_ms": round(span_s, 2), "waves": st["waves"],
-                      "peak_pool_gb": round(st["peak_pool_used"] / 2 ** 30, 3),
-                      "resident_gb": round(st["resident_bytes"] / 2 ** 30, 3),
-                      "max_submit_lag_ms": round(float(lag.max() * 1e3), 3)},
-           "plain": {"p50_ms": p(lat_p, 50), "p99_ms": p(lat_p, 99), "mrays_s": round(pl_m, 1),
-                     "span_ms": round(span_p, 2)},
-           "p99_served_over_plain": round(float(np.percentile(lat_s, 99) / np.percentile(lat_p, 99)), 3),
-           "mrays_served_over_plain": round(srv_m / pl_m, 3),
+                                  "(random incoherent rays), 70% closest / 30% any hit",
+                      "hbm_budget_gb": 120, "staging_pool_gb": 16,
+                      "resident_gb": round(resident / 2 ** 30, 3)},
+           "host_buffers": res["host"], "device_buffers": res["device"],
            "offered_mrays_s": round(total / arrival[-1] / 1e6, 1), "rays": total,
-           "h2d_bytes": total * 32, "d2h_bytes": int(out_off[-1]),
-           "results_equal_plain": same}
+           "h2d_bytes": total * 32, "d2h_bytes": int((nray * esz).sum()), "results_equal_plain": ok}
     print(json.dumps(out), flush=True)
-    return 0 if same else 1
+    return 0 if ok else 1
 
 
 def main():

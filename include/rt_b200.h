@@ -247,6 +247,7 @@ typedef struct {
     int wave_rays;             /* rays per shared wavefront; 0 = 4 Mi */
     int chunk_rays;            /* rays per chunk of a request; 0 = 1 Mi */
     int max_waves;             /* wavefronts in flight, each on its own stream (1..8); 0 = 2 */
+    int prefetch_rays;         /* copied rays waiting for a wavefront, at most; 0 = 2 * wave_rays */
 } RtServerConfig;
 typedef struct {
     double submit_us, admit_us, done_us; /* steady clock, microseconds since rtServer_create */

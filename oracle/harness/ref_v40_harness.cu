@@ -30,6 +30,10 @@ std::string key_of(const Tri& t) { return std::string(reinterpret_cast<const cha
 
 extern "C" {
 
+// Version of this harness's C-ABI; callers check it before binding, so a
+// stale build is refused instead of being called with the wrong arguments.
+int refv40_abi(void) { return 2; }
+
 // Reference BVH2 (32-bin SAH, cuda_rt_v40.cu:790-840) with maxLeaf, collapsed
 // to fp16 BVH4 (cuda_rt_v40.cu:844-871), uploaded the way main() does
 // (cuda_rt_v40.cu:1296-1330), constant-memory top nodes included.
@@ -116,16 +120,18 @@ int refv40_build_cwbvh(void* hv) {
     return h->num_cw;
 }
 
-// traceCWBVH (cuda_rt_v40.cu:142), launched as main() does (:1457).  The
-// kernel reads its scene through __device__ pointers, so set them per call.
-int refv40_trace_cwbvh(void* hv, const void* d_rays, void* d_hits, int n, void* stream) {
+// traceCWBVH (cuda_rt_v40.cu:142): main() launches it as <<<dim3(32, 32),
+// dim3(32, 2)>>> (:1457); its dynamic ray fetch works with any grid, so the
+// grid is a parameter (gx x gy blocks of 32 x 2 threads).  The kernel reads
+// its scene through __device__ pointers, so set them per call.
+int refv40_trace_cwbvh(void* hv, const void* d_rays, void* d_hits, int n, int gx, int gy, void* stream) {
     RefV40* h = static_cast<RefV40*>(hv);
     cudaStream_t s = (cudaStream_t)stream;
     cudaMemcpyToSymbolAsync(d_cwbvhNodes, &h->d_nodes, sizeof(float4*), 0, cudaMemcpyHostToDevice, s);
     cudaMemcpyToSymbolAsync(d_woopTris, &h->d_woop, sizeof(float4*), 0, cudaMemcpyHostToDevice, s);
     cudaMemcpyToSymbolAsync(d_triIndices, &h->d_tri_idx, sizeof(int*), 0, cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(h->d_counter, 0, sizeof(int), s);
-    traceCWBVH<<<dim3(32, 32), dim3(32, 2), 0, s>>>((Ray*)d_rays, (HitCWBVH*)d_hits, n, h->d_counter);
+    traceCWBVH<<<dim3(gx, gy), dim3(32, 2), 0, s>>>((Ray*)d_rays, (HitCWBVH*)d_hits, n, h->d_counter);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -157,3 +157,23 @@ def test_served_admission_limits(served):
     with pytest.raises(lib.RtError):
         tight.add_scene(bvhs[2])
     tight.close()
+
+
+def test_misaligned_device_pointers_are_rejected(served):
+    """Device paths write 16-byte hit records; a misaligned pointer is an
+    argument error reported before any launch, never a GPU fault."""
+    import torch
+    tris, bvhs, reqs, expect = served
+    rays = reqs[0][2][:64]
+    d_r = torch.from_numpy(rays.view(np.uint8).copy()).cuda()
+    d_o = torch.empty(64 * 16 + 16, dtype=torch.uint8, device="cuda")
+    with pytest.raises(lib.RtError):
+        bvhs[0].closest(d_r, 64, d_o[4:])  # hits off by 4 bytes
+    with pytest.raises(lib.RtError):
+        bvhs[0].closest(d_r[8:], 63, d_o)  # rays off by 8 bytes
+    srv = _server(bvhs[:1])
+    with pytest.raises(lib.RtError):
+        srv.submit(0, False, d_r.data_ptr(), 64, d_o.data_ptr() + 4, device=True)
+    srv.close()
+    bvhs[0].closest(d_r, 64, d_o)  # the aligned call still works
+    torch.cuda.synchronize()

@@ -59,6 +59,14 @@ bool ensure_counters(DevBuf<int>& ring) {
     return RT_CUDA(cudaMemset(ring.p, 0, ring.bytes()));
 }
 
+bool check_aligned(const char* who, const void* rays, const void* out, size_t out_align) {
+    if (misaligned(rays, 16) || misaligned(out, out_align)) {
+        set_error("%s: device rays must be 16-byte aligned and results %zu-byte aligned", who, out_align);
+        return false;
+    }
+    return true;
+}
+
 // A fresh zeroed work counter for one launch.  Slots cycle through a ring,
 // so up to kCounterRing launches may be in flight on one handle.
 int* next_counter(DevBuf<int>& ring, unsigned& next, cudaStream_t s) {
@@ -527,6 +535,7 @@ int cudaBVH_traceClosest(CudaBVH_t h, const RtRay* d_rays, int n, RtHit* d_hits,
         set_error("cudaBVH_traceClosest: invalid argument");
         return RT_ERR_INVALID;
     }
+    if (!check_aligned("cudaBVH_traceClosest", d_rays, d_hits, 16)) return RT_ERR_INVALID;
     if (n == 0) return RT_OK;
     cudaStream_t s = (cudaStream_t)stream;
     int* work = next_counter(h->counters, h->counter_next, s);
@@ -540,6 +549,7 @@ int cudaBVH_traceAny(CudaBVH_t h, const RtRay* d_rays, int n, uint8_t* d_occ, vo
         set_error("cudaBVH_traceAny: invalid argument");
         return RT_ERR_INVALID;
     }
+    if (!check_aligned("cudaBVH_traceAny", d_rays, d_occ, 1)) return RT_ERR_INVALID;
     if (n == 0) return RT_OK;
     cudaStream_t s = (cudaStream_t)stream;
     int* work = next_counter(h->counters, h->counter_next, s);
@@ -553,6 +563,7 @@ int cudaBVH_traceCounters(CudaBVH_t h, const RtRay* d_rays, int n, int any, uint
         set_error("cudaBVH_traceCounters: invalid argument");
         return RT_ERR_INVALID;
     }
+    if (!check_aligned("cudaBVH_traceCounters", d_rays, d_counts, 8)) return RT_ERR_INVALID;
     if (n == 0) return RT_OK;
     cudaStream_t s = (cudaStream_t)stream;
     std::lock_guard<std::mutex> g(h->mu);
@@ -605,8 +616,8 @@ HostPipe::~HostPipe() {
 
 namespace {
 
-// Host-buffer trace: the batch is cut into pieces (at least 512K rays, at
-// most HostPipe::kMaxPieces of them); piece k's copy in, trace and copy out
+// Host-buffer trace: the batch is cut into pieces (at least 512K rays by
+// default, at most HostPipe::kMaxPieces of them); piece k's copy in, trace and copy out
 // run on three streams chained by events, so the copy of piece k+1 and the
 // results of piece k-1 cross PCIe while piece k is traced.  Ordered after
 // earlier work on the legacy default stream; returns when the results are
@@ -616,7 +627,12 @@ int trace_host(CudaBVHHandle* h, const RtRay* rays, int n, void* out, bool any) 
     HostPipe& p = h->pipe;
     if (!p.init()) return RT_ERR_CUDA;
     if (!h->stage_rays.ensure(n) || (any ? !h->stage_occ.ensure(n) : !h->stage_hits.ensure(n))) return RT_ERR_NOMEM;
-    constexpr int kMinPiece = 1 << 19;
+    // smallest piece: 512K rays unless RTB200_HOST_PIECE says otherwise (read once)
+    static const int kMinPiece = [] {
+        const char* e = getenv("RTB200_HOST_PIECE");
+        const int v = e ? atoi(e) : 0;
+        return v >= 4096 ? v : (1 << 19);
+    }();
     int piece = std::max(kMinPiece, (n + HostPipe::kMaxPieces - 1) / HostPipe::kMaxPieces);
     piece = (piece + 31) & ~31;
     const size_t es = any ? 1 : sizeof(RtHit);

@@ -84,6 +84,11 @@ int check_trace_args(RtBatchHandle* b, const RtRay* rays, const int* off, int n,
         set_error("%s: invalid argument", who);
         return RT_ERR_INVALID;
     }
+    // closest-hit results are 16-byte records; any-hit results are bytes
+    if (!check_aligned(who, rays, off, 4) || misaligned(out, 16)) {
+        set_error("%s: device rays and results must be 16-byte aligned, offsets 4-byte aligned", who);
+        return RT_ERR_INVALID;
+    }
     return RT_OK;
 }
 

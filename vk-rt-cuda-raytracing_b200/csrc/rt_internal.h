@@ -23,6 +23,12 @@ bool cuda_ok(cudaError_t e, const char* what);
 
 int num_sms();
 
+// Device pointers handed to the kernels are read and written with 16-byte
+// (rays, hit records), 8-byte or 4-byte vector accesses; a misaligned one
+// would fault on the GPU, so entry points reject it first.
+inline bool misaligned(const void* p, size_t a) { return p && (reinterpret_cast<uintptr_t>(p) & (a - 1)) != 0; }
+bool check_aligned(const char* who, const void* rays, const void* out, size_t out_align);
+
 // ---- a typed device buffer ----
 template <class T>
 struct DevBuf {

@@ -482,6 +482,10 @@ int rtPT_render(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* prm, f
         set_error("rtPT_render: invalid argument");
         return RT_ERR_INVALID;
     }
+    if (misaligned(d_rgb, 4)) {
+        set_error("rtPT_render: d_rgb must be 4-byte aligned");
+        return RT_ERR_INVALID;
+    }
     const int64_t P = (int64_t)prm->width * prm->height * prm->spp;
     if (P > (int64_t)INT32_MAX) {
         set_error("rtPT_render: %lld paths exceed 2^31", (long long)P);

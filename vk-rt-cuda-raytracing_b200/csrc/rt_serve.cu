@@ -10,12 +10,15 @@
 //            (rays + results, 256-byte aligned) fits both the staging pool
 //            and the HBM budget left after the resident scenes, and while
 //            fewer than max_inflight requests are admitted; their rays are
-//            copied host->device on the copy stream as they are admitted;
-//   batch    the admitted rays not yet traced are cut into chunks of at most
-//            chunk_rays and packed, oldest request first, into a shared
-//            wavefront of at most wave_rays rays: one persistent
-//            work-stealing launch per hit kind over a segment table, so
-//            requests of different sizes and scenes share the same warps;
+//            copied host->device on the copy stream, oldest first, in
+//            chunk-sized pieces that each record an event, with at most
+//            prefetch_rays copied rays waiting for a wavefront;
+//   batch    the rays whose copy has landed and that are not yet traced are
+//            cut into chunks of at most chunk_rays and packed, oldest
+//            request first, into a shared wavefront of at most wave_rays
+//            rays: one persistent work-stealing launch per hit kind over a
+//            segment table, so requests of different sizes and scenes share
+//            the same warps;
 //   overlap  up to max_waves wavefronts are in flight on their own streams:
 //            a new wavefront's blocks fill the SMs as the previous one
 //            drains, while admission copies of later requests proceed on
@@ -122,6 +125,10 @@ struct Request {
     int n = 0;
     size_t pool_off = 0, pool_bytes = 0;
     int next_ray = 0;        // rays handed to wavefronts so far
+    int ready_rays = 0;      // rays whose host->device copy has completed
+    int issued_rays = 0;     // rays whose host->device copy has been issued
+    std::vector<std::pair<int, cudaEvent_t>> pieces;  // (end ray, copy event) in copy order
+    size_t pieces_ready = 0;
     int chunks_pending = 0;  // chunks in flight
     int waves = 0;
     int status = RT_OK;
@@ -163,7 +170,7 @@ struct RtServerHandle {
     Pool pool;
     // streams
     cudaStream_t copy_in = nullptr, copy_out = nullptr;
-    cudaEvent_t h2d_ev = nullptr;
+    std::vector<cudaEvent_t> spare_events;
     std::vector<std::unique_ptr<WaveSlot>> slots;
     std::deque<WaveSlot*> inflight;  // in launch order
     // requests
@@ -174,6 +181,8 @@ struct RtServerHandle {
     uint64_t next_ticket = 1;
     std::deque<Request*> waiting;  // scheduler-owned: not yet admitted
     std::deque<Request*> staged;   // scheduler-owned: admitted, rays left to trace
+    std::deque<Request*> to_copy;  // scheduler-owned: admitted, copies left to issue
+    int64_t pending_rays = 0;      // copies issued whose rays are not yet in a wavefront
     int admitted = 0;
     // scene additions run on the scheduler thread between wavefronts
     struct SceneJob {
@@ -193,9 +202,31 @@ struct RtServerHandle {
     }
     size_t resident_bytes() const { return nodes.bytes() + tris.bytes(); }
 
+    cudaEvent_t get_event() {
+        if (!spare_events.empty()) {
+            cudaEvent_t e = spare_events.back();
+            spare_events.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        return RT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)) ? e : nullptr;
+    }
+    void update_ready(Request* r) {
+        while (r->pieces_ready < r->pieces.size()) {
+            const cudaError_t q = cudaEventQuery(r->pieces[r->pieces_ready].second);
+            if (q == cudaErrorNotReady) break;
+            if (q != cudaSuccess) {
+                cuda_ok(q, "request copy");
+                r->status = RT_ERR_CUDA;
+            }
+            r->ready_rays = r->pieces[r->pieces_ready].first;
+            r->pieces_ready++;
+        }
+    }
     void loop();
     int add_scene(CudaBVH_t b);
     void admit();
+    void issue_copies();
     bool launch_wave(WaveSlot* w);
     bool retire();
     void complete(Request* r);
@@ -253,6 +284,8 @@ int RtServerHandle::add_scene(CudaBVH_t b) {
 
 void RtServerHandle::complete(Request* r) {
     r->t_done = now_us();
+    for (auto& pc : r->pieces) spare_events.push_back(pc.second);
+    r->pieces.clear();
     if (r->host && r->pool_bytes) {
         pool.release(r->pool_off, r->pool_bytes);
         r->pool_bytes = 0;
@@ -268,8 +301,9 @@ void RtServerHandle::complete(Request* r) {
 }
 
 void RtServerHandle::fail_all(const char* why) {
+    const std::string detail = rtGetLastError();  // this thread's last CUDA error, if any
     std::lock_guard<std::mutex> g(mu);
-    fatal = why;
+    fatal = detail.empty() ? std::string(why) : std::string(why) + ": " + detail;
     for (auto& kv : all) {
         if (!kv.second->done) {
             kv.second->status = RT_ERR_CUDA;
@@ -280,11 +314,36 @@ void RtServerHandle::fail_all(const char* why) {
     submitted.clear();
     waiting.clear();
     staged.clear();
+    to_copy.clear();
     cv_done.notify_all();
 }
 
+// Issues host->device copies of admitted requests in chunk-sized pieces,
+// oldest first, each recording an event, while fewer than prefetch_rays
+// copied rays wait for a wavefront.  The read-ahead bound keeps completions
+// in arrival order: copies of later requests do not take PCIe bandwidth from
+// the results of earlier ones.
+void RtServerHandle::issue_copies() {
+    while (!to_copy.empty() && pending_rays < cfg.prefetch_rays) {
+        Request* r = to_copy.front();
+        const int b = r->issued_rays, e = std::min(r->n, b + cfg.chunk_rays);
+        cudaEvent_t ev = get_event();
+        if (!ev || !RT_CUDA(cudaMemcpyAsync((void*)(r->d_rays + b), r->h_rays + b, (size_t)(e - b) * sizeof(RtRay),
+                                            cudaMemcpyHostToDevice, copy_in)) ||
+            !RT_CUDA(cudaEventRecord(ev, copy_in))) {
+            if (ev) spare_events.push_back(ev);
+            fail_all("request copy could not be issued");
+            stop = true;
+            return;
+        }
+        r->pieces.push_back({e, ev});
+        pending_rays += e - b;
+        r->issued_rays = e;
+        if (e == r->n) to_copy.pop_front();
+    }
+}
+
 void RtServerHandle::admit() {
-    bool copied = false;
     while (!waiting.empty() && admitted < cfg.max_inflight) {
         Request* r = waiting.front();
         if (r->host && r->n > 0) {
@@ -297,18 +356,15 @@ void RtServerHandle::admit() {
             unsigned char* base = pool_mem.p + off;
             r->d_rays = reinterpret_cast<const RtRay*>(base);
             r->d_out = base + align_up((size_t)r->n * sizeof(RtRay));
-            if (!RT_CUDA(cudaMemcpyAsync((void*)r->d_rays, r->h_rays, (size_t)r->n * sizeof(RtRay),
-                                         cudaMemcpyHostToDevice, copy_in))) {
-                r->status = RT_ERR_CUDA;
-            }
-            copied = true;
+            to_copy.push_back(r);
+        } else {
+            r->ready_rays = r->n;
         }
         waiting.pop_front();
         admitted++;
         r->t_admit = now_us();
         staged.push_back(r);
     }
-    if (copied) cudaEventRecord(h2d_ev, copy_in);
 }
 
 bool RtServerHandle::launch_wave(WaveSlot* w) {
@@ -319,11 +375,12 @@ bool RtServerHandle::launch_wave(WaveSlot* w) {
     const uint32_t cap = (uint32_t)cfg.wave_rays;
     for (auto it = staged.begin(); it != staged.end() && tc + ta < cap;) {
         Request* r = *it;
+        update_ready(r);
         int& ns = r->any ? na : nc;
         uint32_t& tk = r->any ? ta : tc;
-        while (r->next_ray < r->n && tc + ta < cap && ns < kMaxSeg) {
-            const int cnt = (int)std::min<uint32_t>({(uint32_t)cfg.chunk_rays, (uint32_t)(r->n - r->next_ray),
-                                                     cap - tc - ta});
+        while (r->next_ray < r->ready_rays && tc + ta < cap && ns < kMaxSeg) {
+            const int cnt = (int)std::min<uint32_t>(
+                {(uint32_t)cfg.chunk_rays, (uint32_t)(r->ready_rays - r->next_ray), cap - tc - ta});
             WaveSeg& sg = w->h_segs[(r->any ? kMaxSeg : 0) + ns];
             sg.rays = r->d_rays + r->next_ray;
             sg.out = r->any ? (void*)((uint8_t*)r->d_out + r->next_ray)
@@ -332,6 +389,7 @@ bool RtServerHandle::launch_wave(WaveSlot* w) {
             sg.root = scenes[r->scene].root;
             sg.pad[0] = sg.pad[1] = 0;
             w->chunks.push_back({r, r->next_ray, cnt});
+            if (r->host) pending_rays -= cnt;
             r->next_ray += cnt;
             r->chunks_pending++;
             ns++;
@@ -345,8 +403,7 @@ bool RtServerHandle::launch_wave(WaveSlot* w) {
     for (const Chunk& c : w->chunks) c.req->waves++;
     w->rays = tc + ta;
     cudaStream_t s = w->stream;
-    bool ok = RT_CUDA(cudaStreamWaitEvent(s, h2d_ev, 0)) &&
-              RT_CUDA(cudaMemcpyAsync(w->d_segs.p, w->h_segs, sizeof(WaveSeg) * 2 * kMaxSeg, cudaMemcpyHostToDevice,
+    bool ok = RT_CUDA(cudaMemcpyAsync(w->d_segs.p, w->h_segs, sizeof(WaveSeg) * 2 * kMaxSeg, cudaMemcpyHostToDevice,
                                       s)) &&
               RT_CUDA(cudaMemsetAsync(w->work.p, 0, 2 * sizeof(int), s)) &&
               RT_CUDA(cudaMemsetAsync(w->status.p, 0, sizeof(int), s));
@@ -428,6 +485,7 @@ void RtServerHandle::loop() {
         while (retire()) progress = true;
         if (stop && !fatal.empty()) break;
         admit();
+        issue_copies();
         bool scene_pending;
         {
             std::lock_guard<std::mutex> g(mu);
@@ -460,7 +518,8 @@ void RtServerHandle::loop() {
             }
             progress = true;
         }
-        if (!progress && !inflight.empty()) std::this_thread::yield();
+        issue_copies();
+        if (!progress) std::this_thread::yield();
     }
     cudaStreamSynchronize(copy_out);
 }
@@ -477,6 +536,7 @@ RtServer_t rtServer_create(const RtServerConfig* cfg_in) {
     if (c.wave_rays <= 0) c.wave_rays = 4 << 20;
     if (c.chunk_rays <= 0) c.chunk_rays = 1 << 20;
     if (c.max_waves <= 0) c.max_waves = 2;
+    if (c.prefetch_rays <= 0) c.prefetch_rays = 2 * c.wave_rays;
     if (c.max_waves > 8 || c.chunk_rays > c.wave_rays || c.pool_bytes > c.hbm_budget_bytes) {
         set_error("rtServer_create: invalid configuration");
         return nullptr;
@@ -488,8 +548,7 @@ RtServer_t rtServer_create(const RtServerConfig* cfg_in) {
     cudaGetDevice(&s->device);
     bool ok = s->pool_mem.alloc(c.pool_bytes) &&
               RT_CUDA(cudaStreamCreateWithFlags(&s->copy_in, cudaStreamNonBlocking)) &&
-              RT_CUDA(cudaStreamCreateWithFlags(&s->copy_out, cudaStreamNonBlocking)) &&
-              RT_CUDA(cudaEventCreateWithFlags(&s->h2d_ev, cudaEventDisableTiming));
+              RT_CUDA(cudaStreamCreateWithFlags(&s->copy_out, cudaStreamNonBlocking));
     s->pool.init(c.pool_bytes);
     for (int i = 0; ok && i < c.max_waves; i++) {
         auto w = std::make_unique<WaveSlot>();
@@ -501,7 +560,6 @@ RtServer_t rtServer_create(const RtServerConfig* cfg_in) {
              RT_CUDA(cudaMallocHost(&w->h_status, sizeof(int)));
         s->slots.push_back(std::move(w));
     }
-    if (ok) ok = RT_CUDA(cudaEventRecord(s->h2d_ev, s->copy_in));
     if (!ok) {
         rtServer_destroy(s.release());
         return nullptr;
@@ -536,6 +594,7 @@ static int submit(RtServer_t s, int scene, int any_hit, const RtRay* rays, int n
         set_error("rtServer_submit: invalid argument");
         return RT_ERR_INVALID;
     }
+    if (!host && !check_aligned("rtServer_submitDevice", rays, out, any_hit ? 1 : 16)) return RT_ERR_INVALID;
     std::unique_ptr<Request> r(new Request());
     r->scene = scene;
     r->any = any_hit != 0;
@@ -611,7 +670,8 @@ int rtServer_wait(RtServer_t s, uint64_t ticket, int timeout_ms, RtRequestInfo* 
         info->waves = r->waves;
     }
     s->all.erase(it);
-    if (st != RT_OK) set_error("rtServer_wait: request failed (%d)", st);
+    if (st != RT_OK) set_error("rtServer_wait: request failed (%d)%s%s", st, s->fatal.empty() ? "" : ": ",
+                               s->fatal.c_str());
     return st;
 }
 
@@ -653,7 +713,9 @@ void rtServer_destroy(RtServer_t s) {
     if (s->copy_out) cudaStreamSynchronize(s->copy_out);
     if (s->copy_in) cudaStreamDestroy(s->copy_in);
     if (s->copy_out) cudaStreamDestroy(s->copy_out);
-    if (s->h2d_ev) cudaEventDestroy(s->h2d_ev);
+    for (cudaEvent_t e : s->spare_events) cudaEventDestroy(e);
+    for (auto& kv : s->all)
+        for (auto& pc : kv.second->pieces) cudaEventDestroy(pc.second);
     delete s;
 }
 

@@ -431,6 +431,11 @@ int cudaTLAS_traceClosest(CudaTLAS_t t, const RtRay* d_rays, int n, RtHit* d_hit
         set_error("cudaTLAS_traceClosest: invalid argument");
         return RT_ERR_INVALID;
     }
+    if (!check_aligned("cudaTLAS_traceClosest", d_rays, d_hits, 16)) return RT_ERR_INVALID;
+    if (misaligned(d_inst, 4)) {
+        set_error("cudaTLAS_traceClosest: d_inst must be 4-byte aligned");
+        return RT_ERR_INVALID;
+    }
     if (n == 0) return RT_OK;
     cudaStream_t s = (cudaStream_t)stream;
     int* work = next_counter(t->counters, t->counter_next, s);
@@ -444,6 +449,7 @@ int cudaTLAS_traceAny(CudaTLAS_t t, const RtRay* d_rays, int n, uint8_t* d_occ, 
         set_error("cudaTLAS_traceAny: invalid argument");
         return RT_ERR_INVALID;
     }
+    if (!check_aligned("cudaTLAS_traceAny", d_rays, d_occ, 1)) return RT_ERR_INVALID;
     if (n == 0) return RT_OK;
     cudaStream_t s = (cudaStream_t)stream;
     int* work = next_counter(t->counters, t->counter_next, s);

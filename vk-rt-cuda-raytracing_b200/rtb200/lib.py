@@ -58,7 +58,7 @@ class RtPTStats(C.Structure):
 
 class RtServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("pool_bytes", C.c_uint64), ("max_inflight", C.c_int),
-                ("wave_rays", C.c_int), ("chunk_rays", C.c_int), ("max_waves", C.c_int)]
+                ("wave_rays", C.c_int), ("chunk_rays", C.c_int), ("max_waves", C.c_int), ("prefetch_rays", C.c_int)]
 
 
 class RtRequestInfo(C.Structure):
@@ -474,8 +474,10 @@ class Server:
     """rtServer_*: resident scenes, requests admitted by footprint and traced
     in shared wavefronts by the library's scheduler thread."""
 
-    def __init__(self, hbm_budget_bytes=0, pool_bytes=0, max_inflight=0, wave_rays=0, chunk_rays=0, max_waves=0):
-        cfg = RtServerConfig(hbm_budget_bytes, pool_bytes, max_inflight, wave_rays, chunk_rays, max_waves)
+    def __init__(self, hbm_budget_bytes=0, pool_bytes=0, max_inflight=0, wave_rays=0, chunk_rays=0, max_waves=0,
+                 prefetch_rays=0):
+        cfg = RtServerConfig(hbm_budget_bytes, pool_bytes, max_inflight, wave_rays, chunk_rays, max_waves,
+                             prefetch_rays)
         self.h = load().rtServer_create(C.byref(cfg))
         if not self.h:
             raise RtError(f"rtServer_create failed: {last_error()}")
