@@ -51,6 +51,23 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(x: float, ws: int, device="cuda") -> float:
+    """The largest of every rank's x (all ranks call it, same order)."""
+    if ws == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_mrays(rays_per_rank: int, ws: int, t_ms_max: float) -> float:
+    """Weak scaling: every rank traces its own batch of rays_per_rank; the
+    job takes as long as the slowest rank."""
+    return ws * rays_per_rank / t_ms_max / 1e3
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -174,43 +191,40 @@ def morton_order(rays):
 
 def reference_gpu_kernel(tris, rays, d_rays, n, torch, steps, flush):
     """The reference's closest-hit kernels rebuilt for sm_100a on its own
-    CPU-built structures of the same scene: traceBVH4Diffuse
-    (cuda_rt_v40.cu:505, fp16 BVH4) and traceCWBVH (cuda_rt_v40.cu:142,
-    8-wide compressed BVH, Woop triangles), each at leaf 3 and 4, three
-    launch shapes, on the rays as given and regrouped in Morton order as the
-    reference's own benchmark does (sort not timed).  The bar is the
-    fastest."""
+    CPU-built BVHs of the same scene: traceBVH4Diffuse (cuda_rt_v40.cu:505,
+    fp16 BVH4) at leaf 3 and 4, three launch shapes, on the rays as given and
+    regrouped in Morton order as the reference's own benchmark does (sort not
+    timed); and the backend's cudaBVH_traceDiffuse path.  The bar is the
+    fastest.  The reference's traceCWBVH is not run:
+    it raised an illegal memory access on this scene with 4-triangle leaves
+    (a limit of its leaf encoding), and reference GPU code that faulted is
+    not run again."""
     import ctypes as C
     path = ROOT / "oracle" / "_ref" / "libref_v40.so"
     if not path.exists():
         return {"unavailable": "oracle/_ref/libref_v40.so not built"}
     R = C.CDLL(str(path))
-    if not hasattr(R, "refv40_abi") or R.refv40_abi() != 2:
-        return {"unavailable": "oracle/_ref/libref_v40.so is stale (harness ABI 2 expected); rebuild: make -C oracle ref"}
+    if not hasattr(R, "refv40_abi") or R.refv40_abi() != 3:
+        return {"unavailable": "oracle/_ref/libref_v40.so is stale (harness ABI 3 expected); rebuild: make -C oracle ref"}
     R.refv40_build.restype = C.c_void_p
     R.refv40_build.argtypes = [C.c_void_p, C.c_int, C.c_int]
     R.refv40_trace_bvh4.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
-    R.refv40_build_cwbvh.argtypes = [C.c_void_p]
-    R.refv40_trace_cwbvh.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
     R.refv40_destroy.argtypes = [C.c_void_p]
     order = morton_order(rays)
     d_sorted = torch.from_numpy(np.ascontiguousarray(rays[order]).view(np.uint8)).cuda()
     d_h = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
     st = torch.cuda.current_stream().cuda_stream
-    out = {"flags": "-O3 --use_fast_math (reference Makefile)", "variants": {}}
+    out = {"flags": "-O3 --use_fast_math (reference Makefile)", "variants": {},
+           "not_run": "traceCWBVH (cuda_rt_v40.cu:142): illegal memory access with 4-triangle leaves"}
     best = None
     for leaf in (3, 4):
         t0 = time.time()
         h = R.refv40_build(tris.ctypes.data, tris.shape[0], leaf)
         out[f"cpu_build_s_leaf{leaf}"] = round(time.time() - t0, 2)
-        R.refv40_build_cwbvh(h)
         for ray_kind, dr in (("as_given", d_rays), ("morton", d_sorted)):
             launches = [("traceBVH4Diffuse", f"{b}x{t}",
                          lambda b=b, t=t: R.refv40_trace_bvh4(h, dr.data_ptr(), d_h.data_ptr(), n, b, t, st))
                         for b, t in ((640, 256), (960, 256), (1280, 128))]
-            launches += [("traceCWBVH", f"({gx},{gy})x64",
-                          lambda gx=gx, gy=gy: R.refv40_trace_cwbvh(h, dr.data_ptr(), d_h.data_ptr(), n, gx, gy, st))
-                         for gx, gy in ((32, 32), (74, 32), (148, 32))]
             for kern, shape, fn in launches:
                 ms = time_steps(torch, fn, steps, 2, flush)
                 v = n / (sum(ms) / len(ms)) / 1e3
@@ -220,6 +234,31 @@ def reference_gpu_kernel(tris, rays, d_rays, n, torch, steps, flush):
                 if best is None or v > best[0]:
                     best = (v, name)
         R.refv40_destroy(h)
+    # the backend's own ABI path (layer/cuda_bvh_backend.cu:1380-1480, built with
+    # BVH_LAYER_MODE=0): it Morton-sorts on the host, then times only its
+    # bk_traceDiffuseArbitrary launch with events and returns that Mrays/s
+    gpu_path = ROOT / "oracle" / "_ref" / "libref_backend_gpu.so"
+    if gpu_path.exists():
+        B = C.CDLL(str(gpu_path))
+        B.cudaBVH_build.restype = C.c_void_p
+        B.cudaBVH_build.argtypes = [C.c_void_p, C.c_int]
+        B.cudaBVH_traceDiffuse.restype = C.c_float
+        B.cudaBVH_traceDiffuse.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 7
+        B.cudaBVH_destroy.argtypes = [C.c_void_p]
+        t0 = time.time()
+        hb = B.cudaBVH_build(tris.ctypes.data, tris.shape[0])
+        out["backend_cpu_build_s"] = round(time.time() - t0, 2)
+        soa = [np.ascontiguousarray(rays["org"][:, k]) for k in range(3)] + \
+              [np.ascontiguousarray(rays["dir"][:, k]) for k in range(3)]
+        ht = np.zeros(n, np.float32)
+        vals = [float(B.cudaBVH_traceDiffuse(hb, n, *[a.ctypes.data for a in soa], ht.ctypes.data))
+                for _ in range(3 + steps)]
+        B.cudaBVH_destroy(hb)
+        v = max(vals[3:])
+        name = "bk_traceDiffuseArbitrary via cudaBVH_traceDiffuse (kernel time it reports)"
+        out["variants"][name] = {"mrays_s": round(v, 1), "hit_fraction": round(float((ht < 1e29).mean()), 4)}
+        if v > best[0]:
+            best = (v, name)
     out.update({"value": round(best[0], 1), "unit": UNIT, "kernel": best[1]})
     return out
 
@@ -299,12 +338,22 @@ def run_ours(args):
     from rtb200 import lib
     lib.load()
     tris = make_workload()
-    t0 = time.time()
-    bvh = lib.BVH(tris)
-    torch.cuda.synchronize()
+    # build time: one small warm-up build (first-use costs of the process),
+    # then the median of three builds of the scene
+    from rtb200 import scenes as _sc
+    lib.BVH(_sc.scene_meshes(2, 5000)).close()
+    builds = []
+    for _ in range(3):
+        t0 = time.time()
+        bvh = lib.BVH(tris)
+        torch.cuda.synchronize()
+        builds.append((bvh.stats()["build_ms"], time.time() - t0))
+        if len(builds) < 3:
+            bvh.close()
     stats = bvh.stats()
-    log(f"build: {stats['build_ms']:.1f} ms device, {time.time() - t0:.2f}s wall, {stats['num_nodes']} nodes, "
-        f"depth {stats['depth']}, SAH {stats['sah_cost']:.2f}")
+    stats["build_ms"] = float(np.median([b[0] for b in builds]))
+    log(f"build: {stats['build_ms']:.1f} ms device (median of 3), {builds[-1][1]:.2f}s wall, {stats['num_nodes']} "
+        f"nodes, depth {stats['depth']}, SAH {stats['sah_cost']:.2f}")
     prim, dif, sha, prim_hit = derive_rays(tris, bvh, torch)
     d_dif = torch.from_numpy(dif.view(np.uint8).copy()).cuda()
     d_sha = torch.from_numpy(sha.view(np.uint8).copy()).cuda()
@@ -327,12 +376,8 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         ms = time_steps(torch, lambda: bvh.closest(d_dif, N_RAYS, d_hits, stream=stream), args.steps, args.warmup,
                         flush)
-    t_step = sum(ms) / len(ms)
-    if ws > 1:
-        tt = torch.tensor([t_step], device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_step = float(tt.item())
-    value = ws * N_RAYS / t_step / 1e3
+    t_step = max_over_ranks(sum(ms) / len(ms), ws)
+    value = whole_job_mrays(N_RAYS, ws, t_step)
     ms_any = time_steps(torch, lambda: bvh.any(d_sha, N_RAYS, d_occ, stream=stream), args.steps, args.warmup, flush)
     any_mrays = N_RAYS / (sum(ms_any) / len(ms_any)) / 1e3
     hits = d_hits.cpu().numpy().view([("t", "<f4"), ("prim", "<i4"), ("u", "<f4"), ("v", "<f4")])
@@ -358,7 +403,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         e2e_step()
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
-    e2e_val = ws * N_RAYS / (sum(e2e_ms) / len(e2e_ms)) / 1e3
+    e2e_val = whole_job_mrays(N_RAYS, ws, max_over_ranks(sum(e2e_ms) / len(e2e_ms), ws))
     assert np.array_equal(h_hits.numpy().view(hits.dtype)["prim"], hits["prim"]), "e2e hits differ"
 
     peak, peak_kind = measured_peaks()

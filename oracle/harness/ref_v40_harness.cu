@@ -1,5 +1,5 @@
-// ref_v40_harness.cu -- drives the reference's own cuda_rt_v40.cu kernels
-// (traceBVH4Diffuse, traceCWBVH) rebuilt for sm_100a.  Comparison arm only: this is
+// ref_v40_harness.cu -- drives the reference's own cuda_rt_v40.cu kernel
+// traceBVH4Diffuse rebuilt for sm_100a.  Comparison arm only: this is
 // how the in-run "rebuilt reference kernel" is timed.  The reference source is
 // #included from where it lies (REF_V40_SOURCE, set by oracle/Makefile); its
 // main() is renamed with -Dmain=ref_v40_main.  Nothing here changes the
@@ -17,10 +17,6 @@ struct RefV40 {
     float* d_tv[9] = {nullptr};
     int* d_counter = nullptr;
     std::vector<int> ordered_orig;  // ordered tri -> input index
-    // CWBVH
-    float4 *d_nodes = nullptr, *d_woop = nullptr;
-    int* d_tri_idx = nullptr;
-    int num_cw = 0;
     BVH2Builder* b2 = nullptr;
     std::vector<Tri> tris;
 };
@@ -32,7 +28,7 @@ extern "C" {
 
 // Version of this harness's C-ABI; callers check it before binding, so a
 // stale build is refused instead of being called with the wrong arguments.
-int refv40_abi(void) { return 2; }
+int refv40_abi(void) { return 3; }
 
 // Reference BVH2 (32-bin SAH, cuda_rt_v40.cu:790-840) with maxLeaf, collapsed
 // to fp16 BVH4 (cuda_rt_v40.cu:844-871), uploaded the way main() does
@@ -103,37 +99,11 @@ int refv40_trace_bvh4(void* hv, const void* d_rays, void* d_hits, int n, int blo
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
-// CWBVH build (cuda_rt_v40.cu:1348-1372: BVH8Builder::collapse + CWBVHData::convert).
-int refv40_build_cwbvh(void* hv) {
-    RefV40* h = static_cast<RefV40*>(hv);
-    BVH8Builder bvh8(*h->b2);
-    bvh8.collapse(0);
-    CWBVHData cw;
-    cw.convert(bvh8, h->b2->ordered.data());
-    h->num_cw = (int)cw.nodeData.size() / 5;
-    cudaMalloc(&h->d_nodes, cw.nodeData.size() * sizeof(float4));
-    cudaMalloc(&h->d_woop, cw.woopTris.size() * sizeof(float4));
-    cudaMalloc(&h->d_tri_idx, cw.triIndices.size() * sizeof(int));
-    cudaMemcpy(h->d_nodes, cw.nodeData.data(), cw.nodeData.size() * sizeof(float4), cudaMemcpyHostToDevice);
-    cudaMemcpy(h->d_woop, cw.woopTris.data(), cw.woopTris.size() * sizeof(float4), cudaMemcpyHostToDevice);
-    cudaMemcpy(h->d_tri_idx, cw.triIndices.data(), cw.triIndices.size() * sizeof(int), cudaMemcpyHostToDevice);
-    return h->num_cw;
-}
-
-// traceCWBVH (cuda_rt_v40.cu:142): main() launches it as <<<dim3(32, 32),
-// dim3(32, 2)>>> (:1457); its dynamic ray fetch works with any grid, so the
-// grid is a parameter (gx x gy blocks of 32 x 2 threads).  The kernel reads
-// its scene through __device__ pointers, so set them per call.
-int refv40_trace_cwbvh(void* hv, const void* d_rays, void* d_hits, int n, int gx, int gy, void* stream) {
-    RefV40* h = static_cast<RefV40*>(hv);
-    cudaStream_t s = (cudaStream_t)stream;
-    cudaMemcpyToSymbolAsync(d_cwbvhNodes, &h->d_nodes, sizeof(float4*), 0, cudaMemcpyHostToDevice, s);
-    cudaMemcpyToSymbolAsync(d_woopTris, &h->d_woop, sizeof(float4*), 0, cudaMemcpyHostToDevice, s);
-    cudaMemcpyToSymbolAsync(d_triIndices, &h->d_tri_idx, sizeof(int*), 0, cudaMemcpyHostToDevice, s);
-    cudaMemsetAsync(h->d_counter, 0, sizeof(int), s);
-    traceCWBVH<<<dim3(gx, gy), dim3(32, 2), 0, s>>>((Ray*)d_rays, (HitCWBVH*)d_hits, n, h->d_counter);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
-}
+// traceCWBVH (cuda_rt_v40.cu:142) is not driven here: it raised an illegal
+// memory access on a 2M-triangle scene built with 4-triangle leaves (its
+// 8-wide conversion, cuda_rt_v40.cu:1086-1088, encodes at most 3 triangles per
+// leaf in unary yet advances the leaf offset by 4, so triangle bits pass bit
+// 24), and the reference's GPU code that faulted is not run again.
 
 void refv40_destroy(void* hv) {
     RefV40* h = static_cast<RefV40*>(hv);
@@ -141,9 +111,6 @@ void refv40_destroy(void* hv) {
     cudaFree(h->d_bvh4);
     for (int c = 0; c < 9; c++) cudaFree(h->d_tv[c]);
     cudaFree(h->d_counter);
-    cudaFree(h->d_nodes);
-    cudaFree(h->d_woop);
-    cudaFree(h->d_tri_idx);
     delete h->b2;
     delete h;
 }
