@@ -589,7 +589,8 @@ namespace rtb {
 bool HostPipe::init() {
     if (ready) return true;
     bool ok = RT_CUDA(cudaStreamCreateWithFlags(&in, cudaStreamNonBlocking)) &&
-              RT_CUDA(cudaStreamCreateWithFlags(&comp, cudaStreamNonBlocking)) &&
+              RT_CUDA(cudaStreamCreateWithFlags(&comp[0], cudaStreamNonBlocking)) &&
+              RT_CUDA(cudaStreamCreateWithFlags(&comp[1], cudaStreamNonBlocking)) &&
               RT_CUDA(cudaStreamCreateWithFlags(&out, cudaStreamNonBlocking)) &&
               RT_CUDA(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
     for (int i = 0; ok && i < kMaxPieces; i++)
@@ -600,7 +601,7 @@ bool HostPipe::init() {
 }
 
 HostPipe::~HostPipe() {
-    for (cudaStream_t s : {in, comp, out})
+    for (cudaStream_t s : {in, comp[0], comp[1], out})
         if (s) {
             cudaStreamSynchronize(s);
             cudaStreamDestroy(s);
@@ -617,11 +618,13 @@ HostPipe::~HostPipe() {
 namespace {
 
 // Host-buffer trace: the batch is cut into pieces (at least 512K rays by
-// default, at most HostPipe::kMaxPieces of them); piece k's copy in, trace and copy out
-// run on three streams chained by events, so the copy of piece k+1 and the
-// results of piece k-1 cross PCIe while piece k is traced.  Ordered after
-// earlier work on the legacy default stream; returns when the results are
-// in host memory.
+// default, at most HostPipe::kMaxPieces of them) whose copy in, trace and
+// copy out run on separate streams chained by events, so the copy of piece
+// k+1 and the results of piece k-1 cross PCIe while piece k is traced.
+// Successive traces alternate between two streams, so a piece's launch can
+// fill the SMs while the slowest rays of the previous piece finish.
+// Ordered after earlier work on the legacy default stream; returns when the
+// results are in host memory.
 int trace_host(CudaBVHHandle* h, const RtRay* rays, int n, void* out, bool any) {
     std::lock_guard<std::mutex> g(h->mu);
     HostPipe& p = h->pipe;
@@ -642,15 +645,16 @@ int trace_host(CudaBVHHandle* h, const RtRay* rays, int n, void* out, bool any) 
     int k = 0;
     for (int b = 0; b < n; b += piece, k++) {
         const int c = std::min(piece, n - b);
+        cudaStream_t comp = p.comp[k & 1];
         if (!RT_CUDA(cudaMemcpyAsync(h->stage_rays.p + b, rays + b, sizeof(RtRay) * (size_t)c, cudaMemcpyHostToDevice,
                                      p.in)) ||
-            !RT_CUDA(cudaEventRecord(p.ev_in[k], p.in)) || !RT_CUDA(cudaStreamWaitEvent(p.comp, p.ev_in[k], 0)))
+            !RT_CUDA(cudaEventRecord(p.ev_in[k], p.in)) || !RT_CUDA(cudaStreamWaitEvent(comp, p.ev_in[k], 0)))
             return RT_ERR_CUDA;
-        int* work = next_counter(h->counters, h->counter_next, p.comp);
+        int* work = next_counter(h->counters, h->counter_next, comp);
         const int rc = launch_trace_blas(h->bvh8, h->stage_rays.p + b, c, any ? nullptr : h->stage_hits.p + b,
-                                         any ? h->stage_occ.p + b : nullptr, nullptr, work, h->status.p, p.comp);
+                                         any ? h->stage_occ.p + b : nullptr, nullptr, work, h->status.p, comp);
         if (rc != RT_OK) return RT_CUDA(cudaGetLastError()) ? rc : RT_ERR_CUDA;
-        if (!RT_CUDA(cudaEventRecord(p.ev_tr[k], p.comp)) || !RT_CUDA(cudaStreamWaitEvent(p.out, p.ev_tr[k], 0)) ||
+        if (!RT_CUDA(cudaEventRecord(p.ev_tr[k], comp)) || !RT_CUDA(cudaStreamWaitEvent(p.out, p.ev_tr[k], 0)) ||
             !RT_CUDA(cudaMemcpyAsync((char*)out + (size_t)b * es, dev_out + (size_t)b * es, (size_t)c * es,
                                      cudaMemcpyDeviceToHost, p.out)))
             return RT_ERR_CUDA;

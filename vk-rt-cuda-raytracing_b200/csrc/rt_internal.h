@@ -114,11 +114,12 @@ float bvh2_sah_cost(const Bvh2Device& b2, cudaStream_t s);
 }  // namespace rtb
 
 namespace rtb {
-// Copy-in / trace / copy-out pipeline of the host-buffer entry points: one
-// non-blocking stream per stage and an event per piece and stage.
+// Copy-in / trace / copy-out pipeline of the host-buffer entry points:
+// non-blocking streams for copy-in, trace (two, alternating) and copy-out,
+// and an event per piece and stage.
 struct HostPipe {
     static constexpr int kMaxPieces = 16;
-    cudaStream_t in = nullptr, comp = nullptr, out = nullptr;
+    cudaStream_t in = nullptr, comp[2] = {nullptr, nullptr}, out = nullptr;
     cudaEvent_t start = nullptr, ev_in[kMaxPieces] = {}, ev_tr[kMaxPieces] = {};
     bool ready = false;
     bool init();

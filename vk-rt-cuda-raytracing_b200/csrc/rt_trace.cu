@@ -59,6 +59,9 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
     __shared__ unsigned long long s_key[TRACE_T];  // owner's best (ordered t, prim)
     __shared__ int s_rec[TRACE_T];                 // set when a worker improved it (any hit: found)
     __shared__ float2 s_uv[TRACE_T];               // barycentrics of the improved best
+#if RTB_RAY_SMEM
+    __shared__ float4 s_ray[2][TRACE_T];           // each lane's ray, read by the lanes testing its triangles
+#endif
     uint2 lstack[LSTACK];
     const int lane = threadIdx.x & 31;
     const int wbase = threadIdx.x & ~31;
@@ -113,6 +116,10 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
                     hprim = -1;
                     hu = hv = 0.f;
                     w.start();
+#if RTB_RAY_SMEM
+                    s_ray[0][threadIdx.x] = make_float4(r.ox, r.oy, r.oz, r.tmin);
+                    s_ray[1][threadIdx.x] = make_float4(r.dx, r.dy, r.dz, r.tmax);
+#endif
                     w.ng = make_uint2(root, (1u << r.oct) | (1u << 8));
                     cn = ct = 0;
                 } else {
@@ -176,11 +183,17 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
                 const int k = g - __shfl_sync(FULL_MASK, excl, o);
                 const uint32_t om = __shfl_sync(FULL_MASK, tmask, o);
                 const uint32_t ob = __shfl_sync(FULL_MASK, tri_base, o);
+#if RTB_RAY_SMEM
+                const float4 ro = s_ray[0][wbase + o], rd = s_ray[1][wbase + o];
+                const float ox = ro.x, oy = ro.y, oz = ro.z, tmn = ro.w;
+                const float dx = rd.x, dy = rd.y, dz = rd.z, tmx = rd.w;
+#else
                 const float ox = __shfl_sync(FULL_MASK, r.ox, o), oy = __shfl_sync(FULL_MASK, r.oy, o),
                             oz = __shfl_sync(FULL_MASK, r.oz, o);
                 const float dx = __shfl_sync(FULL_MASK, r.dx, o), dy = __shfl_sync(FULL_MASK, r.dy, o),
                             dz = __shfl_sync(FULL_MASK, r.dz, o);
                 const float tmn = __shfl_sync(FULL_MASK, r.tmin, o), tmx = __shfl_sync(FULL_MASK, r.tmax, o);
+#endif
                 unsigned long long key = ~0ull;
                 float u = 0.f, v = 0.f;
                 if (g < total) {
