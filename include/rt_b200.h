@@ -226,6 +226,50 @@ void rtPT_destroy(RtPathTracer_t pt);
  * up[3], tan(vfov/2), aspect (14 floats). */
 int rtPT_cameraBasis(const RtCamera* cam, int width, int height, float* out14);
 
+/* ---- Geometry from the application's buffers, refit, blobs ---------------
+ * Survey "next" rows: the reference layer reads every BLAS's vertex and index
+ * buffers back to the host and rebuilds a triangle soup there
+ * (layer/VkLayer_CudaRT.cpp:2961-2981, 3087-3125); refit and a versioned BVH
+ * blob have no counterpart in the reference. */
+#define RT_VERTEX_FLOAT3 0   /* 3 x fp32 per vertex (VK_FORMAT_R32G32B32_SFLOAT) */
+#define RT_VERTEX_HALF3 1    /* 3 x fp16 per vertex (R16G16B16[A16]_SFLOAT) */
+#define RT_INDEX_NONE 0      /* triangle p uses vertices 3p, 3p+1, 3p+2 */
+#define RT_INDEX_UINT16 1
+#define RT_INDEX_UINT32 2
+typedef struct {
+    const void* d_vertices;   /* device address of vertex 0 */
+    uint64_t vertex_stride;   /* bytes from one vertex to the next */
+    int vertex_format;        /* RT_VERTEX_* */
+    int max_vertex;           /* highest vertex index the triangles may use */
+    const void* d_indices;    /* device index buffer, or NULL with RT_INDEX_NONE */
+    int index_type;           /* RT_INDEX_* */
+    int num_triangles;
+    const float* transform;   /* host 3x4 row-major object transform, or NULL */
+} RtGeometry;
+
+/* Builds a BLAS from num_geoms geometries (triangles of all geometries in
+ * order; primitive ids count across them).  Triangles are gathered on the
+ * device; an index above max_vertex is an error, never a read past the
+ * buffer.  NULL on failure. */
+CudaBVH_t cudaBVH_buildGeometries(const RtGeometry* geoms, int num_geoms, void* stream);
+
+/* Refit after the vertices moved: same triangle count and order, new
+ * positions (device CudaTri array, or the geometries as above).  Keeps the
+ * tree's topology and recomputes every box; a TLAS over this BLAS must be
+ * rebuilt afterwards (its instance boxes change).  Must not overlap traces
+ * of the same handle.  RT_OK or an error. */
+int cudaBVH_refit(CudaBVH_t bvh, const CudaTri* d_tris, void* stream);
+int cudaBVH_refitGeometries(CudaBVH_t bvh, const RtGeometry* geoms, int num_geoms, void* stream);
+
+/* Versioned, checksummed host blob of a BLAS (input triangles, binary BVH,
+ * 8-wide nodes, triangle records).  buf == NULL: *size receives the bytes
+ * needed.  RT_ERR_CAPACITY if capacity is too small. */
+int cudaBVH_serialize(CudaBVH_t bvh, void* buf, uint64_t capacity, uint64_t* size);
+/* Loads a blob (no rebuild): NULL with an error for a wrong magic or
+ * version, a truncated or corrupted blob (checksum), or a structure that
+ * fails validation. */
+CudaBVH_t cudaBVH_deserialize(const void* buf, uint64_t size);
+
 /* ---- Served form: a request loop over scenes resident in HBM ------------
  * No counterpart in the reference (its layer calls one synchronous trace per
  * ray batch, layer/cuda_bvh_backend.cu:526-598).  Scenes are copied into one

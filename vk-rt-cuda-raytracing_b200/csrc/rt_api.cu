@@ -403,6 +403,11 @@ AsyncTracer g_async;
 }  // namespace
 
 namespace rtb {
+bool build_handle(CudaBVHHandle* h, cudaStream_t s) { return build_into(h, s); }
+CudaBVHHandle* create_handle(int n) { return new_handle(n); }
+}  // namespace rtb
+
+namespace rtb {
 // Host check of an 8-wide structure: every child index, triangle range and
 // grid exponent in bounds, nodes numbered after their parents (acyclic),
 // every leaf item referenced exactly once, depth within the stack bound.

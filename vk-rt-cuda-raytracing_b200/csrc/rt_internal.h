@@ -168,6 +168,11 @@ struct CudaTLASHandle {
 };
 
 namespace rtb {
+// A new handle for n triangles (h->tris9 not yet allocated), and the build of
+// a handle whose device triangles h->tris9 are in place (BVH2, 8-wide
+// collapse, statistics, per-call scratch); false with the error set.
+CudaBVHHandle* create_handle(int n);
+bool build_handle(CudaBVHHandle* h, cudaStream_t s);
 // Two-level trace; n_dev (optional) supplies the ray count from device memory.
 int launch_trace_tlas(const CudaTLASHandle* t, const RtRay* rays, int n, const int* n_dev, RtHit* hits,
                       int32_t* inst_out, uint8_t* occ, int* work, int* status, cudaStream_t s);

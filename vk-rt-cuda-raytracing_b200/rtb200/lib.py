@@ -56,6 +56,16 @@ class RtPTStats(C.Structure):
                 ("light_area", C.c_double)]
 
 
+class RtGeometry(C.Structure):
+    _fields_ = [("d_vertices", C.c_void_p), ("vertex_stride", C.c_uint64), ("vertex_format", C.c_int),
+                ("max_vertex", C.c_int), ("d_indices", C.c_void_p), ("index_type", C.c_int),
+                ("num_triangles", C.c_int), ("transform", C.c_void_p)]
+
+
+RT_VERTEX_FLOAT3, RT_VERTEX_HALF3 = 0, 1
+RT_INDEX_NONE, RT_INDEX_UINT16, RT_INDEX_UINT32 = 0, 1, 2
+
+
 class RtServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("pool_bytes", C.c_uint64), ("max_inflight", C.c_int),
                 ("wave_rays", C.c_int), ("chunk_rays", C.c_int), ("max_waves", C.c_int), ("prefetch_rays", C.c_int)]
@@ -139,6 +149,11 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "rtBatch_autotune": (i32, [vp, vp, vp, i32, vp, vp, C.POINTER(i32), C.POINTER(i32)]),
         "rtBatch_setTuning": (i32, [vp, i32, i32]),
         "rtBatch_getInfo": (i32, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(f32)]),
+        "cudaBVH_buildGeometries": (vp, [C.POINTER(RtGeometry), i32, vp]),
+        "cudaBVH_refit": (i32, [vp, vp, vp]),
+        "cudaBVH_refitGeometries": (i32, [vp, C.POINTER(RtGeometry), i32, vp]),
+        "cudaBVH_serialize": (i32, [vp, vp, C.c_uint64, C.POINTER(C.c_uint64)]),
+        "cudaBVH_deserialize": (vp, [vp, C.c_uint64]),
         "rtServer_create": (vp, [C.POINTER(RtServerConfig)]),
         "rtServer_addScene": (i32, [vp, vp]),
         "rtServer_submit": (i32, [vp, i32, i32, vp, i32, vp, C.POINTER(C.c_uint64)]),
@@ -200,6 +215,37 @@ class BVH:
             self.h = L.cudaBVH_build(tris.ctypes.data, tris.shape[0])
         if not self.h:
             raise RtError(f"build failed: {last_error()}")
+
+    @classmethod
+    def from_geometries(cls, geoms, stream=None) -> "BVH":
+        """geoms: list of RtGeometry (device pointers inside)."""
+        arr = (RtGeometry * len(geoms))(*geoms)
+        h = load().cudaBVH_buildGeometries(arr, len(geoms), _stream(stream))
+        if not h:
+            raise RtError(f"cudaBVH_buildGeometries failed: {last_error()}")
+        return cls(handle=h)
+
+    def refit(self, d_tris, stream=None):
+        _check(load().cudaBVH_refit(self.h, _ptr(d_tris), _stream(stream)), "cudaBVH_refit")
+
+    def refit_geometries(self, geoms, stream=None):
+        arr = (RtGeometry * len(geoms))(*geoms)
+        _check(load().cudaBVH_refitGeometries(self.h, arr, len(geoms), _stream(stream)), "cudaBVH_refitGeometries")
+
+    def serialize(self) -> bytes:
+        L = load()
+        n = C.c_uint64()
+        _check(L.cudaBVH_serialize(self.h, None, 0, C.byref(n)), "cudaBVH_serialize")
+        buf = (C.c_ubyte * n.value)()
+        _check(L.cudaBVH_serialize(self.h, buf, n.value, C.byref(n)), "cudaBVH_serialize")
+        return bytes(buf)
+
+    @classmethod
+    def deserialize(cls, blob: bytes) -> "BVH":
+        h = load().cudaBVH_deserialize(blob, len(blob))
+        if not h:
+            raise RtError(f"cudaBVH_deserialize failed: {last_error()}")
+        return cls(handle=h)
 
     @classmethod
     def from_aabbs(cls, aabbs: np.ndarray) -> "BVH":
