@@ -412,7 +412,7 @@ bool RtServerHandle::launch_wave(WaveSlot* w) {
     if (ok && nc) ok = launch_trace_wave(nd, tr, w->d_segs.p, nc, (int)tc, false, w->work.p, w->status.p,
                                          TRACE_MINB, s) == RT_OK;
     if (ok && na) ok = launch_trace_wave(nd, tr, w->d_segs.p + kMaxSeg, na, (int)ta, true, w->work.p + 1,
-                                         w->status.p, TRACE_MINB, s) == RT_OK;
+                                         w->status.p, TRACE_MINB_ANY, s) == RT_OK;
     ok = ok && RT_CUDA(cudaMemcpyAsync(w->h_status, w->status.p, sizeof(int), cudaMemcpyDeviceToHost, s)) &&
          RT_CUDA(cudaEventRecord(w->traced, s)) && RT_CUDA(cudaStreamWaitEvent(copy_out, w->traced, 0));
     for (const Chunk& c : w->chunks) {

@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
                 float u = 0.f, v = 0.f;
                 int prim = 0;
                 if (g < total) {
-                    const int rec = (int)ob + (int)__fns(om, 0, k + 1);
+                    const int rec = (int)ob + (int)nth_set_bit(om, (uint32_t)k);
                     const float4* tp = reinterpret_cast<const float4*>(optr) + (size_t)rec * 3;
                     const float4 A = __ldg(tp), B = __ldg(tp + 1), Cc = __ldg(tp + 2);
                     float t;

@@ -50,7 +50,7 @@ __device__ __forceinline__ void* ldg_ptr(const void* p) {
 //   g with segs[g].first <= i, is read from segs[g].rays[i - first], starts
 //   at node segs[g].root and is written to segs[g].out[i - first].
 template <bool ANY, bool COUNT, int MODE, int NITERS>
-__global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
+__global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
     k_trace_blas(const uint4* __restrict__ nodes, const float4* __restrict__ tris, const RtRay* __restrict__ rays,
                  int n, RtHit* __restrict__ hits, uint8_t* __restrict__ occ, uint32_t* __restrict__ counts,
                  int* __restrict__ work, int* __restrict__ status, const int* __restrict__ ray_off,
@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(TRACE_T, TRACE_MINB)
                 unsigned long long key = ~0ull;
                 float u = 0.f, v = 0.f;
                 if (g < total) {
-                    const int rec = (int)ob + (int)__fns(om, 0, k + 1);
+                    const int rec = (int)ob + (int)nth_set_bit(om, (uint32_t)k);
                     const float4* tp = tris + (size_t)rec * 3;
                     const float4 A = __ldg(tp), B = __ldg(tp + 1), Cc = __ldg(tp + 2);
                     float t;
@@ -310,7 +310,7 @@ int launch_trace_multi(const Bvh8Device& b, const RtRay* rays, int n, const int*
                        int node_iters, cudaStream_t s) {
     const uint4* nodes = reinterpret_cast<const uint4*>(b.nodes.p);
     const float4* tris = reinterpret_cast<const float4*>(b.tris.p);
-    const int g = std::max(1, std::min(ctas_per_sm, TRACE_MINB)) * num_sms();
+    const int g = std::max(1, std::min(ctas_per_sm, occ ? TRACE_MINB_ANY : TRACE_MINB)) * num_sms();
     if (occ) {
         if (node_iters == 1)
             k_trace_blas<true, false, MODE_BATCH, 1><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
@@ -332,7 +332,7 @@ int launch_trace_multi(const Bvh8Device& b, const RtRay* rays, int n, const int*
 // One shared wavefront: `n` rays over `nseg` segments, all of one kind.
 int launch_trace_wave(const uint4* nodes, const float4* tris, const WaveSeg* segs, int nseg, int n, bool any,
                       int* work, int* status, int ctas_per_sm, cudaStream_t s) {
-    const int g = std::max(1, std::min(ctas_per_sm, TRACE_MINB)) * num_sms();
+    const int g = std::max(1, std::min(ctas_per_sm, any ? TRACE_MINB_ANY : TRACE_MINB)) * num_sms();
     if (any)
         k_trace_blas<true, false, MODE_WAVE, 2><<<g, TRACE_T, 0, s>>>(nodes, tris, nullptr, n, nullptr, nullptr,
                                                                      nullptr, work, status, nullptr, nullptr, nseg,

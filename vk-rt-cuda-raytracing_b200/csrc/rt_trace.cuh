@@ -17,6 +17,10 @@ constexpr unsigned FULL_MASK = 0xFFFFFFFFu;
 #ifndef RTB_TRACE_MINB
 #define RTB_TRACE_MINB 8
 #endif
+// any hit keeps less state: 9 CTAs per SM (56 registers) measured +1.9 %
+#ifndef RTB_TRACE_MINB_ANY
+#define RTB_TRACE_MINB_ANY 9
+#endif
 #ifndef RTB_SSTACK
 #define RTB_SSTACK 8
 #endif
@@ -63,6 +67,7 @@ __device__ __forceinline__ float min3f(float a, float b, float c) {
 }
 constexpr int TRACE_T = 128;               // threads per persistent CTA
 constexpr int TRACE_MINB = RTB_TRACE_MINB; // CTAs per SM the register budget must allow
+constexpr int TRACE_MINB_ANY = RTB_TRACE_MINB_ANY;
 constexpr int SSTACK = RTB_SSTACK;         // stack entries per thread in shared memory
 constexpr int LSTACK = 64 - SSTACK;        // further entries in local memory (64 total)
 constexpr int SSTACK_TOTAL = SSTACK + LSTACK;
@@ -101,6 +106,26 @@ __device__ __forceinline__ Ray make_ray(float4 a, float4 b) {
 __device__ __forceinline__ Ray load_ray(const RtRay* rays, int i) {
     const float4* p = reinterpret_cast<const float4*>(rays + i);
     return make_ray(__ldg(p), __ldg(p + 1));
+}
+
+// Position of the k-th (0-based) set bit of m (k < popc(m)).  A hit leaf's
+// triangles are one contiguous run of bits, so the common case is
+// ffs - 1 + k; otherwise a five-step popcount search.  Measured +3 % over
+// __fns on the incoherent workload.
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t k) {
+    const uint32_t lo = __ffs(m) - 1, run = m >> lo;
+    if ((run & (run + 1)) == 0) return lo + k;
+    uint32_t pos = 0, c;
+    c = __popc(m & 0xFFFFu);
+    if (k >= c) { k -= c; pos += 16; m >>= 16; }
+    c = __popc(m & 0xFFu);
+    if (k >= c) { k -= c; pos += 8; m >>= 8; }
+    c = __popc(m & 0xFu);
+    if (k >= c) { k -= c; pos += 4; m >>= 4; }
+    c = __popc(m & 0x3u);
+    if (k >= c) { k -= c; pos += 2; m >>= 2; }
+    if (k >= (m & 1u)) pos += 1;
+    return pos;
 }
 
 // Stack of node groups: x = child base, y = hit mask (8 bits, near-to-far
