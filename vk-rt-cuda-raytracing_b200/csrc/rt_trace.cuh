@@ -128,6 +128,14 @@ __device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t k) {
     return pos;
 }
 
+// A mask of `width` bits starting at bit `start` in one instruction (PTX
+// bmsk): a leaf's triangle bits.  width 0 (an empty slot) gives 0.
+__device__ __forceinline__ uint32_t bit_mask(uint32_t start, uint32_t width) {
+    uint32_t r;
+    asm("bmsk.clamp.b32 %0, %1, %2;" : "=r"(r) : "r"(start), "r"(width));
+    return r;
+}
+
 // Stack of node groups: x = child base, y = hit mask (8 bits, near-to-far
 // order) | inner mask << 8 | flags << 16.
 struct Walk {
@@ -228,14 +236,13 @@ __device__ __forceinline__ void visit_node(const uint4* __restrict__ np, const R
         const uint32_t inner = (imask >> s) & 1u;
         const uint32_t hb = hit ? 1u : 0u;
         nh |= (hb & inner) << ((uint32_t)s ^ r.oct);
-        const uint32_t leafm = ((1u << (meta >> 5)) - 1u) << (meta & 31u);
-        th |= leafm & (0u - (hb & (inner ^ 1u)));
+        th |= bit_mask(meta & 31u, meta >> 5) & (0u - (hb & (inner ^ 1u)));
 #else
         if (hit) {
             if ((imask >> s) & 1u) {
                 nh |= 1u << ((uint32_t)s ^ r.oct);
-            } else if (meta) {
-                th |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
+            } else {
+                th |= bit_mask(meta & 31u, meta >> 5);  // empty slot: meta 0, no bits
             }
         }
 #endif
