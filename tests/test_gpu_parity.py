@@ -223,7 +223,7 @@ def test_build_is_deterministic_and_sane(cuda):
     tris = scenes.scene_meshes(2, 120_000)
     a, b = lib.BVH(tris), lib.BVH(tris)
     sa = a.stats()
-    assert sa["num_tris"] == tris.shape[0] and sa["bins"] == 32 and sa["max_leaf"] == 4
+    assert sa["num_tris"] == tris.shape[0] and sa["bins"] == 32 and sa["max_leaf"] == 2
     assert 1 <= sa["depth"] <= 64
     la, lb = a.layout(), b.layout()
     assert la[1] == lb[1] and la[3] == lb[3] == tris.shape[0]

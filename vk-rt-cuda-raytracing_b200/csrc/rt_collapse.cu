@@ -1,15 +1,25 @@
 // rt_collapse.cu -- BVH2 -> compressed 8-wide nodes (top-down, one thread
 // per output node, one launch pair per level).
 //
-// For every 8-wide node: start from the binary node's two children and
+// Which binary nodes become the children of an 8-wide node is decided one
+// of two ways.  Greedy: start from the binary node's two children and
 // repeatedly open the inner child with the largest surface area until there
-// are 8 children or only leaves remain; assign the children to octant slots
+// are 8 children or only leaves remain.  SAH-optimal (the dynamic program of
+// Ylitie, Karras, Laine, HPG 2017): a bottom-up pass computes, for every
+// binary node n and i = 1..8, the least cost of covering n's triangles with
+// at most i subtrees (a subtree is an 8-wide node, cost c_node * area, or
+// one leaf of at most p_max triangles, cost c_prim * area * count), and the
+// top-down pass expands every 8-wide node's children along the recorded
+// choices; small subtrees can thus become one leaf and nodes come out
+// fuller.  Either way: assign the children to octant slots
 // (slot s takes the child nearest along the direction with sign bits s,
 // greedy on the projected-centroid cost); quantise each child box to 8 bits
 // per plane, rounded outward, on the grid p + q * 2^e; write the triangle
 // records of the leaf children contiguously in slot order.
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "rt_internal.h"
@@ -20,11 +30,180 @@ struct Gather {
     int kid[8];  // binary node id per slot, -1 = empty
 };
 
+// Per binary node, for the SAH-optimal collapse.
+struct DPNode {
+    float c[8];          // c[i]: least cost of covering the subtree with at most i + 1 subtrees
+    unsigned char d[8];  // d[0]: 1 if the subtree is best one leaf; d[i], i >= 1: split k for c[i], 0 = as c[i-1]
+    unsigned char s8;    // split of the 8 slots between the children when the node is an 8-wide node
+    unsigned char pad[3];
+    int first, count;    // triangle range in the permutation (first -1: not contiguous)
+};
+
 __device__ __forceinline__ float node_area(const Node2& n) {
     const float dx = n.hi[0] - n.lo[0], dy = n.hi[1] - n.lo[1], dz = n.hi[2] - n.lo[2];
     return dx * dy + dy * dz + dz * dx;
 }
 __device__ __forceinline__ bool is_leaf2(const Node2& n) { return n.b < 0; }
+
+__global__ void k_dp_parents(const Node2* __restrict__ nodes, int slots, int* __restrict__ parent) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= slots) return;
+    const Node2 nd = nodes[i];
+    if (nd.b > 0) {  // inner node (unused reserved slots have b == 0)
+        parent[nd.a] = i;
+        parent[nd.b] = i;
+    }
+}
+
+// Bottom-up: one thread per binary leaf walks toward its root; at every node
+// the second child to arrive fills the node's table (fence before the
+// arrival counter, L2 loads after it).  Depth is bounded by the builder.
+__global__ void k_dp(const Node2* __restrict__ nodes, int slots, const int* __restrict__ parent,
+                     int* __restrict__ arrive, DPNode* __restrict__ dp, float c_node, float c_prim, int p_max,
+                     int* __restrict__ status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= slots) return;
+    const Node2 lf = nodes[i];
+    if (lf.b >= 0) return;  // leaves only
+    {
+        DPNode t;
+        const float v = c_prim * node_area(lf) * (float)(-lf.b);
+        for (int k = 0; k < 8; k++) {
+            t.c[k] = v;
+            t.d[k] = 0;
+        }
+        t.d[0] = 1;
+        t.s8 = 0;
+        t.first = lf.a;
+        t.count = -lf.b;
+        dp[i] = t;
+    }
+    int cur = i;
+    for (int step = 0;; step++) {
+        const int par = parent[cur];
+        if (par < 0) return;
+        if (step >= 256) {  // deeper than any tree the builder makes: give up (greedy collapse instead)
+            atomicOr(status, 1);
+            return;
+        }
+        __threadfence();
+        if (atomicAdd(&arrive[par], 1) == 0) return;
+        __threadfence();
+        const Node2 n = nodes[par];
+        float cl[8], cr[8];
+        for (int k = 0; k < 8; k++) {
+            cl[k] = __ldcg(&dp[n.a].c[k]);
+            cr[k] = __ldcg(&dp[n.b].c[k]);
+        }
+        const int fl = __ldcg(&dp[n.a].first), nl = __ldcg(&dp[n.a].count);
+        const int fr = __ldcg(&dp[n.b].first), nr = __ldcg(&dp[n.b].count);
+        DPNode t;
+        t.count = nl + nr;
+        t.first = (fl >= 0 && fr >= 0 && (fl + nl == fr || fr + nr == fl)) ? min(fl, fr) : -1;
+        float D[9];
+        unsigned char K[9];
+        for (int j = 2; j <= 8; j++) {
+            float best = INFINITY;
+            unsigned char bk = 1;
+            for (int k = 1; k < j; k++) {
+                const float v = cl[k - 1] + cr[j - k - 1];
+                if (v < best) { best = v; bk = (unsigned char)k; }
+            }
+            D[j] = best;
+            K[j] = bk;
+        }
+        const float a = node_area(n);
+        const float c_int = c_node * a + D[8];
+        const float c_leaf = (t.first >= 0 && t.count <= p_max) ? c_prim * a * (float)t.count : INFINITY;
+        t.c[0] = fminf(c_int, c_leaf);
+        t.d[0] = c_leaf <= c_int ? 1 : 0;
+        t.s8 = K[8];
+        for (int k = 1; k < 8; k++) {
+            if (D[k + 1] < t.c[k - 1]) {
+                t.c[k] = D[k + 1];
+                t.d[k] = K[k + 1];
+            } else {
+                t.c[k] = t.c[k - 1];
+                t.d[k] = 0;
+            }
+        }
+        dp[par] = t;
+        cur = par;
+    }
+}
+
+__global__ void k_gather_dp(const Node2* __restrict__ nodes, const DPNode* __restrict__ dp,
+                            const int* __restrict__ level, int L, Gather* __restrict__ out,
+                            int* __restrict__ n_inner, int* __restrict__ n_items) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L) return;
+    const int b2 = level[i];
+    const Node2 me = nodes[b2];
+    int kid[8];
+    int nk = 0;
+    if (is_leaf2(me)) {
+        kid[nk++] = b2;
+    } else {
+        // expand the two children under the 8-slot budget along the recorded splits
+        int sx[16], sj[16], sp = 0;
+        const int k8 = dp[b2].s8;
+        sx[sp] = me.b; sj[sp++] = 8 - k8;
+        sx[sp] = me.a; sj[sp++] = k8;
+        while (sp > 0 && nk < 8) {
+            const int x = sx[--sp];
+            int j = sj[sp];
+            while (j > 1 && dp[x].d[j - 1] == 0) j--;
+            if (j == 1 || sp > 13) {
+                kid[nk++] = x;
+            } else {
+                const int k = dp[x].d[j - 1];
+                const Node2 c = nodes[x];
+                sx[sp] = c.b; sj[sp++] = j - k;
+                sx[sp] = c.a; sj[sp++] = k;
+            }
+        }
+    }
+    // octant slot assignment
+    float pc[3];
+    for (int a = 0; a < 3; a++) pc[a] = (me.lo[a] + me.hi[a]) * 0.5f;
+    float cost[8][8];
+    for (int k = 0; k < nk; k++) {
+        const Node2 c = nodes[kid[k]];
+        float d[3];
+        for (int a = 0; a < 3; a++) d[a] = (c.lo[a] + c.hi[a]) * 0.5f - pc[a];
+        for (int s = 0; s < 8; s++)
+            cost[k][s] = ((s & 1) ? -d[0] : d[0]) + ((s & 2) ? -d[1] : d[1]) + ((s & 4) ? -d[2] : d[2]);
+    }
+    int slot_kid[8];
+    for (int s = 0; s < 8; s++) slot_kid[s] = -1;
+    unsigned used_k = 0, used_s = 0;
+    for (int r = 0; r < nk; r++) {
+        float bc = FLT_MAX;
+        int bk = -1, bs = -1;
+        for (int k = 0; k < nk; k++) {
+            if (used_k & (1u << k)) continue;
+            for (int s = 0; s < 8; s++) {
+                if (used_s & (1u << s)) continue;
+                if (cost[k][s] < bc || bk < 0) { bc = cost[k][s]; bk = k; bs = s; }
+            }
+        }
+        used_k |= 1u << bk;
+        used_s |= 1u << bs;
+        slot_kid[bs] = kid[bk];
+    }
+    Gather g;
+    int ni = 0, nt = 0;
+    for (int s = 0; s < 8; s++) {
+        g.kid[s] = slot_kid[s];
+        if (slot_kid[s] < 0) continue;
+        const int x = slot_kid[s];
+        if (is_leaf2(nodes[x]) || dp[x].d[0]) nt += dp[x].count;
+        else ni++;
+    }
+    out[i] = g;
+    n_inner[i] = ni;
+    n_items[i] = nt;
+}
 
 __global__ void k_gather(const Node2* __restrict__ nodes, const int* __restrict__ level, int L,
                          Gather* __restrict__ out, int* __restrict__ n_inner, int* __restrict__ n_items) {
@@ -112,7 +291,7 @@ __global__ void k_emit(const Node2* __restrict__ nodes, const int* __restrict__ 
                        const int* __restrict__ item_off, int child_base0, int item_base0,
                        const int* __restrict__ perm, const float* __restrict__ tris9,
                        Bvh8Node* __restrict__ out_nodes, int out_base, TriRec* __restrict__ out_tris,
-                       int* __restrict__ out_ids, int* __restrict__ next_level) {
+                       int* __restrict__ out_ids, int* __restrict__ next_level, const DPNode* __restrict__ dp) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= L) return;
     const Gather g = gat[i];
@@ -165,11 +344,15 @@ __global__ void k_emit(const Node2* __restrict__ nodes, const int* __restrict__ 
             qhi[a][s >> 2] |= qh << ((s & 3) * 8);
         }
         uint32_t m;
-        if (is_leaf2(c)) {
-            const int cnt = -c.b;
+        // a leaf child is a binary leaf, or with the SAH-optimal collapse a
+        // subtree chosen to be one leaf (its triangles are contiguous)
+        const bool as_leaf = is_leaf2(c) || (dp && dp[k].d[0]);
+        if (as_leaf) {
+            const int cnt = dp ? dp[k].count : -c.b;
+            const int first = dp ? dp[k].first : c.a;
             m = ((uint32_t)cnt << 5) | (uint32_t)offset;
             for (int j = 0; j < cnt; j++) {
-                const int prim = perm[c.a + j];
+                const int prim = perm[first + j];
                 const int dst = tri_base + offset + j;
                 if (tris9) {
                     const float* t = tris9 + (size_t)prim * 9;
@@ -227,11 +410,48 @@ bool collapse_bvh8(const Bvh2Device& b2, const float* d_tris9, Bvh8Device& out, 
             !RT_CUDA(cudaStreamSynchronize(s)))
             return false;
     }
+    // SAH-optimal collapse for triangle BLASes unless RTB200_COLLAPSE=greedy
+    // (TLAS leaves stay single instances: greedy)
+    static const int mode = [] {
+        const char* e = getenv("RTB200_COLLAPSE");
+        return e && !strcmp(e, "greedy") ? 0 : 1;
+    }();
+    DevBuf<DPNode> dp;
+    if (d_tris9 && mode == 1) {
+        static const float c_prim = [] {
+            const char* e = getenv("RTB200_DP_CPRIM");
+            return e ? (float)atof(e) : 0.5f;
+        }();
+        static const int p_max = [] {
+            const char* e = getenv("RTB200_DP_PMAX");
+            const int v = e ? atoi(e) : 4;
+            return v < 1 ? 1 : (v > 4 ? 4 : v);
+        }();
+        const int slots = b2.num_nodes;
+        DevBuf<int> parent, arrive, st;
+        if (!dp.alloc(slots) || !parent.alloc(slots) || !arrive.alloc(slots) || !st.alloc(1)) return false;
+        int h_st = 0;
+        if (!RT_CUDA(cudaMemsetAsync(parent.p, 0xFF, sizeof(int) * (size_t)slots, s)) ||
+            !RT_CUDA(cudaMemsetAsync(arrive.p, 0, sizeof(int) * (size_t)slots, s)) ||
+            !RT_CUDA(cudaMemsetAsync(st.p, 0, sizeof(int), s)))
+            return false;
+        k_dp_parents<<<(slots + 255) / 256, 256, 0, s>>>(b2.nodes.p, slots, parent.p);
+        k_dp<<<(slots + 255) / 256, 256, 0, s>>>(b2.nodes.p, slots, parent.p, arrive.p, dp.p, 1.0f, c_prim, p_max,
+                                                 st.p);
+        if (!RT_CUDA(cudaGetLastError()) ||
+            !RT_CUDA(cudaMemcpyAsync(&h_st, st.p, sizeof(int), cudaMemcpyDeviceToHost, s)) ||
+            !RT_CUDA(cudaStreamSynchronize(s)))
+            return false;
+        if (h_st) dp.release();  // too deep: greedy collapse
+    }
     int L = R, level_base = 0, items = 0, depth = 0;
     int* cur = lvl_a.p;
     int* nxt = lvl_b.p;
     while (L > 0) {
-        k_gather<<<(L + 127) / 128, 128, 0, s>>>(b2.nodes.p, cur, L, gat.p, n_inner.p, n_items.p);
+        if (dp.p)
+            k_gather_dp<<<(L + 127) / 128, 128, 0, s>>>(b2.nodes.p, dp.p, cur, L, gat.p, n_inner.p, n_items.p);
+        else
+            k_gather<<<(L + 127) / 128, 128, 0, s>>>(b2.nodes.p, cur, L, gat.p, n_inner.p, n_items.p);
         if (!scan_exclusive(n_inner.p, inner_off.p, L, tot.p, s)) return false;
         if (!scan_exclusive(n_items.p, item_off.p, L, tot.p + 1, s)) return false;
         int h[2];
@@ -244,7 +464,7 @@ bool collapse_bvh8(const Bvh2Device& b2, const float* d_tris9, Bvh8Device& out, 
         }
         k_emit<<<(L + 127) / 128, 128, 0, s>>>(b2.nodes.p, cur, L, gat.p, inner_off.p, item_off.p, child_base, items,
                                                b2.perm.p, d_tris9, out.nodes.p, level_base, out.tris.p,
-                                               out.leaf_ids.p, nxt);
+                                               out.leaf_ids.p, nxt, dp.p);
         level_base = child_base;
         items += h[1];
         L = h[0];

@@ -61,7 +61,8 @@ struct DevBuf {
 
 // ---- build configuration ----
 struct BuildConfig {
-    int max_leaf = 4;        // triangles per BVH2 leaf (1..kMaxLeafTris)
+    int max_leaf = 2;        // triangles per BVH2 leaf (1..kMaxLeafTris); the 8-wide
+                             // collapse may merge small subtrees into leaves of up to 4
     int small_task = 1024;   // tasks at or below this size finish in one CTA
     int max_sah_depth = 48;  // deeper tasks fall back to median splits
 };
