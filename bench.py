@@ -542,7 +542,7 @@ def run_batched(args):
         return torch.cuda.Event(enable_timing=True)
 
     # --- ours: one build, autotune once, graph replays
-    b = lib.Batch(tris)
+    b = lib.Batch(all_tris=allt, tri_offsets=tri_off)
     info = b.info()
     ctas, iters = b.autotune(d_rays, d_off, nr, d_hits, stream=stream)
     b.graph(d_rays, d_off, nr, d_hits, stream=stream)
@@ -553,7 +553,7 @@ def run_batched(args):
         flush.zero_()
         torch.cuda.synchronize()
         h0 = time.perf_counter()
-        b = lib.Batch(tris)
+        b = lib.Batch(all_tris=allt, tri_offsets=tri_off)
         torch.cuda.synchronize()
         h1 = time.perf_counter()
         b.set_tuning(ctas, iters)

@@ -468,15 +468,20 @@ class PathTracer:
 class Batch:
     """rtBatch_*: many scenes built and traced together."""
 
-    def __init__(self, scenes_tris, stream=None):
+    def __init__(self, scenes_tris=None, stream=None, *, all_tris=None, tri_offsets=None):
+        """scenes_tris: list of (n_i, 9) arrays; or all_tris (sum n_i, 9) with
+        tri_offsets (num_scenes + 1) already concatenated."""
         L = load()
-        tris = [np.ascontiguousarray(t, np.float32).reshape(-1, 9) for t in scenes_tris]
-        self.tri_off = np.concatenate([[0], np.cumsum([t.shape[0] for t in tris])]).astype(np.int32)
-        allt = np.ascontiguousarray(np.concatenate(tris))
-        self.h = L.rtBatch_build(allt.ctypes.data, self.tri_off.ctypes.data, len(tris), _stream(stream))
+        if all_tris is None:
+            tris = [np.ascontiguousarray(t, np.float32).reshape(-1, 9) for t in scenes_tris]
+            tri_offsets = np.concatenate([[0], np.cumsum([t.shape[0] for t in tris])])
+            all_tris = np.concatenate(tris)
+        self.tri_off = np.ascontiguousarray(tri_offsets, np.int32)
+        allt = np.ascontiguousarray(all_tris, np.float32).reshape(-1, 9)
+        self.h = L.rtBatch_build(allt.ctypes.data, self.tri_off.ctypes.data, len(self.tri_off) - 1, _stream(stream))
         if not self.h:
             raise RtError(f"rtBatch_build failed: {last_error()}")
-        self.num_scenes = len(tris)
+        self.num_scenes = len(self.tri_off) - 1
 
     def info(self):
         a, b, c = C.c_int(), C.c_int(), C.c_float()
