@@ -528,7 +528,13 @@ def run_batched(args):
     tris, rays, off = scenes.batched_workload()
     ntri = np.array([t.shape[0] for t in tris])
     tri_off = np.concatenate([[0], np.cumsum(ntri)]).astype(np.int32)
-    allt = np.ascontiguousarray(np.concatenate(tris))
+    # the triangles sit in pinned host memory, read by both arms (pageable
+    # copies on this path ran 10 GB/s with second-long outliers)
+    nbytes = int(ntri.sum()) * 36
+    pinned = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    allt = pinned.numpy().view(np.float32).reshape(-1, 9)
+    np.concatenate(tris, out=allt)
+    tris = [allt[tri_off[i]:tri_off[i + 1]] for i in range(len(tris))]
     nr = int(rays.shape[0])
     log(f"batched workload: {len(tris)} scenes, {ntri.sum()} tris, {nr} rays in {time.time() - t0:.1f}s")
     stream = torch.cuda.current_stream()
@@ -599,7 +605,7 @@ def run_batched(args):
            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
            "config": {"workload": f"batched_256: 256 scenes of 1K-500K triangles ({int(ntri.sum())} total), "
                                   f"{nr} rays (4K-2M per scene, half primary, half diffuse), closest hit",
-                      "l2": "flushed between steps"},
+                      "l2": "flushed between steps", "host_tris": "pinned, shared by both arms"},
            "ours": {"build_ms": round(bo, 2), "trace_ms": round(to, 3), "trace_mrays_s": round(nr / to / 1e3, 1),
                     "device_build_ms": round(info["build_ms"], 2), "tuning": {"ctas_per_sm": ctas, "node_iters": iters},
                     "launches": "one build pipeline for all scenes, one graph-captured trace launch"},

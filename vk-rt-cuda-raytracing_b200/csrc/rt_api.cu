@@ -51,6 +51,30 @@ int num_sms() {
     return n;
 }
 
+cudaMemPool_t scratch_pool() {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        const char* e = getenv("RTB200_POOL_KEEP_MB");
+        uint64_t keep = (uint64_t)(e ? std::max(0, atoi(e)) : 8192) << 20;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[dev] = pool;
+    }
+    return pools[dev];
+}
+
 constexpr unsigned kCounterRing = 1024;
 
 bool ensure_counters(DevBuf<int>& ring) {
@@ -81,17 +105,13 @@ using namespace rtb;
 
 namespace {
 
-BuildConfig default_config() {
-    BuildConfig c;
-    if (const char* e = getenv("RTB200_MAX_LEAF")) c.max_leaf = std::max(1, std::min(4, atoi(e)));
-    return c;
-}
+BuildConfig default_config() { return default_build_config(); }
 
 // Builds the handle from device triangles it already owns (h->tris9).
 bool build_into(CudaBVHHandle* h, cudaStream_t s) {
     const int n = h->num_tris;
-    DevBuf<float4> lo, hi;
-    if (!lo.alloc(n) || !hi.alloc(n)) return false;
+    TmpBuf<float4> lo, hi;
+    if (!lo.alloc(n, s) || !hi.alloc(n, s)) return false;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);

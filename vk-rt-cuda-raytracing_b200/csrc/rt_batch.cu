@@ -114,11 +114,11 @@ RtBatch_t rtBatch_build(const CudaTri* h_tris, const int* tri_offsets, int num_s
     b->num_tris = tri_offsets[num_scenes];
     b->tri_off.assign(tri_offsets, tri_offsets + num_scenes + 1);
     const int n = b->num_tris;
-    DevBuf<float4> lo, hi;
+    TmpBuf<float4> lo, hi;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    bool ok = b->tris9.alloc((size_t)n * 9) && b->d_tri_off.alloc(num_scenes + 1) && lo.alloc(n) && hi.alloc(n) &&
+    bool ok = b->tris9.alloc((size_t)n * 9) && b->d_tri_off.alloc(num_scenes + 1) && lo.alloc(n, s) && hi.alloc(n, s) &&
               b->work.alloc(2) && b->status.alloc(1) &&
               RT_CUDA(cudaMemcpyAsync(b->tris9.p, h_tris, sizeof(CudaTri) * (size_t)n, cudaMemcpyHostToDevice, s)) &&
               RT_CUDA(cudaMemcpyAsync(b->d_tri_off.p, tri_offsets, sizeof(int) * (num_scenes + 1),
@@ -127,7 +127,7 @@ RtBatch_t rtBatch_build(const CudaTri* h_tris, const int* tri_offsets, int num_s
     if (ok) {
         cudaEventRecord(e0, s);
         launch_tri_bounds(b->tris9.p, n, lo.p, hi.p, s);
-        BuildConfig cfg;
+        const BuildConfig cfg = default_build_config();
         ok = build_bvh2(lo.p, hi.p, n, cfg, b->bvh2, s, &b->tri_off) && collapse_bvh8(b->bvh2, b->tris9.p, b->bvh8, s);
         cudaEventRecord(e1, s);
         ok = ok && RT_CUDA(cudaEventSynchronize(e1));

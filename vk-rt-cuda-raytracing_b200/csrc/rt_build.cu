@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "rt_internal.h"
@@ -103,13 +104,12 @@ bool scan_exclusive(const int* d_in, int* d_out, int n, int* d_total, cudaStream
     if (tiles == 1) {
         k_scan_tiles<<<1, SCAN_T, 0, s>>>(d_in, d_out, n, nullptr);
     } else {
-        int *sums = nullptr, *offs = nullptr;
-        if (!RT_CUDA(cudaMallocAsync(&sums, sizeof(int) * tiles * 2, s))) return false;
-        offs = sums + tiles;
-        k_scan_tiles<<<tiles, SCAN_T, 0, s>>>(d_in, d_out, n, sums);
-        if (!scan_exclusive(sums, offs, tiles, nullptr, s)) return false;
+        TmpBuf<int> sums;
+        if (!sums.alloc((size_t)tiles * 2, s)) return false;
+        int* offs = sums.p + tiles;
+        k_scan_tiles<<<tiles, SCAN_T, 0, s>>>(d_in, d_out, n, sums.p);
+        if (!scan_exclusive(sums.p, offs, tiles, nullptr, s)) return false;
         k_scan_add<<<(n + 255) / 256, 256, 0, s>>>(d_out, n, offs);
-        cudaFreeAsync(sums, s);
     }
     if (d_total) k_scan_total<<<1, 1, 0, s>>>(d_in, d_out, n, d_total);
     return RT_CUDA(cudaGetLastError());
@@ -197,8 +197,13 @@ struct Chunk {
     int task, start, count, first;
 };
 
-// bins per task: [axis][bin] x {cnt, lo3, hi3, clo3, chi3} as ordered uints
-constexpr int BIN_WORDS = 13;
+// bins per task: [axis][bin] x {cnt, lo3, hi3} as ordered uints (the
+// children's centroid bounds are gathered by k_count_left instead)
+constexpr int BIN_WORDS = 7;
+constexpr int PART_IPT = CHUNK / CHUNK_T;  // 8 consecutive positions per thread
+__host__ __device__ __forceinline__ uint32_t bin_init(int w) {
+    return w == 0 ? 0u : (w <= 3 ? 0xFFFFFFFFu : 0u);  // cnt 0, lo: min (from max), hi: max (from 0)
+}
 constexpr int TASK_BIN_WORDS = 3 * kBins * BIN_WORDS;
 
 __global__ void k_chunk_counts(const Task* __restrict__ tasks, int T, int* __restrict__ cnt) {
@@ -225,9 +230,7 @@ __global__ void k_fill_chunks(const Task* __restrict__ tasks, int T, const int* 
 __global__ void k_clear_bins(uint32_t* __restrict__ bins, int T) {
     const size_t total = (size_t)T * TASK_BIN_WORDS;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-        const int w = (int)(i % BIN_WORDS);
-        // cnt:0, lo: min-acc (init max), hi: max-acc (init 0), clo: min, chi: max
-        bins[i] = (w == 0) ? 0u : ((w >= 1 && w <= 3) || (w >= 7 && w <= 9) ? 0xFFFFFFFFu : 0u);
+        bins[i] = bin_init((int)(i % BIN_WORDS));
     }
 }
 
@@ -237,56 +240,74 @@ __global__ void __launch_bounds__(CHUNK_T) k_bin_large(const Chunk* __restrict__
     __shared__ uint32_t sb[TASK_BIN_WORDS];
     const Chunk ch = chunks[blockIdx.x];
     const Task tk = tasks[ch.task];
-    for (int i = threadIdx.x; i < TASK_BIN_WORDS; i += CHUNK_T) {
-        const int w = i % BIN_WORDS;
-        sb[i] = (w == 0) ? 0u : ((w >= 1 && w <= 3) || (w >= 7 && w <= 9) ? 0xFFFFFFFFu : 0u);
-    }
+    for (int i = threadIdx.x; i < TASK_BIN_WORDS; i += CHUNK_T) sb[i] = bin_init(i % BIN_WORDS);
     float k3[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) k3[a] = bin_scale(tk.clo[a], tk.chi[a]);
     __syncthreads();
-    for (int i = threadIdx.x; i < ch.count; i += CHUNK_T) {
-        const int p = perm[ch.start + i];
-        const float4 l = plo[p], h = phi[p];
-        const float L[3] = {l.x, l.y, l.z}, H[3] = {h.x, h.y, h.z};
-        float c[3];
+    // PART_IPT consecutive positions per thread; a run of primitives in the
+    // same bin of an axis (neighbours in a mesh usually are) is merged in
+    // registers and reaches the shared bins as one set of atomics
+    int rb[3] = {-1, -1, -1};
+    uint32_t rc[3] = {0u, 0u, 0u};
+    float rl[3][3], rh[3][3];
+    auto flush = [&](int a) {
+        uint32_t* w = sb + (a * kBins + rb[a]) * BIN_WORDS;
+        atomicAdd(&w[0], rc[a]);
 #pragma unroll
-        for (int a = 0; a < 3; a++) c[a] = centroid(L[a], H[a]);
+        for (int k = 0; k < 3; k++) {
+            atomicMin(&w[1 + k], f2ord(rl[a][k]));
+            atomicMax(&w[4 + k], f2ord(rh[a][k]));
+        }
+    };
 #pragma unroll
-        for (int a = 0; a < 3; a++) {
-            const int b = bin_of(c[a], tk.clo[a], k3[a]);
-            uint32_t* w = sb + (a * kBins + b) * BIN_WORDS;
-            atomicAdd(&w[0], 1u);
+    for (int j = 0; j < PART_IPT; j++) {
+        const int i = threadIdx.x * PART_IPT + j;
+        if (i < ch.count) {
+            const int p = perm[ch.start + i];
+            const float4 l = plo[p], h = phi[p];
+            const float L[3] = {l.x, l.y, l.z}, H[3] = {h.x, h.y, h.z};
 #pragma unroll
-            for (int k = 0; k < 3; k++) {
-                atomicMin(&w[1 + k], f2ord(L[k]));
-                atomicMax(&w[4 + k], f2ord(H[k]));
-                atomicMin(&w[7 + k], f2ord(c[k]));
-                atomicMax(&w[10 + k], f2ord(c[k]));
+            for (int a = 0; a < 3; a++) {
+                const int b = bin_of(centroid(L[a], H[a]), tk.clo[a], k3[a]);
+                if (b != rb[a]) {
+                    if (rb[a] >= 0) flush(a);
+                    rb[a] = b;
+                    rc[a] = 1u;
+#pragma unroll
+                    for (int k = 0; k < 3; k++) { rl[a][k] = L[k]; rh[a][k] = H[k]; }
+                } else {
+                    rc[a]++;
+#pragma unroll
+                    for (int k = 0; k < 3; k++) { rl[a][k] = fminf(rl[a][k], L[k]); rh[a][k] = fmaxf(rh[a][k], H[k]); }
+                }
             }
         }
     }
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+        if (rb[a] >= 0) flush(a);
     __syncthreads();
     uint32_t* g = gbins + (size_t)ch.task * TASK_BIN_WORDS;
     for (int i = threadIdx.x; i < TASK_BIN_WORDS; i += CHUNK_T) {
         const int w = i % BIN_WORDS;
         const uint32_t v = sb[i];
         if (w == 0) { if (v) atomicAdd(&g[i], v); }
-        else if ((w >= 1 && w <= 3) || (w >= 7 && w <= 9)) { if (v != 0xFFFFFFFFu) atomicMin(&g[i], v); }
+        else if (w <= 3) { if (v != 0xFFFFFFFFu) atomicMin(&g[i], v); }
         else if (v) atomicMax(&g[i], v);
     }
 }
 
 struct BinBox {
-    float lo[3], hi[3], clo[3], chi[3];
+    float lo[3], hi[3];
     int cnt;
 };
 
 __device__ __forceinline__ void box_merge(BinBox& a, const BinBox& b) {
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        a.lo[k] = fminf(a.lo[k], b.lo[k]); a.hi[k] = fmaxf(a.hi[k], b.hi[k]);
-        a.clo[k] = fminf(a.clo[k], b.clo[k]); a.chi[k] = fmaxf(a.chi[k], b.chi[k]);
+        a.lo[k] = fminf(a.lo[k], b.lo[k]);
+        a.hi[k] = fmaxf(a.hi[k], b.hi[k]);
     }
     a.cnt += b.cnt;
 }
@@ -296,8 +317,6 @@ __device__ __forceinline__ BinBox shfl_box(const BinBox& v, int src_delta, bool 
     for (int k = 0; k < 3; k++) {
         r.lo[k] = up ? __shfl_up_sync(FULL, v.lo[k], src_delta) : __shfl_down_sync(FULL, v.lo[k], src_delta);
         r.hi[k] = up ? __shfl_up_sync(FULL, v.hi[k], src_delta) : __shfl_down_sync(FULL, v.hi[k], src_delta);
-        r.clo[k] = up ? __shfl_up_sync(FULL, v.clo[k], src_delta) : __shfl_down_sync(FULL, v.clo[k], src_delta);
-        r.chi[k] = up ? __shfl_up_sync(FULL, v.chi[k], src_delta) : __shfl_down_sync(FULL, v.chi[k], src_delta);
     }
     r.cnt = up ? __shfl_up_sync(FULL, v.cnt, src_delta) : __shfl_down_sync(FULL, v.cnt, src_delta);
     return r;
@@ -324,8 +343,6 @@ __device__ BinBox load_bin(const uint32_t* w) {
     for (int k = 0; k < 3; k++) {
         b.lo[k] = b.cnt ? ord2f(w[1 + k]) : FLT_MAX;
         b.hi[k] = b.cnt ? ord2f(w[4 + k]) : -FLT_MAX;
-        b.clo[k] = b.cnt ? ord2f(w[7 + k]) : FLT_MAX;
-        b.chi[k] = b.cnt ? ord2f(w[10 + k]) : -FLT_MAX;
     }
     return b;
 }
@@ -333,8 +350,8 @@ __device__ BinBox load_bin(const uint32_t* w) {
 // One warp per task: best (axis, bin) by SAH; writes the split, the two
 // child nodes (ids base + 2t, base + 2t + 1) and their task descriptors.
 __global__ void k_split_large(const Task* __restrict__ tasks, int T, const uint32_t* __restrict__ gbins,
-                              Split* __restrict__ splits, Task* __restrict__ kids, Node2* __restrict__ nodes,
-                              int node_base, int max_leaf, int max_sah_depth) {
+                              Split* __restrict__ splits, Task* __restrict__ kids, uint32_t* __restrict__ kcb,
+                              Node2* __restrict__ nodes, int node_base, int max_leaf, int max_sah_depth) {
     const int t = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     if (t >= T) return;
     const int lane = threadIdx.x & 31;
@@ -374,9 +391,7 @@ __global__ void k_split_large(const Task* __restrict__ tasks, int T, const uint3
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             L.lo[k] = __shfl_sync(FULL, pre.lo[k], best_bin); L.hi[k] = __shfl_sync(FULL, pre.hi[k], best_bin);
-            L.clo[k] = __shfl_sync(FULL, pre.clo[k], best_bin); L.chi[k] = __shfl_sync(FULL, pre.chi[k], best_bin);
             R.lo[k] = __shfl_sync(FULL, right.lo[k], best_bin); R.hi[k] = __shfl_sync(FULL, right.hi[k], best_bin);
-            R.clo[k] = __shfl_sync(FULL, right.clo[k], best_bin); R.chi[k] = __shfl_sync(FULL, right.chi[k], best_bin);
         }
         nl = __shfl_sync(FULL, pre.cnt, best_bin);
     } else {
@@ -385,8 +400,6 @@ __global__ void k_split_large(const Task* __restrict__ tasks, int T, const uint3
         for (int k = 0; k < 3; k++) {
             L.lo[k] = R.lo[k] = pn.lo[k];
             L.hi[k] = R.hi[k] = pn.hi[k];
-            L.clo[k] = R.clo[k] = tk.clo[k];
-            L.chi[k] = R.chi[k] = tk.chi[k];
         }
     }
     if (lane == 0) {
@@ -414,8 +427,9 @@ __global__ void k_split_large(const Task* __restrict__ tasks, int T, const uint3
             kt.start = st[s];
             kt.count = cnt[s];
             kt.depth = tk.depth + 1;
-            for (int k = 0; k < 3; k++) { kt.clo[k] = B.clo[k]; kt.chi[k] = B.chi[k]; }
+            for (int k = 0; k < 3; k++) { kt.clo[k] = 0.f; kt.chi[k] = 0.f; }  // from kcb, after k_count_left
             kids[2 * t + s] = kt;
+            for (int k = 0; k < 6; k++) kcb[(size_t)(2 * t + s) * 6 + k] = k < 3 ? 0xFFFFFFFFu : 0u;
         }
     }
 }
@@ -429,22 +443,62 @@ __device__ __forceinline__ bool goes_left(const Task& tk, const Split& sp, int p
     return bin_of(centroid(L, H), tk.clo[sp.axis], k) <= sp.bin;
 }
 
-constexpr int PART_IPT = CHUNK / CHUNK_T;  // 8 consecutive positions per thread
 
 __global__ void __launch_bounds__(CHUNK_T) k_count_left(const Chunk* __restrict__ chunks, const Task* __restrict__ tasks,
                                                         const Split* __restrict__ splits, const int* __restrict__ perm,
                                                         const float4* __restrict__ plo, const float4* __restrict__ phi,
-                                                        int* __restrict__ chunk_left) {
+                                                        int* __restrict__ chunk_left, uint32_t* __restrict__ kcb) {
     __shared__ int ws[CHUNK_T / 32];
     const Chunk ch = chunks[blockIdx.x];
     const Task tk = tasks[ch.task];
     const Split sp = splits[ch.task];
     int c = 0;
-    for (int k = 0; k < PART_IPT; k++) {
-        const int i = threadIdx.x * PART_IPT + k;
+    // centroid bounds of each side: [side][min xyz, max xyz]
+    float cb[2][6];
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) { cb[s][k] = FLT_MAX; cb[s][3 + k] = -FLT_MAX; }
+#pragma unroll
+    for (int j = 0; j < PART_IPT; j++) {
+        const int i = threadIdx.x * PART_IPT + j;
         if (i < ch.count) {
             const int p = perm[ch.start + i];
-            c += goes_left(tk, sp, ch.start + i, plo[p], phi[p]);
+            const float4 l = plo[p], h = phi[p];
+            const bool left = goes_left(tk, sp, ch.start + i, l, h);
+            c += left;
+            const float C[3] = {centroid(l.x, h.x), centroid(l.y, h.y), centroid(l.z, h.z)};
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                cb[0][k] = left ? fminf(cb[0][k], C[k]) : cb[0][k];
+                cb[0][3 + k] = left ? fmaxf(cb[0][3 + k], C[k]) : cb[0][3 + k];
+                cb[1][k] = left ? cb[1][k] : fminf(cb[1][k], C[k]);
+                cb[1][3 + k] = left ? cb[1][3 + k] : fmaxf(cb[1][3 + k], C[k]);
+            }
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            float v = cb[s][k];
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                const float y = __shfl_xor_sync(FULL, v, o);
+                v = k < 3 ? fminf(v, y) : fmaxf(v, y);
+            }
+            cb[s][k] = v;
+        }
+    if ((threadIdx.x & 31) < 2) {  // lane s: side s, when the warp saw any of it
+        const int s = threadIdx.x & 31;
+        const float* v = s ? cb[1] : cb[0];
+        if (v[0] <= v[3]) {
+            uint32_t* dst = kcb + (size_t)(2 * ch.task + s) * 6;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                atomicMin(&dst[k], f2ord(v[k]));
+                atomicMax(&dst[3 + k], f2ord(v[3 + k]));
+            }
         }
     }
     int total;
@@ -504,11 +558,17 @@ __global__ void k_classify_flags(const Task* __restrict__ kids, int K, int max_l
 __global__ void k_compact_kids(const Task* __restrict__ kids, int K, const int* __restrict__ is_large,
                                const int* __restrict__ large_off, const int* __restrict__ is_small,
                                const int* __restrict__ small_off, Task* __restrict__ next, Task* __restrict__ small,
-                               const int* __restrict__ small_base) {
+                               const int* __restrict__ small_base, const uint32_t* __restrict__ kcb) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= K) return;
-    if (is_large[i]) next[large_off[i]] = kids[i];
-    if (is_small[i]) small[*small_base + small_off[i]] = kids[i];
+    Task t = kids[i];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        t.clo[k] = ord2f(kcb[(size_t)i * 6 + k]);
+        t.chi[k] = ord2f(kcb[(size_t)i * 6 + 3 + k]);
+    }
+    if (is_large[i]) next[large_off[i]] = t;
+    if (is_small[i]) small[*small_base + small_off[i]] = t;
 }
 
 __global__ void k_add_small(int* small_base, const int* add) { *small_base += *add; }
@@ -519,6 +579,14 @@ __global__ void k_add_small(int* small_base, const int* add) { *small_base += *a
 // in the CTA's fixed processing order (deterministic).
 struct SubTask {
     int node, lstart, count, depth;
+};
+
+// A subtree of at most WARP_TASK primitives handed from k_build_small to
+// k_build_warp: its node (already written by its parent), its range in the
+// permutation, and the first of the 2 * count - 2 node ids reserved for it.
+constexpr int WARP_TASK = 32;
+struct WTask {
+    int node, start, count_depth, nbase;  // count_depth: count | depth << 8
 };
 
 __global__ void k_reserve(const Task* __restrict__ small, int S, int* __restrict__ need) {
@@ -554,7 +622,9 @@ __global__ void __launch_bounds__(SMALL_T) k_build_small(const Task* __restrict_
                                                          int res_base, int* __restrict__ perm,
                                                          const float4* __restrict__ plo, const float4* __restrict__ phi,
                                                          Node2* __restrict__ nodes, int max_leaf, int max_sah_depth,
-                                                         int small_task, int* __restrict__ status) {
+                                                         int small_task, int warp_task, WTask* __restrict__ wq,
+                                                         int wq_cap, int* __restrict__ wq_count,
+                                                         int* __restrict__ status) {
     extern __shared__ float4 smem4[];
     float* sm = reinterpret_cast<float*>(smem4);
     const Task tk = small[blockIdx.x];
@@ -566,7 +636,7 @@ __global__ void __launch_bounds__(SMALL_T) k_build_small(const Task* __restrict_
     unsigned short* pb = pa + small_task;
     uint32_t* bins = reinterpret_cast<uint32_t*>(pb + small_task + (small_task & 1));  // [3][32][7]
     __shared__ SubTask stack[SMALL_STACK];
-    __shared__ int sp_top, next_node, s_axis, s_bin, s_nl, s_done;
+    __shared__ int sp_top, next_node, s_axis, s_bin, s_done;
     __shared__ SubTask cur;
     __shared__ float red[6 * (SMALL_T / 32)];
     __shared__ float s_cost[3];
@@ -601,6 +671,24 @@ __global__ void __launch_bounds__(SMALL_T) k_build_small(const Task* __restrict_
             if (threadIdx.x == 0) {
                 nodes[st.node].a = tk.start + st.lstart;
                 nodes[st.node].b = -st.count;
+            }
+            __syncthreads();
+            continue;
+        }
+        if (st.count <= warp_task) {  // the rest of this subtree goes to one warp (k_build_warp)
+            if (threadIdx.x == 0) {
+                const int slot = atomicAdd(wq_count, 1);
+                if (slot < wq_cap) {
+                    WTask w;
+                    w.node = st.node;
+                    w.start = tk.start + st.lstart;
+                    w.count_depth = st.count | (st.depth << 8);
+                    w.nbase = next_node;
+                    wq[slot] = w;
+                } else {
+                    atomicOr(status, 2);
+                }
+                next_node += 2 * st.count - 2;
             }
             __syncthreads();
             continue;
@@ -652,7 +740,6 @@ __global__ void __launch_bounds__(SMALL_T) k_build_small(const Task* __restrict_
             for (int k = 0; k < 3; k++) {
                 mine.lo[k] = mine.cnt ? ord2f(w[1 + k]) : FLT_MAX;
                 mine.hi[k] = mine.cnt ? ord2f(w[4 + k]) : -FLT_MAX;
-                mine.clo[k] = 0.f; mine.chi[k] = 0.f;
             }
             BinBox pre, suf;
             prefix_suffix(mine, pre, suf);
@@ -763,12 +850,207 @@ __global__ void __launch_bounds__(SMALL_T) k_build_small(const Task* __restrict_
     for (int i = threadIdx.x; i < n; i += SMALL_T) perm[tk.start + i] = gidx[pa[i]];
 }
 
+// One warp finishes a subtree of at most 32 primitives with an exact SAH
+// sweep (every split between consecutive centroids along each axis, cost
+// N_L*A(L) + N_R*A(R) as above).  The primitives are sorted by centroid
+// along each axis once, by a bitonic network over the lanes (ties by
+// primitive slot); a split partitions all three orders stably, so each
+// node's primitives stay a contiguous, still sorted range of every order and
+// no node sorts again.  Per node and axis, the lanes hold the range in
+// order, inclusive prefix and suffix scans give every split's child boxes,
+// and a butterfly picks the cheapest (ties: lower split, then lower axis).
+// Depth-first, left child first; pending right children live one per lane
+// in registers.  Node ids are handed out from the reserved range in that
+// fixed order, so the tree is deterministic.
+constexpr int WB_T = 128;  // 4 warps per CTA, one subtree each at a time
+constexpr int WB_W = WB_T / 32;
+
+__device__ __forceinline__ float box_half_area(const float (&b)[6]) {
+    return half_area(b[0], b[1], b[2], b[3], b[4], b[5]);
+}
+
+__global__ void __launch_bounds__(WB_T) k_build_warp(const WTask* __restrict__ wq, const int* __restrict__ wq_count,
+                                                     int wq_cap, int* __restrict__ perm,
+                                                     const float4* __restrict__ plo, const float4* __restrict__ phi,
+                                                     Node2* __restrict__ nodes, int max_leaf, int max_sah_depth,
+                                                     int* __restrict__ status) {
+    __shared__ float s_box[WB_W][6][32];          // lo xyz, hi xyz per slot
+    __shared__ int s_idx[WB_W][32];               // primitive per slot
+    __shared__ unsigned char s_ord[WB_W][3][32];  // per axis: position -> slot
+    __shared__ unsigned char s_side[WB_W][32];    // per slot: 1 = left of the split
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const int total = min(*wq_count, wq_cap);
+    for (int t = blockIdx.x * WB_W + w; t < total; t += gridDim.x * WB_W) {
+        const WTask wt = wq[t];
+        const int cnt = wt.count_depth & 255;
+        // load this subtree's primitives, one per lane
+        float b[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (lane < cnt) {
+            const int p = perm[wt.start + lane];
+            const float4 l = plo[p], h = phi[p];
+            b[0] = l.x; b[1] = l.y; b[2] = l.z;
+            b[3] = h.x; b[4] = h.y; b[5] = h.z;
+            s_idx[w][lane] = p;
+#pragma unroll
+            for (int k = 0; k < 6; k++) s_box[w][k][lane] = b[k];
+        }
+        // one bitonic sort per axis: (centroid key, slot), idle lanes last
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            uint32_t key = lane < cnt ? f2ord(centroid(b[a], b[3 + a])) : 0xFFFFFFFFu;
+            int val = lane;
+#pragma unroll
+            for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const uint32_t ok = __shfl_xor_sync(FULL, key, j);
+                    const int ov = __shfl_xor_sync(FULL, val, j);
+                    const bool less = ok < key || (ok == key && ov < val);
+                    const bool take = (((lane & j) == 0) == ((lane & k) == 0)) ? less : !less;
+                    if (take) { key = ok; val = ov; }
+                }
+            }
+            s_ord[w][a][lane] = (unsigned char)val;
+        }
+        __syncwarp();
+        // depth-first over the subtree; lane k holds pending entry k
+        int e_node = 0, e_l = 0, e_c = 0, e_d = 0, sp = 0;
+        int c_node = wt.node, c_l = 0, c_c = cnt, c_d = wt.count_depth >> 8;
+        int next = wt.nbase;
+        while (true) {
+            const bool median = c_d >= max_sah_depth;
+            float best = FLT_MAX;
+            int ba = 0, br = c_c / 2 - 1;
+            float bl[6], bR[6];
+            for (int a = 0; a < 3; a++) {
+                if (median && a > 0) break;
+                float pre[6], suf[6];
+                if (lane < c_c) {
+                    const int s = s_ord[w][a][c_l + lane];
+#pragma unroll
+                    for (int k = 0; k < 6; k++) pre[k] = s_box[w][k][s];
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 3; k++) { pre[k] = FLT_MAX; pre[3 + k] = -FLT_MAX; }
+                }
+#pragma unroll
+                for (int k = 0; k < 6; k++) suf[k] = pre[k];
+                // inclusive scans; a lane reading itself at the ends merges its own box (no change)
+                for (int o = 1; o < c_c; o <<= 1) {
+#pragma unroll
+                    for (int k = 0; k < 6; k++) {
+                        const float x = __shfl_up_sync(FULL, pre[k], o);
+                        const float y = __shfl_down_sync(FULL, suf[k], o);
+                        pre[k] = k < 3 ? fminf(pre[k], x) : fmaxf(pre[k], x);
+                        suf[k] = k < 3 ? fminf(suf[k], y) : fmaxf(suf[k], y);
+                    }
+                }
+                float right[6];
+#pragma unroll
+                for (int k = 0; k < 6; k++) right[k] = __shfl_down_sync(FULL, suf[k], 1);
+                // lanes without a split, and NaN costs, read +inf: the lowest lane
+                // then wins every tie, so the chosen split is always a real one
+                float cost = INFINITY;
+                if (lane < c_c - 1) {
+                    cost = (float)(lane + 1) * box_half_area(pre) + (float)(c_c - lane - 1) * box_half_area(right);
+                    if (!(cost <= FLT_MAX)) cost = INFINITY;
+                }
+                int r = lane;
+                if (median) r = c_c / 2 - 1;
+                else {
+                    for (int o = 16; o; o >>= 1) {
+                        const float c2 = __shfl_xor_sync(FULL, cost, o);
+                        const int r2 = __shfl_xor_sync(FULL, r, o);
+                        if (c2 < cost || (c2 == cost && r2 < r)) { cost = c2; r = r2; }
+                    }
+                }
+                if (a == 0 || cost < best) {
+                    best = cost;
+                    ba = a;
+                    br = r;
+#pragma unroll
+                    for (int k = 0; k < 6; k++) {
+                        bl[k] = __shfl_sync(FULL, pre[k], r);
+                        bR[k] = __shfl_sync(FULL, right[k], r);
+                    }
+                }
+            }
+            const int nl = br + 1, nr = c_c - nl;
+            // stable partition of the three orders: the first nl of axis ba go left
+            if (lane < c_c) s_side[w][s_ord[w][ba][c_l + lane]] = lane < nl;
+            __syncwarp();
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                int s = 0, left = 0;
+                if (lane < c_c) {
+                    s = s_ord[w][a][c_l + lane];
+                    left = s_side[w][s];
+                }
+                const unsigned bal = __ballot_sync(FULL, left && lane < c_c);
+                const int below = __popc(bal & lt);
+                const int pos = left ? below : nl + (lane - below);
+                __syncwarp();
+                if (lane < c_c) s_ord[w][a][c_l + pos] = (unsigned char)s;
+            }
+            __syncwarp();
+            const int lid = next, rid = next + 1;
+            next += 2;
+            if (lane == 0) {
+                nodes[c_node].a = lid;
+                nodes[c_node].b = rid;
+                Node2 L, R;
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    L.lo[k] = bl[k]; L.hi[k] = bl[3 + k];
+                    R.lo[k] = bR[k]; R.hi[k] = bR[3 + k];
+                }
+                L.a = wt.start + c_l; L.b = nl > max_leaf ? 0 : -nl;
+                R.a = wt.start + c_l + nl; R.b = nr > max_leaf ? 0 : -nr;
+                nodes[lid] = L;
+                nodes[rid] = R;
+            }
+            const int d = c_d + 1;
+            if (nl > max_leaf) {
+                if (nr > max_leaf) {  // left now, right later
+                    if (sp >= 32) {
+                        if (lane == 0) atomicOr(status, 4);
+                        break;
+                    }
+                    if (lane == sp) { e_node = rid; e_l = c_l + nl; e_c = nr; e_d = d; }
+                    sp++;
+                }
+                c_node = lid; c_c = nl; c_d = d;
+            } else if (nr > max_leaf) {
+                c_node = rid; c_l += nl; c_c = nr; c_d = d;
+            } else {
+                if (sp == 0) break;
+                sp--;
+                c_node = __shfl_sync(FULL, e_node, sp);
+                c_l = __shfl_sync(FULL, e_l, sp);
+                c_c = __shfl_sync(FULL, e_c, sp);
+                c_d = __shfl_sync(FULL, e_d, sp);
+            }
+        }
+        // leaf order = the axis-0 order (every leaf's range holds its primitives)
+        if (lane < cnt) perm[wt.start + lane] = s_idx[w][s_ord[w][0][lane]];
+        __syncwarp();
+    }
+}
+
 __global__ void k_iota(int* __restrict__ p, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) p[i] = i;
 }
 
 // ----------------------------------------------------------- the driver --
+BuildConfig default_build_config() {
+    BuildConfig c;
+    if (const char* e = getenv("RTB200_MAX_LEAF")) c.max_leaf = std::max(1, std::min(4, atoi(e)));
+    if (const char* e = getenv("RTB200_WARP_TASK")) c.warp_task = std::max(0, std::min(WARP_TASK, atoi(e)));
+    return c;
+}
+
 bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig& cfg, Bvh2Device& out,
                 cudaStream_t s, const std::vector<int>* segments) {
     if (n <= 0) {
@@ -797,21 +1079,23 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
     int* perm = out.perm.p;
     // temporaries
     const int maxT = n / (cfg.small_task + 1) + 2;  // large tasks per level
-    DevBuf<int> tmp, dseg;
-    DevBuf<uint32_t> acc;
-    DevBuf<Task> tasks_a, tasks_b, kids, small;
-    DevBuf<Split> splits;
-    DevBuf<uint32_t> gbins;
-    DevBuf<int> flags, status;
+    TmpBuf<int> tmp, dseg;
+    TmpBuf<uint32_t> acc;
+    TmpBuf<Task> tasks_a, tasks_b, kids, small;
+    TmpBuf<Split> splits;
+    TmpBuf<uint32_t> gbins;
+    TmpBuf<int> flags, status;
+    TmpBuf<uint32_t> kcb;  // per kid: centroid min xyz, max xyz (ordered)
     const int maxChunks = n / CHUNK + maxT + 2;
-    DevBuf<Chunk> chunks;
-    DevBuf<int> ccount, coff, cleft, cleftoff;
+    TmpBuf<Chunk> chunks;
+    TmpBuf<int> ccount, coff, cleft, cleftoff;
     const int maxSmall = n / (cfg.max_leaf + 1) + 2;
-    if (!tmp.alloc(n) || !acc.alloc((size_t)12 * S) || !dseg.alloc(S + 1) || !tasks_a.alloc(maxT) ||
-        !tasks_b.alloc(maxT) || !kids.alloc(2 * maxT) || !small.alloc(maxSmall) || !splits.alloc(maxT) ||
-        !gbins.alloc((size_t)maxT * TASK_BIN_WORDS) || !flags.alloc(4 * 2 * maxT + 8) || !chunks.alloc(maxChunks) ||
-        !ccount.alloc(maxT) || !coff.alloc(maxT) || !cleft.alloc(maxChunks) || !cleftoff.alloc(maxChunks) ||
-        !status.alloc(1))
+    if (!tmp.alloc(n, s) || !acc.alloc((size_t)12 * S, s) || !dseg.alloc(S + 1, s) || !tasks_a.alloc(maxT, s) ||
+        !tasks_b.alloc(maxT, s) || !kids.alloc(2 * maxT, s) || !small.alloc(maxSmall, s) ||
+        !splits.alloc(maxT, s) || !gbins.alloc((size_t)maxT * TASK_BIN_WORDS, s) ||
+        !flags.alloc(4 * 2 * maxT + 8, s) || !chunks.alloc(maxChunks, s) || !ccount.alloc(maxT, s) ||
+        !coff.alloc(maxT, s) || !cleft.alloc(maxChunks, s) || !cleftoff.alloc(maxChunks, s) || !status.alloc(1, s) ||
+        !kcb.alloc((size_t)12 * maxT, s))
         return false;
     cudaMemsetAsync(status.p, 0, sizeof(int), s);
     k_iota<<<(n + 255) / 256, 256, 0, s>>>(perm, n);
@@ -893,9 +1177,9 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
         k_fill_chunks<<<T, 128, 0, s>>>(cur, T, coff.p, chunks.p);
         k_clear_bins<<<std::min(T * 8, 4096), 256, 0, s>>>(gbins.p, T);
         k_bin_large<<<C, CHUNK_T, 0, s>>>(chunks.p, cur, perm, d_lo, d_hi, gbins.p);
-        k_split_large<<<(T + 3) / 4, 128, 0, s>>>(cur, T, gbins.p, splits.p, kids.p, out.nodes.p, node_count,
-                                                   cfg.max_leaf, cfg.max_sah_depth);
-        k_count_left<<<C, CHUNK_T, 0, s>>>(chunks.p, cur, splits.p, perm, d_lo, d_hi, cleft.p);
+        k_split_large<<<(T + 3) / 4, 128, 0, s>>>(cur, T, gbins.p, splits.p, kids.p, kcb.p, out.nodes.p,
+                                                   node_count, cfg.max_leaf, cfg.max_sah_depth);
+        k_count_left<<<C, CHUNK_T, 0, s>>>(chunks.p, cur, splits.p, perm, d_lo, d_hi, cleft.p, kcb.p);
         if (!scan_exclusive(cleft.p, cleftoff.p, C, nullptr, s)) return false;
         k_scatter<<<C, CHUNK_T, 0, s>>>(chunks.p, cur, splits.p, perm, d_lo, d_hi, cleftoff.p, tmp.p);
         k_copy_back<<<C, 256, 0, s>>>(chunks.p, tmp.p, perm);
@@ -905,7 +1189,7 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
         if (!scan_exclusive(is_large, large_off, K, d_tot, s)) return false;
         if (!scan_exclusive(is_small, small_off, K, d_tot + 1, s)) return false;
         k_compact_kids<<<(K + 255) / 256, 256, 0, s>>>(kids.p, K, is_large, large_off, is_small, small_off, nxt,
-                                                      small.p, d_small_base);
+                                                      small.p, d_small_base, kcb.p);
         k_add_small<<<1, 1, 0, s>>>(d_small_base, d_tot + 1);
         int h[2];
         cudaMemcpyAsync(h, d_tot, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -919,16 +1203,37 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
         }
     }
     if (num_small > 0) {
-        DevBuf<int> need, off;
-        if (!need.alloc(num_small) || !off.alloc(num_small)) return false;
+        TmpBuf<int> need, off;
+        if (!need.alloc(num_small, s) || !off.alloc(num_small, s)) return false;
         k_reserve<<<(num_small + 255) / 256, 256, 0, s>>>(small.p, num_small, need.p);
         if (!scan_exclusive(need.p, off.p, num_small, d_tot, s)) return false;
         int reserved = 0;
         cudaMemcpyAsync(&reserved, d_tot, sizeof(int), cudaMemcpyDeviceToHost, s);
+        // subtrees of at most warp_task primitives: one warp each (tasks hold
+        // more than max_leaf primitives, so at most n / (max_leaf + 1) of them)
+        const int warp_task = std::min(cfg.warp_task, WARP_TASK);
+        const int wq_cap = warp_task > 0 ? n / (cfg.max_leaf + 1) + 2 : 0;
+        TmpBuf<WTask> wq;
+        if (wq_cap > 0 && !wq.alloc(wq_cap, s)) return false;
+        int* d_wq_count = d_tot + 1;
+        cudaMemsetAsync(d_wq_count, 0, sizeof(int), s);
         const size_t smem = (size_t)cfg.small_task * (6 * 4 + 4 + 2 + 2) + 16 + 3 * kBins * 7 * 4;
         cudaFuncSetAttribute(k_build_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_build_small<<<num_small, SMALL_T, smem, s>>>(small.p, off.p, node_count, perm, d_lo, d_hi, out.nodes.p,
-                                                       cfg.max_leaf, cfg.max_sah_depth, cfg.small_task, status.p);
+                                                       cfg.max_leaf, cfg.max_sah_depth, cfg.small_task, warp_task,
+                                                       wq.p, wq_cap, d_wq_count, status.p);
+        if (warp_task > 0) {
+            static int per_sm = 0, sms = 0;
+            if (!per_sm) {
+                int dev = 0;
+                cudaGetDevice(&dev);
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_warp, WB_T, 0);
+                per_sm = std::max(per_sm, 1);
+            }
+            k_build_warp<<<sms * per_sm, WB_T, 0, s>>>(wq.p, d_wq_count, wq_cap, perm, d_lo, d_hi, out.nodes.p,
+                                                       cfg.max_leaf, cfg.max_sah_depth, status.p);
+        }
         if (!RT_CUDA(cudaStreamSynchronize(s))) return false;
         node_count += reserved;
     }
@@ -936,7 +1241,7 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
     cudaMemcpyAsync(&st, status.p, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (!RT_CUDA(cudaStreamSynchronize(s))) return false;
     if (st) {
-        set_error("build: subtree stack overflow");
+        set_error("build: %s", (st & 2) ? "subtree queue overflow" : "subtree stack overflow");
         return false;
     }
     out.num_nodes = node_count;

@@ -396,11 +396,11 @@ bool collapse_bvh8(const Bvh2Device& b2, const float* d_tris9, Bvh8Device& out, 
     } else {
         if (!out.leaf_ids.alloc(n)) return false;
     }
-    DevBuf<int> lvl_a, lvl_b, n_inner, n_items, inner_off, item_off, tot;
-    DevBuf<Gather> gat;
-    if (!lvl_a.alloc(max_nodes) || !lvl_b.alloc(max_nodes) || !n_inner.alloc(max_nodes) ||
-        !n_items.alloc(max_nodes) || !inner_off.alloc(max_nodes) || !item_off.alloc(max_nodes) ||
-        !gat.alloc(max_nodes) || !tot.alloc(2))
+    TmpBuf<int> lvl_a, lvl_b, n_inner, n_items, inner_off, item_off, tot;
+    TmpBuf<Gather> gat;
+    if (!lvl_a.alloc(max_nodes, s) || !lvl_b.alloc(max_nodes, s) || !n_inner.alloc(max_nodes, s) ||
+        !n_items.alloc(max_nodes, s) || !inner_off.alloc(max_nodes, s) || !item_off.alloc(max_nodes, s) ||
+        !gat.alloc(max_nodes, s) || !tot.alloc(2, s))
         return false;
     {
         // level 0: the roots, binary nodes 0 .. R-1 -> 8-wide nodes 0 .. R-1
@@ -416,7 +416,7 @@ bool collapse_bvh8(const Bvh2Device& b2, const float* d_tris9, Bvh8Device& out, 
         const char* e = getenv("RTB200_COLLAPSE");
         return e && !strcmp(e, "greedy") ? 0 : 1;
     }();
-    DevBuf<DPNode> dp;
+    TmpBuf<DPNode> dp;
     if (d_tris9 && mode == 1) {
         static const float c_prim = [] {
             const char* e = getenv("RTB200_DP_CPRIM");
@@ -428,8 +428,9 @@ bool collapse_bvh8(const Bvh2Device& b2, const float* d_tris9, Bvh8Device& out, 
             return v < 1 ? 1 : (v > 4 ? 4 : v);
         }();
         const int slots = b2.num_nodes;
-        DevBuf<int> parent, arrive, st;
-        if (!dp.alloc(slots) || !parent.alloc(slots) || !arrive.alloc(slots) || !st.alloc(1)) return false;
+        TmpBuf<int> parent, arrive, st;
+        if (!dp.alloc(slots, s) || !parent.alloc(slots, s) || !arrive.alloc(slots, s) || !st.alloc(1, s))
+            return false;
         int h_st = 0;
         if (!RT_CUDA(cudaMemsetAsync(parent.p, 0xFF, sizeof(int) * (size_t)slots, s)) ||
             !RT_CUDA(cudaMemsetAsync(arrive.p, 0, sizeof(int) * (size_t)slots, s)) ||
@@ -492,8 +493,8 @@ __global__ void k_sah(const Node2* __restrict__ nodes, int m, float* __restrict_
 }
 
 float bvh2_sah_cost(const Bvh2Device& b2, cudaStream_t s) {
-    DevBuf<float> acc;
-    if (!acc.alloc(1)) return -1.f;
+    TmpBuf<float> acc;
+    if (!acc.alloc(1, s)) return -1.f;
     cudaMemsetAsync(acc.p, 0, sizeof(float), s);
     k_sah<<<std::min((b2.num_nodes + 255) / 256, 1024), 256, 0, s>>>(b2.nodes.p, b2.num_nodes, acc.p);
     float total = 0.f;

@@ -59,12 +59,54 @@ struct DevBuf {
     size_t bytes() const { return n * sizeof(T); }
 };
 
+// ---- builder temporaries: stream-ordered, from a pool that keeps memory ----
+// The builders need a few bytes to a few GB of scratch per build.  Taking it
+// with cudaMalloc/cudaFree maps and unmaps pages on every build, and every
+// cudaFree waits for the whole device, so the build's timeline fills with
+// idle gaps.  Scratch comes instead from one pool per device that keeps up to
+// `RTB200_POOL_KEEP_MB` (default 8192) MB of freed memory for the next
+// build; allocation and release are ordered on the build's stream.
+cudaMemPool_t scratch_pool();
+
+template <class T>
+struct TmpBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaStream_t s = nullptr;
+    TmpBuf() = default;
+    TmpBuf(const TmpBuf&) = delete;
+    TmpBuf& operator=(const TmpBuf&) = delete;
+    ~TmpBuf() { release(); }
+    bool alloc(size_t count, cudaStream_t st) {
+        release();
+        if (count == 0) return true;
+        cudaMemPool_t pool = scratch_pool();
+        if (!pool || cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(T), pool, st) != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            set_error("scratch allocation of %zu bytes failed", count * sizeof(T));
+            return false;
+        }
+        s = st;
+        n = count;
+        return true;
+    }
+    void release() {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+        n = 0;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
 // ---- build configuration ----
 struct BuildConfig {
     int max_leaf = 2;        // triangles per BVH2 leaf (1..kMaxLeafTris); the 8-wide
                              // collapse may merge small subtrees into leaves of up to 4
     int small_task = 1024;   // tasks at or below this size finish in one CTA
     int max_sah_depth = 48;  // deeper tasks fall back to median splits
+    int warp_task = 32;      // subtrees of at most this many primitives (<= 32) are
+                             // finished by one warp with an exact SAH sweep; 0 = off
 };
 
 // Result of the SAH builder on the device.
@@ -85,6 +127,9 @@ struct Bvh8Device {
     int num_leaf_items = 0;
     int depth = 0;
 };
+
+// Defaults with the environment's overrides (RTB200_MAX_LEAF, RTB200_WARP_TASK).
+BuildConfig default_build_config();
 
 // Builds the binary SAH BVH over primitive boxes (lo/hi float4 per prim).
 // Returns false on failure (error set).  Stream-ordered; synchronises on
