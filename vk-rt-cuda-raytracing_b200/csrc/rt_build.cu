@@ -854,14 +854,14 @@ __global__ void __launch_bounds__(SMALL_T) k_build_small(const Task* __restrict_
 // sweep (every split between consecutive centroids along each axis, cost
 // N_L*A(L) + N_R*A(R) as above).  The primitives are sorted by centroid
 // along each axis once, by a bitonic network over the lanes (ties by
-// primitive slot); a split partitions all three orders stably, so each
-// node's primitives stay a contiguous, still sorted range of every order and
-// no node sorts again.  Per node and axis, the lanes hold the range in
-// order, inclusive prefix and suffix scans give every split's child boxes,
-// and a butterfly picks the cheapest (ties: lower split, then lower axis).
-// Depth-first, left child first; pending right children live one per lane
-// in registers.  Node ids are handed out from the reserved range in that
-// fixed order, so the tree is deterministic.
+// primitive slot); a split partitions all three orders stably, so every
+// node's primitives stay a contiguous, still sorted range of each order.
+// The nodes of one depth own disjoint ranges, so a whole level is split in
+// one pass: lane l works on position l, and prefix/suffix scans, the
+// cheapest-split search (ties: lower split, then lower axis) and the
+// partition are segmented by node range.  Node ids are handed out from the
+// reserved range level by level, in position order, so the tree is
+// deterministic.
 constexpr int WB_T = 128;  // 4 warps per CTA, one subtree each at a time
 constexpr int WB_W = WB_T / 32;
 
@@ -872,12 +872,11 @@ __device__ __forceinline__ float box_half_area(const float (&b)[6]) {
 __global__ void __launch_bounds__(WB_T) k_build_warp(const WTask* __restrict__ wq, const int* __restrict__ wq_count,
                                                      int wq_cap, int* __restrict__ perm,
                                                      const float4* __restrict__ plo, const float4* __restrict__ phi,
-                                                     Node2* __restrict__ nodes, int max_leaf, int max_sah_depth,
-                                                     int* __restrict__ status) {
+                                                     Node2* __restrict__ nodes, int max_leaf, int max_sah_depth) {
     __shared__ float s_box[WB_W][6][32];          // lo xyz, hi xyz per slot
     __shared__ int s_idx[WB_W][32];               // primitive per slot
     __shared__ unsigned char s_ord[WB_W][3][32];  // per axis: position -> slot
-    __shared__ unsigned char s_side[WB_W][32];    // per slot: 1 = left of the split
+    __shared__ unsigned char s_side[WB_W][32];    // per slot: 1 = left of its node's split
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const int total = min(*wq_count, wq_cap);
@@ -914,20 +913,24 @@ __global__ void __launch_bounds__(WB_T) k_build_warp(const WTask* __restrict__ w
             s_ord[w][a][lane] = (unsigned char)val;
         }
         __syncwarp();
-        // depth-first over the subtree; lane k holds pending entry k
-        int e_node = 0, e_l = 0, e_c = 0, e_d = 0, sp = 0;
-        int c_node = wt.node, c_l = 0, c_c = cnt, c_d = wt.count_depth >> 8;
+        // this lane's node: range [s0, s1), id, depth; lanes past cnt own nothing
+        int s0 = lane < cnt ? 0 : lane, s1 = lane < cnt ? cnt : lane + 1;
+        int node = wt.node, depth = wt.count_depth >> 8;
+        bool active = lane < cnt && cnt > max_leaf;
         int next = wt.nbase;
-        while (true) {
-            const bool median = c_d >= max_sah_depth;
-            float best = FLT_MAX;
-            int ba = 0, br = c_c / 2 - 1;
+        while (__any_sync(FULL, active)) {
+            const int len = s1 - s0;
+            const int maxlen = __reduce_max_sync(FULL, active ? len : 0);
+            const bool median = depth >= max_sah_depth;
+            const unsigned seg_ge = ~((1u << s0) - 1u);  // lanes >= s0
+            float best = INFINITY;
+            int br = s0 + len / 2 - 1, ba = 0;
             float bl[6], bR[6];
+#pragma unroll 1
             for (int a = 0; a < 3; a++) {
-                if (median && a > 0) break;
                 float pre[6], suf[6];
-                if (lane < c_c) {
-                    const int s = s_ord[w][a][c_l + lane];
+                if (lane < cnt) {
+                    const int s = s_ord[w][a][lane];
 #pragma unroll
                     for (int k = 0; k < 6; k++) pre[k] = s_box[w][k][s];
                 } else {
@@ -936,100 +939,102 @@ __global__ void __launch_bounds__(WB_T) k_build_warp(const WTask* __restrict__ w
                 }
 #pragma unroll
                 for (int k = 0; k < 6; k++) suf[k] = pre[k];
-                // inclusive scans; a lane reading itself at the ends merges its own box (no change)
-                for (int o = 1; o < c_c; o <<= 1) {
+                // segmented inclusive scans over each node's range
+                for (int o = 1; o < maxlen; o <<= 1) {
+                    const bool up = lane - o >= s0, dn = lane + o < s1;
 #pragma unroll
                     for (int k = 0; k < 6; k++) {
                         const float x = __shfl_up_sync(FULL, pre[k], o);
                         const float y = __shfl_down_sync(FULL, suf[k], o);
-                        pre[k] = k < 3 ? fminf(pre[k], x) : fmaxf(pre[k], x);
-                        suf[k] = k < 3 ? fminf(suf[k], y) : fmaxf(suf[k], y);
+                        if (up) pre[k] = k < 3 ? fminf(pre[k], x) : fmaxf(pre[k], x);
+                        if (dn) suf[k] = k < 3 ? fminf(suf[k], y) : fmaxf(suf[k], y);
                     }
                 }
                 float right[6];
 #pragma unroll
                 for (int k = 0; k < 6; k++) right[k] = __shfl_down_sync(FULL, suf[k], 1);
-                // lanes without a split, and NaN costs, read +inf: the lowest lane
-                // then wins every tie, so the chosen split is always a real one
+                // positions without a right side, idle nodes and NaN costs read
+                // +inf; ties go to the lower position, so a real split is chosen
                 float cost = INFINITY;
-                if (lane < c_c - 1) {
-                    cost = (float)(lane + 1) * box_half_area(pre) + (float)(c_c - lane - 1) * box_half_area(right);
+                if (active && lane < s1 - 1 && !(median && a > 0)) {
+                    cost = (float)(lane - s0 + 1) * box_half_area(pre) + (float)(s1 - lane - 1) * box_half_area(right);
                     if (!(cost <= FLT_MAX)) cost = INFINITY;
                 }
                 int r = lane;
-                if (median) r = c_c / 2 - 1;
-                else {
-                    for (int o = 16; o; o >>= 1) {
-                        const float c2 = __shfl_xor_sync(FULL, cost, o);
-                        const int r2 = __shfl_xor_sync(FULL, r, o);
-                        if (c2 < cost || (c2 == cost && r2 < r)) { cost = c2; r = r2; }
-                    }
+                for (int o = 1; o < maxlen; o <<= 1) {  // segmented suffix minimum: the node's first lane ends with it
+                    const float c2 = __shfl_down_sync(FULL, cost, o);
+                    const int r2 = __shfl_down_sync(FULL, r, o);
+                    if (lane + o < s1 && (c2 < cost || (c2 == cost && r2 < r))) { cost = c2; r = r2; }
                 }
-                if (a == 0 || cost < best) {
+                cost = __shfl_sync(FULL, cost, s0);
+                r = __shfl_sync(FULL, r, s0);
+                if (median) r = s0 + len / 2 - 1;
+                const bool take = active && (a == 0 || cost < best);
+                if (take) {
                     best = cost;
-                    ba = a;
                     br = r;
+                    ba = a;
+                }
+                // each lane reads its own node's split lane
+                const int src = take ? r : lane;
 #pragma unroll
-                    for (int k = 0; k < 6; k++) {
-                        bl[k] = __shfl_sync(FULL, pre[k], r);
-                        bR[k] = __shfl_sync(FULL, right[k], r);
-                    }
+                for (int k = 0; k < 6; k++) {
+                    const float x = __shfl_sync(FULL, pre[k], src);
+                    const float y = __shfl_sync(FULL, right[k], src);
+                    if (take) { bl[k] = x; bR[k] = y; }
                 }
             }
-            const int nl = br + 1, nr = c_c - nl;
-            // stable partition of the three orders: the first nl of axis ba go left
-            if (lane < c_c) s_side[w][s_ord[w][ba][c_l + lane]] = lane < nl;
+            const int nl = br - s0 + 1, nr = len - nl;
+            // stable, segmented partition of the three orders: the first nl
+            // positions of the winning axis' order go left
+            if (active) s_side[w][s_ord[w][ba][lane]] = lane <= br;
             __syncwarp();
 #pragma unroll
             for (int a = 0; a < 3; a++) {
-                int s = 0, left = 0;
-                if (lane < c_c) {
-                    s = s_ord[w][a][c_l + lane];
+                int s = 0;
+                bool left = false;
+                if (active) {
+                    s = s_ord[w][a][lane];
                     left = s_side[w][s];
                 }
-                const unsigned bal = __ballot_sync(FULL, left && lane < c_c);
-                const int below = __popc(bal & lt);
-                const int pos = left ? below : nl + (lane - below);
+                const unsigned bal = __ballot_sync(FULL, left);
+                const int below = __popc(bal & lt & seg_ge);
+                const int pos = left ? s0 + below : s0 + nl + (lane - s0 - below);
                 __syncwarp();
-                if (lane < c_c) s_ord[w][a][c_l + pos] = (unsigned char)s;
+                if (active) s_ord[w][a][pos] = (unsigned char)s;
             }
             __syncwarp();
-            const int lid = next, rid = next + 1;
-            next += 2;
-            if (lane == 0) {
-                nodes[c_node].a = lid;
-                nodes[c_node].b = rid;
+            // two node ids per split node, in position order
+            const bool lead = active && lane == s0;
+            const unsigned leads = __ballot_sync(FULL, lead);
+            const int mine = next + 2 * __popc(leads & lt);
+            next += 2 * __popc(leads);
+            const int lid = __shfl_sync(FULL, mine, s0);
+            if (lead) {
+                nodes[node].a = lid;
+                nodes[node].b = lid + 1;
                 Node2 L, R;
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
                     L.lo[k] = bl[k]; L.hi[k] = bl[3 + k];
                     R.lo[k] = bR[k]; R.hi[k] = bR[3 + k];
                 }
-                L.a = wt.start + c_l; L.b = nl > max_leaf ? 0 : -nl;
-                R.a = wt.start + c_l + nl; R.b = nr > max_leaf ? 0 : -nr;
+                L.a = wt.start + s0; L.b = nl > max_leaf ? 0 : -nl;
+                R.a = wt.start + s0 + nl; R.b = nr > max_leaf ? 0 : -nr;
                 nodes[lid] = L;
-                nodes[rid] = R;
+                nodes[lid + 1] = R;
             }
-            const int d = c_d + 1;
-            if (nl > max_leaf) {
-                if (nr > max_leaf) {  // left now, right later
-                    if (sp >= 32) {
-                        if (lane == 0) atomicOr(status, 4);
-                        break;
-                    }
-                    if (lane == sp) { e_node = rid; e_l = c_l + nl; e_c = nr; e_d = d; }
-                    sp++;
+            if (active) {
+                if (lane < s0 + nl) {
+                    s1 = s0 + nl;
+                    node = lid;
+                    active = nl > max_leaf;
+                } else {
+                    s0 = s0 + nl;
+                    node = lid + 1;
+                    active = nr > max_leaf;
                 }
-                c_node = lid; c_c = nl; c_d = d;
-            } else if (nr > max_leaf) {
-                c_node = rid; c_l += nl; c_c = nr; c_d = d;
-            } else {
-                if (sp == 0) break;
-                sp--;
-                c_node = __shfl_sync(FULL, e_node, sp);
-                c_l = __shfl_sync(FULL, e_l, sp);
-                c_c = __shfl_sync(FULL, e_c, sp);
-                c_d = __shfl_sync(FULL, e_d, sp);
+                depth++;
             }
         }
         // leaf order = the axis-0 order (every leaf's range holds its primitives)
@@ -1232,7 +1237,7 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
                 per_sm = std::max(per_sm, 1);
             }
             k_build_warp<<<sms * per_sm, WB_T, 0, s>>>(wq.p, d_wq_count, wq_cap, perm, d_lo, d_hi, out.nodes.p,
-                                                       cfg.max_leaf, cfg.max_sah_depth, status.p);
+                                                       cfg.max_leaf, cfg.max_sah_depth);
         }
         if (!RT_CUDA(cudaStreamSynchronize(s))) return false;
         node_count += reserved;
