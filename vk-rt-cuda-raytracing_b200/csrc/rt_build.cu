@@ -641,6 +641,7 @@ __global__ void __launch_bounds__(SMALL_T) k_build_small(const Task* __restrict_
     __shared__ float red[6 * (SMALL_T / 32)];
     __shared__ float s_cost[3];
     __shared__ int s_cbin[3];
+    __shared__ float s_cbox[3][12];  // per axis: left box, right box of its best split
     __shared__ int ws[SMALL_T / 32];
 
     for (int i = threadIdx.x; i < n; i += SMALL_T) {
@@ -708,40 +709,55 @@ __global__ void __launch_bounds__(SMALL_T) k_build_small(const Task* __restrict_
         float k3[3];
 #pragma unroll
         for (int a = 0; a < 3; a++) k3[a] = bin_scale(cb[a], cb[3 + a]);
-        for (int i = threadIdx.x; i < 3 * kBins * 7; i += SMALL_T) {
-            const int w = i % 7;
-            bins[i] = w == 0 ? 0u : (w <= 3 ? 0xFFFFFFFFu : 0u);
-        }
+        for (int i = threadIdx.x; i < 3 * kBins * BIN_WORDS; i += SMALL_T) bins[i] = bin_init(i % BIN_WORDS);
         __syncthreads();
-        for (int i = threadIdx.x; i < st.count; i += SMALL_T) {
-            const int q = pa[st.lstart + i];
-            float L[3], H[3];
-#pragma unroll
-            for (int a = 0; a < 3; a++) { L[a] = blo[a * small_task + q]; H[a] = bhi[a * small_task + q]; }
-#pragma unroll
-            for (int a = 0; a < 3; a++) {
-                const int b = bin_of(centroid(L[a], H[a]), cb[a], k3[a]);
-                uint32_t* w = bins + (a * kBins + b) * 7;
-                atomicAdd(&w[0], 1u);
+        // each thread bins `per` consecutive positions; runs in one bin of an
+        // axis are merged in registers first (as in k_bin_large)
+        const int per = (st.count + SMALL_T - 1) / SMALL_T;  // <= small_task / SMALL_T
+        const int i0 = threadIdx.x * per, i1 = min(i0 + per, st.count);
+        {
+            int rb[3] = {-1, -1, -1};
+            uint32_t rc[3] = {0u, 0u, 0u};
+            float rl[3][3], rh[3][3];
+            auto flush = [&](int a) {
+                uint32_t* w = bins + (a * kBins + rb[a]) * BIN_WORDS;
+                atomicAdd(&w[0], rc[a]);
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
-                    atomicMin(&w[1 + k], f2ord(L[k]));
-                    atomicMax(&w[4 + k], f2ord(H[k]));
+                    atomicMin(&w[1 + k], f2ord(rl[a][k]));
+                    atomicMax(&w[4 + k], f2ord(rh[a][k]));
+                }
+            };
+            for (int i = i0; i < i1; i++) {
+                const int q = pa[st.lstart + i];
+                float L[3], H[3];
+#pragma unroll
+                for (int a = 0; a < 3; a++) { L[a] = blo[a * small_task + q]; H[a] = bhi[a * small_task + q]; }
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    const int b = bin_of(centroid(L[a], H[a]), cb[a], k3[a]);
+                    if (b != rb[a]) {
+                        if (rb[a] >= 0) flush(a);
+                        rb[a] = b;
+                        rc[a] = 1u;
+#pragma unroll
+                        for (int k = 0; k < 3; k++) { rl[a][k] = L[k]; rh[a][k] = H[k]; }
+                    } else {
+                        rc[a]++;
+#pragma unroll
+                        for (int k = 0; k < 3; k++) { rl[a][k] = fminf(rl[a][k], L[k]); rh[a][k] = fmaxf(rh[a][k], H[k]); }
+                    }
                 }
             }
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+                if (rb[a] >= 0) flush(a);
         }
         __syncthreads();
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         if (warp < 3) {
-            const uint32_t* w = bins + (warp * kBins + lane) * 7;
-            BinBox mine;
-            mine.cnt = (int)w[0];
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                mine.lo[k] = mine.cnt ? ord2f(w[1 + k]) : FLT_MAX;
-                mine.hi[k] = mine.cnt ? ord2f(w[4 + k]) : -FLT_MAX;
-            }
-            BinBox pre, suf;
+            const uint32_t* w = bins + (warp * kBins + lane) * BIN_WORDS;
+            BinBox mine = load_bin(w), pre, suf;
             prefix_suffix(mine, pre, suf);
             BinBox right = shfl_box(suf, 1, false);
             float cost = FLT_MAX;
@@ -755,6 +771,16 @@ __global__ void __launch_bounds__(SMALL_T) k_build_small(const Task* __restrict_
                 const float c2 = __shfl_xor_sync(FULL, c, o);
                 const int b2 = __shfl_xor_sync(FULL, b, o);
                 if (c2 < c || (c2 == c && b2 < b)) { c = c2; b = b2; }
+            }
+            // the children's boxes: the bins' union on each side of the split
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const float l0 = __shfl_sync(FULL, pre.lo[k], b), l1 = __shfl_sync(FULL, pre.hi[k], b);
+                const float r0 = __shfl_sync(FULL, right.lo[k], b), r1 = __shfl_sync(FULL, right.hi[k], b);
+                if (lane == 0) {
+                    s_cbox[warp][k] = l0; s_cbox[warp][3 + k] = l1;
+                    s_cbox[warp][6 + k] = r0; s_cbox[warp][9 + k] = r1;
+                }
             }
             if (lane == 0) { s_cost[warp] = c; s_cbin[warp] = b; }
         }
@@ -770,55 +796,50 @@ __global__ void __launch_bounds__(SMALL_T) k_build_small(const Task* __restrict_
         }
         __syncthreads();
         const int axis = s_axis, sbin = s_bin;
-        // stable partition of pa[lstart, lstart+count) into pb, then copy back
-        int nl_total = 0;
-        for (int base = 0; base < st.count; base += SMALL_T) {
-            const int i = base + threadIdx.x;
-            int f = 0;
-            int q = 0;
-            if (i < st.count) {
-                q = pa[st.lstart + i];
-                if (axis < 0) f = i < st.count / 2;
-                else f = bin_of(centroid(blo[axis * small_task + q], bhi[axis * small_task + q]), cb[axis], k3[axis]) <= sbin;
-            }
-            int tot;
-            const int r = block_exclusive_scan<SMALL_T>(f, ws, tot);
-            if (i < st.count && f) pb[st.lstart + nl_total + r] = (unsigned short)q;
-            nl_total += tot;
+        // stable partition of pa[lstart, lstart+count) in one scan: each
+        // thread flags its consecutive positions, counts its lefts, and
+        // writes lefts after the lefts before it and rights after all lefts
+        uint32_t fl = 0u;
+        int mine_l = 0;
+        for (int i = i0; i < i1; i++) {
+            const int q = pa[st.lstart + i];
+            const bool f = axis < 0 ? i < st.count / 2
+                                    : bin_of(centroid(blo[axis * small_task + q], bhi[axis * small_task + q]), cb[axis],
+                                             k3[axis]) <= sbin;
+            fl |= (f ? 1u : 0u) << (i - i0);
+            mine_l += f;
         }
-        int nr_done = 0;
-        for (int base = 0; base < st.count; base += SMALL_T) {
-            const int i = base + threadIdx.x;
-            int f = 0;
-            int q = 0;
-            if (i < st.count) {
-                q = pa[st.lstart + i];
-                if (axis < 0) f = !(i < st.count / 2);
-                else f = !(bin_of(centroid(blo[axis * small_task + q], bhi[axis * small_task + q]), cb[axis], k3[axis]) <= sbin);
-            }
-            int tot;
-            const int r = block_exclusive_scan<SMALL_T>(f, ws, tot);
-            if (i < st.count && f) pb[st.lstart + nl_total + nr_done + r] = (unsigned short)q;
-            nr_done += tot;
+        int nl;
+        int lb = block_exclusive_scan<SMALL_T>(mine_l, ws, nl);
+        int rb_ = (i0 - lb);  // rights before my first position
+        for (int i = i0; i < i1; i++) {
+            const unsigned short q = pa[st.lstart + i];
+            if ((fl >> (i - i0)) & 1u) pb[st.lstart + lb++] = q;
+            else pb[st.lstart + nl + rb_++] = q;
         }
         __syncthreads();
         for (int i = threadIdx.x; i < st.count; i += SMALL_T) pa[st.lstart + i] = pb[st.lstart + i];
         __syncthreads();
-        const int nl = nl_total;
-        // child boxes by reduction over each side
-        float bl[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
-        float br[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
-        for (int i = threadIdx.x; i < st.count; i += SMALL_T) {
-            const int q = pa[st.lstart + i];
-            float* B = i < nl ? bl : br;
+        // child boxes: from the bins, or by reduction after a median split
+        float bl[6], br[6];
+        if (axis >= 0) {
 #pragma unroll
-            for (int a = 0; a < 3; a++) {
-                B[a] = fminf(B[a], blo[a * small_task + q]);
-                B[3 + a] = fmaxf(B[3 + a], bhi[a * small_task + q]);
+            for (int k = 0; k < 6; k++) { bl[k] = s_cbox[axis][k]; br[k] = s_cbox[axis][6 + k]; }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 3; k++) { bl[k] = br[k] = FLT_MAX; bl[3 + k] = br[3 + k] = -FLT_MAX; }
+            for (int i = threadIdx.x; i < st.count; i += SMALL_T) {
+                const int q = pa[st.lstart + i];
+                float* B = i < nl ? bl : br;
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    B[a] = fminf(B[a], blo[a * small_task + q]);
+                    B[3 + a] = fmaxf(B[3 + a], bhi[a * small_task + q]);
+                }
             }
+            block_minmax6<SMALL_T>(bl, red);
+            block_minmax6<SMALL_T>(br, red);
         }
-        block_minmax6<SMALL_T>(bl, red);
-        block_minmax6<SMALL_T>(br, red);
         if (threadIdx.x == 0) {
             const int lid = next_node, rid = next_node + 1;
             next_node += 2;
@@ -1064,6 +1085,10 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
     }
     if (cfg.max_leaf < 1 || cfg.max_leaf > 4) {
         set_error("build: max_leaf must be 1..4");
+        return false;
+    }
+    if (cfg.small_task < WARP_TASK || cfg.small_task > 32 * SMALL_T) {  // k_build_small: <= 32 positions per thread
+        set_error("build: small_task must be %d..%d", WARP_TASK, 32 * SMALL_T);
         return false;
     }
     std::vector<int> seg = segments ? *segments : std::vector<int>{0, n};
