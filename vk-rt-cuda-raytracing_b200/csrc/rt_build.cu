@@ -206,15 +206,19 @@ __host__ __device__ __forceinline__ uint32_t bin_init(int w) {
 }
 constexpr int TASK_BIN_WORDS = 3 * kBins * BIN_WORDS;
 
-__global__ void k_chunk_counts(const Task* __restrict__ tasks, int T, int* __restrict__ cnt) {
+// The level loop runs ahead of the host: task and chunk counts stay on the
+// device, grids are sized for upper bounds, and threads past the count exit
+// (or write zeros where a scan covers the whole bound).
+__global__ void k_chunk_counts(const Task* __restrict__ tasks, const int* __restrict__ d_T, int Tb,
+                               int* __restrict__ cnt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < T) cnt[i] = (tasks[i].count + CHUNK - 1) / CHUNK;
+    if (i < Tb) cnt[i] = i < *d_T ? (tasks[i].count + CHUNK - 1) / CHUNK : 0;
 }
 
-__global__ void k_fill_chunks(const Task* __restrict__ tasks, int T, const int* __restrict__ off,
-                              Chunk* __restrict__ chunks) {
+__global__ void k_fill_chunks(const Task* __restrict__ tasks, const int* __restrict__ d_T,
+                              const int* __restrict__ off, Chunk* __restrict__ chunks) {
     const int t = blockIdx.x;
-    if (t >= T) return;
+    if (t >= *d_T) return;
     const Task tk = tasks[t];
     const int nc = (tk.count + CHUNK - 1) / CHUNK;
     for (int c = threadIdx.x; c < nc; c += blockDim.x) {
@@ -227,8 +231,8 @@ __global__ void k_fill_chunks(const Task* __restrict__ tasks, int T, const int* 
     }
 }
 
-__global__ void k_clear_bins(uint32_t* __restrict__ bins, int T) {
-    const size_t total = (size_t)T * TASK_BIN_WORDS;
+__global__ void k_clear_bins(uint32_t* __restrict__ bins, const int* __restrict__ d_T) {
+    const size_t total = (size_t)*d_T * TASK_BIN_WORDS;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
         bins[i] = bin_init((int)(i % BIN_WORDS));
     }
@@ -236,8 +240,10 @@ __global__ void k_clear_bins(uint32_t* __restrict__ bins, int T) {
 
 __global__ void __launch_bounds__(CHUNK_T) k_bin_large(const Chunk* __restrict__ chunks, const Task* __restrict__ tasks,
                                                        const int* __restrict__ perm, const float4* __restrict__ plo,
-                                                       const float4* __restrict__ phi, uint32_t* __restrict__ gbins) {
+                                                       const float4* __restrict__ phi, uint32_t* __restrict__ gbins,
+                                                       const int* __restrict__ d_C) {
     __shared__ uint32_t sb[TASK_BIN_WORDS];
+    if (blockIdx.x >= *d_C) return;
     const Chunk ch = chunks[blockIdx.x];
     const Task tk = tasks[ch.task];
     for (int i = threadIdx.x; i < TASK_BIN_WORDS; i += CHUNK_T) sb[i] = bin_init(i % BIN_WORDS);
@@ -349,11 +355,13 @@ __device__ BinBox load_bin(const uint32_t* w) {
 
 // One warp per task: best (axis, bin) by SAH; writes the split, the two
 // child nodes (ids base + 2t, base + 2t + 1) and their task descriptors.
-__global__ void k_split_large(const Task* __restrict__ tasks, int T, const uint32_t* __restrict__ gbins,
-                              Split* __restrict__ splits, Task* __restrict__ kids, uint32_t* __restrict__ kcb,
-                              Node2* __restrict__ nodes, int node_base, int max_leaf, int max_sah_depth) {
+__global__ void k_split_large(const Task* __restrict__ tasks, const int* __restrict__ d_T,
+                              const uint32_t* __restrict__ gbins, Split* __restrict__ splits, Task* __restrict__ kids,
+                              uint32_t* __restrict__ kcb, Node2* __restrict__ nodes, const int* __restrict__ d_node_base,
+                              int max_leaf, int max_sah_depth) {
     const int t = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-    if (t >= T) return;
+    if (t >= *d_T) return;
+    const int node_base = *d_node_base;
     const int lane = threadIdx.x & 31;
     const Task tk = tasks[t];
     const uint32_t* g = gbins + (size_t)t * TASK_BIN_WORDS;
@@ -447,8 +455,10 @@ __device__ __forceinline__ bool goes_left(const Task& tk, const Split& sp, int p
 __global__ void __launch_bounds__(CHUNK_T) k_count_left(const Chunk* __restrict__ chunks, const Task* __restrict__ tasks,
                                                         const Split* __restrict__ splits, const int* __restrict__ perm,
                                                         const float4* __restrict__ plo, const float4* __restrict__ phi,
-                                                        int* __restrict__ chunk_left, uint32_t* __restrict__ kcb) {
+                                                        int* __restrict__ chunk_left, uint32_t* __restrict__ kcb,
+                                                        const int* __restrict__ d_C) {
     __shared__ int ws[CHUNK_T / 32];
+    if (blockIdx.x >= *d_C) return;  // (the scan over the bound reads stale counts only after the last chunk)
     const Chunk ch = chunks[blockIdx.x];
     const Task tk = tasks[ch.task];
     const Split sp = splits[ch.task];
@@ -509,8 +519,10 @@ __global__ void __launch_bounds__(CHUNK_T) k_count_left(const Chunk* __restrict_
 __global__ void __launch_bounds__(CHUNK_T) k_scatter(const Chunk* __restrict__ chunks, const Task* __restrict__ tasks,
                                                      const Split* __restrict__ splits, const int* __restrict__ perm,
                                                      const float4* __restrict__ plo, const float4* __restrict__ phi,
-                                                     const int* __restrict__ left_off, int* __restrict__ out) {
+                                                     const int* __restrict__ left_off, int* __restrict__ out,
+                                                     const int* __restrict__ d_C) {
     __shared__ int ws[CHUNK_T / 32];
+    if (blockIdx.x >= *d_C) return;
     const Chunk ch = chunks[blockIdx.x];
     const Task tk = tasks[ch.task];
     const Split sp = splits[ch.task];
@@ -541,37 +553,65 @@ __global__ void __launch_bounds__(CHUNK_T) k_scatter(const Chunk* __restrict__ c
     }
 }
 
-__global__ void k_copy_back(const Chunk* __restrict__ chunks, const int* __restrict__ src, int* __restrict__ dst) {
+__global__ void k_copy_back(const Chunk* __restrict__ chunks, const int* __restrict__ src, int* __restrict__ dst,
+                            const int* __restrict__ d_C) {
+    if (blockIdx.x >= *d_C) return;
     const Chunk ch = chunks[blockIdx.x];
     for (int i = threadIdx.x; i < ch.count; i += blockDim.x) dst[ch.start + i] = src[ch.start + i];
 }
 
-__global__ void k_classify_flags(const Task* __restrict__ kids, int K, int max_leaf, int small_task,
-                                 int* __restrict__ is_large, int* __restrict__ is_small) {
+__global__ void k_classify_flags(const Task* __restrict__ kids, const int* __restrict__ d_T, int Kb, int max_leaf,
+                                 int small_task, int* __restrict__ is_large, int* __restrict__ is_small) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= K) return;
+    if (i >= Kb) return;
+    if (i >= 2 * *d_T) {  // past this level's kids: zeros for the scans over the bound
+        is_large[i] = 0;
+        is_small[i] = 0;
+        return;
+    }
     const int c = kids[i].count;
     is_large[i] = c > small_task;
     is_small[i] = c > max_leaf && c <= small_task;
 }
 
-__global__ void k_compact_kids(const Task* __restrict__ kids, int K, const int* __restrict__ is_large,
-                               const int* __restrict__ large_off, const int* __restrict__ is_small,
-                               const int* __restrict__ small_off, Task* __restrict__ next, Task* __restrict__ small,
-                               const int* __restrict__ small_base, const uint32_t* __restrict__ kcb) {
+__global__ void k_compact_kids(const Task* __restrict__ kids, const int* __restrict__ d_T,
+                               const int* __restrict__ is_large, const int* __restrict__ large_off,
+                               const int* __restrict__ is_small, const int* __restrict__ small_off,
+                               Task* __restrict__ next, int max_large, Task* __restrict__ small, int max_small,
+                               const int* __restrict__ small_base, const uint32_t* __restrict__ kcb,
+                               int* __restrict__ status) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= K) return;
+    if (i >= 2 * *d_T) return;
     Task t = kids[i];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         t.clo[k] = ord2f(kcb[(size_t)i * 6 + k]);
         t.chi[k] = ord2f(kcb[(size_t)i * 6 + 3 + k]);
     }
-    if (is_large[i]) next[large_off[i]] = t;
-    if (is_small[i]) small[*small_base + small_off[i]] = t;
+    if (is_large[i]) {
+        if (large_off[i] < max_large) next[large_off[i]] = t;
+        else atomicOr(status, 8);
+    }
+    if (is_small[i]) {
+        const int at = *small_base + small_off[i];
+        if (at < max_small) small[at] = t;
+        else atomicOr(status, 8);
+    }
 }
 
-__global__ void k_add_small(int* small_base, const int* add) { *small_base += *add; }
+// End of a level: node ids advance past this level's kids, the small list
+// grows, the next level's task count becomes current and is logged for the
+// host (which reads it one level behind).
+__global__ void k_level_end(int* __restrict__ d_T, int* __restrict__ d_node_count, int* __restrict__ small_base,
+                            const int* __restrict__ tot, int max_large, int max_small, int* __restrict__ log_T,
+                            int* __restrict__ status) {
+    *d_node_count += 2 * *d_T;
+    *small_base = min(*small_base + tot[1], max_small);
+    const int tn = tot[0];
+    if (tn > max_large) atomicOr(status, 8);
+    *d_T = min(tn, max_large);
+    *log_T = *d_T;
+}
 
 // ----------------------------------------------------------- small tasks --
 // One CTA finishes the subtree of a task of <= small_task primitives in
@@ -1070,6 +1110,41 @@ __global__ void k_iota(int* __restrict__ p, int n) {
 }
 
 // ----------------------------------------------------------- the driver --
+// Per host thread: pinned slots the level loop copies each level's task
+// count into, and an event per level to wait on (created once per thread).
+constexpr int kMaxLevels = 160;  // SAH depth 48, then median splits: far fewer levels
+struct LevelLog {
+    int* count = nullptr;
+    cudaEvent_t ev[kMaxLevels] = {};
+    bool ok = false;
+    LevelLog() {
+        if (cudaHostAlloc(reinterpret_cast<void**>(&count), sizeof(int) * kMaxLevels, cudaHostAllocDefault) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        for (int i = 0; i < kMaxLevels; i++)
+            if (cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                return;
+            }
+        ok = true;
+    }
+    ~LevelLog() {
+        for (int i = 0; i < kMaxLevels; i++)
+            if (ev[i]) cudaEventDestroy(ev[i]);
+        if (count) cudaFreeHost(count);
+    }
+};
+static LevelLog* level_log() {
+    static thread_local LevelLog lg;
+    if (!lg.ok) {
+        set_error("build: pinned level log unavailable");
+        return nullptr;
+    }
+    return &lg;
+}
+
 BuildConfig default_build_config() {
     BuildConfig c;
     if (const char* e = getenv("RTB200_MAX_LEAF")) c.max_leaf = std::max(1, std::min(4, atoi(e)));
@@ -1184,54 +1259,77 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
     if (!small0.empty() &&
         !RT_CUDA(cudaMemcpyAsync(small.p, small0.data(), small0.size() * sizeof(Task), cudaMemcpyHostToDevice, s)))
         return false;
-    int node_count = S;
     int num_small = (int)small0.size();
     int* d_small_base = flags.p + 8 * maxT;  // running count of small tasks
     int* d_tot = d_small_base + 1;           // scratch totals [large, small, chunks]
-    cudaMemcpyAsync(d_small_base, &num_small, sizeof(int), cudaMemcpyHostToDevice, s);
-    int T = (int)large0.size();
-    if (!RT_CUDA(cudaStreamSynchronize(s))) return false;
+    int* d_C = d_tot + 2;
+    // ctl: [0] this level's task count, [1] next node id, [2 + l] task count
+    // of level l + 1 as logged for the host
+    TmpBuf<int> ctl;
+    if (!ctl.alloc(2 + kMaxLevels, s)) return false;
+    int* d_T = ctl.p;
+    int* d_node = ctl.p + 1;
+    const int init[2] = {(int)large0.size(), S};
+    if (!RT_CUDA(cudaMemcpyAsync(d_small_base, &num_small, sizeof(int), cudaMemcpyHostToDevice, s)) ||
+        !RT_CUDA(cudaMemcpyAsync(ctl.p, init, sizeof(init), cudaMemcpyHostToDevice, s)) ||
+        !RT_CUDA(cudaStreamSynchronize(s)))
+        return false;
     Task* cur = tasks_a.p;
     Task* nxt = tasks_b.p;
     int* is_large = flags.p;
     int* is_small = flags.p + 2 * maxT;
     int* large_off = flags.p + 4 * maxT;
     int* small_off = flags.p + 6 * maxT;
-    while (T > 0) {
-        // chunks
-        k_chunk_counts<<<(T + 255) / 256, 256, 0, s>>>(cur, T, ccount.p);
-        if (!scan_exclusive(ccount.p, coff.p, T, d_tot + 2, s)) return false;
-        int C = 0;
-        cudaMemcpyAsync(&C, d_tot + 2, sizeof(int), cudaMemcpyDeviceToHost, s);
-        if (!RT_CUDA(cudaStreamSynchronize(s))) return false;
-        k_fill_chunks<<<T, 128, 0, s>>>(cur, T, coff.p, chunks.p);
-        k_clear_bins<<<std::min(T * 8, 4096), 256, 0, s>>>(gbins.p, T);
-        k_bin_large<<<C, CHUNK_T, 0, s>>>(chunks.p, cur, perm, d_lo, d_hi, gbins.p);
-        k_split_large<<<(T + 3) / 4, 128, 0, s>>>(cur, T, gbins.p, splits.p, kids.p, kcb.p, out.nodes.p,
-                                                   node_count, cfg.max_leaf, cfg.max_sah_depth);
-        k_count_left<<<C, CHUNK_T, 0, s>>>(chunks.p, cur, splits.p, perm, d_lo, d_hi, cleft.p, kcb.p);
-        if (!scan_exclusive(cleft.p, cleftoff.p, C, nullptr, s)) return false;
-        k_scatter<<<C, CHUNK_T, 0, s>>>(chunks.p, cur, splits.p, perm, d_lo, d_hi, cleftoff.p, tmp.p);
-        k_copy_back<<<C, 256, 0, s>>>(chunks.p, tmp.p, perm);
-        node_count += 2 * T;
-        const int K = 2 * T;
-        k_classify_flags<<<(K + 255) / 256, 256, 0, s>>>(kids.p, K, cfg.max_leaf, cfg.small_task, is_large, is_small);
-        if (!scan_exclusive(is_large, large_off, K, d_tot, s)) return false;
-        if (!scan_exclusive(is_small, small_off, K, d_tot + 1, s)) return false;
-        k_compact_kids<<<(K + 255) / 256, 256, 0, s>>>(kids.p, K, is_large, large_off, is_small, small_off, nxt,
-                                                      small.p, d_small_base, kcb.p);
-        k_add_small<<<1, 1, 0, s>>>(d_small_base, d_tot + 1);
-        int h[2];
-        cudaMemcpyAsync(h, d_tot, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
-        if (!RT_CUDA(cudaStreamSynchronize(s))) return false;
-        T = h[0];
-        num_small += h[1];
-        std::swap(cur, nxt);
-        if (num_small > maxSmall) {
-            set_error("build: small-task overflow");
+    // Levels are queued ahead of the host: every launch is sized for an
+    // upper bound (a level has at most twice the tasks of the one before,
+    // and at most maxT), and the host learns each level's count one level
+    // later, while the GPU already works on the next.  A level queued after
+    // the last real one has no tasks and does nothing.
+    LevelLog* lg = level_log();
+    if (!lg) return false;
+    int Tb = (int)large0.size();
+    for (int lvl = 0; Tb > 0; lvl++) {
+        if (lvl >= kMaxLevels) {
+            set_error("build: more than %d levels", kMaxLevels);
             return false;
         }
+        const int Cb = n / CHUNK + Tb + 1;  // sum over tasks of ceil(count / CHUNK) <= n / CHUNK + T
+        const int Kb = 2 * Tb;
+        k_chunk_counts<<<(Tb + 255) / 256, 256, 0, s>>>(cur, d_T, Tb, ccount.p);
+        if (!scan_exclusive(ccount.p, coff.p, Tb, d_C, s)) return false;
+        k_fill_chunks<<<Tb, 128, 0, s>>>(cur, d_T, coff.p, chunks.p);
+        k_clear_bins<<<std::min(Tb * 8, 4096), 256, 0, s>>>(gbins.p, d_T);
+        k_bin_large<<<Cb, CHUNK_T, 0, s>>>(chunks.p, cur, perm, d_lo, d_hi, gbins.p, d_C);
+        k_split_large<<<(Tb + 3) / 4, 128, 0, s>>>(cur, d_T, gbins.p, splits.p, kids.p, kcb.p, out.nodes.p, d_node,
+                                                    cfg.max_leaf, cfg.max_sah_depth);
+        k_count_left<<<Cb, CHUNK_T, 0, s>>>(chunks.p, cur, splits.p, perm, d_lo, d_hi, cleft.p, kcb.p, d_C);
+        if (!scan_exclusive(cleft.p, cleftoff.p, Cb, nullptr, s)) return false;
+        k_scatter<<<Cb, CHUNK_T, 0, s>>>(chunks.p, cur, splits.p, perm, d_lo, d_hi, cleftoff.p, tmp.p, d_C);
+        k_copy_back<<<Cb, 256, 0, s>>>(chunks.p, tmp.p, perm, d_C);
+        k_classify_flags<<<(Kb + 255) / 256, 256, 0, s>>>(kids.p, d_T, Kb, cfg.max_leaf, cfg.small_task, is_large,
+                                                          is_small);
+        if (!scan_exclusive(is_large, large_off, Kb, d_tot, s)) return false;
+        if (!scan_exclusive(is_small, small_off, Kb, d_tot + 1, s)) return false;
+        k_compact_kids<<<(Kb + 255) / 256, 256, 0, s>>>(kids.p, d_T, is_large, large_off, is_small, small_off, nxt,
+                                                        maxT, small.p, maxSmall, d_small_base, kcb.p, status.p);
+        k_level_end<<<1, 1, 0, s>>>(d_T, d_node, d_small_base, d_tot, maxT, maxSmall, ctl.p + 2 + lvl, status.p);
+        if (!RT_CUDA(cudaMemcpyAsync(lg->count + lvl, ctl.p + 2 + lvl, sizeof(int), cudaMemcpyDeviceToHost, s)) ||
+            !RT_CUDA(cudaEventRecord(lg->ev[lvl], s)))
+            return false;
+        std::swap(cur, nxt);
+        Tb = std::min(2 * Tb, maxT);
+        if (lvl >= 1) {
+            if (!RT_CUDA(cudaEventSynchronize(lg->ev[lvl - 1]))) return false;
+            if (lg->count[lvl - 1] == 0) Tb = 0;  // this level had no tasks: done
+        }
     }
+    int hc[2] = {0, 0};
+    if (!RT_CUDA(cudaMemcpyAsync(&hc[0], d_node, sizeof(int), cudaMemcpyDeviceToHost, s)) ||
+        !RT_CUDA(cudaMemcpyAsync(&hc[1], d_small_base, sizeof(int), cudaMemcpyDeviceToHost, s)) ||
+        !RT_CUDA(cudaStreamSynchronize(s)))
+        return false;
+    int node_count = hc[0];
+    num_small = hc[1];
     if (num_small > 0) {
         TmpBuf<int> need, off;
         if (!need.alloc(num_small, s) || !off.alloc(num_small, s)) return false;
@@ -1271,7 +1369,8 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
     cudaMemcpyAsync(&st, status.p, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (!RT_CUDA(cudaStreamSynchronize(s))) return false;
     if (st) {
-        set_error("build: %s", (st & 2) ? "subtree queue overflow" : "subtree stack overflow");
+        set_error("build: %s", (st & 8) ? "task list overflow" : (st & 2) ? "subtree queue overflow"
+                                                                        : "subtree stack overflow");
         return false;
     }
     out.num_nodes = node_count;
