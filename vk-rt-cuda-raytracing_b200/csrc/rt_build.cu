@@ -1,24 +1,26 @@
-// rt_build.cu -- GPU binned-SAH builder (32 bins) and collapse to the
-// compressed 8-wide layout.
+// rt_build.cu -- GPU SAH builder of the binary BVH (the 8-wide collapse is
+// in rt_collapse.cu).
 //
-// Builder (replaces the reference's single-threaded CPU BVH2Builder,
-// layer/cuda_bvh_backend.cu:201-251 / cuda_rt_v40.cu:790-840):
-//   * top-down, level-synchronous for tasks larger than `small_task`
-//     primitives: chunked CTA binning into shared-memory bins (3 axes x 32
-//     bins, order-independent min/max/add atomics, so the result does not
-//     depend on scheduling), one warp per task evaluates the 31 split planes
-//     per axis (lane = bin, prefix/suffix by shuffles), a stable partition by
-//     chunk scans;
-//   * tasks of at most `small_task` primitives finish their whole subtree in
-//     one CTA out of shared memory.
-//   Cost model: C = N_L*A(L) + N_R*A(R) (same split search as the reference);
-//   leaves at <= max_leaf primitives; no valid split or depth >= max_sah_depth
-//   -> object-median split.  Every step is deterministic.
-// Collapse: top-down, one thread per 8-wide node: greedily open the child
-// with the largest surface area until 8 children (Ylitie, Karras, Laine,
-// HPG 2017), assign children to octant slots, quantise child boxes outward
-// to 8 bits per plane against a power-of-two grid, emit triangle records
-// in node order.
+// Replaces the reference's single-threaded CPU BVH2Builder
+// (layer/cuda_bvh_backend.cu:201-251 / cuda_rt_v40.cu:790-840).  Cost model
+// C = N_L*A(L) + N_R*A(R), the reference's split search; leaves at
+// <= max_leaf primitives; depth >= max_sah_depth -> object-median split.
+// Three tiers by task size, every step deterministic:
+//   * tasks > small_task (1024) primitives: level-synchronous over all
+//     tasks (and all scenes of a batch) at once.  Chunked CTA binning into
+//     shared-memory bins (3 axes x 32 bins, count + box per bin, order-
+//     independent atomics; a thread's run of primitives in one bin is
+//     merged in registers first), one warp per task scans the 31 planes per
+//     axis (lane = bin), a stable partition by chunk scans that also gathers
+//     the children's centroid bounds.  The loop is queued ahead of the host:
+//     counts stay on the device and the host reads each level's task count
+//     one level late, so the GPU never waits for it.
+//   * tasks of 33..small_task primitives: one CTA per task, node by node, in
+//     shared memory (binned SAH, single-scan partition, child boxes from the
+//     split's bins).
+//   * subtrees of <= 32 primitives: one warp per subtree, exact SAH sweep
+//     over centroid-sorted orders, a whole level per pass (k_build_warp).
+// Scratch comes from the pooled stream-ordered allocator (TmpBuf).
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
