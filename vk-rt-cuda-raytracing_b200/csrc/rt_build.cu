@@ -1353,16 +1353,16 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
                                                        cfg.max_leaf, cfg.max_sah_depth, cfg.small_task, warp_task,
                                                        wq.p, wq_cap, d_wq_count, status.p);
         if (warp_task > 0) {
-            static int per_sm = 0, sms = 0;
-            if (!per_sm) {
-                int dev = 0;
-                cudaGetDevice(&dev);
-                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_warp, WB_T, 0);
-                per_sm = std::max(per_sm, 1);
-            }
-            k_build_warp<<<sms * per_sm, WB_T, 0, s>>>(wq.p, d_wq_count, wq_cap, perm, d_lo, d_hi, out.nodes.p,
-                                                       cfg.max_leaf, cfg.max_sah_depth);
+            static const int grid = [] {  // persistent: as many CTAs as fit
+                int per_sm = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_build_warp, WB_T, 0) != cudaSuccess) {
+                    cudaGetLastError();
+                    per_sm = 1;
+                }
+                return num_sms() * std::max(per_sm, 1);
+            }();
+            k_build_warp<<<grid, WB_T, 0, s>>>(wq.p, d_wq_count, wq_cap, perm, d_lo, d_hi, out.nodes.p, cfg.max_leaf,
+                                               cfg.max_sah_depth);
         }
         if (!RT_CUDA(cudaStreamSynchronize(s))) return false;
         node_count += reserved;
