@@ -98,7 +98,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = Path(path) if path else LIB_PATH
+    # RTB200_LIB: another build of the library (an A/B of build options)
+    p = Path(path) if path else Path(os.environ.get("RTB200_LIB") or LIB_PATH)
     if not p.exists():
         raise RtError(f"libcudabvh_b200.so not built: {p} (run __graft_entry__.build())")
     L = C.CDLL(str(p))
