@@ -1151,6 +1151,7 @@ BuildConfig default_build_config() {
     BuildConfig c;
     if (const char* e = getenv("RTB200_MAX_LEAF")) c.max_leaf = std::max(1, std::min(4, atoi(e)));
     if (const char* e = getenv("RTB200_WARP_TASK")) c.warp_task = std::max(0, std::min(WARP_TASK, atoi(e)));
+    if (const char* e = getenv("RTB200_SMALL_TASK")) c.small_task = std::max(WARP_TASK, std::min(32 * SMALL_T, atoi(e)));
     return c;
 }
 

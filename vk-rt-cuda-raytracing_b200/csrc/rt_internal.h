@@ -128,7 +128,8 @@ struct Bvh8Device {
     int depth = 0;
 };
 
-// Defaults with the environment's overrides (RTB200_MAX_LEAF, RTB200_WARP_TASK).
+// Defaults with the environment's overrides (RTB200_MAX_LEAF, RTB200_WARP_TASK,
+// RTB200_SMALL_TASK).
 BuildConfig default_build_config();
 
 // Builds the binary SAH BVH over primitive boxes (lo/hi float4 per prim).
