@@ -24,8 +24,6 @@ struct RtBatchHandle {
     int num_tris = 0;
     std::vector<int> tri_off;
     DevBuf<int> d_tri_off;
-    DevBuf<float> tris9;
-    Bvh2Device bvh2;
     Bvh8Device bvh8;
     DevBuf<int> work, status;  // work[0]: plain launches, work[1]: graph launches
     int ctas_per_sm = TRACE_MINB;
@@ -114,21 +112,26 @@ RtBatch_t rtBatch_build(const CudaTri* h_tris, const int* tri_offsets, int num_s
     b->num_tris = tri_offsets[num_scenes];
     b->tri_off.assign(tri_offsets, tri_offsets + num_scenes + 1);
     const int n = b->num_tris;
+    // the input triangles and the binary tree are needed only while building:
+    // pooled scratch and a local tree, gone when the build returns
+    TmpBuf<float> tris9;
     TmpBuf<float4> lo, hi;
+    Bvh2Device bvh2;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    bool ok = b->tris9.alloc((size_t)n * 9) && b->d_tri_off.alloc(num_scenes + 1) && lo.alloc(n, s) && hi.alloc(n, s) &&
+    bool ok = tris9.alloc((size_t)n * 9, s) && b->d_tri_off.alloc(num_scenes + 1) && lo.alloc(n, s) && hi.alloc(n, s) &&
               b->work.alloc(2) && b->status.alloc(1) &&
-              RT_CUDA(cudaMemcpyAsync(b->tris9.p, h_tris, sizeof(CudaTri) * (size_t)n, cudaMemcpyHostToDevice, s)) &&
+              RT_CUDA(cudaMemcpyAsync(tris9.p, h_tris, sizeof(CudaTri) * (size_t)n, cudaMemcpyHostToDevice, s)) &&
               RT_CUDA(cudaMemcpyAsync(b->d_tri_off.p, tri_offsets, sizeof(int) * (num_scenes + 1),
                                       cudaMemcpyHostToDevice, s)) &&
               RT_CUDA(cudaMemsetAsync(b->status.p, 0, sizeof(int), s));
     if (ok) {
         cudaEventRecord(e0, s);
-        launch_tri_bounds(b->tris9.p, n, lo.p, hi.p, s);
-        const BuildConfig cfg = default_build_config();
-        ok = build_bvh2(lo.p, hi.p, n, cfg, b->bvh2, s, &b->tri_off) && collapse_bvh8(b->bvh2, b->tris9.p, b->bvh8, s);
+        launch_tri_bounds(tris9.p, n, lo.p, hi.p, s);
+        BuildConfig cfg = default_build_config();
+        cfg.transient = true;
+        ok = build_bvh2(lo.p, hi.p, n, cfg, bvh2, s, &b->tri_off) && collapse_bvh8(bvh2, tris9.p, b->bvh8, s);
         cudaEventRecord(e1, s);
         ok = ok && RT_CUDA(cudaEventSynchronize(e1));
         if (ok) cudaEventElapsedTime(&b->build_ms, e0, e1);

@@ -1182,7 +1182,9 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
         }
     out.num_prims = n;
     out.num_roots = S;
-    if (!out.nodes.alloc((size_t)2 * n + 2) || !out.perm.alloc(n)) return false;
+    if (cfg.transient ? (!out.nodes.alloc_on((size_t)2 * n + 2, s) || !out.perm.alloc_on(n, s))
+                      : (!out.nodes.alloc((size_t)2 * n + 2) || !out.perm.alloc(n)))
+        return false;
     cudaMemsetAsync(out.nodes.p, 0, out.nodes.bytes(), s);
     int* perm = out.perm.p;
     // temporaries

@@ -34,6 +34,8 @@ template <class T>
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
+    cudaStream_t pool_stream = nullptr;  // set when the memory came from scratch_pool()
+    bool pooled = false;
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
@@ -50,11 +52,18 @@ struct DevBuf {
         n = count;
         return true;
     }
+    // From the scratch pool, ordered on `st` (allocation and release): for
+    // buffers that die before the stream's work is done with them.
+    bool alloc_on(size_t count, cudaStream_t st);
     bool ensure(size_t count) { return count <= n ? true : alloc(count); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (pooled) cudaFreeAsync(p, pool_stream);
+            else cudaFree(p);
+        }
         p = nullptr;
         n = 0;
+        pooled = false;
     }
     size_t bytes() const { return n * sizeof(T); }
 };
@@ -99,6 +108,23 @@ struct TmpBuf {
     size_t bytes() const { return n * sizeof(T); }
 };
 
+template <class T>
+bool DevBuf<T>::alloc_on(size_t count, cudaStream_t st) {
+    release();
+    if (count == 0) return true;
+    cudaMemPool_t pool = scratch_pool();
+    if (!pool || cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(T), pool, st) != cudaSuccess) {
+        cudaGetLastError();
+        p = nullptr;
+        set_error("scratch allocation of %zu bytes failed", count * sizeof(T));
+        return false;
+    }
+    pooled = true;
+    pool_stream = st;
+    n = count;
+    return true;
+}
+
 // ---- build configuration ----
 struct BuildConfig {
     int max_leaf = 2;        // triangles per BVH2 leaf (1..kMaxLeafTris); the 8-wide
@@ -107,6 +133,8 @@ struct BuildConfig {
     int max_sah_depth = 48;  // deeper tasks fall back to median splits
     int warp_task = 32;      // subtrees of at most this many primitives (<= 32) are
                              // finished by one warp with an exact SAH sweep; 0 = off
+    bool transient = false;  // the binary tree comes from the scratch pool (a caller
+                             // that drops it right after the collapse)
 };
 
 // Result of the SAH builder on the device.
