@@ -28,6 +28,8 @@
 #include <cstring>
 #include <vector>
 
+#include <cuda/atomic>
+
 #include "rt_internal.h"
 
 using namespace rtb;
@@ -184,9 +186,9 @@ __global__ void k_refit(Node2* __restrict__ nodes, int slots, const int* __restr
             atomicOr(status, 1);
             return;
         }
-        __threadfence();
-        if (atomicAdd(&arrive[par], 1) == 0) return;
-        __threadfence();
+        // release our box, acquire the sibling's: the second arrival sees both
+        cuda::atomic_ref<int, cuda::thread_scope_device> arr(arrive[par]);
+        if (arr.fetch_add(1, cuda::memory_order_acq_rel) == 0) return;
         const int a = __ldcg(&nodes[par].a), b = __ldcg(&nodes[par].b);
         float bl[3], bh[3];
         for (int k = 0; k < 3; k++) {
@@ -208,9 +210,10 @@ bool refit_handle(CudaBVHHandle* h, cudaStream_t s) {
         set_error("cudaBVH_refit: handle has %d roots", b2.num_roots);
         return false;
     }
-    DevBuf<float4> lo, hi;
-    DevBuf<int> parent, arrive, status;
-    if (!lo.alloc(n) || !hi.alloc(n) || !parent.alloc(slots) || !arrive.alloc(slots) || !status.alloc(1))
+    TmpBuf<float4> lo, hi;
+    TmpBuf<int> parent, arrive, status;
+    if (!lo.alloc(n, s) || !hi.alloc(n, s) || !parent.alloc(slots, s) || !arrive.alloc(slots, s) ||
+        !status.alloc(1, s))
         return false;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -379,8 +382,8 @@ CudaBVH_t cudaBVH_buildGeometries(const RtGeometry* geoms, int num_geoms, void* 
     cudaStream_t s = (cudaStream_t)stream;
     CudaBVHHandle* h = create_handle((int)n);
     if (!h) return nullptr;
-    DevBuf<int> bad;
-    const bool ok = h->tris9.alloc((size_t)n * 9) && bad.alloc(1) &&
+    TmpBuf<int> bad;
+    const bool ok = h->tris9.alloc((size_t)n * 9) && bad.alloc(1, s) &&
                     RT_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s)) &&
                     gather_geometries(geoms, num_geoms, h->tris9.p, bad.p, s, "cudaBVH_buildGeometries") &&
                     build_handle(h, s);
@@ -418,9 +421,9 @@ int cudaBVH_refitGeometries(CudaBVH_t h, const RtGeometry* geoms, int num_geoms,
     }
     cudaStream_t s = (cudaStream_t)stream;
     std::lock_guard<std::mutex> g(h->mu);
-    DevBuf<float> tmp;
-    DevBuf<int> bad;
-    if (!tmp.alloc((size_t)h->num_tris * 9) || !bad.alloc(1) ||
+    TmpBuf<float> tmp;
+    TmpBuf<int> bad;
+    if (!tmp.alloc((size_t)h->num_tris * 9, s) || !bad.alloc(1, s) ||
         !RT_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s)))
         return RT_ERR_NOMEM;
     if (!gather_geometries(geoms, num_geoms, tmp.p, bad.p, s, "cudaBVH_refitGeometries")) return RT_ERR_INVALID;
