@@ -56,6 +56,17 @@ using namespace rtb;
 namespace {
 
 constexpr size_t kAlign = 256;
+
+// A wavefront's segment table moves host->device and its status word
+// device->host through the SMs, reading and writing the pinned staging
+// directly: the copy engines carry request rays and results in large
+// pieces, and a small copy queued behind them held each wavefront's launch
+// (measured on the 256-request trace: trace streams busy 200+ ms of a
+// 220 ms span while the kernels themselves needed far less).
+__global__ void k_fetch_segs(const uint4* __restrict__ src, uint4* __restrict__ dst, int n16) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n16; i += gridDim.x * blockDim.x) dst[i] = src[i];
+}
+__global__ void k_put_status(const int* __restrict__ src, int* __restrict__ dst) { *dst = *src; }
 constexpr int kMaxSeg = 512;  // segments per hit kind in one wavefront
 
 size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
@@ -147,6 +158,10 @@ struct WaveSlot {
     DevBuf<WaveSeg> d_segs;
     WaveSeg* h_segs = nullptr;  // pinned staging of the segment table
     int* h_status = nullptr;    // pinned status word of this wavefront
+    // the same two pinned buffers as the device addresses them (mapped), or
+    // null where the device cannot: then copy engines move them instead
+    const uint4* m_segs = nullptr;
+    int* m_status = nullptr;
     DevBuf<int> work;           // [0] closest, [1] any
     DevBuf<int> status;
     std::vector<Chunk> chunks;
@@ -403,9 +418,16 @@ bool RtServerHandle::launch_wave(WaveSlot* w) {
     for (const Chunk& c : w->chunks) c.req->waves++;
     w->rays = tc + ta;
     cudaStream_t s = w->stream;
-    bool ok = RT_CUDA(cudaMemcpyAsync(w->d_segs.p, w->h_segs, sizeof(WaveSeg) * 2 * kMaxSeg, cudaMemcpyHostToDevice,
-                                      s)) &&
-              RT_CUDA(cudaMemsetAsync(w->work.p, 0, 2 * sizeof(int), s)) &&
+    bool ok = true;
+    if (w->m_segs) {
+        static_assert(sizeof(WaveSeg) % 16 == 0, "segment table moves as 16-byte words");
+        k_fetch_segs<<<8, 256, 0, s>>>(w->m_segs, reinterpret_cast<uint4*>(w->d_segs.p),
+                                       (int)(sizeof(WaveSeg) * 2 * kMaxSeg / 16));
+        ok = RT_CUDA(cudaGetLastError());
+    } else {
+        ok = RT_CUDA(cudaMemcpyAsync(w->d_segs.p, w->h_segs, sizeof(WaveSeg) * 2 * kMaxSeg, cudaMemcpyHostToDevice, s));
+    }
+    ok = ok && RT_CUDA(cudaMemsetAsync(w->work.p, 0, 2 * sizeof(int), s)) &&
               RT_CUDA(cudaMemsetAsync(w->status.p, 0, sizeof(int), s));
     const uint4* nd = reinterpret_cast<const uint4*>(nodes.p);
     const float4* tr = reinterpret_cast<const float4*>(tris.p);
@@ -413,8 +435,13 @@ bool RtServerHandle::launch_wave(WaveSlot* w) {
                                          TRACE_MINB, s) == RT_OK;
     if (ok && na) ok = launch_trace_wave(nd, tr, w->d_segs.p + kMaxSeg, na, (int)ta, true, w->work.p + 1,
                                          w->status.p, TRACE_MINB_ANY, s) == RT_OK;
-    ok = ok && RT_CUDA(cudaMemcpyAsync(w->h_status, w->status.p, sizeof(int), cudaMemcpyDeviceToHost, s)) &&
-         RT_CUDA(cudaEventRecord(w->traced, s)) && RT_CUDA(cudaStreamWaitEvent(copy_out, w->traced, 0));
+    if (ok && w->m_status) {
+        k_put_status<<<1, 1, 0, s>>>(w->status.p, w->m_status);
+        ok = RT_CUDA(cudaGetLastError());
+    } else if (ok) {
+        ok = RT_CUDA(cudaMemcpyAsync(w->h_status, w->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    }
+    ok = ok && RT_CUDA(cudaEventRecord(w->traced, s)) && RT_CUDA(cudaStreamWaitEvent(copy_out, w->traced, 0));
     for (const Chunk& c : w->chunks) {
         if (!ok) break;
         Request* r = c.req;
@@ -558,6 +585,17 @@ RtServer_t rtServer_create(const RtServerConfig* cfg_in) {
              w->work.alloc(2) && w->status.alloc(1) &&
              RT_CUDA(cudaMallocHost(&w->h_segs, sizeof(WaveSeg) * 2 * kMaxSeg)) &&
              RT_CUDA(cudaMallocHost(&w->h_status, sizeof(int)));
+        if (ok) {  // device addresses of the pinned staging (unified addressing maps it)
+            void *ds = nullptr, *dst = nullptr;
+            if (cudaHostGetDevicePointer(&ds, w->h_segs, 0) == cudaSuccess &&
+                cudaHostGetDevicePointer(&dst, w->h_status, 0) == cudaSuccess && ds && dst &&
+                reinterpret_cast<uintptr_t>(ds) % 16 == 0) {
+                w->m_segs = static_cast<const uint4*>(ds);
+                w->m_status = static_cast<int*>(dst);
+            } else {
+                cudaGetLastError();
+            }
+        }
         s->slots.push_back(std::move(w));
     }
     if (!ok) {
