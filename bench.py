@@ -498,7 +498,11 @@ def run_ours(args):
         "hit_fraction": {"primary": round(prim_hit, 4), "diffuse": round(float((hits["prim"] >= 0).mean()), 4)},
         "clocks": clk.summary(),
     }
-    if rank == 0 and not args.no_baselines:
+    # the baseline legs run at N=1 only: under torchrun the other ranks would
+    # wait for them at the closing barrier, inside the process-group timeout
+    if ws > 1 and not args.no_baselines:
+        out["baselines"] = "reported by the N=1 run"
+    if rank == 0 and ws == 1 and not args.no_baselines:
         out["reference_gpu_kernel"] = reference_gpu_kernel(tris, dif, d_dif, N_RAYS, torch, max(3, args.steps // 2),
                                                            flush)
         if "value" in out["reference_gpu_kernel"]:
