@@ -385,3 +385,34 @@ def test_batched_scenes_equal_per_scene_calls(cuda):
     b.graph(d_rays, d_off, n, d_g)
     torch.cuda.synchronize()
     assert np.array_equal(d_g.cpu().numpy(), d_h.cpu().numpy())
+
+
+def test_pipelined_host_calls_equal_device_calls(cuda):
+    """Host-buffer calls larger than one 512K-ray piece run as a pipeline of
+    pieces (copy in, trace on two alternating streams, copy out): results
+    equal the device-buffer path's, for pinned and pageable host memory,
+    closest and any hit, with a ragged last piece."""
+    import torch
+    tris = scenes.scene_meshes(61, 100_000, box=40.0)
+    bvh = lib.BVH(tris)
+    rays = scenes.random_rays(62, 1_200_001, box=50.0)
+    n = rays.shape[0]
+    d_rays = _dev(torch, rays)
+    d_h = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
+    d_o = torch.empty(n, dtype=torch.uint8, device="cuda")
+    bvh.closest(d_rays, n, d_h)
+    bvh.any(d_rays, n, d_o)
+    torch.cuda.synchronize()
+    ref_h, ref_o = d_h.cpu().numpy(), d_o.cpu().numpy()
+    L = lib.load()
+    p_r = torch.empty(n * 32, dtype=torch.uint8, pin_memory=True)
+    p_r.numpy()[:] = rays.view(np.uint8).reshape(-1)
+    p_h = torch.zeros(n * 16, dtype=torch.uint8, pin_memory=True)
+    p_o = torch.zeros(n, dtype=torch.uint8, pin_memory=True)
+    for _ in range(2):  # repeated calls reuse the staging buffers and events
+        assert L.cudaBVH_traceClosestHost(bvh.h, p_r.data_ptr(), n, p_h.data_ptr()) == 0, lib.last_error()
+        assert L.cudaBVH_traceAnyHost(bvh.h, p_r.data_ptr(), n, p_o.data_ptr()) == 0, lib.last_error()
+        assert np.array_equal(p_h.numpy(), ref_h) and np.array_equal(p_o.numpy(), ref_o)
+    assert np.array_equal(bvh.closest_host(rays).view(np.uint8).reshape(-1), ref_h)  # pageable
+    assert np.array_equal(bvh.any_host(rays), ref_o)
+    assert 0.05 < (ref_h.view(HIT_DTYPE)["prim"] >= 0).mean() < 0.95
