@@ -107,7 +107,13 @@ __global__ void k_pt_generate(PtCam c, int W, int H, int spp, uint32_t seed, RtR
     if (path == 0) *count = (int)P;
 }
 
-__global__ void __launch_bounds__(PT_T) k_pt_shade(PtScene sc, int spp, int bounce, int max_bounces, int rr_start,
+// Shading waits on scattered loads (hit triangles, instances, lights): 6
+// CTAs per SM (40 registers, some spilled) hide more of it than 4 at 64
+// registers, +0.9 % on the frame; 8 (32 registers) +0.4 %.
+#ifndef RTB_SHADE_MINB
+#define RTB_SHADE_MINB 6
+#endif
+__global__ void __launch_bounds__(PT_T, RTB_SHADE_MINB) k_pt_shade(PtScene sc, int spp, int bounce, int max_bounces, int rr_start,
                                                    uint32_t seed, const int* __restrict__ in_count,
                                                    const RtRay* __restrict__ rays, const int* __restrict__ pid,
                                                    const RtHit* __restrict__ hits, const int32_t* __restrict__ hinst,
