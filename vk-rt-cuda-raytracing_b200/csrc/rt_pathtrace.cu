@@ -109,7 +109,9 @@ __global__ void k_pt_generate(PtCam c, int W, int H, int spp, uint32_t seed, RtR
 
 // Shading waits on scattered loads (hit triangles, instances, lights): 6
 // CTAs per SM (40 registers, some spilled) hide more of it than 4 at 64
-// registers, +0.9 % on the frame; 8 (32 registers) +0.4 %.
+// registers, +0.9 % on the frame; 8 (32 registers) +0.4 %.  The grid-stride
+// launch is sized to exactly the resident CTAs (no ragged second wave:
+// another +2.0 %).
 #ifndef RTB_SHADE_MINB
 #define RTB_SHADE_MINB 6
 #endif
@@ -531,7 +533,7 @@ int rtPT_render(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* prm, f
         if (launch_trace_tlas(t, pt->rays[cur].p, 0, cnt + cur, pt->hits.p, pt->hinst.p, nullptr, w1, t->status.p,
                               s) != RT_OK)
             return RT_CUDA(cudaGetLastError()) ? RT_ERR_CUDA : RT_ERR_CUDA;
-        k_pt_shade<<<shade_blocks, PT_T, 0, s>>>(sc, prm->spp, b, prm->max_bounces, prm->rr_start, prm->seed,
+        k_pt_shade<<<num_sms() * RTB_SHADE_MINB, PT_T, 0, s>>>(sc, prm->spp, b, prm->max_bounces, prm->rr_start, prm->seed,
                                                  cnt + cur, pt->rays[cur].p, pt->pid[cur].p, pt->hits.p,
                                                  pt->hinst.p, pt->tp.p, pt->L.p, pt->rays[nxt].p, pt->pid[nxt].p,
                                                  cnt + nxt, pt->srays.p, pt->spid.p, pt->scontrib.p, cnt + 2);
