@@ -458,7 +458,7 @@ __global__ void __launch_bounds__(CHUNK_T) k_count_left(const Chunk* __restrict_
                                                         const Split* __restrict__ splits, const int* __restrict__ perm,
                                                         const float4* __restrict__ plo, const float4* __restrict__ phi,
                                                         int* __restrict__ chunk_left, uint32_t* __restrict__ kcb,
-                                                        const int* __restrict__ d_C) {
+                                                        const int* __restrict__ d_C, uint8_t* __restrict__ side) {
     __shared__ int ws[CHUNK_T / 32];
     if (blockIdx.x >= *d_C) return;  // (the scan over the bound reads stale counts only after the last chunk)
     const Chunk ch = chunks[blockIdx.x];
@@ -478,6 +478,7 @@ __global__ void __launch_bounds__(CHUNK_T) k_count_left(const Chunk* __restrict_
             const int p = perm[ch.start + i];
             const float4 l = plo[p], h = phi[p];
             const bool left = goes_left(tk, sp, ch.start + i, l, h);
+            side[ch.start + i] = left;  // k_scatter reads this instead of the boxes
             c += left;
             const float C[3] = {centroid(l.x, h.x), centroid(l.y, h.y), centroid(l.z, h.z)};
 #pragma unroll
@@ -520,9 +521,8 @@ __global__ void __launch_bounds__(CHUNK_T) k_count_left(const Chunk* __restrict_
 
 __global__ void __launch_bounds__(CHUNK_T) k_scatter(const Chunk* __restrict__ chunks, const Task* __restrict__ tasks,
                                                      const Split* __restrict__ splits, const int* __restrict__ perm,
-                                                     const float4* __restrict__ plo, const float4* __restrict__ phi,
-                                                     const int* __restrict__ left_off, int* __restrict__ out,
-                                                     const int* __restrict__ d_C) {
+                                                     const uint8_t* __restrict__ side, const int* __restrict__ left_off,
+                                                     int* __restrict__ out, const int* __restrict__ d_C) {
     __shared__ int ws[CHUNK_T / 32];
     if (blockIdx.x >= *d_C) return;
     const Chunk ch = chunks[blockIdx.x];
@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(CHUNK_T) k_scatter(const Chunk* __restrict__ c
         pv[k] = -1;
         if (i < ch.count) {
             pv[k] = perm[ch.start + i];
-            f[k] = goes_left(tk, sp, ch.start + i, plo[pv[k]], phi[pv[k]]);
+            f[k] = side[ch.start + i] != 0;
             c += f[k];
         }
     }
@@ -1196,6 +1196,7 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
     TmpBuf<uint32_t> gbins;
     TmpBuf<int> flags, status;
     TmpBuf<uint32_t> kcb;  // per kid: centroid min xyz, max xyz (ordered)
+    TmpBuf<uint8_t> side;  // per position: 1 = goes left at this level (k_count_left -> k_scatter)
     const int maxChunks = n / CHUNK + maxT + 2;
     TmpBuf<Chunk> chunks;
     TmpBuf<int> ccount, coff, cleft, cleftoff;
@@ -1205,7 +1206,7 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
         !splits.alloc(maxT, s) || !gbins.alloc((size_t)maxT * TASK_BIN_WORDS, s) ||
         !flags.alloc(4 * 2 * maxT + 8, s) || !chunks.alloc(maxChunks, s) || !ccount.alloc(maxT, s) ||
         !coff.alloc(maxT, s) || !cleft.alloc(maxChunks, s) || !cleftoff.alloc(maxChunks, s) || !status.alloc(1, s) ||
-        !kcb.alloc((size_t)12 * maxT, s))
+        !kcb.alloc((size_t)12 * maxT, s) || !side.alloc(n, s))
         return false;
     cudaMemsetAsync(status.p, 0, sizeof(int), s);
     k_iota<<<(n + 255) / 256, 256, 0, s>>>(perm, n);
@@ -1307,9 +1308,9 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
         k_bin_large<<<Cb, CHUNK_T, 0, s>>>(chunks.p, cur, perm, d_lo, d_hi, gbins.p, d_C);
         k_split_large<<<(Tb + 3) / 4, 128, 0, s>>>(cur, d_T, gbins.p, splits.p, kids.p, kcb.p, out.nodes.p, d_node,
                                                     cfg.max_leaf, cfg.max_sah_depth);
-        k_count_left<<<Cb, CHUNK_T, 0, s>>>(chunks.p, cur, splits.p, perm, d_lo, d_hi, cleft.p, kcb.p, d_C);
+        k_count_left<<<Cb, CHUNK_T, 0, s>>>(chunks.p, cur, splits.p, perm, d_lo, d_hi, cleft.p, kcb.p, d_C, side.p);
         if (!scan_exclusive(cleft.p, cleftoff.p, Cb, nullptr, s)) return false;
-        k_scatter<<<Cb, CHUNK_T, 0, s>>>(chunks.p, cur, splits.p, perm, d_lo, d_hi, cleftoff.p, tmp.p, d_C);
+        k_scatter<<<Cb, CHUNK_T, 0, s>>>(chunks.p, cur, splits.p, perm, side.p, cleftoff.p, tmp.p, d_C);
         k_copy_back<<<Cb, 256, 0, s>>>(chunks.p, tmp.p, perm, d_C);
         k_classify_flags<<<(Kb + 255) / 256, 256, 0, s>>>(kids.p, d_T, Kb, cfg.max_leaf, cfg.small_task, is_large,
                                                           is_small);
