@@ -2,7 +2,7 @@
  *
  * TEST INFRASTRUCTURE ONLY.  Nothing in the product library links or calls
  * this code; only tests/, __graft_entry__.smoke() and bench.py's CPU baseline
- * leg load it, as the checker.
+ * leg load it, to verify results against.
  *
  * What it restates (reference paths are relative to the reference project):
  *   - BVH2Builder::build/buildRec, binned SAH, layer/cuda_bvh_backend.cu:201-251

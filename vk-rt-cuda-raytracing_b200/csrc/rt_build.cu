@@ -1111,7 +1111,7 @@ __global__ void k_iota(int* __restrict__ p, int n) {
     if (i < n) p[i] = i;
 }
 
-// ----------------------------------------------------------- the driver --
+// ------------------------------------------------------ host-side build --
 // Per host thread: pinned slots the level loop copies each level's task
 // count into, and an event per level to wait on (created once per thread).
 constexpr int kMaxLevels = 160;  // SAH depth 48, then median splits: far fewer levels
