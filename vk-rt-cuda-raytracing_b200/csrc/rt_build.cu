@@ -26,6 +26,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
+#include <new>
 
 #include "rt_internal.h"
 
@@ -1139,12 +1141,21 @@ struct LevelLog {
     }
 };
 static LevelLog* level_log() {
-    static thread_local LevelLog lg;
-    if (!lg.ok) {
+    // one per device: events belong to the device that was current at creation
+    constexpr int kDevices = 16;
+    static thread_local std::unique_ptr<LevelLog> lg[kDevices];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevices) {
+        cudaGetLastError();
+        set_error("build: no usable device for the level log");
+        return nullptr;
+    }
+    if (!lg[dev]) lg[dev].reset(new (std::nothrow) LevelLog());
+    if (!lg[dev] || !lg[dev]->ok) {
         set_error("build: pinned level log unavailable");
         return nullptr;
     }
-    return &lg;
+    return lg[dev].get();
 }
 
 BuildConfig default_build_config() {
