@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
                 if (g < total) {
                     const int rec = (int)ob + (int)nth_set_bit(om, (uint32_t)k);
                     const float4* tp = tris + (size_t)rec * 3;
-                    const float4 A = __ldg(tp), B = __ldg(tp + 1), Cc = __ldg(tp + 2);
+                    const float4 A = ld_tri(tp), B = ld_tri(tp + 1), Cc = ld_tri(tp + 2);
                     float t;
                     if (intersect_tri(ox, oy, oz, dx, dy, dz, A, B, Cc, t, u, v) && t > tmn && t < tmx) {
                         if (ANY) s_rec[wbase + o] = 1;
@@ -254,10 +254,14 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
                 if (ANY) {
                     occ[ray] = found_any ? 1 : 0;
                 } else {
-                    reinterpret_cast<float4*>(hits)[ray] =
-                        make_float4(hprim >= 0 ? thit : __int_as_float(0x7f800000),
-                                    __int_as_float(hprim >= 0 ? hprim - prim_base : -1),
-                                    hprim >= 0 ? hu : 0.f, hprim >= 0 ? hv : 0.f);
+                    const float4 hv4 = make_float4(hprim >= 0 ? thit : __int_as_float(0x7f800000),
+                                                   __int_as_float(hprim >= 0 ? hprim - prim_base : -1),
+                                                   hprim >= 0 ? hu : 0.f, hprim >= 0 ? hv : 0.f);
+#if RTB_RAY_CS
+                    __stcs(reinterpret_cast<float4*>(hits) + ray, hv4);
+#else
+                    reinterpret_cast<float4*>(hits)[ray] = hv4;
+#endif
                 }
                 if (COUNT) reinterpret_cast<uint2*>(counts)[ray] = make_uint2(cn, ct);
                 ray = -1;
