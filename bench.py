@@ -489,6 +489,9 @@ def run_ours(args):
                      "bytes_per_ray": round(bytes_per_ray, 1), "nodes_per_ray": round(n_node, 2),
                      "tris_per_ray": round(n_tri, 2),
                      "formula": "32 ray + 16 hit + nodes*80 + tris*36",
+                     "counts": "node visits and triangle tests per ray from cudaBVH_traceCounters on this "
+                               "launch's rays; ray for ray equal to the CPU oracle's restated walk on committed "
+                               "fixtures (tests/test_oracle_bvh8.py)",
                      "dram_gbs_from_traffic": round(traffic / (t_step * 1e-3) / 1e9, 1) if traffic else None,
                      "note": "BVH and triangles stay in the 126 MB L2; DRAM carries rays, hits and misses; "
                              "the kernel is issue-bound (profiles/trace_closest_incoherent_2m.md)"},

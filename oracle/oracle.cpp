@@ -560,6 +560,198 @@ void trace_two_level_one(const uint32_t* tlas, int tn, const int* tord, const fl
     inst_out = best_i;
 }
 
+// ---------------- 8-wide compressed walk, with work counts ----------------
+// The engine's own closest-hit / any-hit walk over its 8-wide nodes (the
+// traceCWBVH scheme of cuda_rt_v37.cu:146-373: a node group is a child base
+// plus an 8-bit hit mask, children taken in ray-octant order, child boxes
+// quantised to 8 bits on the grid p + q * 2^e), restated step for step so
+// that the node visits and triangle tests per ray -- the algorithmic bytes
+// bench.py charges a launch -- and the results also come from the CPU.
+//
+// Node, 20 words:  [0..2] p (float), [3] exponent bytes x | y << 8 | z << 16
+//   and the inner-child mask << 24, [4] first child node, [5] first triangle
+//   record, [6] [7] one meta byte per slot 0-3 / 4-7 (inner 0xFF, leaf
+//   count << 5 | offset, empty 0), [8..11] x planes (lo of slots 0-3, lo
+//   4-7, hi 0-3, hi 4-7), [12..15] y, [16..19] z.
+// Triangle record, 12 floats: v0 and the primitive id (int bits), e1, 0,
+//   e2, 0.
+// One round of the walk: up to `niters` node visits (none once a visited
+// node gave triangles; a visited node with nothing hit pops the next
+// group), then every triangle of the hit leaves is tested and the least
+// (t, primitive) key kept, then the next group is popped if the current
+// one is spent.  Box test: t = q * (s / d) + (p - o) / d with an absolute
+// slack of 2^-22 |(p - o) / d| on the offsets and 2^-21 |t_far| on the
+// comparison; 1/d of a component with |d| <= 2^-64 uses +-2^-64.
+struct Walk8Out {
+    float t, u, v;
+    int prim;
+    uint8_t occ;
+    uint32_t nodes, tris;
+    bool bad;  // an index past the arrays (not a valid tree)
+};
+
+inline float as_f(uint32_t u) {
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+inline uint32_t ord_of(float f) {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+inline float from_ord(uint32_t u) { return as_f((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u); }
+inline uint32_t bit_run(uint32_t start, uint32_t width) {
+    return width ? (uint32_t)((((1ull << width) - 1ull) << start) & 0xFFFFFFFFull) : 0u;
+}
+
+void visit8(const uint32_t* W, const float o[3], const float inv[3], uint32_t oct, float tmin, float thit,
+            uint32_t& tri_base, uint32_t& tmask, uint32_t& ngx, uint32_t& ngy) {
+    const uint32_t e = W[3], imask = e >> 24;
+    float S[3], On[3], Of[3];
+    for (int a = 0; a < 3; a++) {
+        const float sc = as_f(((e >> (8 * a)) & 0xFFu) << 23);
+        S[a] = sc * inv[a];
+        const float O = (as_f(W[a]) - o[a]) * inv[a];
+        On[a] = fmaf(-fabsf(O), 0x1p-22f, O);
+        Of[a] = fmaf(fabsf(O), 0x1p-22f, O);
+    }
+    uint32_t nh = 0, th = 0;
+    for (int s = 0; s < 8; s++) {
+        float tn[3], tf[3];
+        for (int a = 0; a < 3; a++) {
+            const uint32_t* P = W + 8 + 4 * a;
+            const bool neg = (oct >> a) & 1u;  // near plane: lo for a positive 1/d, hi otherwise
+            const uint32_t nw = neg ? P[2 + (s >> 2)] : P[s >> 2];
+            const uint32_t fw = neg ? P[s >> 2] : P[2 + (s >> 2)];
+            tn[a] = fmaf((float)((nw >> (8 * (s & 3))) & 0xFFu), S[a], On[a]);
+            tf[a] = fmaf((float)((fw >> (8 * (s & 3))) & 0xFFu), S[a], Of[a]);
+        }
+        const float tnear = fmaxf(fmaxf(tn[0], tn[1]), fmaxf(tn[2], tmin));
+        const float tfar = fminf(fminf(tf[0], tf[1]), fminf(tf[2], thit));
+        if (!(tnear <= fmaf(fabsf(tfar), 0x1p-21f, tfar))) continue;
+        if ((imask >> s) & 1u) {
+            nh |= 1u << ((uint32_t)s ^ oct);
+        } else {
+            const uint32_t meta = (W[6 + (s >> 2)] >> (8 * (s & 3))) & 0xFFu;
+            th |= bit_run(meta & 31u, meta >> 5);
+        }
+    }
+    tri_base = W[5];
+    tmask = th;
+    ngx = W[4];
+    ngy = nh | (imask << 8);
+}
+
+void walk8_one(const uint32_t* nodes, int nnodes, const float* recs, int nrecs, const OrcRay& ray, bool any,
+               int niters, Walk8Out& out) {
+    const float* o = ray.org;
+    const float* d = ray.dir;
+    float inv[3];
+    for (int a = 0; a < 3; a++) inv[a] = 1.0f / (fabsf(d[a]) > 0x1p-64f ? d[a] : copysignf(0x1p-64f, d[a]));
+    const uint32_t oct =
+        (std::signbit(inv[0]) ? 1u : 0u) | (std::signbit(inv[1]) ? 2u : 0u) | (std::signbit(inv[2]) ? 4u : 0u);
+    float thit = ray.tmax, hu = 0.f, hv = 0.f;
+    int hprim = -1;
+    uint32_t cn = 0, ct = 0;
+    uint32_t stx[64], sty[64];
+    int sp = 0;
+    bool overflow = false, found = false;
+    uint32_t ngx = 0, ngy = (1u << oct) | (1u << 8);  // the root as slot 0 of a one-child group
+    out.bad = false;
+    for (;;) {
+        uint32_t tri_base = 0, tmask = 0;
+        for (int it = 0; it < niters; it++) {
+            if (tmask != 0 || overflow || (ngy & 0xFFu) == 0) continue;
+            uint32_t hitsm = ngy & 0xFFu;
+            const uint32_t imask = (ngy >> 8) & 0xFFu;
+            const uint32_t k = (uint32_t)__builtin_ctz(hitsm);
+            hitsm &= hitsm - 1;
+            const uint32_t slot = k ^ oct;
+            const uint32_t ni = ngx + (uint32_t)__builtin_popcount(imask & ((1u << slot) - 1u));
+            if (hitsm) {
+                if (sp < 64) {
+                    stx[sp] = ngx;
+                    sty[sp] = hitsm | (imask << 8);
+                    sp++;
+                } else {
+                    overflow = true;
+                }
+            }
+            cn++;
+            if (ni >= (uint32_t)nnodes) {
+                out.bad = true;
+                return;
+            }
+            visit8(nodes + (size_t)ni * 20, o, inv, oct, ray.tmin, thit, tri_base, tmask, ngx, ngy);
+            if (niters > 1 && tmask == 0 && (ngy & 0xFFu) == 0 && sp > 0) {
+                sp--;
+                ngx = stx[sp];
+                ngy = sty[sp];
+            }
+        }
+        ct += (uint32_t)__builtin_popcount(tmask);
+        if (tmask) {
+            uint64_t best = ((uint64_t)ord_of(thit) << 32) | (uint32_t)(hprim >= 0 ? hprim : -1);
+            float bu = 0.f, bv = 0.f;
+            bool improved = false;
+            for (uint32_t m = tmask; m; m &= m - 1) {
+                const uint32_t rec = tri_base + (uint32_t)__builtin_ctz(m);
+                if (rec >= (uint32_t)nrecs) {
+                    out.bad = true;
+                    return;
+                }
+                const float* R = recs + (size_t)rec * 12;
+                float t, u, v;
+                if (!mt(o, d, R, R + 4, R + 8, t, u, v) || !(t > ray.tmin && t < ray.tmax)) continue;
+                if (any) {
+                    found = true;
+                } else {
+                    uint32_t pid;
+                    memcpy(&pid, R + 3, 4);
+                    const uint64_t key = ((uint64_t)ord_of(t) << 32) | pid;
+                    if (key < best) {
+                        best = key;
+                        bu = u;
+                        bv = v;
+                        improved = true;
+                    }
+                }
+            }
+            if (improved) {
+                thit = from_ord((uint32_t)(best >> 32));
+                hprim = (int)(uint32_t)best;
+                hu = bu;
+                hv = bv;
+            }
+        }
+        bool done = overflow || (any && found);
+        if (!done && (ngy & 0xFFu) == 0) {
+            if (sp == 0) {
+                done = true;
+            } else {
+                sp--;
+                ngx = stx[sp];
+                ngy = sty[sp];
+            }
+        }
+        if (done) {
+            if (overflow) {
+                hprim = -1;
+                found = false;
+            }
+            out.t = hprim >= 0 ? thit : INFINITY;
+            out.prim = hprim;
+            out.u = hprim >= 0 ? hu : 0.f;
+            out.v = hprim >= 0 ? hv : 0.f;
+            out.occ = found ? 1 : 0;
+            out.nodes = cn;
+            out.tris = ct;
+            return;
+        }
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -763,6 +955,31 @@ int orc_fix_skips(uint32_t* dfs, int n) {
     }
     return changed;
 }
+
+// 8-wide walk over the engine's own nodes (walk8_one).  hits (closest hit)
+// or occluded (any hit) may be null; counts: node visits and triangle tests
+// per ray (2 x u32).  Returns how many rays' walks left the arrays (0 for a
+// valid tree; those rays get counts 0xFFFFFFFF).
+int orc_walk_bvh8(const uint32_t* nodes, int nnodes, const float* recs, int nrecs, const OrcRay* rays, int nrays,
+                  int any, int niters, OrcHit* hits, uint8_t* occluded, uint32_t* counts, int nthreads) {
+    std::atomic<int> bad(0);
+    parallel_for(nrays, nthreads, 256, [&](int i) {
+        Walk8Out w;
+        walk8_one(nodes, nnodes, recs, nrecs, rays[i], any != 0, niters, w);
+        if (w.bad) {
+            bad.fetch_add(1);
+            w = Walk8Out{INFINITY, 0.f, 0.f, -1, 0, 0xFFFFFFFFu, 0xFFFFFFFFu, true};
+        }
+        if (hits) hits[i] = OrcHit{w.t, w.prim, w.u, w.v};
+        if (occluded) occluded[i] = w.occ;
+        if (counts) {
+            counts[2 * i] = w.nodes;
+            counts[2 * i + 1] = w.tris;
+        }
+    });
+    return bad.load();
+}
+
 
 }  // extern "C"
 

@@ -14,7 +14,10 @@
  *   - stackless traversal, layer/shaders/bvh2_stackless.comp:37-76, with the
  *     Moller-Trumbore arithmetic of layer/cuda_bvh_backend.cu:143-157;
  *   - two-level TLAS->BLAS traversal, layer/rt_ir_exec.cu:81-189;
- *   - Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11).
+ *   - Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11);
+ *   - the engine's 8-wide compressed walk with its work counts, after the
+ *     traceCWBVH scheme of cuda_rt_v37.cu:146-373 (node visits and triangle
+ *     tests per ray, the basis of the algorithmic bytes per ray).
  *
  * Parity pinning: tests compare this restatement byte-for-byte against the
  * reference's own builder compiled from its sources into oracle/_ref/ and
@@ -56,6 +59,15 @@ void orc_trace_closest_dfs(const uint32_t* dfs, int nnodes, const float* packed,
                            int nthreads, uint64_t* stats);
 void orc_trace_any_dfs(const uint32_t* dfs, int nnodes, const float* packed,
                        const OrcRay* rays, int nrays, uint8_t* occluded, int nthreads);
+/* The engine's own 8-wide walk (nodes of 20 words, triangle records of 12
+ * floats, as the library lays them out in device memory), restated with the
+ * kernel's node-visit and triangle-test counts per ray (2 x u32 in counts).
+ * any = 0: closest hit into hits; 1: occlusion flags into occluded.  niters:
+ * node visits per round of the walk (the kernel's RTB_NODE_ITERS).  Returns
+ * the number of rays whose walk left the arrays (0 for a valid tree). */
+int orc_walk_bvh8(const uint32_t* nodes, int nnodes, const float* recs, int nrecs, const OrcRay* rays,
+                  int nrays, int any, int niters, OrcHit* hits, uint8_t* occluded, uint32_t* counts,
+                  int nthreads);
 void orc_brute_closest(const float* tris9, int ntris, const OrcRay* rays, int nrays,
                        OrcHit* hits, int nthreads);
 void orc_brute_any(const float* tris9, int ntris, const OrcRay* rays, int nrays,

@@ -60,6 +60,8 @@ def lib() -> C.CDLL:
         L.orc_f2h_rn.restype = C.c_uint16
         L.orc_f2h_rn.argtypes = [C.c_float]
         L.orc_pt_pixels.argtypes = [vp, vp, vp, vp, i32, vp, i32, vp]
+        L.orc_walk_bvh8.restype = i32
+        L.orc_walk_bvh8.argtypes = [vp, i32, vp, i32, vp, i32, i32, i32, vp, vp, vp, i32]
         _lib = L
     return _lib
 
@@ -112,6 +114,25 @@ def trace_closest_dfs(dfs, packed, rays, nthreads=0, stats=False):
     lib().orc_trace_closest_dfs(_p(dfs), dfs.size // 8, _p(packed), _p(rays), rays.shape[0], _p(hits),
                                 nthreads, _p(st) if stats else None)
     return (hits, st) if stats else hits
+
+
+def walk_bvh8(nodes, recs, rays, any_hit=False, niters=2, nthreads=0):
+    """The engine's 8-wide walk restated on the CPU (orc_walk_bvh8).  nodes:
+    (N, 20) u32 as laid out on the device; recs: (M, 12) f32 triangle
+    records.  Returns (hits or occlusion flags, counts (n, 2) u32 of node
+    visits and triangle tests per ray); raises if a walk leaves the arrays."""
+    rays = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
+    nodes = np.ascontiguousarray(nodes, dtype=np.uint32).reshape(-1, 20)
+    recs = np.ascontiguousarray(recs, dtype=np.float32).reshape(-1, 12)
+    n = rays.shape[0]
+    counts = np.zeros((n, 2), dtype=np.uint32)
+    out = np.zeros(n, dtype=np.uint8) if any_hit else np.zeros(n, dtype=HIT_DTYPE)
+    bad = lib().orc_walk_bvh8(_p(nodes), nodes.shape[0], _p(recs), recs.shape[0], _p(rays), n, int(any_hit),
+                              niters, None if any_hit else _p(out), _p(out) if any_hit else None, _p(counts),
+                              nthreads)
+    if bad:
+        raise ValueError(f"walk_bvh8: {bad} walks left the node or record arrays")
+    return out, counts
 
 
 def trace_any_dfs(dfs, packed, rays, nthreads=0):
