@@ -138,6 +138,17 @@ typedef struct {
 CudaTLAS_t cudaTLAS_build(const CudaBVH_t* blas, int numBlas, const RtInstance* instances, int numInstances);
 void cudaTLAS_destroy(CudaTLAS_t tlas);
 
+/* Per-frame instance update (replaces the layer's TLAS rebuild in
+ * processPendingTLAS, layer/VkLayer_CudaRT.cpp:3418, paced by
+ * CUDA_RT_TLAS_EVERY_N): new transforms and BLAS choices for the same number
+ * of instances (over the BLAS array given to cudaTLAS_build); the top level
+ * is rebuilt in place, the BLASes are untouched, and traces afterwards equal
+ * those of a TLAS built with the new instances.  Waits for the device first
+ * (traces in flight finish on the old instances).  On failure the TLAS keeps
+ * its previous instances.  A path tracer created on the TLAS must be created
+ * again (rtPT_render refuses a TLAS changed since rtPT_create). */
+int cudaTLAS_setTransforms(CudaTLAS_t tlas, const RtInstance* instances, int numInstances);
+
 /* Closest hit over all instances: d_hits[i].prim is the primitive index in
  * the hit instance's BLAS, d_inst[i] the instance index (-1 on a miss; may
  * be NULL).  Rays are transformed by the inverse instance transform without

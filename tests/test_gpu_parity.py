@@ -305,6 +305,55 @@ def test_tlas_two_level_vs_oracle(cuda):
         L.cudaTLAS_destroy(tl)
 
 
+def test_tlas_set_transforms_equals_a_fresh_build(cuda):
+    """cudaTLAS_setTransforms moves every instance and changes BLAS choices in
+    place: traces afterwards are byte-identical to those of a TLAS built with
+    the new instances, and a path tracer created before the update refuses
+    to render (it copied the old transforms)."""
+    import torch
+    rs = np.random.RandomState(8)
+    blases = [lib.BVH(scenes.scene_meshes(20 + i, 2000, box=6.0, lo=200, hi=800, ground=False)) for i in range(3)]
+    n = 16
+
+    def instances(seed):
+        r = np.random.RandomState(seed)
+        xf = [np.concatenate([scenes.rotations(r.uniform(size=(1, 3)))[0] * r.uniform(0.5, 2.0),
+                              r.uniform(-30, 30, 3)[:, None]], 1).astype(np.float32) for _ in range(n)]
+        return np.array(xf), r.randint(0, 3, n)
+
+    xa, ba = instances(1)
+    xb, bb = instances(2)
+    moved = lib.TLAS(blases, xa, ba)
+    pt = lib.PathTracer(moved, np.full((n, 3), 0.5, np.float32), np.zeros((n, 3), np.float32))
+    moved.set_transforms(xb, bb)
+    fresh = lib.TLAS(blases, xb, bb)
+    try:
+        assert np.array_equal(moved.inverse(), fresh.inverse())
+        rays = scenes.random_rays(61, 20000)
+        d = xb[rs.randint(0, n, rays.shape[0]), :, 3] + rs.normal(0, 1.0, (rays.shape[0], 3)) - rays["org"]
+        rays["dir"] = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+        d_rays = _dev(torch, rays)
+        out = []
+        for tl in (moved, fresh):
+            d_hits = torch.empty(rays.shape[0] * 16, dtype=torch.uint8, device="cuda")
+            d_inst = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+            d_occ = torch.empty(rays.shape[0], dtype=torch.uint8, device="cuda")
+            tl.closest(d_rays, rays.shape[0], d_hits, d_inst)
+            tl.any(d_rays, rays.shape[0], d_occ)
+            torch.cuda.synchronize()
+            out.append((d_hits.cpu().numpy(), d_inst.cpu().numpy(), d_occ.cpu().numpy()))
+        for a, b in zip(*out):
+            assert np.array_equal(a, b)
+        assert (out[0][1] >= 0).mean() > 0.05  # 9 % of these rays hit
+        d_rgb = torch.zeros(64 * 36 * 3, dtype=torch.float32, device="cuda")
+        with pytest.raises(lib.RtError):
+            pt.render(lib.make_camera((0.0, 0.0, -80.0), (0.0, 0.0, 0.0)), 64, 36, 1, d_rgb=d_rgb)
+    finally:
+        pt.close()
+        fresh.close()
+        moved.close()
+
+
 def test_counters_match_closest_results(cuda, small_scene):
     import torch
     bvh = lib.BVH(small_scene)

@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -66,6 +67,12 @@ struct DevBuf {
         pooled = false;
     }
     size_t bytes() const { return n * sizeof(T); }
+    void swap(DevBuf& o) {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
+        std::swap(pool_stream, o.pool_stream);
+        std::swap(pooled, o.pooled);
+    }
 };
 
 // ---- builder temporaries: stream-ordered, from a pool that keeps memory ----
@@ -144,6 +151,13 @@ struct Bvh2Device {
     int num_nodes = 0;       // slots used (incl. unused reservations)
     int num_prims = 0;
     int num_roots = 1;       // one root per segment, nodes 0 .. num_roots-1
+    void swap(Bvh2Device& o) {
+        nodes.swap(o.nodes);
+        perm.swap(o.perm);
+        std::swap(num_nodes, o.num_nodes);
+        std::swap(num_prims, o.num_prims);
+        std::swap(num_roots, o.num_roots);
+    }
 };
 
 // The compressed 8-wide structure the traversal kernels read.
@@ -154,6 +168,14 @@ struct Bvh8Device {
     int num_nodes = 0;
     int num_leaf_items = 0;
     int depth = 0;
+    void swap(Bvh8Device& o) {
+        nodes.swap(o.nodes);
+        tris.swap(o.tris);
+        leaf_ids.swap(o.leaf_ids);
+        std::swap(num_nodes, o.num_nodes);
+        std::swap(num_leaf_items, o.num_leaf_items);
+        std::swap(depth, o.depth);
+    }
 };
 
 // Defaults with the environment's overrides (RTB200_MAX_LEAF, RTB200_WARP_TASK,
@@ -236,6 +258,7 @@ struct CudaTLASHandle {
     rtb::Bvh8Device bvh8;
     rtb::DevBuf<float4> inst;     // per instance: inv xform (3 float4), BLAS ptrs, id base
     std::vector<float> h_inv;     // 12 floats per instance
+    unsigned long long generation = 0;  // bumped by every cudaTLAS_setTransforms
     rtb::DevBuf<int> counters;
     unsigned counter_next = 0;
     rtb::DevBuf<int> status;

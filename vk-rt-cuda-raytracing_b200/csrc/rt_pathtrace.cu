@@ -316,6 +316,7 @@ using namespace rtb;
 
 struct RtPathTracerHandle {
     CudaTLAS_t tlas = nullptr;
+    unsigned long long tlas_generation = 0;  // the TLAS's instances this tracer copied
     int ninst = 0;
     DevBuf<float4> mat;
     DevBuf<float> fwd, inv;
@@ -405,6 +406,7 @@ RtPathTracer_t rtPT_create(CudaTLAS_t tlas, const RtMaterial* mats, int nmat, co
     RtPathTracerHandle* pt = new (std::nothrow) RtPathTracerHandle();
     if (!pt) return nullptr;
     pt->tlas = tlas;
+    pt->tlas_generation = tlas->generation;
     const int ni = nmat;
     pt->ninst = ni;
     std::vector<float4> mat((size_t)2 * ni);
@@ -492,6 +494,11 @@ int rtPT_render(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* prm, f
     }
     if (misaligned(d_rgb, 4)) {
         set_error("rtPT_render: d_rgb must be 4-byte aligned");
+        return RT_ERR_INVALID;
+    }
+    // transforms, light areas and BLAS choices were copied at creation
+    if (pt->tlas->generation != pt->tlas_generation) {
+        set_error("rtPT_render: the TLAS's instances changed since rtPT_create; create the path tracer again");
         return RT_ERR_INVALID;
     }
     const int64_t P = (int64_t)prm->width * prm->height * prm->spp;

@@ -336,44 +336,31 @@ static bool invert34(const float* m, double* inv) {
     return true;
 }
 
-}  // namespace rtb
-
-using namespace rtb;
-
-extern "C" {
-
-CudaTLAS_t cudaTLAS_build(const CudaBVH_t* blas, int nb, const RtInstance* inst, int ni) {
-    clear_error();
-    if (!blas || nb <= 0 || !inst || ni <= 0) {
-        set_error("cudaTLAS_build: empty input");
-        return nullptr;
-    }
-    for (int i = 0; i < nb; i++)
-        if (!blas[i]) {
-            set_error("cudaTLAS_build: BLAS %d is NULL", i);
-            return nullptr;
-        }
-    CudaTLASHandle* t = new (std::nothrow) CudaTLASHandle();
-    if (!t) return nullptr;
-    t->num_instances = ni;
-    t->blas.assign(blas, blas + nb);
-    t->h_inv.resize((size_t)ni * 12);
-    std::vector<float4> rec((size_t)ni * INST_F4), lo(ni), hi(ni);
+// Per instance: the inverse transform (12 floats), the record the kernels
+// read (inverse as 3 float4, BLAS node / record pointers, tie-break id
+// base) and the padded world box of its BLAS.  False, with the error set,
+// on a bad instance.
+static bool instance_data(const std::vector<CudaBVH_t>& blas, const RtInstance* inst, int ni, const char* who,
+                          std::vector<float>& h_inv, std::vector<float4>& rec, std::vector<float4>& lo,
+                          std::vector<float4>& hi) {
+    const int nb = (int)blas.size();
+    h_inv.assign((size_t)ni * 12, 0.f);
+    rec.assign((size_t)ni * INST_F4, make_float4(0.f, 0.f, 0.f, 0.f));
+    lo.resize(ni);
+    hi.resize(ni);
     unsigned long long id_base = 0;
     for (int k = 0; k < ni; k++) {
         const RtInstance& I = inst[k];
         if (I.blas < 0 || I.blas >= nb) {
-            set_error("cudaTLAS_build: instance %d names BLAS %d of %d", k, I.blas, nb);
-            delete t;
-            return nullptr;
+            set_error("%s: instance %d names BLAS %d of %d", who, k, I.blas, nb);
+            return false;
         }
         double inv[12];
         if (!invert34(I.xform, inv)) {
-            set_error("cudaTLAS_build: instance %d transform is singular", k);
-            delete t;
-            return nullptr;
+            set_error("%s: instance %d transform is singular", who, k);
+            return false;
         }
-        float* fi = &t->h_inv[(size_t)k * 12];
+        float* fi = &h_inv[(size_t)k * 12];
         for (int j = 0; j < 12; j++) fi[j] = (float)inv[j];
         const CudaBVHHandle* b = blas[I.blas];
         double wl[3] = {1e300, 1e300, 1e300}, wh[3] = {-1e300, -1e300, -1e300}, mag = 0.0;
@@ -403,27 +390,90 @@ CudaTLAS_t cudaTLAS_build(const CudaBVH_t* blas, int nb, const RtInstance* inst,
                                              bits_f((uint32_t)(tp >> 32)));
     }
     if (id_base >= 0xFFFFFFFFull) {
-        set_error("cudaTLAS_build: %llu instance primitives exceed the 32-bit tie-break id", id_base);
-        delete t;
-        return nullptr;
+        set_error("%s: %llu instance primitives exceed the 32-bit tie-break id", who, id_base);
+        return false;
     }
+    return true;
+}
+
+// The top-level tree over the instance boxes: binned SAH with leaves of one
+// instance, collapsed greedily to 8-wide nodes.
+static bool build_top(const std::vector<float4>& lo, const std::vector<float4>& hi, Bvh2Device& b2, Bvh8Device& b8) {
+    const int ni = (int)lo.size();
     DevBuf<float4> dlo, dhi;
     BuildConfig cfg;
     cfg.max_leaf = 1;
-    bool ok = t->inst.alloc(rec.size()) && dlo.alloc(ni) && dhi.alloc(ni) &&
+    return dlo.alloc(ni) && dhi.alloc(ni) &&
+           RT_CUDA(cudaMemcpy(dlo.p, lo.data(), ni * sizeof(float4), cudaMemcpyHostToDevice)) &&
+           RT_CUDA(cudaMemcpy(dhi.p, hi.data(), ni * sizeof(float4), cudaMemcpyHostToDevice)) &&
+           build_bvh2(dlo.p, dhi.p, ni, cfg, b2, 0) && collapse_bvh8(b2, nullptr, b8, 0) &&
+           RT_CUDA(cudaDeviceSynchronize()) &&
+           (!getenv("RTB200_VALIDATE") || !atoi(getenv("RTB200_VALIDATE")) ||
+            validate_bvh8(b8, b8.num_leaf_items, ni));
+}
+
+}  // namespace rtb
+
+using namespace rtb;
+
+extern "C" {
+
+CudaTLAS_t cudaTLAS_build(const CudaBVH_t* blas, int nb, const RtInstance* inst, int ni) {
+    clear_error();
+    if (!blas || nb <= 0 || !inst || ni <= 0) {
+        set_error("cudaTLAS_build: empty input");
+        return nullptr;
+    }
+    for (int i = 0; i < nb; i++)
+        if (!blas[i]) {
+            set_error("cudaTLAS_build: BLAS %d is NULL", i);
+            return nullptr;
+        }
+    CudaTLASHandle* t = new (std::nothrow) CudaTLASHandle();
+    if (!t) return nullptr;
+    t->num_instances = ni;
+    t->blas.assign(blas, blas + nb);
+    std::vector<float4> rec, lo, hi;
+    bool ok = instance_data(t->blas, inst, ni, "cudaTLAS_build", t->h_inv, rec, lo, hi) &&
+              t->inst.alloc(rec.size()) &&
               RT_CUDA(cudaMemcpy(t->inst.p, rec.data(), rec.size() * sizeof(float4), cudaMemcpyHostToDevice)) &&
-              RT_CUDA(cudaMemcpy(dlo.p, lo.data(), ni * sizeof(float4), cudaMemcpyHostToDevice)) &&
-              RT_CUDA(cudaMemcpy(dhi.p, hi.data(), ni * sizeof(float4), cudaMemcpyHostToDevice)) &&
-              build_bvh2(dlo.p, dhi.p, ni, cfg, t->bvh2, 0) && collapse_bvh8(t->bvh2, nullptr, t->bvh8, 0) &&
-              ensure_counters(t->counters) && t->status.alloc(1) &&
-              RT_CUDA(cudaMemset(t->status.p, 0, sizeof(int))) && RT_CUDA(cudaDeviceSynchronize()) &&
-              (!getenv("RTB200_VALIDATE") || !atoi(getenv("RTB200_VALIDATE")) ||
-               validate_bvh8(t->bvh8, t->bvh8.num_leaf_items, ni));
+              build_top(lo, hi, t->bvh2, t->bvh8) && ensure_counters(t->counters) && t->status.alloc(1) &&
+              RT_CUDA(cudaMemset(t->status.p, 0, sizeof(int))) && RT_CUDA(cudaDeviceSynchronize());
     if (!ok) {
         delete t;
         return nullptr;
     }
     return t;
+}
+
+// Per-frame instance update (the layer's processPendingTLAS,
+// layer/VkLayer_CudaRT.cpp:3418, rebuilds its TLAS every CUDA_RT_TLAS_EVERY_N
+// frames): new transforms and BLAS choices for the same number of
+// instances, the top-level tree rebuilt in place; the BLASes are untouched.
+int cudaTLAS_setTransforms(CudaTLAS_t t, const RtInstance* inst, int ni) {
+    clear_error();
+    if (!t || !inst || ni != t->num_instances) {
+        set_error("cudaTLAS_setTransforms: need one instance record per TLAS instance (%d)",
+                  t ? t->num_instances : 0);
+        return RT_ERR_INVALID;
+    }
+    std::lock_guard<std::mutex> g(t->mu);
+    std::vector<float> h_inv;
+    std::vector<float4> rec, lo, hi;
+    if (!instance_data(t->blas, inst, ni, "cudaTLAS_setTransforms", h_inv, rec, lo, hi)) return RT_ERR_INVALID;
+    // the new tree is built aside, so a failure leaves the TLAS as it was
+    Bvh2Device b2;
+    Bvh8Device b8;
+    if (!build_top(lo, hi, b2, b8)) return RT_ERR_CUDA;
+    // traces still in flight read the current arrays: let them finish
+    if (!RT_CUDA(cudaDeviceSynchronize()) ||
+        !RT_CUDA(cudaMemcpy(t->inst.p, rec.data(), rec.size() * sizeof(float4), cudaMemcpyHostToDevice)))
+        return RT_ERR_CUDA;
+    t->bvh2.swap(b2);
+    t->bvh8.swap(b8);
+    t->h_inv.swap(h_inv);
+    t->generation++;
+    return RT_OK;
 }
 
 void cudaTLAS_destroy(CudaTLAS_t t) {

@@ -142,6 +142,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "cudaTLAS_traceClosest": (i32, [vp, vp, i32, vp, vp, vp]),
         "cudaTLAS_traceAny": (i32, [vp, vp, i32, vp, vp]),
         "cudaTLAS_getInverseTransforms": (i32, [vp, vp, i32]),
+        "cudaTLAS_setTransforms": (i32, [vp, vp, i32]),
         "rtBatch_build": (vp, [vp, vp, i32, vp]),
         "rtBatch_destroy": (None, [vp]),
         "rtBatch_traceClosest": (i32, [vp, vp, vp, i32, vp, vp]),
@@ -389,6 +390,15 @@ class TLAS:
         if not self.h:
             raise RtError(f"cudaTLAS_build failed: {last_error()}")
         self.n = n
+
+    def set_transforms(self, xforms: np.ndarray, blas_index: np.ndarray):
+        """cudaTLAS_setTransforms: new instance transforms / BLAS choices, same count."""
+        inst = (RtInstance * self.n)()
+        for k in range(self.n):
+            inst[k].xform[:] = np.asarray(xforms[k], np.float32).ravel().tolist()
+            inst[k].blas = int(blas_index[k])
+        _check(load().cudaTLAS_setTransforms(self.h, inst, self.n), "cudaTLAS_setTransforms")
+        self.instances = inst
 
     def inverse(self) -> np.ndarray:
         out = np.zeros((self.n, 12), np.float32)
