@@ -145,8 +145,8 @@ void cudaTLAS_destroy(CudaTLAS_t tlas);
  * is rebuilt in place, the BLASes are untouched, and traces afterwards equal
  * those of a TLAS built with the new instances.  Waits for the device first
  * (traces in flight finish on the old instances).  On failure the TLAS keeps
- * its previous instances.  A path tracer created on the TLAS must be created
- * again (rtPT_render refuses a TLAS changed since rtPT_create). */
+ * its previous instances.  A path tracer created on the TLAS reloads the
+ * transforms, BLAS choices and light areas at its next rtPT_render. */
 int cudaTLAS_setTransforms(CudaTLAS_t tlas, const RtInstance* instances, int numInstances);
 
 /* Closest hit over all instances: d_hits[i].prim is the primitive index in

@@ -308,11 +308,12 @@ def test_tlas_two_level_vs_oracle(cuda):
 def test_tlas_set_transforms_equals_a_fresh_build(cuda):
     """cudaTLAS_setTransforms moves every instance and changes BLAS choices in
     place: traces afterwards are byte-identical to those of a TLAS built with
-    the new instances, and a path tracer created before the update refuses
-    to render (it copied the old transforms)."""
+    the new instances, and a path tracer created before the move renders
+    exactly what one created on the new TLAS renders (it reloads transforms
+    and light areas at its next render)."""
     import torch
     rs = np.random.RandomState(8)
-    blases = [lib.BVH(scenes.scene_meshes(20 + i, 2000, box=6.0, lo=200, hi=800, ground=False)) for i in range(3)]
+    blases = [lib.BVH(scenes.scene_meshes(20 + i, 2000, box=30.0, lo=200, hi=800, ground=False)) for i in range(3)]
     n = 16
 
     def instances(seed):
@@ -323,10 +324,18 @@ def test_tlas_set_transforms_equals_a_fresh_build(cuda):
 
     xa, ba = instances(1)
     xb, bb = instances(2)
+    alb = np.full((n, 3), 0.6, np.float32)
+    emi = np.zeros((n, 3), np.float32)
+    emi[[0, 5]] = 5.0
+    cam = lib.make_camera((0.0, 0.0, -90.0), (0.0, 0.0, 0.0))
+    W, H = 128, 72
+    img = [torch.zeros(W * H * 3, dtype=torch.float32, device="cuda") for _ in range(3)]
     moved = lib.TLAS(blases, xa, ba)
-    pt = lib.PathTracer(moved, np.full((n, 3), 0.5, np.float32), np.zeros((n, 3), np.float32))
+    pt = lib.PathTracer(moved, alb, emi)
+    pt.render(cam, W, H, 2, d_rgb=img[0])
     moved.set_transforms(xb, bb)
     fresh = lib.TLAS(blases, xb, bb)
+    pt_fresh = lib.PathTracer(fresh, alb, emi)
     try:
         assert np.array_equal(moved.inverse(), fresh.inverse())
         rays = scenes.random_rays(61, 20000)
@@ -344,11 +353,16 @@ def test_tlas_set_transforms_equals_a_fresh_build(cuda):
             out.append((d_hits.cpu().numpy(), d_inst.cpu().numpy(), d_occ.cpu().numpy()))
         for a, b in zip(*out):
             assert np.array_equal(a, b)
-        assert (out[0][1] >= 0).mean() > 0.05  # 9 % of these rays hit
-        d_rgb = torch.zeros(64 * 36 * 3, dtype=torch.float32, device="cuda")
-        with pytest.raises(lib.RtError):
-            pt.render(lib.make_camera((0.0, 0.0, -80.0), (0.0, 0.0, 0.0)), 64, 36, 1, d_rgb=d_rgb)
+        assert (out[0][1] >= 0).mean() > 0.05
+        pt.render(cam, W, H, 2, d_rgb=img[1])
+        pt_fresh.render(cam, W, H, 2, d_rgb=img[2])
+        torch.cuda.synchronize()
+        a, b, f = (x.cpu().numpy() for x in img)
+        assert np.array_equal(b.view(np.uint32), f.view(np.uint32))
+        assert b.sum() > 0 and not np.array_equal(a, b)
+        assert pt.stats()["light_tris"] == pt_fresh.stats()["light_tris"]
     finally:
+        pt_fresh.close()
         pt.close()
         fresh.close()
         moved.close()

@@ -258,6 +258,8 @@ struct CudaTLASHandle {
     rtb::Bvh8Device bvh8;
     rtb::DevBuf<float4> inst;     // per instance: inv xform (3 float4), BLAS ptrs, id base
     std::vector<float> h_inv;     // 12 floats per instance
+    std::vector<float> h_fwd;     // 12 floats per instance: the object -> world transforms
+    std::vector<int> h_blas;      // BLAS index per instance
     unsigned long long generation = 0;  // bumped by every cudaTLAS_setTransforms
     rtb::DevBuf<int> counters;
     unsigned counter_next = 0;

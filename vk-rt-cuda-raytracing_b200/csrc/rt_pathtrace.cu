@@ -318,6 +318,8 @@ struct RtPathTracerHandle {
     CudaTLAS_t tlas = nullptr;
     unsigned long long tlas_generation = 0;  // the TLAS's instances this tracer copied
     int ninst = 0;
+    std::vector<char> emissive;                  // per instance
+    std::vector<std::vector<float>> host_tris;   // per BLAS, emissive ones only (light table)
     DevBuf<float4> mat;
     DevBuf<float> fwd, inv;
     DevBuf<const float*> tris9;
@@ -385,6 +387,69 @@ double tri_area_world(const float* m, const float* v) {
 
 }  // namespace
 
+// Instance-dependent state of a tracer, from the transforms (12 floats per
+// instance) and BLAS choices given: forward / inverse transforms, each
+// instance's BLAS triangles, and the emissive triangles weighted by world
+// area (an exact integer CDF).  Host copies of emissive BLASes are kept for
+// later reloads.
+static bool load_instances(RtPathTracerHandle* pt, const float* fwd12, const int* blas_idx, const char* who) {
+    const CudaTLASHandle* tlas = pt->tlas;
+    const int ni = pt->ninst;
+    std::vector<const float*> t9(ni);
+    std::vector<double> areas;
+    std::vector<int2> lights;
+    for (int k = 0; k < ni; k++) {
+        const int b = blas_idx[k];
+        if (b < 0 || b >= (int)tlas->blas.size()) {
+            set_error("%s: instance %d names BLAS %d", who, k, b);
+            return false;
+        }
+        const CudaBVHHandle* bh = tlas->blas[b];
+        t9[k] = bh->tris9.p;
+        if (pt->emissive[k]) {
+            std::vector<float>& ht = pt->host_tris[b];
+            if (ht.empty()) {
+                ht.resize((size_t)bh->num_tris * 9);
+                if (!RT_CUDA(cudaMemcpy(ht.data(), bh->tris9.p, ht.size() * 4, cudaMemcpyDeviceToHost))) return false;
+            }
+            for (int p = 0; p < bh->num_tris; p++) {
+                areas.push_back(tri_area_world(fwd12 + (size_t)12 * k, &ht[(size_t)p * 9]));
+                lights.push_back(make_int2(k, p));
+            }
+        }
+    }
+    pt->total_q = 0;
+    pt->light_area = 0.0;
+    // exact integer CDF: q_i = floor(area_i * 2^K), K from count and max area
+    pt->num_lights = (int)lights.size();
+    std::vector<unsigned long long> cdf(lights.size());
+    if (!lights.empty()) {
+        double amax = 0.0;
+        for (double a : areas) amax = std::max(amax, a);
+        const int K = (int)floor(61.0 - log2((double)areas.size() * std::max(amax, 1e-300)));
+        unsigned long long run = 0;
+        for (size_t i = 0; i < areas.size(); i++) {
+            run += (unsigned long long)floor(ldexp(areas[i], K));
+            cdf[i] = run;
+        }
+        pt->total_q = run;
+        pt->light_area = ldexp((double)run, -K);
+    }
+    const size_t nl = std::max<size_t>(lights.size(), 1);
+    bool ok = pt->fwd.ensure((size_t)12 * ni) && pt->inv.ensure((size_t)12 * ni) && pt->tris9.ensure(ni) &&
+              pt->cdf.ensure(nl) && pt->lights.ensure(nl) &&
+              RT_CUDA(cudaMemcpy(pt->fwd.p, fwd12, (size_t)12 * ni * 4, cudaMemcpyHostToDevice)) &&
+              RT_CUDA(cudaMemcpy(pt->inv.p, tlas->h_inv.data(), (size_t)12 * ni * 4, cudaMemcpyHostToDevice)) &&
+              RT_CUDA(cudaMemcpy(pt->tris9.p, t9.data(), t9.size() * sizeof(void*), cudaMemcpyHostToDevice));
+    if (ok && !lights.empty())
+        ok = RT_CUDA(cudaMemcpy(pt->cdf.p, cdf.data(), cdf.size() * 8, cudaMemcpyHostToDevice)) &&
+             RT_CUDA(cudaMemcpy(pt->lights.p, lights.data(), lights.size() * 8, cudaMemcpyHostToDevice));
+    if (!ok) return false;
+    pt->stats.light_tris = pt->num_lights;
+    pt->stats.light_area = pt->light_area;
+    return true;
+}
+
 extern "C" {
 
 int rtPT_cameraBasis(const RtCamera* cam, int width, int height, float* out14) {
@@ -411,72 +476,24 @@ RtPathTracer_t rtPT_create(CudaTLAS_t tlas, const RtMaterial* mats, int nmat, co
     pt->ninst = ni;
     std::vector<float4> mat((size_t)2 * ni);
     std::vector<float> fwd((size_t)12 * ni);
-    std::vector<const float*> t9(ni);
-    std::vector<double> areas;
-    std::vector<int2> lights;
-    std::vector<std::vector<float>> host_tris(tlas->blas.size());
+    std::vector<int> bidx(ni);
+    pt->emissive.assign(ni, 0);
+    pt->host_tris.assign(tlas->blas.size(), std::vector<float>());
     for (int k = 0; k < ni; k++) {
         mat[2 * k] = make_float4(mats[k].albedo[0], mats[k].albedo[1], mats[k].albedo[2], 0.f);
         mat[2 * k + 1] = make_float4(mats[k].emission[0], mats[k].emission[1], mats[k].emission[2], 0.f);
         memcpy(&fwd[(size_t)12 * k], instances[k].xform, 48);
-        const int b = instances[k].blas;
-        if (b < 0 || b >= (int)tlas->blas.size()) {
-            set_error("rtPT_create: instance %d names BLAS %d", k, b);
-            delete pt;
-            return nullptr;
-        }
-        const CudaBVHHandle* bh = tlas->blas[b];
-        t9[k] = bh->tris9.p;
-        const bool emissive = mats[k].emission[0] > 0.f || mats[k].emission[1] > 0.f || mats[k].emission[2] > 0.f;
-        if (emissive) {
-            std::vector<float>& ht = host_tris[b];
-            if (ht.empty()) {
-                ht.resize((size_t)bh->num_tris * 9);
-                if (!RT_CUDA(cudaMemcpy(ht.data(), bh->tris9.p, ht.size() * 4, cudaMemcpyDeviceToHost))) {
-                    delete pt;
-                    return nullptr;
-                }
-            }
-            for (int p = 0; p < bh->num_tris; p++) {
-                areas.push_back(tri_area_world(instances[k].xform, &ht[(size_t)p * 9]));
-                lights.push_back(make_int2(k, p));
-            }
-        }
+        bidx[k] = instances[k].blas;
+        pt->emissive[k] = mats[k].emission[0] > 0.f || mats[k].emission[1] > 0.f || mats[k].emission[2] > 0.f;
     }
-    // exact integer CDF: q_i = floor(area_i * 2^K), K from count and max area
-    pt->num_lights = (int)lights.size();
-    std::vector<unsigned long long> cdf(lights.size());
-    if (!lights.empty()) {
-        double amax = 0.0;
-        for (double a : areas) amax = std::max(amax, a);
-        const int K = (int)floor(61.0 - log2((double)areas.size() * std::max(amax, 1e-300)));
-        unsigned long long run = 0;
-        for (size_t i = 0; i < areas.size(); i++) {
-            run += (unsigned long long)floor(ldexp(areas[i], K));
-            cdf[i] = run;
-        }
-        pt->total_q = run;
-        pt->light_area = ldexp((double)run, -K);
-    }
-    std::vector<float> inv((size_t)12 * ni);
-    memcpy(inv.data(), tlas->h_inv.data(), inv.size() * 4);
-    const size_t nl = std::max<size_t>(lights.size(), 1);
-    bool ok = pt->mat.alloc(mat.size()) && pt->fwd.alloc(fwd.size()) && pt->inv.alloc(inv.size()) &&
-              pt->tris9.alloc(ni) && pt->cdf.alloc(nl) && pt->lights.alloc(nl) && pt->counts.alloc(8) &&
-              pt->work.alloc(1024) && pt->bcounts.alloc(2 * kMaxBounces) &&
+    bool ok = pt->mat.alloc(mat.size()) && pt->counts.alloc(8) && pt->work.alloc(1024) &&
+              pt->bcounts.alloc(2 * kMaxBounces) &&
               RT_CUDA(cudaMemcpy(pt->mat.p, mat.data(), mat.size() * 16, cudaMemcpyHostToDevice)) &&
-              RT_CUDA(cudaMemcpy(pt->fwd.p, fwd.data(), fwd.size() * 4, cudaMemcpyHostToDevice)) &&
-              RT_CUDA(cudaMemcpy(pt->inv.p, inv.data(), inv.size() * 4, cudaMemcpyHostToDevice)) &&
-              RT_CUDA(cudaMemcpy(pt->tris9.p, t9.data(), t9.size() * sizeof(void*), cudaMemcpyHostToDevice));
-    if (ok && !lights.empty())
-        ok = RT_CUDA(cudaMemcpy(pt->cdf.p, cdf.data(), cdf.size() * 8, cudaMemcpyHostToDevice)) &&
-             RT_CUDA(cudaMemcpy(pt->lights.p, lights.data(), lights.size() * 8, cudaMemcpyHostToDevice));
+              load_instances(pt, fwd.data(), bidx.data(), "rtPT_create");
     if (!ok) {
         delete pt;
         return nullptr;
     }
-    pt->stats.light_tris = pt->num_lights;
-    pt->stats.light_area = pt->light_area;
     return pt;
 }
 
@@ -496,10 +513,13 @@ int rtPT_render(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* prm, f
         set_error("rtPT_render: d_rgb must be 4-byte aligned");
         return RT_ERR_INVALID;
     }
-    // transforms, light areas and BLAS choices were copied at creation
+    // the TLAS's instances moved (cudaTLAS_setTransforms): reload the copies
+    // once renders still in flight are done with them
     if (pt->tlas->generation != pt->tlas_generation) {
-        set_error("rtPT_render: the TLAS's instances changed since rtPT_create; create the path tracer again");
-        return RT_ERR_INVALID;
+        const CudaTLASHandle* t = pt->tlas;
+        if (!RT_CUDA(cudaDeviceSynchronize()) || !load_instances(pt, t->h_fwd.data(), t->h_blas.data(), "rtPT_render"))
+            return RT_ERR_CUDA;
+        pt->tlas_generation = t->generation;
     }
     const int64_t P = (int64_t)prm->width * prm->height * prm->spp;
     if (P > (int64_t)INT32_MAX) {

@@ -396,6 +396,16 @@ static bool instance_data(const std::vector<CudaBVH_t>& blas, const RtInstance* 
     return true;
 }
 
+// The instances as given: transform (12 floats) and BLAS index each.
+static void instance_copy(const RtInstance* inst, int ni, std::vector<float>& fwd, std::vector<int>& blas) {
+    fwd.resize((size_t)ni * 12);
+    blas.resize(ni);
+    for (int k = 0; k < ni; k++) {
+        memcpy(&fwd[(size_t)k * 12], inst[k].xform, 12 * sizeof(float));
+        blas[k] = inst[k].blas;
+    }
+}
+
 // The top-level tree over the instance boxes: binned SAH with leaves of one
 // instance, collapsed greedily to 8-wide nodes.
 static bool build_top(const std::vector<float4>& lo, const std::vector<float4>& hi, Bvh2Device& b2, Bvh8Device& b8) {
@@ -434,6 +444,7 @@ CudaTLAS_t cudaTLAS_build(const CudaBVH_t* blas, int nb, const RtInstance* inst,
     t->num_instances = ni;
     t->blas.assign(blas, blas + nb);
     std::vector<float4> rec, lo, hi;
+    instance_copy(inst, ni, t->h_fwd, t->h_blas);
     bool ok = instance_data(t->blas, inst, ni, "cudaTLAS_build", t->h_inv, rec, lo, hi) &&
               t->inst.alloc(rec.size()) &&
               RT_CUDA(cudaMemcpy(t->inst.p, rec.data(), rec.size() * sizeof(float4), cudaMemcpyHostToDevice)) &&
@@ -450,6 +461,7 @@ CudaTLAS_t cudaTLAS_build(const CudaBVH_t* blas, int nb, const RtInstance* inst,
 // layer/VkLayer_CudaRT.cpp:3418, rebuilds its TLAS every CUDA_RT_TLAS_EVERY_N
 // frames): new transforms and BLAS choices for the same number of
 // instances, the top-level tree rebuilt in place; the BLASes are untouched.
+// A path tracer on the TLAS reloads the instances at its next render.
 int cudaTLAS_setTransforms(CudaTLAS_t t, const RtInstance* inst, int ni) {
     clear_error();
     if (!t || !inst || ni != t->num_instances) {
@@ -472,6 +484,7 @@ int cudaTLAS_setTransforms(CudaTLAS_t t, const RtInstance* inst, int ni) {
     t->bvh2.swap(b2);
     t->bvh8.swap(b8);
     t->h_inv.swap(h_inv);
+    instance_copy(inst, ni, t->h_fwd, t->h_blas);
     t->generation++;
     return RT_OK;
 }
