@@ -48,6 +48,9 @@ def test_null_and_empty_inputs_fail_cleanly():
     assert L.cudaBVH_tracePrimary(None, 16, 0.0, 0.0, 0.0, None) == 0.0
     pn = C.POINTER(C.c_uint32)()
     assert L.cudaBVH_buildTLASFast(None, 3, C.byref(pn), None) == 0
+    assert L.cudaTLAS_build(None, 0, None, 0) is None
+    assert L.cudaTLAS_setTransforms(None, None, 0) == -1
+    assert "one instance record per TLAS instance" in lib.last_error()
 
 
 @pytest.mark.parametrize("path", sorted(GOLD.glob("ref_tlasfast_*.npz")), ids=lambda p: p.stem)
