@@ -21,13 +21,14 @@ def test_library_loads_and_exports_every_declared_symbol():
 
 
 def test_reference_header_symbols_all_present():
-    # the 22 entry points of the reference's layer/cuda_bvh_backend.h:21-141
+    # the 21 entry points of the reference's layer/cuda_bvh_backend.h:21-141
     ref = ["cudaBVH_build", "cudaBVH_destroy", "cudaBVH_tracePrimary", "cudaBVH_traceDiffuse",
            "cudaBVH_traceToRGBA", "cudaBVH_traceToGPUPtr", "cudaBVH_traceToGPUAsync", "cudaBVH_traceToHostPtr",
            "cudaBVH_importBufferFd", "cudaBVH_getBounds", "cudaBVH_getNumTris", "cudaBVH_getNumBVH4Nodes",
            "cudaBVH_getNumCWBVHNodes", "cudaBVH_getNodeData", "cudaBVH_getTriData", "cudaBVH_getStacklessBVH2",
            "cudaBVH_getPackedTris", "cudaBVH_resetDevice", "cudaBVH_buildFromAABBs", "cudaBVH_buildTLASFast",
            "cudaBVH_readGPUMemoryFd"]
+    assert len(set(ref)) == 21
     L = lib.load()
     assert all(hasattr(L, s) for s in ref)
 
