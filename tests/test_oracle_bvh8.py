@@ -152,3 +152,62 @@ def test_walk_reproduces_the_kernel(path):
     # the algorithmic bytes per ray bench.py charges, from the oracle's counts
     per_ray = 32 + 16 + cnt[:, 0].mean() * 80 + cnt[:, 1].mean() * 36
     assert per_ray > 48
+
+
+def _slot_boxes(node):
+    """Decoded child boxes of one 8-wide node (float64): lo, hi (8, 3)."""
+    p = node[0:3].view(np.float32).astype(np.float64)
+    e = int(node[3])
+    scale = np.array([math.ldexp(1.0, ((e >> (8 * a)) & 0xFF) - 127) if (e >> (8 * a)) & 0xFF else 0.0
+                      for a in range(3)])
+    lo, hi = np.zeros((8, 3)), np.zeros((8, 3))
+    for a in range(3):
+        w = [int(x) for x in node[8 + 4 * a: 12 + 4 * a]]
+        for s in range(8):
+            ql = (w[s >> 2] >> (8 * (s & 3))) & 0xFF
+            qh = (w[2 + (s >> 2)] >> (8 * (s & 3))) & 0xFF
+            lo[s, a], hi[s, a] = p[a] + ql * scale[a], p[a] + qh * scale[a]
+    return lo, hi
+
+
+@pytest.mark.parametrize("path", sorted(GOLD.glob("bvh8_walk_*.npz")), ids=lambda p: p.stem)
+def test_quantised_boxes_hold_their_triangles(path):
+    """The builder's 8-bit child boxes are rounded outward: every triangle
+    reachable through a slot lies inside that slot's decoded box (the tree
+    the kernel walked, as written on the GPU)."""
+    g = np.load(path)
+    nodes, recs = g["nodes"], g["recs"].astype(np.float64)
+    v0 = recs[:, 0:3]
+    verts = np.stack([v0, v0 + recs[:, 4:7], v0 + recs[:, 8:11]], 1)  # the triangle the kernel tests
+    memo = {}
+
+    def slot_records(ni):
+        node = nodes[ni]
+        imask, child_base, tri_base = int(node[3]) >> 24, int(node[4]), int(node[5])
+        per_slot = []
+        for s in range(8):
+            meta = (int(node[6 + (s >> 2)]) >> (8 * (s & 3))) & 0xFF
+            if (imask >> s) & 1:
+                c = child_base + bin(imask & ((1 << s) - 1)).count("1")
+                per_slot.append(subtree(c))
+            else:
+                per_slot.append(np.arange(tri_base + (meta & 31), tri_base + (meta & 31) + (meta >> 5)))
+        return per_slot
+
+    def subtree(ni):
+        if ni not in memo:
+            memo[ni] = np.concatenate(slot_records(ni))
+        return memo[ni]
+
+    checked = 0
+    for ni in range(nodes.shape[0]):
+        lo, hi = _slot_boxes(nodes[ni])
+        for s, r in enumerate(slot_records(ni)):
+            if r.size == 0:
+                continue
+            v = verts[r].reshape(-1, 3)
+            tol = 1e-6 * (np.abs(v).max() + 1.0)  # the stored edges are rounded differences
+            assert (v >= lo[s] - tol).all() and (v <= hi[s] + tol).all(), (ni, s)
+            checked += 1
+    assert sorted(subtree(0).tolist()) == list(range(recs.shape[0]))  # every record under the root once
+    assert checked > nodes.shape[0]
