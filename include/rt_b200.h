@@ -66,6 +66,17 @@ int cudaBVH_traceClosest(CudaBVH_t bvh, const RtRay* d_rays, int n, RtHit* d_hit
  * with tmin < t < tmax, else 0. */
 int cudaBVH_traceAny(CudaBVH_t bvh, const RtRay* d_rays, int n, uint8_t* d_occluded, void* stream);
 
+/* Traversal status of the device-pointer calls on this handle.  The trace
+ * calls above return as soon as the kernel is queued, so a stack overflow
+ * inside it (RT_ERR_STACK: the BVH is deeper than the 64-entry traversal
+ * stack; never silent) is recorded in the handle's status word instead.
+ * This call waits for `stream`, reads the word, clears it and returns
+ * RT_OK or RT_ERR_STACK (or RT_ERR_CUDA).  The word is shared by every call
+ * on the handle since the last check, from any thread or stream.  The
+ * reference has no counterpart (its trace calls only print CUDA errors,
+ * layer/cuda_bvh_backend.cu:25). */
+int cudaBVH_getStatus(CudaBVH_t bvh, void* stream);
+
 /* The same two calls on host buffers: copies in, traces, copies out and
  * waits.  Staging buffers are owned by the handle. */
 int cudaBVH_traceClosestHost(CudaBVH_t bvh, const RtRay* h_rays, int n, RtHit* h_hits);
@@ -118,6 +129,22 @@ int cudaBVH_getDeviceLayout(CudaBVH_t bvh, const void** d_nodes, int* num_nodes,
 int cudaBVH_traceCounters(CudaBVH_t bvh, const RtRay* d_rays, int n, int any, uint32_t* d_counts,
                           void* stream);
 
+/* Test hook, no counterpart in the reference: after `after` more device
+ * allocations by the library (handle buffers, staging, build scratch), every
+ * further one fails as if the device were out of memory, until the hook is
+ * called again; after < 0 turns it off.  The failing call returns
+ * RT_ERR_NOMEM (or NULL for a build) with the reason in rtGetLastError(),
+ * and the library stays usable.  Process-wide. */
+int rtDebug_failAllocations(int after);
+
+/* Measurement helper, no counterpart in the reference: read bandwidth of
+ * this GPU in GB/s, streaming a `bytes` buffer (allocated and freed by the
+ * call) `reps` times in one launch with 16-byte loads cached in L2 only,
+ * timed with events after two warm-up passes.  A buffer well under the 126 MB L2 gives
+ * the L2 read bandwidth that bounds traversal of an L2-resident BVH; one
+ * far above it gives the HBM read bandwidth.  Changes no device setting. */
+int rtProbe_readBandwidth(uint64_t bytes, int reps, float* out_gbs);
+
 /* ---------------- instanced scenes (TLAS over BLASes) ---------------- */
 typedef struct CudaTLASHandle* CudaTLAS_t;
 
@@ -146,7 +173,10 @@ void cudaTLAS_destroy(CudaTLAS_t tlas);
  * those of a TLAS built with the new instances.  Waits for the device first
  * (traces in flight finish on the old instances).  On failure the TLAS keeps
  * its previous instances.  A path tracer created on the TLAS reloads the
- * transforms, BLAS choices and light areas at its next rtPT_render. */
+ * transforms, BLAS choices and light areas at its next rtPT_render.  Safe
+ * against traces and renders of the same TLAS on other threads: each takes
+ * the TLAS's lock while it launches, so it runs wholly on the old or wholly
+ * on the new instances. */
 int cudaTLAS_setTransforms(CudaTLAS_t tlas, const RtInstance* instances, int numInstances);
 
 /* Closest hit over all instances: d_hits[i].prim is the primitive index in
@@ -156,6 +186,9 @@ int cudaTLAS_setTransforms(CudaTLAS_t tlas, const RtInstance* instances, int num
 int cudaTLAS_traceClosest(CudaTLAS_t tlas, const RtRay* d_rays, int n, RtHit* d_hits, int32_t* d_inst,
                           void* stream);
 int cudaTLAS_traceAny(CudaTLAS_t tlas, const RtRay* d_rays, int n, uint8_t* d_occluded, void* stream);
+
+/* Status word of the TLAS's device-pointer traces, as cudaBVH_getStatus. */
+int cudaTLAS_getStatus(CudaTLAS_t tlas, void* stream);
 
 /* Inverse transforms (12 floats per instance) the TLAS uses, host copy. */
 int cudaTLAS_getInverseTransforms(CudaTLAS_t tlas, float* out, int numInstances);

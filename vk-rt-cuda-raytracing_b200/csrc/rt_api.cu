@@ -41,6 +41,16 @@ bool cuda_ok(cudaError_t e, const char* what) {
     return false;
 }
 
+// Allocations left before injected failures begin; negative = injection off.
+static std::atomic<long long> g_alloc_budget{-1};
+
+bool alloc_fail_injected() {
+    long long b = g_alloc_budget.load(std::memory_order_relaxed);
+    while (b > 0 && !g_alloc_budget.compare_exchange_weak(b, b - 1, std::memory_order_relaxed)) {
+    }
+    return b == 0;
+}
+
 int num_sms() {
     static const int n = [] {
         int d = 0, v = 0;
@@ -92,11 +102,24 @@ bool check_aligned(const char* who, const void* rays, const void* out, size_t ou
 }
 
 // A fresh zeroed work counter for one launch.  Slots cycle through a ring,
-// so up to kCounterRing launches may be in flight on one handle.
-int* next_counter(DevBuf<int>& ring, unsigned& next, cudaStream_t s) {
-    int* p = ring.p + (next++ % kCounterRing);
+// so up to kCounterRing launches may be in flight on one handle; the index
+// is an atomic, so concurrent callers never share a slot.
+int* next_counter(DevBuf<int>& ring, std::atomic<unsigned>& next, cudaStream_t s) {
+    int* p = ring.p + (next.fetch_add(1, std::memory_order_relaxed) % kCounterRing);
     cudaMemsetAsync(p, 0, sizeof(int), s);
     return p;
+}
+
+int read_status(int* d_status, cudaStream_t s, const char* who) {
+    int st = 0;
+    if (!RT_CUDA(cudaStreamSynchronize(s)) ||
+        !RT_CUDA(cudaMemcpy(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost)))
+        return RT_ERR_CUDA;
+    if (st & RT_STATUS_STACK) {
+        set_error("%s: traversal stack overflow", who);
+        return RT_CUDA(cudaMemset(d_status, 0, sizeof(int))) ? RT_ERR_STACK : RT_ERR_CUDA;
+    }
+    return RT_OK;
 }
 
 }  // namespace rtb
@@ -329,7 +352,7 @@ bool render_rgba(CudaBVHHandle* h, int w, int ht, float cx, float cy, float cz, 
     launch_gen_lookat(h->stage_rays.p, w, ht, lookat_basis(h, cx, cy, cz), s);
     int* work = next_counter(h->counters, h->counter_next, s);
     if (launch_trace_blas(h->bvh8, h->stage_rays.p, n, h->stage_hits.p, nullptr, nullptr, work, h->status.p, s) != RT_OK)
-        return RT_CUDA(cudaGetLastError());
+        return false;
     launch_shade(h->stage_rays.p, h->stage_hits.p, h->tris9.p, w, ht, out, fmt, s);
     return RT_CUDA(cudaGetLastError());
 }
@@ -565,7 +588,6 @@ int cudaBVH_traceClosest(CudaBVH_t h, const RtRay* d_rays, int n, RtHit* d_hits,
     cudaStream_t s = (cudaStream_t)stream;
     int* work = next_counter(h->counters, h->counter_next, s);
     const int rc = launch_trace_blas(h->bvh8, d_rays, n, d_hits, nullptr, nullptr, work, h->status.p, s);
-    if (rc != RT_OK) RT_CUDA(cudaGetLastError());
     return rc;
 }
 
@@ -579,7 +601,6 @@ int cudaBVH_traceAny(CudaBVH_t h, const RtRay* d_rays, int n, uint8_t* d_occ, vo
     cudaStream_t s = (cudaStream_t)stream;
     int* work = next_counter(h->counters, h->counter_next, s);
     const int rc = launch_trace_blas(h->bvh8, d_rays, n, nullptr, d_occ, nullptr, work, h->status.p, s);
-    if (rc != RT_OK) RT_CUDA(cudaGetLastError());
     return rc;
 }
 
@@ -598,15 +619,19 @@ int cudaBVH_traceCounters(CudaBVH_t h, const RtRay* d_rays, int n, int any, uint
                              d_counts, work, h->status.p, s);
 }
 
-static int check_status(CudaBVHHandle* h) {
-    int st = 0;
-    if (!RT_CUDA(cudaMemcpy(&st, h->status.p, sizeof(int), cudaMemcpyDeviceToHost))) return RT_ERR_CUDA;
-    if (st & 1) {
-        set_error("traversal stack overflow");
-        cudaMemset(h->status.p, 0, sizeof(int));
-        return RT_ERR_STACK;
-    }
+static int check_status(CudaBVHHandle* h) { return read_status(h->status.p, 0, "trace"); }
+
+int rtDebug_failAllocations(int after) {
+    g_alloc_budget.store(after < 0 ? -1 : after, std::memory_order_relaxed);
     return RT_OK;
+}
+
+int cudaBVH_getStatus(CudaBVH_t h, void* stream) {
+    if (!h) {
+        set_error("cudaBVH_getStatus: invalid argument");
+        return RT_ERR_INVALID;
+    }
+    return read_status(h->status.p, (cudaStream_t)stream, "cudaBVH_getStatus");
 }
 
 namespace rtb {
@@ -678,7 +703,7 @@ int trace_host(CudaBVHHandle* h, const RtRay* rays, int n, void* out, bool any) 
         int* work = next_counter(h->counters, h->counter_next, comp);
         const int rc = launch_trace_blas(h->bvh8, h->stage_rays.p + b, c, any ? nullptr : h->stage_hits.p + b,
                                          any ? h->stage_occ.p + b : nullptr, nullptr, work, h->status.p, comp);
-        if (rc != RT_OK) return RT_CUDA(cudaGetLastError()) ? rc : RT_ERR_CUDA;
+        if (rc != RT_OK) return rc;
         if (!RT_CUDA(cudaEventRecord(p.ev_tr[k], comp)) || !RT_CUDA(cudaStreamWaitEvent(p.out, p.ev_tr[k], 0)) ||
             !RT_CUDA(cudaMemcpyAsync((char*)out + (size_t)b * es, dev_out + (size_t)b * es, (size_t)c * es,
                                      cudaMemcpyDeviceToHost, p.out)))
@@ -944,6 +969,8 @@ int cudaBVH_readGPUMemoryFd(int fd, uint64_t allocationSize, uint64_t offset, ui
 
 void cudaBVH_resetDevice(void) {
     cudaDeviceSynchronize();
+    // the reset ends this context: the scratch address looked up in it is void
+    noalloc_forget_current_device();
     cudaDeviceReset();
 }
 

@@ -161,7 +161,6 @@ int rtBatch_traceClosest(RtBatch_t b, const RtRay* d_rays, const int* d_ray_offs
     cudaMemsetAsync(b->work.p, 0, sizeof(int), s);
     rc = launch_trace_multi(b->bvh8, d_rays, n, d_ray_offsets, b->d_tri_off.p, b->num_scenes, d_hits, nullptr,
                             b->work.p, b->status.p, b->ctas_per_sm, b->node_iters, s);
-    if (rc != RT_OK) RT_CUDA(cudaGetLastError());
     return rc;
 }
 
@@ -173,7 +172,6 @@ int rtBatch_traceAny(RtBatch_t b, const RtRay* d_rays, const int* d_ray_offsets,
     cudaMemsetAsync(b->work.p, 0, sizeof(int), s);
     rc = launch_trace_multi(b->bvh8, d_rays, n, d_ray_offsets, b->d_tri_off.p, b->num_scenes, nullptr, d_occ,
                             b->work.p, b->status.p, b->ctas_per_sm, b->node_iters, s);
-    if (rc != RT_OK) RT_CUDA(cudaGetLastError());
     return rc;
 }
 

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -24,6 +25,10 @@ bool cuda_ok(cudaError_t e, const char* what);
 
 int num_sms();
 
+// Host-side allocation-failure injection for tests (rtDebug_failAllocations):
+// true when the allocation about to be made must fail.
+bool alloc_fail_injected();
+
 // Device pointers handed to the kernels are read and written with 16-byte
 // (rays, hit records), 8-byte or 4-byte vector accesses; a misaligned one
 // would fault on the GPU, so entry points reject it first.
@@ -44,6 +49,10 @@ struct DevBuf {
     bool alloc(size_t count) {
         release();
         if (count == 0) return true;
+        if (alloc_fail_injected()) {
+            set_error("cudaMalloc of %zu bytes failed (injected)", count * sizeof(T));
+            return false;
+        }
         if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) {
             cudaGetLastError();
             p = nullptr;
@@ -96,6 +105,10 @@ struct TmpBuf {
     bool alloc(size_t count, cudaStream_t st) {
         release();
         if (count == 0) return true;
+        if (alloc_fail_injected()) {
+            set_error("scratch allocation of %zu bytes failed (injected)", count * sizeof(T));
+            return false;
+        }
         cudaMemPool_t pool = scratch_pool();
         if (!pool || cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(T), pool, st) != cudaSuccess) {
             cudaGetLastError();
@@ -119,6 +132,10 @@ template <class T>
 bool DevBuf<T>::alloc_on(size_t count, cudaStream_t st) {
     release();
     if (count == 0) return true;
+    if (alloc_fail_injected()) {
+        set_error("scratch allocation of %zu bytes failed (injected)", count * sizeof(T));
+        return false;
+    }
     cudaMemPool_t pool = scratch_pool();
     if (!pool || cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(T), pool, st) != cudaSuccess) {
         cudaGetLastError();
@@ -240,9 +257,10 @@ struct CudaBVHHandle {
     std::vector<float> h_soa[9];
     bool exports_ready = false;
     int num_bvh4 = -1;
-    // per-call scratch: work counters (ring) and host staging
+    // per-call scratch: work counters (ring; the index is taken atomically so
+    // host threads tracing one handle draw distinct slots) and host staging
     rtb::DevBuf<int> counters;
-    unsigned counter_next = 0;
+    std::atomic<unsigned> counter_next{0};
     rtb::DevBuf<RtRay> stage_rays;
     rtb::DevBuf<RtHit> stage_hits;
     rtb::DevBuf<uint8_t> stage_occ;
@@ -260,10 +278,12 @@ struct CudaTLASHandle {
     std::vector<float> h_inv;     // 12 floats per instance
     std::vector<float> h_fwd;     // 12 floats per instance: the object -> world transforms
     std::vector<int> h_blas;      // BLAS index per instance
-    unsigned long long generation = 0;  // bumped by every cudaTLAS_setTransforms
+    std::atomic<unsigned long long> generation{0};  // bumped by every cudaTLAS_setTransforms
     rtb::DevBuf<int> counters;
-    unsigned counter_next = 0;
+    std::atomic<unsigned> counter_next{0};
     rtb::DevBuf<int> status;
+    // held by cudaTLAS_setTransforms while it swaps the instances and the top
+    // level, and by every trace and render while it launches on them
     std::mutex mu;
 };
 
@@ -276,6 +296,12 @@ bool build_handle(CudaBVHHandle* h, cudaStream_t s);
 // Two-level trace; n_dev (optional) supplies the ray count from device memory.
 int launch_trace_tlas(const CudaTLASHandle* t, const RtRay* rays, int n, const int* n_dev, RtHit* hits,
                       int32_t* inst_out, uint8_t* occ, int* work, int* status, cudaStream_t s);
-int* next_counter(rtb::DevBuf<int>& ring, unsigned& next, cudaStream_t s);
+int* next_counter(rtb::DevBuf<int>& ring, std::atomic<unsigned>& next, cudaStream_t s);
+// Reads and clears a handle's status word once `s` has finished its work:
+// RT_OK, RT_ERR_STACK (some trace overflowed its stack) or RT_ERR_CUDA.
+int read_status(int* d_status, cudaStream_t s, const char* who);
+// Forgets the cached device address of the allocation-free entry point's
+// scratch array on the current device (a device reset invalidates it).
+void noalloc_forget_current_device();
 bool ensure_counters(rtb::DevBuf<int>& ring);
 }  // namespace rtb

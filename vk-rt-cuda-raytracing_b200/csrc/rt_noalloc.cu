@@ -62,6 +62,20 @@ NoAllocScratch* scratch_for_current_device() {
 
 }  // namespace
 
+namespace rtb {
+
+void noalloc_forget_current_device() {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        cudaGetLastError();
+        return;
+    }
+    std::lock_guard<std::mutex> g(g_mu);
+    g_addr[dev] = nullptr;
+}
+
+}  // namespace rtb
+
 extern "C" int cudaBVH_traceClosestHostNoAlloc(CudaBVH_t bvh, const RtRay* h_rays, int n, RtHit* h_hits,
                                                void* stream) {
     if (!bvh || n < 0 || (n > 0 && (!h_rays || !h_hits))) {
@@ -82,7 +96,7 @@ extern "C" int cudaBVH_traceClosestHostNoAlloc(CudaBVH_t bvh, const RtRay* h_ray
         return RT_ERR_CUDA;
     if (rtb::launch_trace_blas(bvh->bvh8, sc->rays, n, sc->hits, nullptr, nullptr, &sc->work, &sc->status, s) !=
         RT_OK)
-        return RT_CUDA(cudaGetLastError()) ? RT_ERR_CUDA : RT_ERR_CUDA;
+        return RT_ERR_CUDA;
     int status = 0;
     if (!RT_CUDA(cudaMemcpyAsync(h_hits, sc->hits, sizeof(RtHit) * (size_t)n, cudaMemcpyDeviceToHost, s)) ||
         !RT_CUDA(cudaMemcpyAsync(&status, &sc->status, sizeof(int), cudaMemcpyDeviceToHost, s)) ||

@@ -513,6 +513,10 @@ int rtPT_render(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* prm, f
         set_error("rtPT_render: d_rgb must be 4-byte aligned");
         return RT_ERR_INVALID;
     }
+    // The TLAS lock is held from the reload check to the last launch, so a
+    // cudaTLAS_setTransforms on another thread cannot swap the instances or
+    // the top level between this render's launches.
+    std::lock_guard<std::mutex> tlas_lock(pt->tlas->mu);
     // the TLAS's instances moved (cudaTLAS_setTransforms): reload the copies
     // once renders still in flight are done with them
     if (pt->tlas->generation != pt->tlas_generation) {
@@ -559,7 +563,7 @@ int rtPT_render(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* prm, f
         cudaMemsetAsync(w1, 0, sizeof(int), s);
         if (launch_trace_tlas(t, pt->rays[cur].p, 0, cnt + cur, pt->hits.p, pt->hinst.p, nullptr, w1, t->status.p,
                               s) != RT_OK)
-            return RT_CUDA(cudaGetLastError()) ? RT_ERR_CUDA : RT_ERR_CUDA;
+            return RT_ERR_CUDA;
         k_pt_shade<<<num_sms() * RTB_SHADE_MINB, PT_T, 0, s>>>(sc, prm->spp, b, prm->max_bounces, prm->rr_start, prm->seed,
                                                  cnt + cur, pt->rays[cur].p, pt->pid[cur].p, pt->hits.p,
                                                  pt->hinst.p, pt->tp.p, pt->L.p, pt->rays[nxt].p, pt->pid[nxt].p,
@@ -567,7 +571,7 @@ int rtPT_render(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* prm, f
         int* w2 = pt->work.p + (pt->work_next++ % 1024);
         cudaMemsetAsync(w2, 0, sizeof(int), s);
         if (launch_trace_tlas(t, pt->srays.p, 0, cnt + 2, nullptr, nullptr, pt->socc.p, w2, t->status.p, s) != RT_OK)
-            return RT_CUDA(cudaGetLastError()) ? RT_ERR_CUDA : RT_ERR_CUDA;
+            return RT_ERR_CUDA;
         k_pt_accum<<<shade_blocks, 256, 0, s>>>(cnt + 2, pt->spid.p, pt->scontrib.p, pt->socc.p, pt->L.p);
         // ray counts of this bounce for the statistics
         cudaMemcpyAsync(pt->bcounts.p + 2 * b, cnt + cur, sizeof(int), cudaMemcpyDeviceToDevice, s);

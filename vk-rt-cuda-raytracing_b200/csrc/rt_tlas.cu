@@ -70,6 +70,12 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
     __shared__ unsigned long long s_key[TRACE_T];
     __shared__ int s_rec[TRACE_T];
     __shared__ int4 s_res[TRACE_T];  // u, v bits, instance, primitive of the improved best
+#if RTB_SLOTMASK
+    __shared__ uint8_t s_oct_perm[OCT_PERM_BYTES];
+    init_oct_perm(s_oct_perm);
+#else
+    const uint8_t* s_oct_perm = nullptr;
+#endif
     if (n_dev) n = *n_dev;  // ray count produced on the device by an earlier stage
     uint2 lstack[LSTACK];
     const int lane = threadIdx.x & 31;
@@ -154,7 +160,7 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
                 break;
             }
             uint32_t nh, tb, tm;
-            visit_node((top ? tnodes : bnodes) + (size_t)ni * 5, cr, thit, nh, tb, tm, w.ng);
+            visit_node((top ? tnodes : bnodes) + (size_t)ni * 5, cr, thit, nh, tb, tm, w.ng, s_oct_perm);
             if (top) {
                 w.ng.y |= G_TOP;
                 if (tm) {
@@ -307,7 +313,7 @@ int launch_trace_tlas(const CudaTLASHandle* t, const RtRay* rays, int n, const i
         k_trace_tlas<false><<<g, TRACE_T, 0, s>>>(nodes, t->bvh8.leaf_ids.p, t->inst.p, rays, n, n_dev, hits,
                                                   inst_out, occ, work, status);
     }
-    return cudaGetLastError() == cudaSuccess ? RT_OK : RT_ERR_CUDA;
+    return RT_CUDA(cudaGetLastError()) ? RT_OK : RT_ERR_CUDA;
 }
 
 static float bits_f(uint32_t u) {
@@ -507,10 +513,9 @@ int cudaTLAS_traceClosest(CudaTLAS_t t, const RtRay* d_rays, int n, RtHit* d_hit
     }
     if (n == 0) return RT_OK;
     cudaStream_t s = (cudaStream_t)stream;
+    std::lock_guard<std::mutex> g(t->mu);  // not while cudaTLAS_setTransforms swaps the instances
     int* work = next_counter(t->counters, t->counter_next, s);
-    const int rc = launch_trace_tlas(t, d_rays, n, nullptr, d_hits, d_inst, nullptr, work, t->status.p, s);
-    if (rc != RT_OK) RT_CUDA(cudaGetLastError());
-    return rc;
+    return launch_trace_tlas(t, d_rays, n, nullptr, d_hits, d_inst, nullptr, work, t->status.p, s);
 }
 
 int cudaTLAS_traceAny(CudaTLAS_t t, const RtRay* d_rays, int n, uint8_t* d_occ, void* stream) {
@@ -521,10 +526,17 @@ int cudaTLAS_traceAny(CudaTLAS_t t, const RtRay* d_rays, int n, uint8_t* d_occ, 
     if (!check_aligned("cudaTLAS_traceAny", d_rays, d_occ, 1)) return RT_ERR_INVALID;
     if (n == 0) return RT_OK;
     cudaStream_t s = (cudaStream_t)stream;
+    std::lock_guard<std::mutex> g(t->mu);
     int* work = next_counter(t->counters, t->counter_next, s);
-    const int rc = launch_trace_tlas(t, d_rays, n, nullptr, nullptr, nullptr, d_occ, work, t->status.p, s);
-    if (rc != RT_OK) RT_CUDA(cudaGetLastError());
-    return rc;
+    return launch_trace_tlas(t, d_rays, n, nullptr, nullptr, nullptr, d_occ, work, t->status.p, s);
+}
+
+int cudaTLAS_getStatus(CudaTLAS_t t, void* stream) {
+    if (!t) {
+        set_error("cudaTLAS_getStatus: invalid argument");
+        return RT_ERR_INVALID;
+    }
+    return read_status(t->status.p, (cudaStream_t)stream, "cudaTLAS_getStatus");
 }
 
 int cudaTLAS_getInverseTransforms(CudaTLAS_t t, float* out, int n) {

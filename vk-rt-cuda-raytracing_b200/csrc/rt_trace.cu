@@ -35,7 +35,38 @@
 #include "rt_legacy.h"
 #include "rt_trace.cuh"
 
+// Analysis builds only (all default to 0; the release kernels are unchanged):
+//   RTB_STATS     per-warp event counters (iterations, lanes per phase,
+//                 triangle rounds) in g_trace_stats, read by rtStats_read;
+//   RTB_DUP_NODE  every node visit done twice (the second result discarded
+//                 through a value the compiler cannot know is zero), and
+//   RTB_DUP_TRI   every triangle phase done twice (idempotent): the
+//                 instruction count of one phase is then the difference to
+//                 the release kernel's.
+#ifndef RTB_STATS
+#define RTB_STATS 0
+#endif
+#ifndef RTB_DUP_NODE
+#define RTB_DUP_NODE 0
+#endif
+#ifndef RTB_DUP_TRI
+#define RTB_DUP_TRI 0
+#endif
+
 namespace rtb {
+
+#if RTB_STATS
+__device__ unsigned long long g_trace_stats[16];
+#define RTB_STAT(k, v)                                                             \
+    do {                                                                           \
+        const unsigned long long _v = (unsigned long long)(v);                     \
+        if (lane == 0 && _v) atomicAdd(&g_trace_stats[k], _v);                   \
+    } while (0)
+#else
+#define RTB_STAT(k, v) \
+    do {               \
+    } while (0)
+#endif
 
 __device__ __forceinline__ void* ldg_ptr(const void* p) {
     return reinterpret_cast<void*>(__ldg(reinterpret_cast<const unsigned long long*>(p)));
@@ -62,6 +93,12 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
 #if RTB_RAY_SMEM
     __shared__ float4 s_ray[2][TRACE_T];           // each lane's ray, read by the lanes testing its triangles
 #endif
+#if RTB_SLOTMASK
+    __shared__ uint8_t s_oct_perm[OCT_PERM_BYTES];
+    init_oct_perm(s_oct_perm);
+#else
+    const uint8_t* s_oct_perm = nullptr;
+#endif
     uint2 lstack[LSTACK];
     const int lane = threadIdx.x & 31;
     const int wbase = threadIdx.x & ~31;
@@ -78,6 +115,7 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
         // ---- refill idle lanes ----
         const bool need = ray < 0 && !exhausted;
         const unsigned want = __ballot_sync(FULL_MASK, need);
+        RTB_STAT(10, __popc(want));
         if (want) {
             const int leader = __ffs(want) - 1;
             int base = 0;
@@ -128,12 +166,30 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
             }
         }
         if (__all_sync(FULL_MASK, ray < 0)) break;
+        RTB_STAT(0, 1);
+        RTB_STAT(1, __popc(__ballot_sync(FULL_MASK, ray >= 0)));
         // ---- node phase ----
         uint32_t tri_base = 0, tmask = 0;
+#if RTB_TWO_SETS
+        uint32_t tri_base2 = 0, tmask2 = 0;  // a second visit's leaves while the first set waits
+#else
+        constexpr uint32_t tmask2 = 0;
+#endif
         bool overflow = false;
 #pragma unroll 1
         for (int it = 0; it < NITERS; it++) {
+#if RTB_STATS
+            {
+                const unsigned act = __ballot_sync(FULL_MASK, ray >= 0 && tmask == 0 && !overflow && (w.ng.y & 0xFFu));
+                RTB_STAT(2 + 2 * it, act ? 1 : 0);
+                RTB_STAT(3 + 2 * it, __popc(act));
+            }
+#endif
+#if RTB_TWO_SETS
+            if (ray >= 0 && tmask2 == 0 && !overflow && (w.ng.y & 0xFFu)) {
+#else
             if (ray >= 0 && tmask == 0 && !overflow && (w.ng.y & 0xFFu)) {
+#endif
                 uint32_t hitsm = w.ng.y & 0xFFu;
                 const uint32_t imask = (w.ng.y >> 8) & 0xFFu;
                 const int k = __ffs(hitsm) - 1;
@@ -143,23 +199,61 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
                 if (hitsm && !w.push(make_uint2(w.ng.x, hitsm | (imask << 8)), sstack, lstack)) overflow = true;
                 if (COUNT) cn++;
                 uint32_t nmask;
-                visit_node(nodes + (size_t)ni * 5, r, thit, nmask, tri_base, tmask, w.ng);
+#if RTB_TWO_SETS
+                uint32_t vb, vm;
+                visit_node(nodes + (size_t)ni * 5, r, thit, nmask, vb, vm, w.ng, s_oct_perm);
+                if (tmask == 0) {
+                    tri_base = vb;
+                    tmask = vm;
+                } else {
+                    tri_base2 = vb;
+                    tmask2 = vm;
+                }
+#else
+                visit_node(nodes + (size_t)ni * 5, r, thit, nmask, tri_base, tmask, w.ng, s_oct_perm);
+#endif
+#if RTB_DUP_NODE
+                {
+                    uint32_t nm2, tb2, tm2;
+                    uint2 ng2;
+                    visit_node(nodes + (size_t)ni * 5, r, thit, nm2, tb2, tm2, ng2, s_oct_perm);
+                    const uint32_t z = (uint32_t)(n >> 31);  // 0 for n >= 0, unknown at compile time
+                    tmask |= tm2 & z;
+                    tri_base |= tb2 & z;
+                    w.ng.x |= ng2.x & z;
+                    w.ng.y |= ng2.y & z;
+                }
+#endif
                 prefetch_next(nodes, w.ng, r.oct);
+#if RTB_TWO_SETS
+                if (NITERS > 1 && (w.ng.y & 0xFFu) == 0 && w.sp > 0) {
+#else
                 if (NITERS > 1 && tmask == 0 && (w.ng.y & 0xFFu) == 0 && w.sp > 0) {
+#endif
                     w.ng = w.pop(sstack, lstack);
                 }
             }
         }
         // ---- triangle phase: pooled over the warp ----
-        const int cnt = __popc(tmask);
-        int incl = cnt;
+        const int cnt = __popc(tmask) + __popc(tmask2);
+        int incl = cnt, total = 0;
+        // RTB_TRI_VOTE: one warp vote skips the scan when no lane holds triangles
+        if (!RTB_TRI_VOTE || __any_sync(FULL_MASK, tmask != 0)) {
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(FULL_MASK, incl, o);
-            if (lane >= o) incl += y;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(FULL_MASK, incl, o);
+                if (lane >= o) incl += y;
+            }
+            total = __shfl_sync(FULL_MASK, incl, 31);
         }
-        const int total = __shfl_sync(FULL_MASK, incl, 31);
         bool found_any = false;
+        RTB_STAT(6, total ? 1 : 0);
+        RTB_STAT(7, (total + 31) / 32);
+        RTB_STAT(8, total);
+#if RTB_DUP_TRI
+#pragma unroll 1
+        for (int rep = 0; rep < 2; rep++)
+#endif
         if (total) {
             const int excl = incl - cnt;
             if (COUNT) ct += cnt;
@@ -180,9 +274,23 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
                     if (v <= g) o += s;
                 }
                 o = min(o, 31);
-                const int k = g - __shfl_sync(FULL_MASK, excl, o);
+                const int k0 = g - __shfl_sync(FULL_MASK, excl, o);
+#if RTB_TWO_SETS
+                uint32_t om = __shfl_sync(FULL_MASK, tmask, o);
+                uint32_t ob = __shfl_sync(FULL_MASK, tri_base, o);
+                const uint32_t om2 = __shfl_sync(FULL_MASK, tmask2, o);
+                const uint32_t ob2 = __shfl_sync(FULL_MASK, tri_base2, o);
+                const int c1 = __popc(om);
+                const int k = k0 < c1 ? k0 : k0 - c1;
+                if (k0 >= c1) {
+                    om = om2;
+                    ob = ob2;
+                }
+#else
+                const int k = k0;
                 const uint32_t om = __shfl_sync(FULL_MASK, tmask, o);
                 const uint32_t ob = __shfl_sync(FULL_MASK, tri_base, o);
+#endif
 #if RTB_RAY_SMEM
                 const float4 ro = s_ray[0][wbase + o], rd = s_ray[1][wbase + o];
                 const float ox = ro.x, oy = ro.y, oz = ro.z, tmn = ro.w;
@@ -280,6 +388,19 @@ static int persistent_grid(K kernel, int threads) {
     return per_sm * num_sms();
 }
 
+#if RTB_STATS
+extern "C" int rtStats_read(unsigned long long* out16, int reset) {
+    if (cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpyFromSymbol(out16, g_trace_stats, sizeof(unsigned long long) * 16) != cudaSuccess)
+        return -1;
+    if (reset) {
+        static const unsigned long long zero[16] = {};
+        if (cudaMemcpyToSymbol(g_trace_stats, zero, sizeof(zero)) != cudaSuccess) return -1;
+    }
+    return 0;
+}
+#endif
+
 int launch_trace_blas(const Bvh8Device& b, const RtRay* rays, int n, RtHit* hits, uint8_t* occ,
                       uint32_t* counts, int* work, int* status, cudaStream_t s) {
     const uint4* nodes = reinterpret_cast<const uint4*>(b.nodes.p);
@@ -304,7 +425,7 @@ int launch_trace_blas(const Bvh8Device& b, const RtRay* rays, int n, RtHit* hits
         k_trace_blas<false, false, MODE_SINGLE, NI><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, counts, work,
                                                                    status, nullptr, nullptr, 1, nullptr);
     }
-    return cudaGetLastError() == cudaSuccess ? RT_OK : RT_ERR_CUDA;
+    return RT_CUDA(cudaGetLastError()) ? RT_OK : RT_ERR_CUDA;
 }
 
 // Many scenes in one persistent launch: ctas_per_sm (1..TRACE_MINB) sets the
@@ -330,7 +451,7 @@ int launch_trace_multi(const Bvh8Device& b, const RtRay* rays, int n, const int*
             k_trace_blas<false, false, MODE_BATCH, 2><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
                                                                      status, ray_off, tri_off, nscenes, nullptr);
     }
-    return cudaGetLastError() == cudaSuccess ? RT_OK : RT_ERR_CUDA;
+    return RT_CUDA(cudaGetLastError()) ? RT_OK : RT_ERR_CUDA;
 }
 
 // One shared wavefront: `n` rays over `nseg` segments, all of one kind.
@@ -345,7 +466,7 @@ int launch_trace_wave(const uint4* nodes, const float4* tris, const WaveSeg* seg
         k_trace_blas<false, false, MODE_WAVE, 2><<<g, TRACE_T, 0, s>>>(nodes, tris, nullptr, n, nullptr, nullptr,
                                                                       nullptr, work, status, nullptr, nullptr, nseg,
                                                                       segs);
-    return cudaGetLastError() == cudaSuccess ? RT_OK : RT_ERR_CUDA;
+    return RT_CUDA(cudaGetLastError()) ? RT_OK : RT_ERR_CUDA;
 }
 
 // Copies one scene's 8-wide nodes into an arena at node offset `node_off`,

@@ -51,6 +51,9 @@ constexpr unsigned FULL_MASK = 0xFFFFFFFFu;
 #ifndef RTB_RAY_CS
 #define RTB_RAY_CS 1
 #endif
+#ifndef RTB_TRI_VOTE
+#define RTB_TRI_VOTE 0
+#endif
 // pooled triangle phase reads the owner's ray from shared memory (1) or
 // gathers it with eight shuffles (0)
 #ifndef RTB_RAY_SMEM
@@ -81,7 +84,14 @@ constexpr int TRACE_T = 128;               // threads per persistent CTA
 constexpr int TRACE_MINB = RTB_TRACE_MINB; // CTAs per SM the register budget must allow
 constexpr int TRACE_MINB_ANY = RTB_TRACE_MINB_ANY;
 constexpr int SSTACK = RTB_SSTACK;         // stack entries per thread in shared memory
-constexpr int LSTACK = 64 - SSTACK;        // further entries in local memory (64 total)
+// Stack entries per ray in total (shared + local).  64 holds any tree the
+// builder makes (validation rejects deeper ones); a test build lowers it to
+// reach the overflow path, which reports RT_ERR_STACK.
+#ifndef RTB_STACK_TOTAL
+#define RTB_STACK_TOTAL 64
+#endif
+static_assert(RTB_STACK_TOTAL > RTB_SSTACK, "the local part of the stack needs at least one entry");
+constexpr int LSTACK = RTB_STACK_TOTAL - SSTACK;  // further entries in local memory
 constexpr int SSTACK_TOTAL = SSTACK + LSTACK;
 constexpr int RT_STATUS_STACK = 1;
 constexpr int RT_STATUS_TIMEOUT = 2;
@@ -168,6 +178,40 @@ __device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t k) {
     return pos;
 }
 
+// RTB_SLOTMASK: the node test keeps one hit bit per child slot (a
+// predicated OR, no branch), takes a leaf's triangle bits with one
+// predicated OR, and moves the inner hits into the ray's octant order once
+// per node with a table lookup (oct_perm, 2 KB of shared memory per CTA)
+// instead of a shift per child.
+#ifndef RTB_SLOTMASK
+#define RTB_SLOTMASK 0
+#endif
+// RTB_TWO_SETS: a lane keeps up to two pending triangle sets, so a node
+// visit that finds leaves does not stop the lane's second visit.
+#ifndef RTB_TWO_SETS
+#define RTB_TWO_SETS 0
+#endif
+constexpr int OCT_PERM_BYTES = 8 * 256;
+// Fills the table: entry (o << 8) | x is x with bit i moved to bit i ^ o.
+// Called by every thread of the CTA before its first node visit.
+__device__ __forceinline__ void init_oct_perm(uint8_t* perm) {
+    for (int idx = threadIdx.x; idx < OCT_PERM_BYTES; idx += blockDim.x) {
+        const uint32_t o = (uint32_t)idx >> 8, x = (uint32_t)idx & 0xFFu;
+        uint32_t y = 0;
+        for (uint32_t i = 0; i < 8; i++) y |= ((x >> i) & 1u) << (i ^ o);
+        perm[idx] = (uint8_t)y;
+    }
+    __syncthreads();
+}
+
+// A mask of `width` bits starting at bit `start` (mod 32) in one
+// instruction; the start's bits above bit 4 are ignored.
+__device__ __forceinline__ uint32_t bit_mask_wrap(uint32_t start, uint32_t width) {
+    uint32_t r;
+    asm("bmsk.wrap.b32 %0, %1, %2;" : "=r"(r) : "r"(start), "r"(width));
+    return r;
+}
+
 // A mask of `width` bits starting at bit `start` in one instruction (PTX
 // bmsk): a leaf's triangle bits.  width 0 (an empty slot) gives 0.
 __device__ __forceinline__ uint32_t bit_mask(uint32_t start, uint32_t width) {
@@ -212,7 +256,21 @@ __device__ __forceinline__ float qbyte_p(uint32_t w, int k) {
 #ifndef RTB_PRMT_PLANES
 #define RTB_PRMT_PLANES 2
 #endif
+// Byte k of w as the exact float 2^15 + byte, built by one byte permute:
+// bits 0x47 00 qq 00 are exponent 142 and mantissa q << 8, i.e.
+// 2^15 (1 + q 2^-15).  The node test folds the 2^15 bias into its offsets
+// (RTB_DECODE15), so a plane costs one integer op and its FMA.
+__device__ __forceinline__ float qbyte15(uint32_t w, int k) {
+    return __uint_as_float(__byte_perm(w, 0x47000000u, 0x7604u | ((uint32_t)k << 4)));
+}
+#ifndef RTB_DECODE15
+#define RTB_DECODE15 0
+#endif
+#if RTB_DECODE15
+#define RTB_QB(w, k, plane) qbyte15((w), (k))
+#else
 #define RTB_QB(w, k, plane) ((plane) < RTB_PRMT_PLANES ? qbyte_p((w), (k)) : qbyte((w), (k)))
+#endif
 
 // Pulls the node a group will visit next toward L1 (80-byte nodes may span
 // two 128-byte lines).
@@ -235,7 +293,8 @@ __device__ __forceinline__ void prefetch_next(const uint4* nodes, uint2 ng, uint
 // segment [tmin, thit].  Outputs the node group of hit inner children
 // (`ng`), and the triangle base + 32-bit mask of hit leaf triangles.
 __device__ __forceinline__ void visit_node(const uint4* __restrict__ np, const Ray& r, float thit,
-                                           uint32_t& inner_hits, uint32_t& tri_base, uint32_t& tmask, uint2& ng) {
+                                           uint32_t& inner_hits, uint32_t& tri_base, uint32_t& tmask, uint2& ng,
+                                           const uint8_t* __restrict__ oct_perm = nullptr) {
     const uint4 w0 = ld_node(np), w1 = ld_node(np + 1), w2 = ld_node(np + 2), w3 = ld_node(np + 3),
                 w4 = ld_node(np + 4);
     const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
@@ -247,15 +306,32 @@ __device__ __forceinline__ void visit_node(const uint4* __restrict__ np, const R
     // per axis: S = s/d, O = (p - o)/d, slack E = 2^-22 |O|
     const float Sx = sx * r.ix, Sy = sy * r.iy, Sz = sz * r.iz;
     const float Ox = (px - r.ox) * r.ix, Oy = (py - r.oy) * r.iy, Oz = (pz - r.oz) * r.iz;
+#if RTB_DECODE15
+    // planes decode to 2^15 + q, so the offsets carry -B = -2^15 S (exact:
+    // a power-of-two scaling).  C = O - B is rounded once, by at most
+    // 2^-24 (|O| + |B|), and C -+ E once more; the slack
+    // E = 2^-21 |O| + 2^-22 |B| covers both roundings and the error of O
+    // itself with a factor of two to spare, so the test stays conservative.
+    const float Bx = Sx * 32768.f, By = Sy * 32768.f, Bz = Sz * 32768.f;
+    const float Cx = Ox - Bx, Cy = Oy - By, Cz = Oz - Bz;
+    const float Ex = fmaf(fabsf(Bx), 0x1p-22f, fabsf(Ox) * 0x1p-21f);
+    const float Ey = fmaf(fabsf(By), 0x1p-22f, fabsf(Oy) * 0x1p-21f);
+    const float Ez = fmaf(fabsf(Bz), 0x1p-22f, fabsf(Oz) * 0x1p-21f);
+    const float Onx = Cx - Ex, Ofx = Cx + Ex, Ony = Cy - Ey, Ofy = Cy + Ey, Onz = Cz - Ez, Ofz = Cz + Ez;
+#else
     const float Onx = fmaf(-fabsf(Ox), 0x1p-22f, Ox), Ofx = fmaf(fabsf(Ox), 0x1p-22f, Ox);
     const float Ony = fmaf(-fabsf(Oy), 0x1p-22f, Oy), Ofy = fmaf(fabsf(Oy), 0x1p-22f, Oy);
     const float Onz = fmaf(-fabsf(Oz), 0x1p-22f, Oz), Ofz = fmaf(fabsf(Oz), 0x1p-22f, Oz);
+#endif
     // near plane = lo for a positive 1/d, hi otherwise
     const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
     const uint32_t qnx0 = nx ? w2.z : w2.x, qnx1 = nx ? w2.w : w2.y, qfx0 = nx ? w2.x : w2.z, qfx1 = nx ? w2.y : w2.w;
     const uint32_t qny0 = ny ? w3.z : w3.x, qny1 = ny ? w3.w : w3.y, qfy0 = ny ? w3.x : w3.z, qfy1 = ny ? w3.y : w3.w;
     const uint32_t qnz0 = nz ? w4.z : w4.x, qnz1 = nz ? w4.w : w4.y, qfz0 = nz ? w4.x : w4.z, qfz1 = nz ? w4.y : w4.w;
     uint32_t nh = 0, th = 0;
+#if RTB_SLOTMASK
+    uint32_t hm = 0;  // hit children in slot order
+#endif
 #pragma unroll
     for (int s = 0; s < 8; s++) {
         const int sh = (s & 3) * 8;
@@ -271,6 +347,15 @@ __device__ __forceinline__ void visit_node(const uint4* __restrict__ np, const R
         const float tn = max3f(tnx, tny, fmaxf(tnz, r.tmin));
         const float tf = min3f(tfx, tfy, fminf(tfz, thit));
         const bool hit = tn <= fmaf(fabsf(tf), 0x1p-21f, tf);
+#if RTB_SLOTMASK
+        // leaf run from the meta byte (count << 5 | offset); inner slots (meta
+        // 0xFF) are excluded by the inner bit, empty slots have count 0
+        const uint32_t mw = s < 4 ? w1.z : w1.w;
+        const uint32_t run = bit_mask_wrap(mw >> sh, (mw >> (sh + 5)) & 7u);
+        if (hit) hm |= 1u << s;
+        if (hit && !((imask >> s) & 1u)) th |= run;
+        continue;
+#endif
         const uint32_t meta = ((s < 4 ? w1.z : w1.w) >> sh) & 0xFFu;
 #if RTB_BRANCHLESS
         const uint32_t inner = (imask >> s) & 1u;
@@ -287,6 +372,9 @@ __device__ __forceinline__ void visit_node(const uint4* __restrict__ np, const R
         }
 #endif
     }
+#if RTB_SLOTMASK
+    nh = oct_perm[(r.oct << 8) | (hm & imask)];
+#endif
     inner_hits = nh;
     tri_base = w1.y;
     tmask = th;

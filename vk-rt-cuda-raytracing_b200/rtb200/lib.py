@@ -116,6 +116,9 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "cudaBVH_traceAnyHost": (i32, [vp, vp, i32, vp]),
         "cudaBVH_traceCounters": (i32, [vp, vp, i32, i32, vp, vp]),
         "cudaBVH_traceClosestHostNoAlloc": (i32, [vp, vp, i32, vp, vp]),
+        "cudaBVH_getStatus": (i32, [vp, vp]),
+        "rtDebug_failAllocations": (i32, [i32]),
+        "rtProbe_readBandwidth": (i32, [C.c_uint64, i32, C.POINTER(f32)]),
         "cudaBVH_validate": (i32, [vp]),
         "cudaBVH_getBuildStats": (i32, [vp, C.POINTER(RtBuildStats)]),
         "cudaBVH_getDeviceLayout": (i32, [vp, C.POINTER(vp), C.POINTER(i32), C.POINTER(vp), C.POINTER(i32)]),
@@ -143,6 +146,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "cudaTLAS_traceAny": (i32, [vp, vp, i32, vp, vp]),
         "cudaTLAS_getInverseTransforms": (i32, [vp, vp, i32]),
         "cudaTLAS_setTransforms": (i32, [vp, vp, i32]),
+        "cudaTLAS_getStatus": (i32, [vp, vp]),
         "rtBatch_build": (vp, [vp, vp, i32, vp]),
         "rtBatch_destroy": (None, [vp]),
         "rtBatch_traceClosest": (i32, [vp, vp, vp, i32, vp, vp]),
@@ -178,6 +182,13 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
     if path is None:
         _lib = L
     return L
+
+
+def read_bandwidth_gbs(nbytes: int, reps: int = 20) -> float:
+    """rtProbe_readBandwidth: streamed read GB/s over an nbytes device buffer."""
+    v = C.c_float()
+    _check(load().rtProbe_readBandwidth(nbytes, reps, C.byref(v)), "rtProbe_readBandwidth")
+    return float(v.value)
 
 
 def last_error() -> str:
@@ -275,6 +286,10 @@ class BVH:
 
     def any(self, d_rays, n: int, d_occ, stream=None):
         _check(load().cudaBVH_traceAny(self.h, _ptr(d_rays), n, _ptr(d_occ), _stream(stream)), "cudaBVH_traceAny")
+
+    def status(self, stream=None) -> int:
+        """cudaBVH_getStatus: RT_OK or RT_ERR_STACK for the device-pointer traces so far."""
+        return load().cudaBVH_getStatus(self.h, _stream(stream))
 
     def counters(self, d_rays, n: int, d_counts, any_hit: bool = False, stream=None):
         _check(load().cudaBVH_traceCounters(self.h, _ptr(d_rays), n, int(any_hit), _ptr(d_counts), _stream(stream)),
