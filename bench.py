@@ -68,6 +68,41 @@ def whole_job_mrays(rays_per_rank: int, ws: int, t_ms_max: float) -> float:
     return ws * rays_per_rank / t_ms_max / 1e3
 
 
+TRACE_SOURCES = ("vk-rt-cuda-raytracing_b200/csrc/rt_trace.cu", "vk-rt-cuda-raytracing_b200/csrc/rt_trace.cuh",
+                 "vk-rt-cuda-raytracing_b200/csrc/rt_common.cuh")
+TRAFFIC_PROFILE = "profiles/trace_closest_incoherent_2m.md"
+
+
+def trace_source_sha():
+    """SHA-256 over the closest-hit kernel's source files (the profile's
+    capture records the same digest)."""
+    import hashlib
+    h = hashlib.sha256()
+    for f in TRACE_SOURCES:
+        h.update((ROOT / f).read_bytes())
+    return h.hexdigest()
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the closest-hit kernel from the committed ncu
+    summary, with whether that capture was taken on the current kernel source
+    (its recorded source digest equals the digest of the files now)."""
+    prof = ROOT / TRAFFIC_PROFILE
+    traffic, sha, commit = None, None, None
+    if prof.exists():
+        for line in prof.read_text().splitlines():
+            cells = [c.strip() for c in line.split("|")]
+            if len(cells) > 2 and cells[1] == "dram_bytes_per_launch":
+                traffic = int(cells[2])
+            elif len(cells) > 2 and cells[1] == "kernel_source_sha256":
+                sha = cells[2].strip("`")
+            elif len(cells) > 2 and cells[1] == "captured_at_commit":
+                commit = cells[2].strip("`")
+    now = trace_source_sha()
+    return traffic, {"profile": TRAFFIC_PROFILE, "captured_at_commit": commit, "kernel_source_sha256": sha,
+                     "matches_current_source": sha == now if sha else False}
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -139,19 +174,43 @@ def make_workload(seed_scene=1):
     return tris
 
 
-def derive_rays(tris, bvh, torch):
-    """Primary 1080p hits (traced by the GPU) -> diffuse + shadow batches."""
-    from rtb200 import scenes
+LIGHT = dict(light_center=(0.0, 80.0, 0.0), light_size=1.0)
+
+
+def derive_rays(bvh, torch, steps, flush):
+    """Primary 1080p hits, then the 2M diffuse and 2M shadow rays made from
+    them on the GPU by cudaBVH_generateRays (the reference's genAndCompact,
+    multi_bounce.cu:281-362): cosine-weighted bounces with a 0.001 * normal
+    origin offset, and rays toward a 1 x 1 area light; output k leaves the
+    (k mod hits)-th hit.  Also times the generator."""
+    from rtb200 import lib, scenes
     prim = scenes.primary_1080p()
+    n = prim.shape[0]
     d_prim = torch.from_numpy(prim.view(np.uint8).copy()).cuda()
-    d_hits = torch.empty(prim.shape[0] * 16, dtype=torch.uint8, device="cuda")
-    bvh.closest(d_prim, prim.shape[0], d_hits)
+    d_hits = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
+    bvh.closest(d_prim, n, d_hits)
+    d_dif = torch.empty(N_RAYS * 32, dtype=torch.uint8, device="cuda")
+    d_sha = torch.empty(N_RAYS * 32, dtype=torch.uint8, device="cuda")
+    d_cnt = torch.zeros(2, dtype=torch.int32, device="cuda")
+    st = torch.cuda.current_stream()
+
+    def gen(kind, out, cnt, seed):
+        bvh.generate_rays(d_prim, d_hits, n, out, cnt, kind=kind, count=N_RAYS, seed=seed, eps=1e-3, tmin=1e-3,
+                          stream=st, **LIGHT)
+
+    gen(lib.RT_GEN_DIFFUSE, d_dif, d_cnt[0:1], 3)
+    gen(lib.RT_GEN_SHADOW, d_sha, d_cnt[1:2], 4)
     torch.cuda.synchronize()
+    assert d_cnt.tolist() == [N_RAYS, N_RAYS], d_cnt.tolist()
+    ms = time_steps(torch, lambda: gen(lib.RT_GEN_DIFFUSE, d_dif, d_cnt[0:1], 3), steps, 3, flush)
     ph = d_hits.cpu().numpy().view(scenes.HIT_DTYPE)
-    p, n = scenes.hit_frame(tris, prim, ph)
-    dif = scenes.diffuse_rays(p, n, N_RAYS, seed=3)
-    sha = scenes.shadow_rays(p, n, N_RAYS, seed=4)
-    return prim, dif, sha, float((ph["prim"] >= 0).mean())
+    dif = d_dif.cpu().numpy().view(scenes.RAY_DTYPE)
+    sha = d_sha.cpu().numpy().view(scenes.RAY_DTYPE)
+    info = {"primary_hit_fraction": round(float((ph["prim"] >= 0).mean()), 4),
+            "diffuse_2m_ms": round(sum(ms) / len(ms), 4),
+            "diffuse_mrays_s": round(N_RAYS / (sum(ms) / len(ms)) / 1e3, 1),
+            "entry_point": "cudaBVH_generateRays (2,073,600 primary hits in, 2M compacted bounce rays out)"}
+    return prim, dif, sha, d_dif, d_sha, info
 
 
 def time_steps(torch, fn, steps, warmup, flush):
@@ -204,8 +263,8 @@ def reference_gpu_kernel(tris, rays, d_rays, n, torch, steps, flush):
     if not path.exists():
         return {"unavailable": "oracle/_ref/libref_v40.so not built"}
     R = C.CDLL(str(path))
-    if not hasattr(R, "refv40_abi") or R.refv40_abi() != 3:
-        return {"unavailable": "oracle/_ref/libref_v40.so is stale (harness ABI 3 expected); rebuild: make -C oracle ref"}
+    if not hasattr(R, "refv40_abi") or R.refv40_abi() != 4:
+        return {"unavailable": "oracle/_ref/libref_v40.so is stale (harness ABI 4 expected); rebuild: make -C oracle ref"}
     R.refv40_build.restype = C.c_void_p
     R.refv40_build.argtypes = [C.c_void_p, C.c_int, C.c_int]
     R.refv40_trace_bvh4.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
@@ -319,6 +378,107 @@ def reference_anyhit_kernel(tris, rays, d_rays, n, torch, steps, flush, d_ours):
     return out
 
 
+CFG0_SIDE = 1440                 # 1440^2 = 2,073,600 rays, the ray count of a 1920x1080 frame
+CFG0_CAM = (0.0, 0.0, -100.0)    # square camera looking +z at the 100^3 sphere scene
+
+
+def square_rays(side, cam):
+    """The reference's primary camera (cuda_rt_v40.cu:441-449,
+    layer/cuda_bvh_backend.cu:69-74): pixel p -> u, v = (p + 0.5)/side*2 - 1,
+    direction (u, v, 1) normalised, origin cam; in float32 as
+    cudaBVH_tracePrimary generates them."""
+    from rtb200 import scenes
+    i = np.arange(side * side)
+    px, py = (i % side).astype(np.float32), (i // side).astype(np.float32)
+    u = (px + np.float32(0.5)) / np.float32(side) * np.float32(2) - np.float32(1)
+    v = (py + np.float32(0.5)) / np.float32(side) * np.float32(2) - np.float32(1)
+    rl = np.float32(1) / np.sqrt(u * u + v * v + np.float32(1))
+    rays = np.zeros(side * side, scenes.RAY_DTYPE)
+    rays["org"] = cam
+    rays["dir"] = np.stack([u * rl, v * rl, rl], 1)
+    rays["tmax"] = 1e30
+    return rays
+
+
+def config0_primary(torch, steps, flush):
+    """Config 0: primary rays on the 100,002-triangle scene (200 UV spheres of
+    500 triangles + a 2-triangle ground plane).  Ours: 1920x1080 pinhole rays
+    and the reference's square camera (side 1440, the same ray count) through
+    cudaBVH_traceClosest, device-timed.  Reference, rebuilt for sm_100a in
+    this run on its own CPU-built fp16 BVH4 (leaf 3 and 4): its primary
+    pipeline resetCounters + broadphaseRoot + tracePrimaryDense
+    (cuda_rt_v40.cu:1401-1421, rays generated in its kernels from the same
+    camera), timed with the same events; and the backend's
+    cudaBVH_tracePrimary (bk_broadphaseRoot + bk_tracePrimaryDense,
+    layer/cuda_bvh_backend.cu:57-183, built with BVH_LAYER_MODE=0), which
+    reports the Mrays/s of its own kernels."""
+    import ctypes as C
+    from rtb200 import lib, scenes
+    tris = scenes.scene_spheres_100k(0)
+    bvh = lib.BVH(tris)
+    st = torch.cuda.current_stream()
+    out = {"workload": "primary_100k: 100,002 triangles (200 UV spheres x 500 + ground plane)",
+           "square_camera": {"side": CFG0_SIDE, "eye": CFG0_CAM, "looking": "+z"}}
+    n_pin = None
+    for name, rays in (("pinhole_1080p", scenes.primary_1080p()), ("square_1440", square_rays(CFG0_SIDE, CFG0_CAM))):
+        n = rays.shape[0]
+        d_r = torch.from_numpy(rays.view(np.uint8).copy()).cuda()
+        d_h = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
+        ms = time_steps(torch, lambda: bvh.closest(d_r, n, d_h, stream=st), steps, 3, flush)
+        hit = float((d_h.view(torch.int32).view(-1, 4)[:, 1] >= 0).float().mean().item())
+        out[f"ours_{name}"] = {"mrays_s": round(n / (sum(ms) / len(ms)) / 1e3, 1), "rays": n,
+                               "hit_fraction": round(hit, 4)}
+        n_pin = n if n_pin is None else n_pin
+    ours_sq = out["ours_square_1440"]["mrays_s"]
+    # our cudaBVH_tracePrimary, timed the way the reference's entry point times itself
+    Lb = lib.load()
+    vals = [float(Lb.cudaBVH_tracePrimary(bvh.h, CFG0_SIDE, *CFG0_CAM, None)) for _ in range(3 + steps)]
+    out["ours_cudaBVH_tracePrimary_reported"] = round(max(vals[3:]), 1)
+    ref = {}
+    path = ROOT / "oracle" / "_ref" / "libref_v40.so"
+    R = C.CDLL(str(path)) if path.exists() else None
+    if R is not None and hasattr(R, "refv40_abi") and R.refv40_abi() == 4:
+        R.refv40_build.restype = C.c_void_p
+        R.refv40_build.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        R.refv40_trace_primary.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_float, C.c_void_p,
+                                           C.c_void_p]
+        R.refv40_destroy.argtypes = [C.c_void_p]
+        n = CFG0_SIDE * CFG0_SIDE
+        d_h = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
+        for leaf in (3, 4):
+            h = R.refv40_build(tris.ctypes.data, tris.shape[0], leaf)
+            d_h.fill_(0xFF)  # rays culled at the root keep this: t = NaN, tri = -1
+            ms = time_steps(torch, lambda: R.refv40_trace_primary(h, CFG0_SIDE, *CFG0_CAM, d_h.data_ptr(),
+                                                                  st.cuda_stream), steps, 3, flush)
+            hit = float((d_h.view(torch.int32).view(-1, 4)[:, 1] >= 0).float().mean().item())
+            ref[f"broadphaseRoot+tracePrimaryDense leaf{leaf}"] = {"mrays_s": round(n / (sum(ms) / len(ms)) / 1e3, 1),
+                                                                   "hit_fraction": round(hit, 4)}
+            R.refv40_destroy(h)
+    else:
+        ref["v40"] = {"unavailable": "oracle/_ref/libref_v40.so missing or stale (harness ABI 4 expected)"}
+    gpu_path = ROOT / "oracle" / "_ref" / "libref_backend_gpu.so"
+    if gpu_path.exists():
+        B = C.CDLL(str(gpu_path))
+        B.cudaBVH_build.restype = C.c_void_p
+        B.cudaBVH_build.argtypes = [C.c_void_p, C.c_int]
+        B.cudaBVH_tracePrimary.restype = C.c_float
+        B.cudaBVH_tracePrimary.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_float, C.c_void_p]
+        B.cudaBVH_destroy.argtypes = [C.c_void_p]
+        hb = B.cudaBVH_build(tris.ctypes.data, tris.shape[0])
+        ht = np.zeros(CFG0_SIDE * CFG0_SIDE, np.float32)
+        vals = [float(B.cudaBVH_tracePrimary(hb, CFG0_SIDE, *CFG0_CAM, ht.ctypes.data)) for _ in range(3 + steps)]
+        B.cudaBVH_destroy(hb)
+        ref["bk_broadphaseRoot+bk_tracePrimaryDense via cudaBVH_tracePrimary (kernel Mrays/s it reports)"] = {
+            "mrays_s": round(max(vals[3:]), 1), "hit_fraction": round(float((ht < 1e29).mean()), 4)}
+    out["reference"] = ref
+    vals = [v["mrays_s"] for v in ref.values() if "mrays_s" in v]
+    if vals:
+        out["reference_best_mrays_s"] = max(vals)
+        out["speedup_square_vs_reference_best"] = round(ours_sq / max(vals), 3)
+    bvh.close()
+    return out
+
+
 def cpu_baseline(tris, dif, budget_s=20.0):
     """The restated scalar traversal (oracle) on the host cores over the
     restated reference builder's BVH (32 bins, leaf 4), bounded sample."""
@@ -359,8 +519,9 @@ def run_reference_arm(args):
         dfs, packed, bvh_src = ob.dfs, ob.packed, "restated reference builder (16 bins, leaf 3)"
     prim = scenes.primary_1080p()
     ph = O.trace_closest_dfs(dfs, packed, prim, threads)
-    p, n = scenes.hit_frame(tris, prim, ph)
-    dif = scenes.diffuse_rays(p, n, N_RAYS, seed=3)
+    # the same 2M bounce rays the GPU arm makes (the oracle restates
+    # cudaBVH_generateRays bit for bit)
+    dif, _ = O.generate_rays(tris, prim, ph, 0, count=N_RAYS, seed=3, eps=1e-3, tmin=1e-3, **LIGHT)
     sample = 250_000
     for _ in range(args.warmup):
         O.trace_closest_dfs(dfs, packed, dif[:20_000], threads)
@@ -410,12 +571,11 @@ def run_ours(args):
     stats["build_ms"] = float(np.median([b[0] for b in builds]))
     log(f"build: {stats['build_ms']:.1f} ms device (median of 3), {builds[-1][1]:.2f}s wall, {stats['num_nodes']} "
         f"nodes, depth {stats['depth']}, SAH {stats['sah_cost']:.2f}")
-    prim, dif, sha, prim_hit = derive_rays(tris, bvh, torch)
-    d_dif = torch.from_numpy(dif.view(np.uint8).copy()).cuda()
-    d_sha = torch.from_numpy(sha.view(np.uint8).copy()).cuda()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    prim, dif, sha, d_dif, d_sha, raygen = derive_rays(bvh, torch, args.steps, flush)
+    prim_hit = raygen["primary_hit_fraction"]
     d_hits = torch.empty(N_RAYS * 16, dtype=torch.uint8, device="cuda")
     d_occ = torch.empty(N_RAYS, dtype=torch.uint8, device="cuda")
-    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
 
     # algorithmic bytes per ray from the per-ray work counters (outside timing)
@@ -464,12 +624,12 @@ def run_ours(args):
 
     peak, peak_kind = measured_peaks()
     achieved = bytes_per_ray * N_RAYS / (t_step * 1e-3) / 1e9
-    traffic = None
-    prof = ROOT / "profiles" / "trace_closest_incoherent_2m.md"
-    if prof.exists():  # DRAM bytes of one launch from the committed ncu capture
-        for line in prof.read_text().splitlines():
-            if line.startswith("| dram_bytes_per_launch |"):
-                traffic = int(line.split("|")[2].strip())
+    # read bandwidth of this GPU measured now by the library's probe kernel: a
+    # 64 MiB buffer stays in L2 (the BVH and triangles of this scene do too), a
+    # 4 GiB one streams from HBM
+    l2_gbs = lib.read_bandwidth_gbs(64 << 20, 50)
+    hbm_read_gbs = lib.read_bandwidth_gbs(4 << 30, 5)
+    traffic, prov = profile_traffic()
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t_step, 4), "higher_is_better": True, "scaling": "weak",
@@ -493,12 +653,18 @@ def run_ours(args):
                                "launch's rays; ray for ray equal to the CPU oracle's restated walk on committed "
                                "fixtures (tests/test_oracle_bvh8.py)",
                      "dram_gbs_from_traffic": round(traffic / (t_step * 1e-3) / 1e9, 1) if traffic else None,
+                     "traffic_source": prov,
+                     "l2_peak_gbs": round(l2_gbs, 1), "l2_frac": round(achieved / l2_gbs, 4),
+                     "l2_probe": "rtProbe_readBandwidth: 64 MiB buffer, 16-byte L2-cached loads, 50 passes "
+                                 "after 2 warm-up passes, events; measured in this run",
+                     "hbm_read_probe_gbs": round(hbm_read_gbs, 1),
                      "note": "BVH and triangles stay in the 126 MB L2; DRAM carries rays, hits and misses; "
                              "the kernel is issue-bound (profiles/trace_closest_incoherent_2m.md)"},
         "anyhit_shadow_mrays": round(any_mrays, 1),
         "build": {"device_ms": round(stats["build_ms"], 2), "nodes": stats["num_nodes"], "depth": stats["depth"],
                   "sah_cost": round(stats["sah_cost"], 3)},
         "hit_fraction": {"primary": round(prim_hit, 4), "diffuse": round(float((hits["prim"] >= 0).mean()), 4)},
+        "raygen": raygen,
         "clocks": clk.summary(),
     }
     # the baseline legs run at N=1 only: under torchrun the other ranks would
@@ -515,6 +681,15 @@ def run_ours(args):
         if "value" in out["reference_anyhit_kernel"]:
             out["speedup_anyhit_vs_reference_kernel"] = round(any_mrays / out["reference_anyhit_kernel"]["value"], 3)
         out["cpu_baseline"] = cpu_baseline(tris, dif)
+        out["config0_primary"] = config0_primary(torch, max(3, args.steps // 2), flush)
+    # the metric's second half (p99 served vs plain) on one GPU, at the
+    # configured arrival rate and at 2x and 4x it (saturating)
+    if ws > 1 and not args.no_served:
+        out["served"] = "reported by the N=1 run"
+    if rank == 0 and ws == 1 and not args.no_served:
+        del d_dif, d_sha, d_hits, d_occ, h_rays, h_hits
+        torch.cuda.empty_cache()
+        out["served"] = served_legs(rates=(SERVED_RATE, 2 * SERVED_RATE, 4 * SERVED_RATE))
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -539,6 +714,8 @@ def run_pathtrace(args):
     bvhs = [lib.BVH(t) for t in blases]
     tl = lib.TLAS(bvhs, xf, bidx)
     pt = lib.PathTracer(tl, alb, emi)
+    if args.pt_regroup:
+        pt.set_regroup(args.pt_regroup)
     W, H, spp = 1920, 1080, 8
     cam = lib.make_camera(scenes.PT_CAM_EYE, scenes.PT_CAM_TARGET, vfov=50.0)
     d_rgb = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
@@ -555,7 +732,9 @@ def run_pathtrace(args):
            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
            "config": {"workload": "pathtrace_tlas_5m: 1920x1080, 8 spp, <=4 bounces, RR from bounce 2, 64 instances "
                                   "over 16 BLASes (5,000,000 triangles), Lambertian, 5% emissive",
-                      "l2": "flushed between timed frames"},
+                      "l2": "flushed between timed frames",
+                      "regroup": (f"bounce rays regrouped by a {args.pt_regroup}-bit octant+Morton key before each "
+                                  "extension trace (rtPT_setRegroup)") if args.pt_regroup else "off"},
            "rays_per_frame": {"extension": st["extension_rays"], "shadow": st["shadow_rays"]},
            "light_triangles": st["light_tris"], "mean_radiance": float(img.mean())}
     if not args.no_baselines:
@@ -684,160 +863,169 @@ def run_batched(args):
     return 0 if same else 1
 
 
-def run_served(args):
-    """Served form: 16 resident scenes (30M triangles, 200K-5M each), a
-    Poisson trace of 256 requests at 2,000 requests/s (scene uniform, rays
-    log-uniform 1K-8M, 70% closest / 30% any hit), replayed twice per arm:
-    with pinned host buffers (rays in, results out across PCIe) and with
-    device buffers (rays produced and results consumed on the GPU).
-    Served: every request submitted to one rtServer at its arrival time
-    (admission under a 120 GB HBM budget, shared wavefronts).  Plain: the
-    same trace through the per-call C-ABI (cudaBVH_traceClosestHost /
-    cudaBVH_traceAnyHost, or cudaBVH_traceClosest / cudaBVH_traceAny and a
-    synchronize), one call at a time in arrival order.  Latency = results
-    ready - scheduled arrival; aggregate = all rays / (last completion -
-    first arrival)."""
-    import threading
-    import zlib
+SERVED_RATE = 2000.0  # requests/s of the served configuration
+SERVED_NREQ = 256
+
+
+def served_legs(rates=(SERVED_RATE,), modes=("host", "device")):
+    """Served form against the plain per-call path on Poisson request traces.
+
+    16 resident scenes (30M triangles, 200K-5M each); for each arrival rate a
+    trace of 256 requests (scene uniform, rays log-uniform 1K-8M, 70% closest
+    / 30% any hit) is replayed per mode: pinned host buffers (rays in and
+    results out across PCIe) and device buffers.  Served: every request
+    submitted to one rtServer at its arrival time (admission under a 120 GB
+    HBM budget, shared wavefronts).  Plain: the same trace through the
+    per-call C-ABI (cudaBVH_traceClosestHost / cudaBVH_traceAnyHost, or
+    cudaBVH_traceClosest / cudaBVH_traceAny and a synchronize), one call at a
+    time in arrival order (layer/cuda_bvh_backend.cu:1379-1497 is the
+    reference's per-call path).  Latency = results ready - scheduled
+    arrival; aggregate = all rays / (last completion - first arrival).  Both
+    arms' results are compared byte for byte on the GPU."""
     import torch
     from rtb200 import lib, scenes
-    ws, rank, local = dist_env()
-    torch.cuda.set_device(local)
-    NREQ, RATE = 256, 2000.0
     t0 = time.time()
     tris = scenes.served_scenes()
     pool_c, pool_a = scenes.served_ray_pools()
-    arrival, scene, nray, anyh, start = scenes.served_trace(NREQ, rate=RATE, pool=pool_c.shape[0])
-    log(f"served workload: {sum(t.shape[0] for t in tris)} tris, {NREQ} requests, {int(nray.sum())} rays "
-        f"in {time.time() - t0:.1f}s")
+    log(f"served workload: {sum(t.shape[0] for t in tris)} tris in {time.time() - t0:.1f}s")
     t0 = time.time()
     bvhs = [lib.BVH(t) for t in tris]
     torch.cuda.synchronize()
     log(f"16 BVH builds: {time.time() - t0:.2f}s")
-    esz = np.where(anyh, 1, 16)
-    # each request's result slot starts on a 16-byte boundary (hit records
-    # are written as 16-byte vectors by the device paths)
-    out_off = np.concatenate([[0], np.cumsum((nray * esz + 15) // 16 * 16)]).astype(np.int64)
-    total = int(nray.sum())
     L = lib.load()
-    bufs = {}
-    for mode in ("host", "device"):
-        if mode == "host":
-            ic = torch.empty(pool_c.nbytes, dtype=torch.uint8, pin_memory=True)
-            ia = torch.empty(pool_a.nbytes, dtype=torch.uint8, pin_memory=True)
-            ic.numpy()[:] = pool_c.view(np.uint8)
-            ia.numpy()[:] = pool_a.view(np.uint8)
-            out = torch.empty(int(out_off[-1]), dtype=torch.uint8, pin_memory=True)
-        else:
-            ic, ia = bufs["host"][0].cuda(), bufs["host"][1].cuda()
-            out = torch.empty(int(out_off[-1]), dtype=torch.uint8, device="cuda")
-        bufs[mode] = (ic, ia, out)
+    ic_h = torch.empty(pool_c.nbytes, dtype=torch.uint8, pin_memory=True)
+    ia_h = torch.empty(pool_a.nbytes, dtype=torch.uint8, pin_memory=True)
+    ic_h.numpy()[:] = pool_c.view(np.uint8)
+    ia_h.numpy()[:] = pool_a.view(np.uint8)
+    ins = {"host": (ic_h, ia_h), "device": (ic_h.cuda(), ia_h.cuda())}
     srv = lib.Server(hbm_budget_bytes=120 << 30, pool_bytes=16 << 30)
     for b in bvhs:
         srv.add_scene(b)
-    res = {}
-    for mode in ("host", "device"):
-        ic, ia, outb = bufs[mode]
-        dev = mode == "device"
-        base_out = outb.data_ptr()
+    out = {"config": {"workload": "served_16x30m: 16 resident scenes (30,000,000 triangles, 200K-5M each), "
+                                  f"{SERVED_NREQ} Poisson requests per trace, rays log-uniform 1K-8M (random "
+                                  "incoherent rays), 70% closest / 30% any hit",
+                      "hbm_budget_gb": 120, "staging_pool_gb": 16},
+           "rates": {}}
+    for rate in rates:
+        arrival, scene, nray, anyh, start = scenes.served_trace(SERVED_NREQ, rate=rate, pool=pool_c.shape[0])
+        esz = np.where(anyh, 1, 16)
+        # each request's result slot starts on a 16-byte boundary (hit records
+        # are written as 16-byte vectors by the device paths)
+        out_off = np.concatenate([[0], np.cumsum((nray * esz + 15) // 16 * 16)]).astype(np.int64)
+        total = int(nray.sum())
+        row = {"offered_mrays_s": round(total / arrival[-1] / 1e6, 1), "rays": total,
+               "h2d_bytes": total * 32, "d2h_bytes": int((nray * esz).sum())}
+        for mode in modes:
+            dev = mode == "device"
+            ic, ia = ins[mode]
+            # zeroed, like the plain arm's buffer below: the 16-byte padding
+            # between result slots is then equal in both arms' byte comparison
+            outb = (torch.zeros(int(out_off[-1]), dtype=torch.uint8, device="cuda") if dev else
+                    torch.zeros(int(out_off[-1]), dtype=torch.uint8, pin_memory=True))
+            base_out = outb.data_ptr()
 
-        def rays_ptr(i):
-            return (ia if anyh[i] else ic).data_ptr() + int(start[i]) * 32
+            def rays_ptr(i):
+                return (ia if anyh[i] else ic).data_ptr() + int(start[i]) * 32
 
-        def out_ptr(i):
-            return base_out + int(out_off[i])
+            def out_ptr(i):
+                return base_out + int(out_off[i])
 
-        def crcs():
-            o = outb.cpu().numpy() if dev else outb.numpy()
-            return [zlib.crc32(o[out_off[i]:out_off[i] + nray[i] * esz[i]]) for i in range(NREQ)]
+            # ---- served arm
+            for i in range(4):  # warm-up: largest requests of each kind
+                k = int(np.argmax(nray * (anyh == bool(i & 1))))
+                srv.wait(srv.submit(int(scene[k]), bool(anyh[k]), rays_ptr(k), int(nray[k]), out_ptr(k), device=dev))
+            w0 = srv.stats()["waves"]
+            tickets, lag = [0] * SERVED_NREQ, np.zeros(SERVED_NREQ)
 
-        # ---- served arm
-        for i in range(4):  # warm-up: largest requests of each kind
-            k = int(np.argmax(nray * (anyh == bool(i & 1))))
-            srv.wait(srv.submit(int(scene[k]), bool(anyh[k]), rays_ptr(k), int(nray[k]), out_ptr(k), device=dev))
-        w0 = srv.stats()["waves"]
-        tickets, lag = [0] * NREQ, np.zeros(NREQ)
+            def submitter():
+                T0 = time.perf_counter()
+                for i in range(SERVED_NREQ):
+                    ta = T0 + arrival[i]
+                    while time.perf_counter() < ta:
+                        pass
+                    tickets[i] = srv.submit(int(scene[i]), bool(anyh[i]), rays_ptr(i), int(nray[i]), out_ptr(i),
+                                            device=dev)
+                    lag[i] = time.perf_counter() - ta
 
-        def submitter():
+            th = threading.Thread(target=submitter)
+            th.start()
+            th.join()
+            infos = [srv.wait(t, timeout_ms=600_000) for t in tickets]
+            bad_status = sum(1 for f in infos if f["status"] != 0)
+            st = srv.stats()
+            lat_s = np.array([(f["done_us"] - f["submit_us"]) / 1e3 for f in infos]) + lag * 1e3
+            first = infos[0]["submit_us"] - lag[0] * 1e6
+            span_s = (max(f["done_us"] for f in infos) - first) / 1e3
+            snap = outb.cuda() if not dev else outb.clone()  # served results, kept on the GPU
+            # ---- plain arm: the per-call path, one call at a time
+            if dev:
+                fc, fa = L.cudaBVH_traceClosest, L.cudaBVH_traceAny
+            else:
+                fc, fa = L.cudaBVH_traceClosestHost, L.cudaBVH_traceAnyHost
+
+            def call(i):
+                f = fa if anyh[i] else fc
+                args_ = (bvhs[scene[i]].h, rays_ptr(i), int(nray[i]), out_ptr(i)) + ((None,) if dev else ())
+                rc = f(*args_)
+                if dev:
+                    torch.cuda.synchronize()
+                if rc != 0:
+                    raise RuntimeError(lib.last_error())
+
+            for sc in range(len(bvhs)):  # warm-up: each scene's staging sized by its largest request
+                for kind in (False, True):
+                    m = np.nonzero((scene == sc) & (anyh == kind))[0]
+                    if m.size:
+                        call(int(m[np.argmax(nray[m])]))
+            outb.zero_()
+            torch.cuda.synchronize()
+            lat_p = np.zeros(SERVED_NREQ)
             T0 = time.perf_counter()
-            for i in range(NREQ):
+            for i in range(SERVED_NREQ):
                 ta = T0 + arrival[i]
                 while time.perf_counter() < ta:
                     pass
-                tickets[i] = srv.submit(int(scene[i]), bool(anyh[i]), rays_ptr(i), int(nray[i]), out_ptr(i),
-                                        device=dev)
-                lag[i] = time.perf_counter() - ta
-
-        th = threading.Thread(target=submitter)
-        th.start()
-        th.join()
-        infos = [srv.wait(t, timeout_ms=600_000) for t in tickets]
-        st = srv.stats()
-        lat_s = np.array([(f["done_us"] - f["submit_us"]) / 1e3 for f in infos]) + lag * 1e3
-        first = infos[0]["submit_us"] - lag[0] * 1e6
-        span_s = (max(f["done_us"] for f in infos) - first) / 1e3
-        crc_srv = crcs()
-        # ---- plain arm: the per-call path, one call at a time
-        if dev:
-            fc, fa = L.cudaBVH_traceClosest, L.cudaBVH_traceAny
-        else:
-            fc, fa = L.cudaBVH_traceClosestHost, L.cudaBVH_traceAnyHost
-
-        def call(i):
-            f = fa if anyh[i] else fc
-            args_ = (bvhs[scene[i]].h, rays_ptr(i), int(nray[i]), out_ptr(i)) + ((None,) if dev else ())
-            rc = f(*args_)
-            if dev:
-                torch.cuda.synchronize()
-            if rc != 0:
-                raise RuntimeError(lib.last_error())
-
-        for sc in range(len(bvhs)):  # warm-up: each scene's staging sized by its largest request
-            for kind in (False, True):
-                m = np.nonzero((scene == sc) & (anyh == kind))[0]
-                if m.size:
-                    call(int(m[np.argmax(nray[m])]))
-        outb.zero_()
-        torch.cuda.synchronize()
-        lat_p = np.zeros(NREQ)
-        T0 = time.perf_counter()
-        for i in range(NREQ):
-            ta = T0 + arrival[i]
-            while time.perf_counter() < ta:
-                pass
-            call(i)
-            lat_p[i] = (time.perf_counter() - ta) * 1e3
-        span_p = (time.perf_counter() - T0) * 1e3
-        same = crcs() == crc_srv
-        srv_m, pl_m = total / span_s / 1e3, total / span_p / 1e3
-        pc = lambda a, q: round(float(np.percentile(a, q)), 3)
-        res[mode] = {
-            "served": {"p50_ms": pc(lat_s, 50), "p99_ms": pc(lat_s, 99), "mrays_s": round(srv_m, 1),
-                       "span_ms": round(span_s, 2), "waves": st["waves"] - w0,
-                       "peak_pool_gb": round(st["peak_pool_used"] / 2 ** 30, 3),
-                       "max_submit_lag_ms": round(float(lag.max() * 1e3), 3)},
-            "plain": {"p50_ms": pc(lat_p, 50), "p99_ms": pc(lat_p, 99), "mrays_s": round(pl_m, 1),
-                      "span_ms": round(span_p, 2)},
-            "p99_served_over_plain": round(float(np.percentile(lat_s, 99) / np.percentile(lat_p, 99)), 3),
-            "mrays_served_over_plain": round(srv_m / pl_m, 3),
-            "results_equal_plain": same}
-        log(f"{mode}: {json.dumps(res[mode])}")
-    resident = srv.stats()["resident_bytes"]
+                call(i)
+                lat_p[i] = (time.perf_counter() - ta) * 1e3
+            span_p = (time.perf_counter() - T0) * 1e3
+            same = bool(torch.equal(snap, outb.cuda() if not dev else outb))
+            del snap
+            srv_m, pl_m = total / span_s / 1e3, total / span_p / 1e3
+            pc = lambda a, q: round(float(np.percentile(a, q)), 3)
+            row[mode] = {
+                "served": {"p50_ms": pc(lat_s, 50), "p99_ms": pc(lat_s, 99), "mrays_s": round(srv_m, 1),
+                           "span_ms": round(span_s, 2), "waves": st["waves"] - w0,
+                           "peak_pool_gb": round(st["peak_pool_used"] / 2 ** 30, 3),
+                           "max_submit_lag_ms": round(float(lag.max() * 1e3), 3)},
+                "plain": {"p50_ms": pc(lat_p, 50), "p99_ms": pc(lat_p, 99), "mrays_s": round(pl_m, 1),
+                          "span_ms": round(span_p, 2)},
+                "p99_served_over_plain": round(float(np.percentile(lat_s, 99) / np.percentile(lat_p, 99)), 3),
+                "mrays_served_over_plain": round(srv_m / pl_m, 3),
+                "results_equal_plain": same and bad_status == 0}
+            log(f"served rate {rate:.0f}/s {mode}: {json.dumps(row[mode])}")
+            del outb
+        out["rates"][f"{rate:.0f}"] = row
+    out["config"]["resident_gb"] = round(srv.stats()["resident_bytes"] / 2 ** 30, 3)
     srv.close()
-    ok = all(r["results_equal_plain"] for r in res.values())
+    out["results_equal_plain"] = all(r[m]["results_equal_plain"] for r in out["rates"].values() for m in modes)
+    return out
+
+
+def run_served(args):
+    """Served form alone: served_legs at the configured 2,000 requests/s and
+    at 2x and 4x that rate (saturating arrivals); value = p99 latency of the
+    served arm with host buffers at 2,000 requests/s."""
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    res = served_legs(rates=(SERVED_RATE, 2 * SERVED_RATE, 4 * SERVED_RATE))
+    base = res["rates"][f"{SERVED_RATE:.0f}"]
     out = {"metric": "p99 trace latency served vs plain (ms), 256-request Poisson trace, host buffers",
-           "value": res["host"]["served"]["p99_ms"], "unit": "ms", "n_gpus": 1, "steps": 1, "warmup": 4,
-           "higher_is_better": False, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": "served_16x30m: 16 resident scenes (30,000,000 triangles, 200K-5M each), "
-                                  f"{NREQ} requests Poisson at {RATE:.0f}/s, rays log-uniform 1K-8M "
-                                  "(random incoherent rays), 70% closest / 30% any hit",
-                      "hbm_budget_gb": 120, "staging_pool_gb": 16,
-                      "resident_gb": round(resident / 2 ** 30, 3)},
-           "host_buffers": res["host"], "device_buffers": res["device"],
-           "offered_mrays_s": round(total / arrival[-1] / 1e6, 1), "rays": total,
-           "h2d_bytes": total * 32, "d2h_bytes": int((nray * esz).sum()), "results_equal_plain": ok}
+           "value": base["host"]["served"]["p99_ms"], "unit": "ms", "n_gpus": 1, "steps": 1, "warmup": 4,
+           "higher_is_better": False, "dtype": "f32", "data": "synthetic", "config": res["config"],
+           "served": res, "results_equal_plain": res["results_equal_plain"]}
     print(json.dumps(out), flush=True)
-    return 0 if ok else 1
+    return 0 if res["results_equal_plain"] else 1
 
 
 def main():
@@ -847,6 +1035,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-baselines", action="store_true", help="skip the reference-kernel and CPU legs")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-vs-plain legs of the default run")
+    ap.add_argument("--pt-regroup", type=int, default=0, choices=[0, 16, 32],
+                    help="pathtrace: regroup bounce rays by a 16- or 32-bit octant+Morton key before each extension")
     ap.add_argument("--workload", choices=["incoherent", "pathtrace", "batched", "served"], default="incoherent",
                     help="incoherent = 2M diffuse rays vs 2M triangles (headline); pathtrace = 1080p 8 spp TLAS "
                          "path tracer; batched = 256 scenes built and traced together; served = request "

@@ -66,6 +66,43 @@ int cudaBVH_traceClosest(CudaBVH_t bvh, const RtRay* d_rays, int n, RtHit* d_hit
  * with tmin < t < tmax, else 0. */
 int cudaBVH_traceAny(CudaBVH_t bvh, const RtRay* d_rays, int n, uint8_t* d_occluded, void* stream);
 
+/* ---- Next-bounce rays made on the device (the reference's genAndCompact,
+ * multi_bounce.cu:281-362) ----
+ * From a closest-hit batch traced on this BVH: for every input ray i whose
+ * hit names one of this BVH's triangles, the hit point p = o + t d and the
+ * triangle's geometric normal n turned to face the ray; the new ray starts
+ * at p + eps n and goes
+ *   RT_GEN_DIFFUSE: in a cosine-weighted direction about n (Malley's method:
+ *     the first of eight Philox uniform points of [-1,1)^2 that lies in the
+ *     unit disk, lifted to the hemisphere), over [tmin, tmax];
+ *   RT_GEN_SHADOW: toward a uniform point of a light_size x light_size square
+ *     parallel to xz centred at light_center, over [tmin, 0.9999 * distance].
+ * Misses are dropped and the survivors compacted in input order (warp ballot
+ * and block scan; deterministic).  count == 0: one ray per hit, output k from
+ * the k-th hit; count > 0: exactly count rays, output k from the
+ * (k mod hits)-th hit (none when there are no hits).  Random numbers: Philox
+ * key (seed, 3) diffuse / (seed, 4) shadow, counter (k, block, 0, 0).  All
+ * arithmetic is correctly rounded single precision without contraction, so
+ * a CPU restatement reproduces every bit.  d_out holds n rays (count == 0)
+ * or count rays; d_src (optional) receives each output's input index;
+ * *d_count (device) the number of rays written.  Stream-ordered; scratch
+ * comes from the library's stream-ordered pool.  The reference's version
+ * uses PCG, rsqrtf and sin/cos, and an atomic per block (output order
+ * varies run to run). */
+#define RT_GEN_DIFFUSE 0
+#define RT_GEN_SHADOW 1
+typedef struct {
+    int kind;               /* RT_GEN_DIFFUSE or RT_GEN_SHADOW */
+    int count;              /* 0: one ray per hit; > 0: exactly this many */
+    uint32_t seed;          /* Philox key word 0 */
+    float eps;              /* origin offset along the facing normal (0.001 in the reference) */
+    float tmin, tmax;       /* diffuse: the new rays' interval; shadow: tmin only */
+    float light_center[3];  /* shadow rays: centre of the square light */
+    float light_size;       /* shadow rays: side of the square light */
+} RtRayGen;
+int cudaBVH_generateRays(CudaBVH_t bvh, const RtRay* d_rays, const RtHit* d_hits, int n, const RtRayGen* gen,
+                         RtRay* d_out, int32_t* d_src, int* d_count, void* stream);
+
 /* Traversal status of the device-pointer calls on this handle.  The trace
  * calls above return as soon as the kernel is queued, so a stack overflow
  * inside it (RT_ERR_STACK: the BVH is deeper than the 64-entry traversal
@@ -144,6 +181,22 @@ int rtDebug_failAllocations(int after);
  * the L2 read bandwidth that bounds traversal of an L2-resident BVH; one
  * far above it gives the HBM read bandwidth.  Changes no device setting. */
 int rtProbe_readBandwidth(uint64_t bytes, int reps, float* out_gbs);
+
+/* ---- Ray regrouping (the reference's Morton sort of ray origins before
+ * tracing: CUB radix sort in cuda_rt_v40.cu:94-124,1226-1239, and a host
+ * radix sort in its per-call path, layer/cuda_bvh_backend.cu:1387-1433) ----
+ * d_out[k] = d_in[perm[k]] ordered by a key per ray: RT_REGROUP_MORTON, the
+ * 30-bit Morton code of the origin in box6 = {lo x, y, z, hi x, y, z} (10
+ * bits per axis, as the reference); RT_REGROUP_OCTANT_MORTON, the direction
+ * octant above the top 29 bits of that code.  key_bits 16 sorts by the
+ * key's top 16 bits only (2 passes of the radix sort instead of 4).  The
+ * sort is stable (equal keys keep their input order) and runs on the device
+ * with the library's own radix sort; d_perm (optional) receives the source
+ * index of every output ray.  d_in and d_out must not overlap. */
+#define RT_REGROUP_MORTON 0
+#define RT_REGROUP_OCTANT_MORTON 1
+int rtRays_regroup(const RtRay* d_in, int n, const float* box6, int kind, int key_bits, RtRay* d_out,
+                   int32_t* d_perm, void* stream);
 
 /* ---------------- instanced scenes (TLAS over BLASes) ---------------- */
 typedef struct CudaTLASHandle* CudaTLAS_t;
@@ -265,6 +318,11 @@ RtPathTracer_t rtPT_create(CudaTLAS_t tlas, const RtMaterial* materials, int num
  * are owned by the handle and grow to W*H*spp paths. */
 int rtPT_render(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* params, float* d_rgb, void* stream);
 int rtPT_getStats(RtPathTracer_t pt, RtPTStats* out);
+/* Regroups each bounce's extension rays (after the camera rays) with
+ * rtRays_regroup's key (kind, key_bits 16 or 32; 0 = off, the default)
+ * before they are traced.  Paths are independent, so the image is the same
+ * either way; only the order the rays are traced in changes. */
+int rtPT_setRegroup(RtPathTracer_t pt, int kind, int key_bits);
 void rtPT_destroy(RtPathTracer_t pt);
 /* The fp32 camera basis the renderer uses: eye[3], forward[3], right[3],
  * up[3], tan(vfov/2), aspect (14 floats). */

@@ -1,5 +1,6 @@
-// ref_v40_harness.cu -- drives the reference's own cuda_rt_v40.cu kernel
-// traceBVH4Diffuse rebuilt for sm_100a.  Comparison arm only: this is
+// ref_v40_harness.cu -- drives the reference's own cuda_rt_v40.cu kernels
+// traceBVH4Diffuse and the primary pipeline (broadphaseRoot +
+// tracePrimaryDense) rebuilt for sm_100a.  Comparison arm only: this is
 // how the in-run "rebuilt reference kernel" is timed.  The reference source is
 // #included from where it lies (REF_V40_SOURCE, set by oracle/Makefile); its
 // main() is renamed with -Dmain=ref_v40_main.  Nothing here changes the
@@ -16,6 +17,9 @@ struct RefV40 {
     int4* d_bvh4 = nullptr;
     float* d_tv[9] = {nullptr};
     int* d_counter = nullptr;
+    int* d_survivors = nullptr;     // primary pipeline: surviving ray indices
+    int* d_num_survivors = nullptr;
+    int survivors_cap = 0;
     std::vector<int> ordered_orig;  // ordered tri -> input index
     BVH2Builder* b2 = nullptr;
     std::vector<Tri> tris;
@@ -28,7 +32,7 @@ extern "C" {
 
 // Version of this harness's C-ABI; callers check it before binding, so a
 // stale build is refused instead of being called with the wrong arguments.
-int refv40_abi(void) { return 3; }
+int refv40_abi(void) { return 4; }
 
 // Reference BVH2 (32-bin SAH, cuda_rt_v40.cu:790-840) with maxLeaf, collapsed
 // to fp16 BVH4 (cuda_rt_v40.cu:844-871), uploaded the way main() does
@@ -99,6 +103,30 @@ int refv40_trace_bvh4(void* hv, const void* d_rays, void* d_hits, int n, int blo
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
+// The reference's primary pass for a side x side square camera looking +z
+// from cam (cuda_rt_v40.cu:1401-1421): resetCounters, broadphaseRoot
+// <<<640,256>>> (root test, survivors compacted by warp ballot), then
+// tracePrimaryDense <<<320,256>>> over the survivors (CSWAP-ordered BVH4
+// closest hit).  d_hits: Hit {t, tri (ordered index), u, v} per pixel; rays
+// that miss the root keep whatever d_hits held.  Stream-ordered on `stream`.
+int refv40_trace_primary(void* hv, int side, float cx, float cy, float cz, void* d_hits, void* stream) {
+    RefV40* h = static_cast<RefV40*>(hv);
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n = side * side;
+    if (n > h->survivors_cap) {
+        cudaFree(h->d_survivors);
+        if (cudaMalloc(&h->d_survivors, (size_t)n * sizeof(int)) != cudaSuccess) return -1;
+        h->survivors_cap = n;
+    }
+    if (!h->d_num_survivors && cudaMalloc(&h->d_num_survivors, sizeof(int)) != cudaSuccess) return -1;
+    resetCounters<<<1, 1, 0, s>>>(h->d_num_survivors);
+    broadphaseRoot<<<640, 256, 0, s>>>(h->d_survivors, h->d_num_survivors, n, side, cx, cy, cz);
+    tracePrimaryDense<<<320, 256, 0, s>>>(h->d_bvh4, h->num_b4 * 4, h->d_tv[0], h->d_tv[1], h->d_tv[2], h->d_tv[3],
+                                          h->d_tv[4], h->d_tv[5], h->d_tv[6], h->d_tv[7], h->d_tv[8],
+                                          h->d_survivors, h->d_num_survivors, (Hit*)d_hits, side, cx, cy, cz);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 // traceCWBVH (cuda_rt_v40.cu:142) is not driven here: it raised an illegal
 // memory access on a 2M-triangle scene built with 4-triangle leaves (its
 // 8-wide conversion, cuda_rt_v40.cu:1086-1088, encodes at most 3 triangles per
@@ -111,6 +139,8 @@ void refv40_destroy(void* hv) {
     cudaFree(h->d_bvh4);
     for (int c = 0; c < 9; c++) cudaFree(h->d_tv[c]);
     cudaFree(h->d_counter);
+    cudaFree(h->d_survivors);
+    cudaFree(h->d_num_survivors);
     delete h->b2;
     delete h;
 }

@@ -980,6 +980,116 @@ int orc_walk_bvh8(const uint32_t* nodes, int nnodes, const float* recs, int nrec
     return bad.load();
 }
 
+// ---- next-bounce ray generation, restating the library's
+// cudaBVH_generateRays (itself after genAndCompact, multi_bounce.cu:281-362:
+// hit point, facing geometric normal, tangent frame branching on the larger
+// of |nx| |ny|, origin offset eps * n).  Every step is one correctly rounded
+// single-precision operation in the same order as the GPU (this file is
+// compiled with -ffp-contract=off); random numbers are Philox4x32-10 with
+// key (seed, 3) for diffuse and (seed, 4) for shadow rays and counter
+// (output index, block, 0, 0); the cosine-weighted direction is Malley's
+// method on the first of eight uniform points of [-1,1)^2 inside the unit
+// disk.  Survivors (hits whose primitive is < ntris) keep input order.
+static inline float gen_u01(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+
+static void gen_one_ray(const float* tris9, const OrcRay& ray, const OrcHit& h, uint32_t item, int kind,
+                        uint32_t seed, float eps, float tmin, float tmax, const float* lc, float lsize,
+                        OrcRay& r) {
+    const float px = ray.org[0] + h.t * ray.dir[0], py = ray.org[1] + h.t * ray.dir[1],
+                pz = ray.org[2] + h.t * ray.dir[2];
+    const float* v = tris9 + (size_t)h.prim * 9;
+    const float e1x = v[3] - v[0], e1y = v[4] - v[1], e1z = v[5] - v[2];
+    const float e2x = v[6] - v[0], e2y = v[7] - v[1], e2z = v[8] - v[2];
+    float nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+    const float nl = 1.0f / sqrtf(fmaxf(nx * nx + ny * ny + nz * nz, 1e-30f));
+    nx = nx * nl;
+    ny = ny * nl;
+    nz = nz * nl;
+    if (nx * ray.dir[0] + ny * ray.dir[1] + nz * ray.dir[2] > 0.f) {
+        nx = -nx;
+        ny = -ny;
+        nz = -nz;
+    }
+    const float ox = px + eps * nx, oy = py + eps * ny, oz = pz + eps * nz;
+    r.org[0] = ox;
+    r.org[1] = oy;
+    r.org[2] = oz;
+    const uint32_t key[2] = {seed, kind == 0 ? 3u : 4u};
+    if (kind == 0) {
+        float tx, ty, tz;
+        if (fabsf(nx) > fabsf(ny)) {
+            const float il = 1.0f / sqrtf(nx * nx + nz * nz);
+            tx = -nz * il;
+            ty = 0.f;
+            tz = nx * il;
+        } else {
+            const float il = 1.0f / sqrtf(ny * ny + nz * nz);
+            tx = 0.f;
+            ty = nz * il;
+            tz = -ny * il;
+        }
+        const float bx = ny * tz - nz * ty, by = nz * tx - nx * tz, bz = nx * ty - ny * tx;
+        float x = 0.f, y = 0.f;
+        for (uint32_t blk = 0; blk < 4; blk++) {
+            const uint32_t ctr[4] = {item, blk, 0u, 0u};
+            uint32_t b[4];
+            orc_philox4x32_10(ctr, key, b);
+            const float a0 = 2.f * gen_u01(b[0]) - 1.f, b0 = 2.f * gen_u01(b[1]) - 1.f;
+            const float a1 = 2.f * gen_u01(b[2]) - 1.f, b1 = 2.f * gen_u01(b[3]) - 1.f;
+            if (a0 * a0 + b0 * b0 < 1.f) {
+                x = a0;
+                y = b0;
+                break;
+            }
+            if (a1 * a1 + b1 * b1 < 1.f) {
+                x = a1;
+                y = b1;
+                break;
+            }
+        }
+        const float z = sqrtf(fmaxf(1.f - x * x - y * y, 0.f));
+        const float dx = x * tx + y * bx + z * nx, dy = x * ty + y * by + z * ny, dz = x * tz + y * bz + z * nz;
+        const float dl = 1.0f / sqrtf(dx * dx + dy * dy + dz * dz);
+        r.dir[0] = dx * dl;
+        r.dir[1] = dy * dl;
+        r.dir[2] = dz * dl;
+        r.tmin = tmin;
+        r.tmax = tmax;
+    } else {
+        const uint32_t ctr[4] = {item, 0u, 0u, 0u};
+        uint32_t b[4];
+        orc_philox4x32_10(ctr, key, b);
+        const float lx = lc[0] + (gen_u01(b[0]) - 0.5f) * lsize, ly = lc[1], lz = lc[2] + (gen_u01(b[1]) - 0.5f) * lsize;
+        const float dx = lx - ox, dy = ly - oy, dz = lz - oz;
+        const float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+        r.dir[0] = dx / dist;
+        r.dir[1] = dy / dist;
+        r.dir[2] = dz / dist;
+        r.tmin = tmin;
+        r.tmax = dist * 0.9999f;
+    }
+}
+
+// Returns the number of rays written (count if count > 0 and there are hits,
+// the number of hits if count == 0).
+int orc_generate_rays(const float* tris9, int ntris, const OrcRay* rays, const OrcHit* hits, int n, int kind,
+                      int count, uint32_t seed, float eps, float tmin, float tmax, const float* light_center,
+                      float light_size, OrcRay* out, int32_t* src, int nthreads) {
+    std::vector<int> surv;
+    surv.reserve(n);
+    for (int i = 0; i < n; i++)
+        if (hits[i].prim >= 0 && hits[i].prim < ntris) surv.push_back(i);
+    const int m = (int)surv.size();
+    const int total = m == 0 ? 0 : (count > 0 ? count : m);
+    parallel_for(total, nthreads, 4096, [&](int k) {
+        const int s = surv[k % m];
+        gen_one_ray(tris9, rays[s], hits[s], (uint32_t)k, kind, seed, eps, tmin, tmax, light_center, light_size,
+                    out[k]);
+        if (src) src[k] = s;
+    });
+    return total;
+}
+
 
 }  // extern "C"
 

@@ -92,6 +92,13 @@ void orc_trace_any_two_level(const uint32_t* tlas, int tlas_nodes, const int* tl
                              const float* blas_packed, const int* tri_off,
                              const OrcRay* rays, int nrays, uint8_t* occluded, int nthreads);
 
+/* ---- next-bounce ray generation (restates cudaBVH_generateRays) ----
+ * kind 0: cosine-weighted diffuse, 1: shadow rays toward a square light.
+ * Returns the number of rays written to out (and input indices to src). */
+int orc_generate_rays(const float* tris9, int ntris, const OrcRay* rays, const OrcHit* hits, int n, int kind,
+                      int count, uint32_t seed, float eps, float tmin, float tmax, const float* light_center,
+                      float light_size, OrcRay* out, int32_t* src, int nthreads);
+
 /* ---- Philox4x32-10 ---- */
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 

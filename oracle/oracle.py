@@ -62,6 +62,10 @@ def lib() -> C.CDLL:
         L.orc_pt_pixels.argtypes = [vp, vp, vp, vp, i32, vp, i32, vp]
         L.orc_walk_bvh8.restype = i32
         L.orc_walk_bvh8.argtypes = [vp, i32, vp, i32, vp, i32, i32, i32, vp, vp, vp, i32]
+        f32 = C.c_float
+        L.orc_generate_rays.restype = i32
+        L.orc_generate_rays.argtypes = [vp, i32, vp, vp, i32, i32, i32, C.c_uint32, f32, f32, f32, vp, f32, vp, vp,
+                                        i32]
         _lib = L
     return _lib
 
@@ -182,6 +186,23 @@ def fix_skips(dfs: np.ndarray) -> np.ndarray:
     if lib().orc_fix_skips(_p(out), out.size // 8) < 0:
         raise ValueError("not a preorder binary tree")
     return out
+
+
+def generate_rays(tris, rays, hits, kind, count=0, seed=3, eps=1e-3, tmin=1e-3, tmax=1e30,
+                  light_center=(0.0, 80.0, 0.0), light_size=1.0, nthreads=0):
+    """Restated cudaBVH_generateRays: (rays, src) of the next bounce from a
+    closest-hit batch; kind 0 diffuse, 1 shadow."""
+    tris = np.ascontiguousarray(tris, dtype=np.float32).reshape(-1, 9)
+    rays = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
+    hits = np.ascontiguousarray(hits, dtype=HIT_DTYPE)
+    n = rays.shape[0]
+    cap = count if count > 0 else n
+    out = np.zeros(cap, dtype=RAY_DTYPE)
+    src = np.zeros(cap, dtype=np.int32)
+    lc = np.ascontiguousarray(light_center, dtype=np.float32)
+    m = lib().orc_generate_rays(_p(tris), tris.shape[0], _p(rays), _p(hits), n, int(kind), int(count),
+                                seed & 0xFFFFFFFF, eps, tmin, tmax, _p(lc), light_size, _p(out), _p(src), nthreads)
+    return out[:m], src[:m]
 
 
 def philox4x32_10(ctr, key):

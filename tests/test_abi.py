@@ -65,3 +65,35 @@ def test_tlas_fast_matches_reference_except_skips(path):
     mine = nodes.reshape(-1, 8)
     assert np.array_equal(mine[:, :7], ref[:, :7])
     assert np.array_equal(nodes, O.fix_skips(g["nodes"]))
+
+
+REF_OUT = Path(__file__).resolve().parents[1] / "oracle" / "_ref"
+
+
+def _nm(path, *flags):
+    import subprocess
+    r = subprocess.run(["nm", "-D", *flags, str(path)], capture_output=True, text=True, check=True)
+    return {ln.split()[-1].split("@")[0] for ln in r.stdout.splitlines() if ln.strip()}
+
+
+def test_reference_caller_and_shim_link_against_the_library():
+    """The reference's own C-ABI caller (layer/bvh_bench.cu, compiled unchanged
+    against include/cuda_bvh_backend.h) and its OptiX shim (linked as
+    OptiX_Shim/build_shim.sh:18-21 does, with this library in place of
+    cuda_bvh_backend.o) resolve every backend symbol they import from
+    libcudabvh_b200.so.  Built by `make -C oracle ref` from the reference
+    sources; the GPU run of the caller is tests/test_gpu_dropin.py."""
+    import subprocess
+    bench, shim = REF_OUT / "bvh_bench_b200", REF_OUT / "libnvoptix_shim_b200.so"
+    if not bench.exists() or not shim.exists():
+        pytest.skip("oracle/_ref caller and shim are built only where the reference sources are mounted")
+    exported = _nm(lib.LIB_PATH, "--defined-only")
+    wanted = {s for s in _nm(bench, "--undefined-only") if s.startswith("cudaBVH_")}
+    assert {"cudaBVH_build", "cudaBVH_tracePrimary", "cudaBVH_traceToRGBA", "cudaBVH_destroy"} <= wanted
+    assert wanted <= exported, wanted - exported
+    for f in (bench, shim):
+        ldd = subprocess.run(["ldd", str(f)], capture_output=True, text=True, check=True).stdout
+        line = next(ln for ln in ldd.splitlines() if "libcudabvh_b200.so" in ln)
+        assert "not found" not in line and Path(line.split("=>")[1].split("(")[0].strip()).resolve() == \
+            lib.LIB_PATH.resolve()
+    assert "optixQueryFunctionTable" in _nm(shim, "--defined-only")

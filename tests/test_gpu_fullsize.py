@@ -4,7 +4,9 @@ Config 1 (the headline workload, the same seeds and sizes bench.py times):
 a 2,000,000-triangle scene of sphere and box meshes, the 1920x1080 primary
 pass, then 2M cosine-weighted diffuse bounce rays with a 0.001 * normal
 origin offset (multi_bounce.cu:343-356 form; closest hit) and 2M area-light
-shadow rays (any hit).  Every ray is compared with the oracle's restated
+shadow rays (any hit), both made on the GPU by cudaBVH_generateRays from
+the primary hits and checked bit for bit against the oracle's restatement
+of the generator.  Every ray is compared with the oracle's restated
 traversal (layer/shaders/bvh2_stackless.comp:37-76 with the Moller-Trumbore
 arithmetic of layer/cuda_bvh_backend.cu:143-157) over the restated
 reference builder's BVH: primitive ids, t, u and v bit-identical, occlusion
@@ -55,9 +57,20 @@ def test_config1_fullsize_every_ray(cuda):
     prim = scenes.primary_1080p()
     ph = _trace(torch, bvh, prim)
     _assert_bitexact(ph, ob.closest(prim), "primary 1080p")
-    p, nrm = scenes.hit_frame(tris, prim, ph)
-    dif = scenes.diffuse_rays(p, nrm, N_RAYS, seed=3)
-    sha = scenes.shadow_rays(p, nrm, N_RAYS, seed=4)
+    d_prim = torch.from_numpy(prim.view(np.uint8).copy()).cuda()
+    d_ph = torch.from_numpy(ph.view(np.uint8).copy()).cuda()
+    made = []
+    for kind, seed in ((lib.RT_GEN_DIFFUSE, 3), (lib.RT_GEN_SHADOW, 4)):
+        d_out = torch.empty(N_RAYS * 32, dtype=torch.uint8, device="cuda")
+        d_cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+        bvh.generate_rays(d_prim, d_ph, prim.shape[0], d_out, d_cnt, kind=kind, count=N_RAYS, seed=seed)
+        torch.cuda.synchronize()
+        assert int(d_cnt.item()) == N_RAYS
+        rays = d_out.cpu().numpy().view(scenes.RAY_DTYPE)
+        ref, _ = O.generate_rays(tris, prim, ph, kind, count=N_RAYS, seed=seed)
+        assert np.array_equal(rays.view(np.uint32), ref.view(np.uint32)), f"generated rays (kind {kind}) differ"
+        made.append(rays)
+    dif, sha = made
     got = _trace(torch, bvh, dif)
     _assert_bitexact(got, ob.closest(dif), "2M diffuse closest hit")
     assert 0.3 < (got["prim"] >= 0).mean() < 0.6

@@ -297,6 +297,11 @@ bool build_handle(CudaBVHHandle* h, cudaStream_t s);
 int launch_trace_tlas(const CudaTLASHandle* t, const RtRay* rays, int n, const int* n_dev, RtHit* hits,
                       int32_t* inst_out, uint8_t* occ, int* work, int* status, cudaStream_t s);
 int* next_counter(rtb::DevBuf<int>& ring, std::atomic<unsigned>& next, cudaStream_t s);
+// Stable radix sort of rays[0 .. n) by regrouping key into out (payload
+// gathered alongside, perm[k] = source index; both optional); n from d_n
+// when given (at most cap).  Scratch from the stream-ordered pool.
+bool regroup_rays(const RtRay* rays, const int* payload, int cap, const int* d_n, int n_host, const float* box6,
+                  int kind, int key_bits, RtRay* out, int* payload_out, int32_t* perm, cudaStream_t s);
 // Reads and clears a handle's status word once `s` has finished its work:
 // RT_OK, RT_ERR_STACK (some trace overflowed its stack) or RT_ERR_CUDA.
 int read_status(int* d_status, cudaStream_t s, const char* who);

@@ -340,6 +340,12 @@ struct RtPathTracerHandle {
     unsigned work_next = 0;
     DevBuf<int> bcounts;      // per bounce: extension rays, shadow rays
     RtPTStats stats{};
+    // extension-queue regrouping (rtPT_setRegroup): key kind and bits (0 = off),
+    // the world box the origin Morton codes are taken in, sorted queue copies
+    int regroup_kind = RT_REGROUP_OCTANT_MORTON, regroup_bits = 0;
+    float world_box[6] = {0, 0, 0, 0, 0, 0};
+    DevBuf<RtRay> rays_sorted;
+    DevBuf<int> pid_sorted;
 };
 
 namespace {
@@ -392,6 +398,17 @@ double tri_area_world(const float* m, const float* v) {
 // instance's BLAS triangles, and the emissive triangles weighted by world
 // area (an exact integer CDF).  Host copies of emissive BLASes are kept for
 // later reloads.
+// World box of the TLAS (its binary root), for the regrouping keys.
+static bool load_world_box(RtPathTracerHandle* pt) {
+    Node2 root;
+    if (!RT_CUDA(cudaMemcpy(&root, pt->tlas->bvh2.nodes.p, sizeof(Node2), cudaMemcpyDeviceToHost))) return false;
+    for (int a = 0; a < 3; a++) {
+        pt->world_box[a] = root.lo[a];
+        pt->world_box[3 + a] = root.hi[a];
+    }
+    return true;
+}
+
 static bool load_instances(RtPathTracerHandle* pt, const float* fwd12, const int* blas_idx, const char* who) {
     const CudaTLASHandle* tlas = pt->tlas;
     const int ni = pt->ninst;
@@ -489,12 +506,23 @@ RtPathTracer_t rtPT_create(CudaTLAS_t tlas, const RtMaterial* mats, int nmat, co
     bool ok = pt->mat.alloc(mat.size()) && pt->counts.alloc(8) && pt->work.alloc(1024) &&
               pt->bcounts.alloc(2 * kMaxBounces) &&
               RT_CUDA(cudaMemcpy(pt->mat.p, mat.data(), mat.size() * 16, cudaMemcpyHostToDevice)) &&
-              load_instances(pt, fwd.data(), bidx.data(), "rtPT_create");
+              load_instances(pt, fwd.data(), bidx.data(), "rtPT_create") && load_world_box(pt);
     if (!ok) {
         delete pt;
         return nullptr;
     }
     return pt;
+}
+
+int rtPT_setRegroup(RtPathTracer_t pt, int kind, int key_bits) {
+    if (!pt || (key_bits != 0 && key_bits != 16 && key_bits != 32) ||
+        (kind != RT_REGROUP_MORTON && kind != RT_REGROUP_OCTANT_MORTON)) {
+        set_error("rtPT_setRegroup: invalid argument");
+        return RT_ERR_INVALID;
+    }
+    pt->regroup_kind = kind;
+    pt->regroup_bits = key_bits;
+    return RT_OK;
 }
 
 void rtPT_destroy(RtPathTracer_t pt) {
@@ -521,7 +549,8 @@ int rtPT_render(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* prm, f
     // once renders still in flight are done with them
     if (pt->tlas->generation != pt->tlas_generation) {
         const CudaTLASHandle* t = pt->tlas;
-        if (!RT_CUDA(cudaDeviceSynchronize()) || !load_instances(pt, t->h_fwd.data(), t->h_blas.data(), "rtPT_render"))
+        if (!RT_CUDA(cudaDeviceSynchronize()) || !load_instances(pt, t->h_fwd.data(), t->h_blas.data(), "rtPT_render") ||
+            !load_world_box(pt))
             return RT_ERR_CUDA;
         pt->tlas_generation = t->generation;
     }
@@ -537,7 +566,10 @@ int rtPT_render(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* prm, f
                         pt->tp.alloc(P) && pt->L.alloc(P) && pt->scontrib.alloc(P) && pt->socc.alloc(P);
         if (!ok) return RT_ERR_NOMEM;
         pt->cap = P;
+        pt->rays_sorted.release();
+        pt->pid_sorted.release();
     }
+    if (pt->regroup_bits && (!pt->rays_sorted.ensure(pt->cap) || !pt->pid_sorted.ensure(pt->cap))) return RT_ERR_NOMEM;
     CudaTLASHandle* t = pt->tlas;
     PtScene sc;
     sc.mat = pt->mat.p;
@@ -561,11 +593,22 @@ int rtPT_render(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* prm, f
         k_zero2<<<1, 1, 0, s>>>(cnt + nxt, cnt + 2);
         int* w1 = pt->work.p + (pt->work_next++ % 1024);
         cudaMemsetAsync(w1, 0, sizeof(int), s);
-        if (launch_trace_tlas(t, pt->rays[cur].p, 0, cnt + cur, pt->hits.p, pt->hinst.p, nullptr, w1, t->status.p,
-                              s) != RT_OK)
+        // bounce rays leave scattered surface points in all directions: regroup
+        // them (direction octant, origin Morton code) before the extension trace;
+        // camera rays (bounce 0) are already in pixel order
+        RtRay* qrays = pt->rays[cur].p;
+        int* qpid = pt->pid[cur].p;
+        if (pt->regroup_bits && b > 0) {
+            if (!regroup_rays(qrays, qpid, (int)pt->cap, cnt + cur, 0, pt->world_box, pt->regroup_kind,
+                              pt->regroup_bits, pt->rays_sorted.p, pt->pid_sorted.p, nullptr, s))
+                return RT_ERR_CUDA;
+            qrays = pt->rays_sorted.p;
+            qpid = pt->pid_sorted.p;
+        }
+        if (launch_trace_tlas(t, qrays, 0, cnt + cur, pt->hits.p, pt->hinst.p, nullptr, w1, t->status.p, s) != RT_OK)
             return RT_ERR_CUDA;
         k_pt_shade<<<num_sms() * RTB_SHADE_MINB, PT_T, 0, s>>>(sc, prm->spp, b, prm->max_bounces, prm->rr_start, prm->seed,
-                                                 cnt + cur, pt->rays[cur].p, pt->pid[cur].p, pt->hits.p,
+                                                 cnt + cur, qrays, qpid, pt->hits.p,
                                                  pt->hinst.p, pt->tp.p, pt->L.p, pt->rays[nxt].p, pt->pid[nxt].p,
                                                  cnt + nxt, pt->srays.p, pt->spid.p, pt->scontrib.p, cnt + 2);
         int* w2 = pt->work.p + (pt->work_next++ % 1024);

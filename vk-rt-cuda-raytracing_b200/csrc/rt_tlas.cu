@@ -71,10 +71,11 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
     __shared__ int s_rec[TRACE_T];
     __shared__ int4 s_res[TRACE_T];  // u, v bits, instance, primitive of the improved best
 #if RTB_SLOTMASK
-    __shared__ uint8_t s_oct_perm[OCT_PERM_BYTES];
-    init_oct_perm(s_oct_perm);
+    __shared__ NodeLuts s_luts;
+    init_node_luts(&s_luts);
+    const NodeLuts* s_oct_perm = &s_luts;
 #else
-    const uint8_t* s_oct_perm = nullptr;
+    const NodeLuts* s_oct_perm = nullptr;
 #endif
     if (n_dev) n = *n_dev;  // ray count produced on the device by an earlier stage
     uint2 lstack[LSTACK];

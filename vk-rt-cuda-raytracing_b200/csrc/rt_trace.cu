@@ -94,10 +94,11 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
     __shared__ float4 s_ray[2][TRACE_T];           // each lane's ray, read by the lanes testing its triangles
 #endif
 #if RTB_SLOTMASK
-    __shared__ uint8_t s_oct_perm[OCT_PERM_BYTES];
-    init_oct_perm(s_oct_perm);
+    __shared__ NodeLuts s_luts;
+    init_node_luts(&s_luts);
+    const NodeLuts* s_oct_perm = &s_luts;
 #else
-    const uint8_t* s_oct_perm = nullptr;
+    const NodeLuts* s_oct_perm = nullptr;
 #endif
     uint2 lstack[LSTACK];
     const int lane = threadIdx.x & 31;
@@ -180,9 +181,14 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
         for (int it = 0; it < NITERS; it++) {
 #if RTB_STATS
             {
-                const unsigned act = __ballot_sync(FULL_MASK, ray >= 0 && tmask == 0 && !overflow && (w.ng.y & 0xFFu));
-                RTB_STAT(2 + 2 * it, act ? 1 : 0);
-                RTB_STAT(3 + 2 * it, __popc(act));
+#if RTB_TWO_SETS
+                const bool visit = ray >= 0 && tmask2 == 0 && !overflow && (w.ng.y & 0xFFu);
+#else
+                const bool visit = ray >= 0 && tmask == 0 && !overflow && (w.ng.y & 0xFFu);
+#endif
+                const unsigned act = __ballot_sync(FULL_MASK, visit);
+                RTB_STAT(2 + 2 * it, act ? 1 : 0);  // visit it: warp executions (it < 5)
+                RTB_STAT(3 + 2 * it, __popc(act));  //           lanes
             }
 #endif
 #if RTB_TWO_SETS
@@ -247,9 +253,9 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
             total = __shfl_sync(FULL_MASK, incl, 31);
         }
         bool found_any = false;
-        RTB_STAT(6, total ? 1 : 0);
-        RTB_STAT(7, (total + 31) / 32);
-        RTB_STAT(8, total);
+        RTB_STAT(12, total ? 1 : 0);
+        RTB_STAT(13, (total + 31) / 32);
+        RTB_STAT(14, total);
 #if RTB_DUP_TRI
 #pragma unroll 1
         for (int rep = 0; rep < 2; rep++)

@@ -182,7 +182,9 @@ __device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t k) {
 // predicated OR, no branch), takes a leaf's triangle bits with one
 // predicated OR, and moves the inner hits into the ray's octant order once
 // per node with a table lookup (oct_perm, 2 KB of shared memory per CTA)
-// instead of a shift per child.
+// instead of a shift per child.  1: a leaf's bits from bmsk of its meta
+// byte; 2: from a 256-entry table indexed by the meta byte (1 KB of shared
+// memory; inner slots' meta 0xFF and empty slots' 0 map to no bits).
 #ifndef RTB_SLOTMASK
 #define RTB_SLOTMASK 0
 #endif
@@ -192,14 +194,23 @@ __device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t k) {
 #define RTB_TWO_SETS 0
 #endif
 constexpr int OCT_PERM_BYTES = 8 * 256;
-// Fills the table: entry (o << 8) | x is x with bit i moved to bit i ^ o.
-// Called by every thread of the CTA before its first node visit.
-__device__ __forceinline__ void init_oct_perm(uint8_t* perm) {
+// Lookup tables of the node test in shared memory (RTB_SLOTMASK).
+struct NodeLuts {
+    uint32_t meta_run[256];        // meta byte -> triangle bits of the leaf slot
+    uint8_t oct_perm[OCT_PERM_BYTES];  // (o << 8) | x -> x with bit i moved to bit i ^ o
+};
+// Fills the tables; called by every thread of the CTA before its first node visit.
+__device__ __forceinline__ void init_node_luts(NodeLuts* t) {
     for (int idx = threadIdx.x; idx < OCT_PERM_BYTES; idx += blockDim.x) {
         const uint32_t o = (uint32_t)idx >> 8, x = (uint32_t)idx & 0xFFu;
         uint32_t y = 0;
         for (uint32_t i = 0; i < 8; i++) y |= ((x >> i) & 1u) << (i ^ o);
-        perm[idx] = (uint8_t)y;
+        t->oct_perm[idx] = (uint8_t)y;
+    }
+    for (int m = threadIdx.x; m < 256; m += blockDim.x) {
+        // leaf: count << 5 | offset; 0xFF marks an inner child, 0 an empty slot
+        const uint32_t off = (uint32_t)m & 31u, cnt = (uint32_t)m >> 5;
+        t->meta_run[m] = (m == 0xFF || off + cnt > 32) ? 0u : (cnt ? ((0xFFFFFFFFu >> (32 - cnt)) << off) : 0u);
     }
     __syncthreads();
 }
@@ -294,7 +305,7 @@ __device__ __forceinline__ void prefetch_next(const uint4* nodes, uint2 ng, uint
 // (`ng`), and the triangle base + 32-bit mask of hit leaf triangles.
 __device__ __forceinline__ void visit_node(const uint4* __restrict__ np, const Ray& r, float thit,
                                            uint32_t& inner_hits, uint32_t& tri_base, uint32_t& tmask, uint2& ng,
-                                           const uint8_t* __restrict__ oct_perm = nullptr) {
+                                           const NodeLuts* __restrict__ luts = nullptr) {
     const uint4 w0 = ld_node(np), w1 = ld_node(np + 1), w2 = ld_node(np + 2), w3 = ld_node(np + 3),
                 w4 = ld_node(np + 4);
     const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
@@ -347,13 +358,20 @@ __device__ __forceinline__ void visit_node(const uint4* __restrict__ np, const R
         const float tn = max3f(tnx, tny, fmaxf(tnz, r.tmin));
         const float tf = min3f(tfx, tfy, fminf(tfz, thit));
         const bool hit = tn <= fmaf(fabsf(tf), 0x1p-21f, tf);
-#if RTB_SLOTMASK
+#if RTB_SLOTMASK == 1
         // leaf run from the meta byte (count << 5 | offset); inner slots (meta
         // 0xFF) are excluded by the inner bit, empty slots have count 0
         const uint32_t mw = s < 4 ? w1.z : w1.w;
         const uint32_t run = bit_mask_wrap(mw >> sh, (mw >> (sh + 5)) & 7u);
         if (hit) hm |= 1u << s;
         if (hit && !((imask >> s) & 1u)) th |= run;
+        continue;
+#elif RTB_SLOTMASK == 2
+        const uint32_t mw = s < 4 ? w1.z : w1.w;
+        if (hit) {
+            hm |= 1u << s;
+            th |= luts->meta_run[(mw >> sh) & 0xFFu];
+        }
         continue;
 #endif
         const uint32_t meta = ((s < 4 ? w1.z : w1.w) >> sh) & 0xFFu;
@@ -373,7 +391,7 @@ __device__ __forceinline__ void visit_node(const uint4* __restrict__ np, const R
 #endif
     }
 #if RTB_SLOTMASK
-    nh = oct_perm[(r.oct << 8) | (hm & imask)];
+    nh = luts->oct_perm[(r.oct << 8) | (hm & imask)];
 #endif
     inner_hits = nh;
     tri_base = w1.y;

@@ -33,6 +33,24 @@ class RtBuildStats(C.Structure):
                 ("node_bytes", C.c_uint64), ("tri_bytes", C.c_uint64)]
 
 
+class RtRayGen(C.Structure):
+    _fields_ = [("kind", C.c_int), ("count", C.c_int), ("seed", C.c_uint32), ("eps", C.c_float),
+                ("tmin", C.c_float), ("tmax", C.c_float), ("light_center", C.c_float * 3),
+                ("light_size", C.c_float)]
+
+
+RT_GEN_DIFFUSE, RT_GEN_SHADOW = 0, 1
+RT_REGROUP_MORTON, RT_REGROUP_OCTANT_MORTON = 0, 1
+
+
+def regroup_rays(d_in, n: int, box6, d_out, kind: int = RT_REGROUP_OCTANT_MORTON, key_bits: int = 32, d_perm=None,
+                 stream=None):
+    """rtRays_regroup: d_out = d_in reordered by (octant,) origin Morton key; stable."""
+    box = np.ascontiguousarray(box6, dtype=np.float32)
+    _check(load().rtRays_regroup(_ptr(d_in), n, box.ctypes.data, kind, key_bits, _ptr(d_out),
+                                 _ptr(d_perm) if d_perm is not None else None, _stream(stream)), "rtRays_regroup")
+
+
 class RtInstance(C.Structure):
     _fields_ = [("xform", C.c_float * 12), ("blas", C.c_int32), ("mask", C.c_uint32), ("custom", C.c_uint32),
                 ("pad", C.c_uint32)]
@@ -117,6 +135,9 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "cudaBVH_traceCounters": (i32, [vp, vp, i32, i32, vp, vp]),
         "cudaBVH_traceClosestHostNoAlloc": (i32, [vp, vp, i32, vp, vp]),
         "cudaBVH_getStatus": (i32, [vp, vp]),
+        "cudaBVH_generateRays": (i32, [vp, vp, vp, i32, C.POINTER(RtRayGen), vp, vp, vp, vp]),
+        "rtRays_regroup": (i32, [vp, i32, vp, i32, i32, vp, vp, vp]),
+        "rtPT_setRegroup": (i32, [vp, i32, i32]),
         "rtDebug_failAllocations": (i32, [i32]),
         "rtProbe_readBandwidth": (i32, [C.c_uint64, i32, C.POINTER(f32)]),
         "cudaBVH_validate": (i32, [vp]),
@@ -286,6 +307,15 @@ class BVH:
 
     def any(self, d_rays, n: int, d_occ, stream=None):
         _check(load().cudaBVH_traceAny(self.h, _ptr(d_rays), n, _ptr(d_occ), _stream(stream)), "cudaBVH_traceAny")
+
+    def generate_rays(self, d_rays, d_hits, n: int, d_out, d_count, kind: int = RT_GEN_DIFFUSE, count: int = 0,
+                      seed: int = 3, eps: float = 1e-3, tmin: float = 1e-3, tmax: float = 1e30,
+                      light_center=(0.0, 80.0, 0.0), light_size: float = 1.0, d_src=None, stream=None):
+        """cudaBVH_generateRays: next-bounce rays from a closest-hit batch (device buffers)."""
+        g = RtRayGen(kind, count, seed & 0xFFFFFFFF, eps, tmin, tmax, (C.c_float * 3)(*light_center), light_size)
+        _check(load().cudaBVH_generateRays(self.h, _ptr(d_rays), _ptr(d_hits), n, C.byref(g), _ptr(d_out),
+                                           _ptr(d_src) if d_src is not None else None, _ptr(d_count),
+                                           _stream(stream)), "cudaBVH_generateRays")
 
     def status(self, stream=None) -> int:
         """cudaBVH_getStatus: RT_OK or RT_ERR_STACK for the device-pointer traces so far."""
@@ -473,6 +503,10 @@ class PathTracer:
                seed: int = 1, d_rgb=None, stream=None):
         p = RtPTParams(w, h, spp, max_bounces, rr_start, seed)
         _check(load().rtPT_render(self.h, C.byref(cam), C.byref(p), _ptr(d_rgb), _stream(stream)), "rtPT_render")
+
+    def set_regroup(self, key_bits: int, kind: int = RT_REGROUP_OCTANT_MORTON):
+        """rtPT_setRegroup: regroup bounce rays before each extension trace (0 = off)."""
+        _check(load().rtPT_setRegroup(self.h, kind, key_bits), "rtPT_setRegroup")
 
     def stats(self) -> dict:
         s = RtPTStats()
