@@ -797,6 +797,7 @@ def run_batched(args):
     b = lib.Batch(all_tris=allt, tri_offsets=tri_off)
     info = b.info()
     ctas, iters = b.autotune(d_rays, d_off, nr, d_hits, stream=stream)
+    shape = b.tuning()
     b.graph(d_rays, d_off, nr, d_hits, stream=stream)
     torch.cuda.synchronize()
     b.close()
@@ -808,7 +809,7 @@ def run_batched(args):
         b = lib.Batch(all_tris=allt, tri_offsets=tri_off)
         torch.cuda.synchronize()
         h1 = time.perf_counter()
-        b.set_tuning(ctas, iters)
+        b.set_tuning_ex(shape["warps_per_sm"], shape["node_iters"], shape["block"], shape["shared_stack"])
         e0, e1 = ev(), ev()
         e0.record(stream)
         b.graph(d_rays, d_off, nr, d_hits, stream=stream)
@@ -853,7 +854,7 @@ def run_batched(args):
                                   f"{nr} rays (4K-2M per scene, half primary, half diffuse), closest hit",
                       "l2": "flushed between steps", "host_tris": "pinned, shared by both arms"},
            "ours": {"build_ms": round(bo, 2), "trace_ms": round(to, 3), "trace_mrays_s": round(nr / to / 1e3, 1),
-                    "device_build_ms": round(info["build_ms"], 2), "tuning": {"ctas_per_sm": ctas, "node_iters": iters},
+                    "device_build_ms": round(info["build_ms"], 2), "tuning": shape,
                     "launches": "one build pipeline for all scenes, one graph-captured trace launch"},
            "plain": {"build_ms": round(bp, 2), "trace_ms": round(tp, 3), "trace_mrays_s": round(nr / tp / 1e3, 1),
                      "value": round(nr / (bp + tp) / 1e3, 1), "steps": psteps,

@@ -265,12 +265,27 @@ int rtBatch_traceAny(RtBatch_t batch, const RtRay* d_rays, const int* d_ray_offs
  * any != 0: d_out is uint8_t occlusion, else RtHit. */
 int rtBatch_traceGraph(RtBatch_t batch, const RtRay* d_rays, const int* d_ray_offsets, int n, void* d_out, int any,
                        void* stream);
-/* Autotuner: times persistent CTAs per SM {2,4,6,8} x node visits per
- * iteration {1,2} on this batch and keeps the fastest.  With the environment
- * variable RTB200_TUNE_CACHE=<file> the choice is stored and reused. */
+/* Launch shape of the batched trace. */
+typedef struct {
+    int warps_per_sm;   /* persistent worker warps per SM (8..32 at 128 threads per CTA) */
+    int node_iters;     /* node visits per lane between pooled triangle phases (2..4) */
+    int block;          /* threads per CTA: 64, 128 or 256 */
+    int shared_stack;   /* traversal stack entries per ray kept in shared memory: 4, 8 or 12 */
+} RtBatchTuning;
+/* Autotuner: times the batch's closest-hit trace over the launch shape, one
+ * dimension at a time from the default (worker warps per SM {8, 16, 24, 32},
+ * node visits per iteration {2, 3, 4}, threads per CTA {64, 128, 256}, shared
+ * stack entries {4, 8, 12}), keeping the fastest value of each before the
+ * next.  With the environment variable RTB200_TUNE_CACHE=<file> the choice is
+ * stored and reused.  out_ctas_per_sm reports the worker count as CTAs of
+ * 128 threads; rtBatch_getTuning gives the whole shape. */
 int rtBatch_autotune(RtBatch_t batch, const RtRay* d_rays, const int* d_ray_offsets, int n, RtHit* d_hits,
                      void* stream, int* out_ctas_per_sm, int* out_node_iters);
+/* Worker count as CTAs of 128 threads per SM (1..8) and node visits (1..4);
+ * block and shared stack keep their values. */
 int rtBatch_setTuning(RtBatch_t batch, int ctas_per_sm, int node_iters);
+int rtBatch_setTuningEx(RtBatch_t batch, const RtBatchTuning* tuning);
+int rtBatch_getTuning(RtBatch_t batch, RtBatchTuning* out);
 int rtBatch_getInfo(RtBatch_t batch, int* num_scenes, int* num_nodes, float* build_ms);
 
 /* ---------------- wavefront path tracer ----------------
@@ -323,6 +338,18 @@ int rtPT_getStats(RtPathTracer_t pt, RtPTStats* out);
  * before they are traced.  Paths are independent, so the image is the same
  * either way; only the order the rays are traced in changes. */
 int rtPT_setRegroup(RtPathTracer_t pt, int kind, int key_bits);
+/* Wavefront queue capacity: the frame's W*H*spp paths are traced in slices
+ * of at most `paths` paths (contiguous path ids, each slice through all its
+ * bounces before the next starts); 0 = the whole frame in one slice (the
+ * default).  Queues take about 150 bytes per path of capacity.  The image
+ * does not depend on it: every path keeps its own radiance slot. */
+int rtPT_setQueueCapacity(RtPathTracer_t pt, int64_t paths);
+/* Times renders of this frame with the whole frame, 1/2, 1/4 and 1/8 of it
+ * per slice (slices that would not fill the GPU are skipped), keeps the
+ * fastest capacity and returns it in *out_paths (0 = whole frame).  Renders
+ * into d_rgb. */
+int rtPT_autotune(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* params, float* d_rgb, void* stream,
+                  int64_t* out_paths);
 void rtPT_destroy(RtPathTracer_t pt);
 /* The fp32 camera basis the renderer uses: eye[3], forward[3], right[3],
  * up[3], tan(vfov/2), aspect (14 floats). */

@@ -444,10 +444,21 @@ def test_batched_scenes_equal_per_scene_calls(cuda):
         assert_hits_equal(got[off[i]:off[i + 1]], ref, f"scene {i}")
         assert np.array_equal(occ[off[i]:off[i + 1]], O.brute_any(t, rays[i]))
     ctas, iters = b.autotune(d_rays, d_off, n, d_h)
-    assert 1 <= ctas <= 8 and iters in (1, 2)
+    t = b.tuning()
+    assert 1 <= ctas <= 8 and iters in (2, 3, 4) and t["node_iters"] == iters
+    assert t["block"] in (64, 128, 256) and t["shared_stack"] in (4, 8, 12) and 8 <= t["warps_per_sm"] <= 32
     b.graph(d_rays, d_off, n, d_g)
     torch.cuda.synchronize()
     assert np.array_equal(d_g.cpu().numpy(), d_h.cpu().numpy())
+    # every launch shape the tuner can pick gives the same records
+    for shape in ((8, 2, 64, 8), (32, 4, 256, 8), (16, 3, 128, 8), (24, 4, 128, 4), (32, 2, 128, 12)):
+        b.set_tuning_ex(*shape)
+        d_x = torch.empty_like(d_h)
+        b.closest(d_rays, d_off, n, d_x)
+        d_y = torch.empty_like(d_g)
+        b.graph(d_rays, d_off, n, d_y)
+        torch.cuda.synchronize()
+        assert torch.equal(d_x, d_h) and torch.equal(d_y, d_h), shape
 
 
 def test_pipelined_host_calls_equal_device_calls(cuda):

@@ -163,7 +163,11 @@ def test_regroup_sorts_stably_and_keeps_every_ray(cuda):
     assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
 
 
-def test_path_tracer_image_does_not_depend_on_regrouping(cuda):
+def test_path_tracer_image_does_not_depend_on_regrouping_or_queue_capacity(cuda):
+    """Paths are independent and each keeps its own radiance slot, so the
+    image and the ray counts are bit-identical whether bounce rays are
+    regrouped or not and whatever the wavefront queue capacity (the frame in
+    one slice, or in slices of any size, uneven last slice included)."""
     import torch
     blases, xf, bidx, alb, emi = scenes.instanced_scene(2, 200_000, nblas=4, ninst=16, world=40.0,
                                                         emissive_frac=0.25)
@@ -172,9 +176,10 @@ def test_path_tracer_image_does_not_depend_on_regrouping(cuda):
     cam = lib.make_camera((0.0, 10.0, -70.0), (0.0, 0.0, 0.0), vfov=50.0)
     W, H, spp = 320, 180, 4
     imgs = []
-    for bits in (0, 16, 32):
+    for bits, cap in ((0, 0), (16, 0), (32, 0), (0, 77_777), (32, 50_000), (0, 4_099)):
         pt = lib.PathTracer(tl, alb, emi)
         pt.set_regroup(bits)
+        pt.set_queue_capacity(cap)
         d_rgb = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
         pt.render(cam, W, H, spp, 4, 2, 1, d_rgb)
         torch.cuda.synchronize()
@@ -185,3 +190,23 @@ def test_path_tracer_image_does_not_depend_on_regrouping(cuda):
         assert st["extension_rays"] == imgs[0][1]["extension_rays"]
         assert st["shadow_rays"] == imgs[0][1]["shadow_rays"]
     assert imgs[0][0].sum() > 0
+
+
+def test_path_tracer_autotune_keeps_the_image(cuda):
+    import torch
+    blases, xf, bidx, alb, emi = scenes.instanced_scene(3, 400_000, nblas=4, ninst=16, world=40.0,
+                                                        emissive_frac=0.25)
+    bvhs = [lib.BVH(t) for t in blases]
+    tl = lib.TLAS(bvhs, xf, bidx)
+    cam = lib.make_camera((0.0, 10.0, -70.0), (0.0, 0.0, 0.0), vfov=50.0)
+    W, H, spp = 640, 360, 8
+    pt = lib.PathTracer(tl, alb, emi)
+    a = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
+    b = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
+    pt.render(cam, W, H, spp, 4, 2, 1, a)
+    cap = pt.autotune(cam, W, H, spp, 4, 2, 1, d_rgb=b)
+    assert cap == 0 or (cap % spp == 0 and cap < W * H * spp)
+    b.zero_()
+    pt.render(cam, W, H, spp, 4, 2, 1, b)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)

@@ -4,8 +4,10 @@
 // stage's launches; all ray batches are traced by one persistent,
 // work-stealing launch in which every lane starts at its own scene's root;
 // that launch can be captured once into a CUDA graph and replayed.  The
-// autotuner times the persistent worker count and the node visits per
-// iteration on the caller's batch and keeps the fastest.
+// autotuner times the launch shape on the caller's batch (persistent worker
+// warps, node visits per iteration, threads per CTA, shared stack entries)
+// and keeps the fastest.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -26,8 +28,7 @@ struct RtBatchHandle {
     DevBuf<int> d_tri_off;
     Bvh8Device bvh8;
     DevBuf<int> work, status;  // work[0]: plain launches, work[1]: graph launches
-    int ctas_per_sm = TRACE_MINB;
-    int node_iters = 2;
+    RtBatchTuning tune{TRACE_MINB * TRACE_T / 32, RTB_NODE_ITERS, TRACE_T, SSTACK};
     float build_ms = 0.f;
     // captured graph and the arguments it was captured with
     cudaGraphExec_t gexec = nullptr;
@@ -35,7 +36,8 @@ struct RtBatchHandle {
     const void* g_rays = nullptr;
     const void* g_off = nullptr;
     void* g_out = nullptr;
-    int g_n = -1, g_any = -1, g_ctas = -1, g_iters = -1;
+    int g_n = -1, g_any = -1;
+    RtBatchTuning g_tune{-1, -1, -1, -1};
     ~RtBatchHandle() {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (cap_stream) cudaStreamDestroy(cap_stream);
@@ -43,6 +45,12 @@ struct RtBatchHandle {
 };
 
 namespace {
+
+bool valid_tuning(const RtBatchTuning& t) {
+    return t.warps_per_sm >= 1 && t.warps_per_sm <= 64 && t.node_iters >= 1 && t.node_iters <= 4 &&
+           (t.block == 64 || t.block == 128 || t.block == 256) &&
+           (t.shared_stack == 4 || t.shared_stack == 8 || t.shared_stack == 12);
+}
 
 bool tune_from_cache(RtBatchHandle* b, int n) {
     const char* path = getenv("RTB200_TUNE_CACHE");
@@ -56,11 +64,11 @@ bool tune_from_cache(RtBatchHandle* b, int n) {
     while (fgets(line, sizeof(line), f)) {
         const char* k = strstr(line, key);
         if (!k) continue;
-        int c = 0, it = 0;
-        if (sscanf(k + strlen(key), " : [%d, %d]", &c, &it) == 2 && c >= 1 && c <= TRACE_MINB &&
-            (it == 1 || it == 2)) {
-            b->ctas_per_sm = c;
-            b->node_iters = it;
+        RtBatchTuning t;
+        if (sscanf(k + strlen(key), " : [%d, %d, %d, %d]", &t.warps_per_sm, &t.node_iters, &t.block,
+                   &t.shared_stack) == 4 &&
+            valid_tuning(t)) {
+            b->tune = t;
             found = true;
         }
     }
@@ -73,7 +81,8 @@ void tune_to_cache(const RtBatchHandle* b, int n) {
     if (!path) return;
     FILE* f = fopen(path, "a");
     if (!f) return;
-    fprintf(f, "{\"batch:%d:%d:%d\" : [%d, %d]}\n", b->num_scenes, b->num_tris, n, b->ctas_per_sm, b->node_iters);
+    fprintf(f, "{\"batch:%d:%d:%d\" : [%d, %d, %d, %d]}\n", b->num_scenes, b->num_tris, n, b->tune.warps_per_sm,
+            b->tune.node_iters, b->tune.block, b->tune.shared_stack);
     fclose(f);
 }
 
@@ -160,7 +169,7 @@ int rtBatch_traceClosest(RtBatch_t b, const RtRay* d_rays, const int* d_ray_offs
     cudaStream_t s = (cudaStream_t)stream;
     cudaMemsetAsync(b->work.p, 0, sizeof(int), s);
     rc = launch_trace_multi(b->bvh8, d_rays, n, d_ray_offsets, b->d_tri_off.p, b->num_scenes, d_hits, nullptr,
-                            b->work.p, b->status.p, b->ctas_per_sm, b->node_iters, s);
+                            b->work.p, b->status.p, b->tune, s);
     return rc;
 }
 
@@ -171,7 +180,7 @@ int rtBatch_traceAny(RtBatch_t b, const RtRay* d_rays, const int* d_ray_offsets,
     cudaStream_t s = (cudaStream_t)stream;
     cudaMemsetAsync(b->work.p, 0, sizeof(int), s);
     rc = launch_trace_multi(b->bvh8, d_rays, n, d_ray_offsets, b->d_tri_off.p, b->num_scenes, nullptr, d_occ,
-                            b->work.p, b->status.p, b->ctas_per_sm, b->node_iters, s);
+                            b->work.p, b->status.p, b->tune, s);
     return rc;
 }
 
@@ -181,7 +190,7 @@ int rtBatch_traceGraph(RtBatch_t b, const RtRay* d_rays, const int* d_ray_offset
     if (rc != RT_OK || n == 0) return rc;
     cudaStream_t s = (cudaStream_t)stream;
     const bool same = b->gexec && b->g_rays == d_rays && b->g_off == d_ray_offsets && b->g_out == d_out &&
-                      b->g_n == n && b->g_any == any && b->g_ctas == b->ctas_per_sm && b->g_iters == b->node_iters;
+                      b->g_n == n && b->g_any == any && memcmp(&b->g_tune, &b->tune, sizeof(RtBatchTuning)) == 0;
     if (!same) {
         if (b->gexec) {
             cudaGraphExecDestroy(b->gexec);
@@ -194,7 +203,7 @@ int rtBatch_traceGraph(RtBatch_t b, const RtRay* d_rays, const int* d_ray_offset
         cudaMemsetAsync(b->work.p + 1, 0, sizeof(int), b->cap_stream);
         const int lrc = launch_trace_multi(b->bvh8, d_rays, n, d_ray_offsets, b->d_tri_off.p, b->num_scenes,
                                            any ? nullptr : (RtHit*)d_out, any ? (uint8_t*)d_out : nullptr,
-                                           b->work.p + 1, b->status.p, b->ctas_per_sm, b->node_iters, b->cap_stream);
+                                           b->work.p + 1, b->status.p, b->tune, b->cap_stream);
         const bool ended = RT_CUDA(cudaStreamEndCapture(b->cap_stream, &g));
         if (lrc != RT_OK || !ended) {
             if (g) cudaGraphDestroy(g);
@@ -208,8 +217,7 @@ int rtBatch_traceGraph(RtBatch_t b, const RtRay* d_rays, const int* d_ray_offset
         b->g_out = d_out;
         b->g_n = n;
         b->g_any = any;
-        b->g_ctas = b->ctas_per_sm;
-        b->g_iters = b->node_iters;
+        b->g_tune = b->tune;
     }
     return RT_CUDA(cudaGraphLaunch(b->gexec, s)) ? RT_OK : RT_ERR_CUDA;
 }
@@ -221,51 +229,79 @@ int rtBatch_autotune(RtBatch_t b, const RtRay* d_rays, const int* d_ray_offsets,
     if (n > 0 && !tune_from_cache(b, n)) {
         cudaStream_t s = (cudaStream_t)stream;
         cudaEvent_t e0, e1;
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
-        float best = 1e30f;
-        int bc = b->ctas_per_sm, bi = b->node_iters;
-        const int cands[] = {2, 4, 6, TRACE_MINB};
-        for (int c : cands) {
-            for (int it = 1; it <= 2; it++) {
-                b->ctas_per_sm = c;
-                b->node_iters = it;
-                rtBatch_traceClosest(b, d_rays, d_ray_offsets, n, d_hits, stream);  // warm
+        if (!RT_CUDA(cudaEventCreate(&e0)) || !RT_CUDA(cudaEventCreate(&e1))) return RT_ERR_CUDA;
+        // median of three timed launches after a warm one
+        auto time_shape = [&](const RtBatchTuning& t, float& ms_out) -> int {
+            b->tune = t;
+            int r = rtBatch_traceClosest(b, d_rays, d_ray_offsets, n, d_hits, stream);
+            float ms[3];
+            for (int k = 0; k < 3 && r == RT_OK; k++) {
                 cudaEventRecord(e0, s);
-                for (int k = 0; k < 3; k++) rtBatch_traceClosest(b, d_rays, d_ray_offsets, n, d_hits, stream);
+                r = rtBatch_traceClosest(b, d_rays, d_ray_offsets, n, d_hits, stream);
                 cudaEventRecord(e1, s);
-                if (!RT_CUDA(cudaEventSynchronize(e1))) {
-                    cudaEventDestroy(e0);
-                    cudaEventDestroy(e1);
-                    return RT_ERR_CUDA;
-                }
+                if (r == RT_OK && (!RT_CUDA(cudaEventSynchronize(e1)) || !RT_CUDA(cudaEventElapsedTime(&ms[k], e0, e1))))
+                    r = RT_ERR_CUDA;
+            }
+            if (r == RT_OK) ms_out = std::max(std::min(ms[0], ms[1]), std::min(std::max(ms[0], ms[1]), ms[2]));
+            return r;
+        };
+        RtBatchTuning best = b->tune;
+        float best_ms = 1e30f;
+        rc = time_shape(best, best_ms);
+        const int warps[] = {8, 16, 24, 32}, iters[] = {2, 3, 4}, blocks[] = {64, 128, 256}, stacks[] = {4, 8, 12};
+        for (int dim = 0; dim < 4 && rc == RT_OK; dim++) {
+            const int* vals = dim == 0 ? warps : dim == 1 ? iters : dim == 2 ? blocks : stacks;
+            const int nv = dim == 0 ? 4 : 3;
+            for (int i = 0; i < nv && rc == RT_OK; i++) {
+                RtBatchTuning t = best;
+                int& f = dim == 0 ? t.warps_per_sm : dim == 1 ? t.node_iters : dim == 2 ? t.block : t.shared_stack;
+                if (f == vals[i]) continue;
+                f = vals[i];
+                if (dim == 1 && t.node_iters == 3 && (t.block != 128 || t.shared_stack != 8)) continue;
                 float ms = 0.f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (ms < best) {
-                    best = ms;
-                    bc = c;
-                    bi = it;
+                rc = time_shape(t, ms);
+                if (rc == RT_OK && ms < best_ms) {
+                    best_ms = ms;
+                    best = t;
                 }
             }
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        b->ctas_per_sm = bc;
-        b->node_iters = bi;
+        b->tune = best;
+        if (rc != RT_OK) return rc;
         tune_to_cache(b, n);
     }
-    if (out_ctas_per_sm) *out_ctas_per_sm = b->ctas_per_sm;
-    if (out_node_iters) *out_node_iters = b->node_iters;
+    if (out_ctas_per_sm) *out_ctas_per_sm = std::max(1, b->tune.warps_per_sm * 32 / TRACE_T);
+    if (out_node_iters) *out_node_iters = b->tune.node_iters;
     return RT_OK;
 }
 
 int rtBatch_setTuning(RtBatch_t b, int ctas_per_sm, int node_iters) {
-    if (!b || ctas_per_sm < 1 || ctas_per_sm > TRACE_MINB || node_iters < 1 || node_iters > 2) {
+    if (!b || ctas_per_sm < 1 || ctas_per_sm > TRACE_MINB || node_iters < 1 || node_iters > 4) {
         set_error("rtBatch_setTuning: invalid argument");
         return RT_ERR_INVALID;
     }
-    b->ctas_per_sm = ctas_per_sm;
-    b->node_iters = node_iters;
+    b->tune.warps_per_sm = ctas_per_sm * TRACE_T / 32;
+    b->tune.node_iters = node_iters;
+    return RT_OK;
+}
+
+int rtBatch_setTuningEx(RtBatch_t b, const RtBatchTuning* t) {
+    if (!b || !t || !valid_tuning(*t)) {
+        set_error("rtBatch_setTuningEx: invalid argument");
+        return RT_ERR_INVALID;
+    }
+    b->tune = *t;
+    return RT_OK;
+}
+
+int rtBatch_getTuning(RtBatch_t b, RtBatchTuning* out) {
+    if (!b || !out) {
+        set_error("rtBatch_getTuning: invalid argument");
+        return RT_ERR_INVALID;
+    }
+    *out = b->tune;
     return RT_OK;
 }
 

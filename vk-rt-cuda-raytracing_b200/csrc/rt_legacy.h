@@ -21,9 +21,11 @@ void launch_shade(const RtRay* rays, const RtHit* hits, const float* tris9, int 
 struct Bvh8Device;
 int launch_trace_blas(const Bvh8Device& b, const RtRay* rays, int n, RtHit* hits, uint8_t* occ,
                       uint32_t* counts, int* work, int* status, cudaStream_t s);
+// Launch shape of the batched trace (the autotuner's choice).
+using BatchShape = RtBatchTuning;
 int launch_trace_multi(const Bvh8Device& b, const RtRay* rays, int n, const int* ray_off, const int* tri_off,
-                       int nscenes, RtHit* hits, uint8_t* occ, int* work, int* status, int ctas_per_sm,
-                       int node_iters, cudaStream_t s);
+                       int nscenes, RtHit* hits, uint8_t* occ, int* work, int* status, const BatchShape& shape,
+                       cudaStream_t s);
 
 // A shared-wavefront segment: rays [first, next.first) of the launch are
 // rays[0 ..] of this segment, traced from arena node `root`, results to out.

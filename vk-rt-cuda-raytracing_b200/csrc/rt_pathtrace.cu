@@ -26,6 +26,7 @@
 // geometric quantities (rays, hit points, normals, light points, RR
 // probability) use explicitly rounded fp32 operations, so the oracle's paths
 // are the same paths; only radiance differs (fp32 here, fp64 there).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -81,12 +82,14 @@ __device__ __forceinline__ int warp_append(bool want, int* counter) {
     return want ? base + __popc(m & ((1u << lane) - 1)) : -1;
 }
 
-__global__ void k_pt_generate(PtCam c, int W, int H, int spp, uint32_t seed, RtRay* __restrict__ rays,
-                              int* __restrict__ pid, float4* __restrict__ tp, float4* __restrict__ L,
-                              int* __restrict__ count) {
-    const int64_t path = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t P = (int64_t)W * H * spp;
-    if (path >= P) return;
+// Camera paths p0 .. p0 + np - 1 (path = pixel * spp + sample) into queue
+// slots 0 .. np - 1; throughput and radiance are indexed by path.
+__global__ void k_pt_generate(PtCam c, int W, int H, int spp, uint32_t seed, int64_t p0, int np,
+                              RtRay* __restrict__ rays, int* __restrict__ pid, float4* __restrict__ tp,
+                              float4* __restrict__ L, int* __restrict__ count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    const int64_t path = p0 + i;
     const uint32_t pixel = (uint32_t)(path / spp), s = (uint32_t)(path % spp);
     const uint32_t px = pixel % W, py = pixel / W;
     const uint4 rr = pt_rand(pixel, s, 0, 0, seed);
@@ -100,11 +103,17 @@ __global__ void k_pt_generate(PtCam c, int W, int H, int spp, uint32_t seed, RtR
     RtRay r;
     r.org[0] = c.eye[0]; r.org[1] = c.eye[1]; r.org[2] = c.eye[2]; r.tmin = 0.f;
     r.dir[0] = dv(dx, len); r.dir[1] = dv(dy, len); r.dir[2] = dv(dz, len); r.tmax = 1e30f;
-    rays[path] = r;
-    pid[path] = (int)path;
+    rays[i] = r;
+    pid[i] = (int)path;
     tp[path] = make_float4(1.f, 1.f, 1.f, 0.f);
     L[path] = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (path == 0) *count = (int)P;
+    if (i == 0) *count = np;
+}
+
+// Per-bounce ray counts of one slice added to the frame's totals.
+__global__ void k_pt_count(const int* __restrict__ ext, const int* __restrict__ shadow, int* __restrict__ acc2) {
+    acc2[0] += *ext;
+    acc2[1] += *shadow;
 }
 
 // Shading waits on scattered loads (hit triangles, instances, lights): 6
@@ -328,8 +337,10 @@ struct RtPathTracerHandle {
     int num_lights = 0;
     unsigned long long total_q = 0;
     double light_area = 0.0;
-    // per-render buffers
-    int64_t cap = 0;
+    // per-render buffers: queues for `cap` paths (a slice of the frame), per-path
+    // throughput and radiance for `cap_paths` (the whole frame)
+    int64_t cap = 0, cap_paths = 0;
+    int64_t queue_paths = 0;  // rtPT_setQueueCapacity: paths per slice, 0 = the whole frame
     DevBuf<RtRay> rays[2], srays;
     DevBuf<int> pid[2], spid, counts;
     DevBuf<RtHit> hits;
@@ -514,6 +525,54 @@ RtPathTracer_t rtPT_create(CudaTLAS_t tlas, const RtMaterial* mats, int nmat, co
     return pt;
 }
 
+int rtPT_setQueueCapacity(RtPathTracer_t pt, int64_t paths) {
+    if (!pt || paths < 0) {
+        set_error("rtPT_setQueueCapacity: invalid argument");
+        return RT_ERR_INVALID;
+    }
+    pt->queue_paths = paths;
+    return RT_OK;
+}
+
+int rtPT_autotune(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* prm, float* d_rgb, void* stream,
+                  int64_t* out_paths) {
+    if (!pt || !cam || !prm || !d_rgb || prm->width <= 0 || prm->height <= 0 || prm->spp <= 0) {
+        set_error("rtPT_autotune: invalid argument");
+        return RT_ERR_INVALID;
+    }
+    const int64_t P = (int64_t)prm->width * prm->height * prm->spp;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (!RT_CUDA(cudaEventCreate(&e0)) || !RT_CUDA(cudaEventCreate(&e1))) return RT_ERR_CUDA;
+    int64_t best_q = 0;
+    float best = 1e30f;
+    int rc = RT_OK;
+    // the whole frame, then slices of 1/2, 1/4 and 1/8 of it (whole pixels)
+    for (int div : {1, 2, 4, 8}) {
+        const int64_t q = div == 1 ? 0 : ((P / div + prm->spp - 1) / prm->spp) * prm->spp;
+        if (div > 1 && q < (int64_t)num_sms() * 4096) break;  // too small a slice to fill the GPU
+        pt->queue_paths = q;
+        if ((rc = rtPT_render(pt, cam, prm, d_rgb, stream)) != RT_OK) break;  // warm (allocates)
+        if (!RT_CUDA(cudaEventRecord(e0, s))) { rc = RT_ERR_CUDA; break; }
+        if ((rc = rtPT_render(pt, cam, prm, d_rgb, stream)) != RT_OK) break;
+        float ms = 0.f;
+        if (!RT_CUDA(cudaEventRecord(e1, s)) || !RT_CUDA(cudaEventSynchronize(e1)) ||
+            !RT_CUDA(cudaEventElapsedTime(&ms, e0, e1))) {
+            rc = RT_ERR_CUDA;
+            break;
+        }
+        if (ms < best) {
+            best = ms;
+            best_q = q;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    pt->queue_paths = best_q;
+    if (out_paths) *out_paths = best_q;
+    return rc;
+}
+
 int rtPT_setRegroup(RtPathTracer_t pt, int kind, int key_bits) {
     if (!pt || (key_bits != 0 && key_bits != 16 && key_bits != 32) ||
         (kind != RT_REGROUP_MORTON && kind != RT_REGROUP_OCTANT_MORTON)) {
@@ -560,12 +619,18 @@ int rtPT_render(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* prm, f
         return RT_ERR_CAPACITY;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    if (P > pt->cap) {
-        const bool ok = pt->rays[0].alloc(P) && pt->rays[1].alloc(P) && pt->srays.alloc(P) && pt->pid[0].alloc(P) &&
-                        pt->pid[1].alloc(P) && pt->spid.alloc(P) && pt->hits.alloc(P) && pt->hinst.alloc(P) &&
-                        pt->tp.alloc(P) && pt->L.alloc(P) && pt->scontrib.alloc(P) && pt->socc.alloc(P);
+    // queues hold one slice of Q paths; the frame is traced slice after slice
+    const int64_t Q = pt->queue_paths > 0 ? std::min(pt->queue_paths, P) : P;
+    if (P > pt->cap_paths) {
+        if (!pt->tp.alloc(P) || !pt->L.alloc(P)) return RT_ERR_NOMEM;
+        pt->cap_paths = P;
+    }
+    if (Q > pt->cap) {
+        const bool ok = pt->rays[0].alloc(Q) && pt->rays[1].alloc(Q) && pt->srays.alloc(Q) && pt->pid[0].alloc(Q) &&
+                        pt->pid[1].alloc(Q) && pt->spid.alloc(Q) && pt->hits.alloc(Q) && pt->hinst.alloc(Q) &&
+                        pt->scontrib.alloc(Q) && pt->socc.alloc(Q);
         if (!ok) return RT_ERR_NOMEM;
-        pt->cap = P;
+        pt->cap = Q;
         pt->rays_sorted.release();
         pt->pid_sorted.release();
     }
@@ -584,43 +649,45 @@ int rtPT_render(RtPathTracer_t pt, const RtCamera* cam, const RtPTParams* prm, f
     const PtCam c = make_cam(*cam, prm->width, prm->height);
     int* cnt = pt->counts.p;  // [0],[1]: ray queues, [2]: shadow queue
     cudaMemsetAsync(pt->bcounts.p, 0, sizeof(int) * 2 * kMaxBounces, s);
-    k_pt_generate<<<(unsigned)((P + 255) / 256), 256, 0, s>>>(c, prm->width, prm->height, prm->spp, prm->seed,
-                                                             pt->rays[0].p, pt->pid[0].p, pt->tp.p, pt->L.p, cnt);
-    int cur = 0;
     const int shade_blocks = num_sms() * 8;
-    for (int b = 0; b < prm->max_bounces; b++) {
-        const int nxt = cur ^ 1;
-        k_zero2<<<1, 1, 0, s>>>(cnt + nxt, cnt + 2);
-        int* w1 = pt->work.p + (pt->work_next++ % 1024);
-        cudaMemsetAsync(w1, 0, sizeof(int), s);
-        // bounce rays leave scattered surface points in all directions: regroup
-        // them (direction octant, origin Morton code) before the extension trace;
-        // camera rays (bounce 0) are already in pixel order
-        RtRay* qrays = pt->rays[cur].p;
-        int* qpid = pt->pid[cur].p;
-        if (pt->regroup_bits && b > 0) {
-            if (!regroup_rays(qrays, qpid, (int)pt->cap, cnt + cur, 0, pt->world_box, pt->regroup_kind,
-                              pt->regroup_bits, pt->rays_sorted.p, pt->pid_sorted.p, nullptr, s))
+    for (int64_t p0 = 0; p0 < P; p0 += Q) {
+        const int np = (int)std::min(Q, P - p0);
+        k_pt_generate<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(c, prm->width, prm->height, prm->spp, prm->seed, p0,
+                                                                  np, pt->rays[0].p, pt->pid[0].p, pt->tp.p, pt->L.p, cnt);
+        int cur = 0;
+        for (int b = 0; b < prm->max_bounces; b++) {
+            const int nxt = cur ^ 1;
+            k_zero2<<<1, 1, 0, s>>>(cnt + nxt, cnt + 2);
+            int* w1 = pt->work.p + (pt->work_next++ % 1024);
+            cudaMemsetAsync(w1, 0, sizeof(int), s);
+            // bounce rays leave scattered surface points in all directions: regroup
+            // them (direction octant, origin Morton code) before the extension trace;
+            // camera rays (bounce 0) are already in pixel order
+            RtRay* qrays = pt->rays[cur].p;
+            int* qpid = pt->pid[cur].p;
+            if (pt->regroup_bits && b > 0) {
+                if (!regroup_rays(qrays, qpid, (int)pt->cap, cnt + cur, 0, pt->world_box, pt->regroup_kind,
+                                  pt->regroup_bits, pt->rays_sorted.p, pt->pid_sorted.p, nullptr, s))
+                    return RT_ERR_CUDA;
+                qrays = pt->rays_sorted.p;
+                qpid = pt->pid_sorted.p;
+            }
+            if (launch_trace_tlas(t, qrays, 0, cnt + cur, pt->hits.p, pt->hinst.p, nullptr, w1, t->status.p, s) != RT_OK)
                 return RT_ERR_CUDA;
-            qrays = pt->rays_sorted.p;
-            qpid = pt->pid_sorted.p;
+            k_pt_shade<<<num_sms() * RTB_SHADE_MINB, PT_T, 0, s>>>(sc, prm->spp, b, prm->max_bounces, prm->rr_start, prm->seed,
+                                                     cnt + cur, qrays, qpid, pt->hits.p,
+                                                     pt->hinst.p, pt->tp.p, pt->L.p, pt->rays[nxt].p, pt->pid[nxt].p,
+                                                     cnt + nxt, pt->srays.p, pt->spid.p, pt->scontrib.p, cnt + 2);
+            int* w2 = pt->work.p + (pt->work_next++ % 1024);
+            cudaMemsetAsync(w2, 0, sizeof(int), s);
+            if (launch_trace_tlas(t, pt->srays.p, 0, cnt + 2, nullptr, nullptr, pt->socc.p, w2, t->status.p, s) != RT_OK)
+                return RT_ERR_CUDA;
+            k_pt_accum<<<shade_blocks, 256, 0, s>>>(cnt + 2, pt->spid.p, pt->scontrib.p, pt->socc.p, pt->L.p);
+            // ray counts of this bounce for the statistics
+            k_pt_count<<<1, 1, 0, s>>>(cnt + cur, cnt + 2, pt->bcounts.p + 2 * b);
+            cur = nxt;
         }
-        if (launch_trace_tlas(t, qrays, 0, cnt + cur, pt->hits.p, pt->hinst.p, nullptr, w1, t->status.p, s) != RT_OK)
-            return RT_ERR_CUDA;
-        k_pt_shade<<<num_sms() * RTB_SHADE_MINB, PT_T, 0, s>>>(sc, prm->spp, b, prm->max_bounces, prm->rr_start, prm->seed,
-                                                 cnt + cur, qrays, qpid, pt->hits.p,
-                                                 pt->hinst.p, pt->tp.p, pt->L.p, pt->rays[nxt].p, pt->pid[nxt].p,
-                                                 cnt + nxt, pt->srays.p, pt->spid.p, pt->scontrib.p, cnt + 2);
-        int* w2 = pt->work.p + (pt->work_next++ % 1024);
-        cudaMemsetAsync(w2, 0, sizeof(int), s);
-        if (launch_trace_tlas(t, pt->srays.p, 0, cnt + 2, nullptr, nullptr, pt->socc.p, w2, t->status.p, s) != RT_OK)
-            return RT_ERR_CUDA;
-        k_pt_accum<<<shade_blocks, 256, 0, s>>>(cnt + 2, pt->spid.p, pt->scontrib.p, pt->socc.p, pt->L.p);
-        // ray counts of this bounce for the statistics
-        cudaMemcpyAsync(pt->bcounts.p + 2 * b, cnt + cur, sizeof(int), cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(pt->bcounts.p + 2 * b + 1, cnt + 2, sizeof(int), cudaMemcpyDeviceToDevice, s);
-        cur = nxt;
-    }
+    }  // slices
     const int pixels = prm->width * prm->height;
     k_pt_finalize<<<(pixels + 255) / 256, 256, 0, s>>>(pt->L.p, pixels, prm->spp, d_rgb);
     return RT_CUDA(cudaGetLastError()) ? RT_OK : RT_ERR_CUDA;

@@ -60,6 +60,18 @@ __device__ __forceinline__ InstView load_inst(const float4* __restrict__ inst, i
 #ifndef RTB_TLAS_MINB
 #define RTB_TLAS_MINB 7
 #endif
+// Steps per lane per iteration of this kernel (a step is a node visit or
+// entering an instance) and its node test's slot-mask mode (RTB_SLOTMASK in
+// rt_trace.cuh), tuned apart from the single-level kernel on the path
+// tracer (1080p x 8 spp, 5M triangles): 2 steps 1,323 Mrays/s, 3: 1,393,
+// 4: 1,466, 6: 1,503; with the meta-byte table (mode 2) 3: 1,425, 4: 1,495,
+// 6: 1,527.
+#ifndef RTB_TLAS_ITERS
+#define RTB_TLAS_ITERS 6
+#endif
+#ifndef RTB_TLAS_SLOTMASK
+#define RTB_TLAS_SLOTMASK 2
+#endif
 template <bool ANY>
 __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
     k_trace_tlas(const uint4* __restrict__ tnodes, const int* __restrict__ leaf_ids, const float4* __restrict__ inst,
@@ -70,7 +82,7 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
     __shared__ unsigned long long s_key[TRACE_T];
     __shared__ int s_rec[TRACE_T];
     __shared__ int4 s_res[TRACE_T];  // u, v bits, instance, primitive of the improved best
-#if RTB_SLOTMASK
+#if RTB_TLAS_SLOTMASK
     __shared__ NodeLuts s_luts;
     init_node_luts(&s_luts);
     const NodeLuts* s_oct_perm = &s_luts;
@@ -124,7 +136,7 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
         uint32_t tri_base = 0, tmask = 0;
         bool overflow = false;
 #pragma unroll 1
-        for (int it = 0; it < RTB_NODE_ITERS; it++) {
+        for (int it = 0; it < RTB_TLAS_ITERS; it++) {
             if (ray < 0 || tmask || overflow) break;
             if (w.ng.y & G_INST) {
                 // enter the next instance of an instance group
@@ -161,7 +173,8 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
                 break;
             }
             uint32_t nh, tb, tm;
-            visit_node((top ? tnodes : bnodes) + (size_t)ni * 5, cr, thit, nh, tb, tm, w.ng, s_oct_perm);
+            visit_node<RTB_TLAS_SLOTMASK>((top ? tnodes : bnodes) + (size_t)ni * 5, cr, thit, nh, tb, tm, w.ng,
+                                          s_oct_perm);
             if (top) {
                 w.ng.y |= G_TOP;
                 if (tm) {

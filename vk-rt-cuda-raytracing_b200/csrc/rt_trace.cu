@@ -80,18 +80,21 @@ __device__ __forceinline__ void* ldg_ptr(const void* p) {
 //   against scenes resident in one arena); ray i belongs to the last segment
 //   g with segs[g].first <= i, is read from segs[g].rays[i - first], starts
 //   at node segs[g].root and is written to segs[g].out[i - first].
-template <bool ANY, bool COUNT, int MODE, int NITERS>
-__global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
+// T threads per CTA and SS shared stack entries per thread are template
+// parameters so the batched form's autotuner can choose them; the CTA count
+// the register budget must allow scales with T (the same 64 registers).
+template <bool ANY, bool COUNT, int MODE, int NITERS, int T = TRACE_T, int SS = SSTACK>
+__global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE_T / T)
     k_trace_blas(const uint4* __restrict__ nodes, const float4* __restrict__ tris, const RtRay* __restrict__ rays,
                  int n, RtHit* __restrict__ hits, uint8_t* __restrict__ occ, uint32_t* __restrict__ counts,
                  int* __restrict__ work, int* __restrict__ status, const int* __restrict__ ray_off,
                  const int* __restrict__ tri_off, int nscenes, const WaveSeg* __restrict__ segs) {
-    __shared__ uint2 sstack[SSTACK][TRACE_T];
-    __shared__ unsigned long long s_key[TRACE_T];  // owner's best (ordered t, prim)
-    __shared__ int s_rec[TRACE_T];                 // set when a worker improved it (any hit: found)
-    __shared__ float2 s_uv[TRACE_T];               // barycentrics of the improved best
+    __shared__ uint2 sstack[SS][T];
+    __shared__ unsigned long long s_key[T];  // owner's best (ordered t, prim)
+    __shared__ int s_rec[T];                 // set when a worker improved it (any hit: found)
+    __shared__ float2 s_uv[T];               // barycentrics of the improved best
 #if RTB_RAY_SMEM
-    __shared__ float4 s_ray[2][TRACE_T];           // each lane's ray, read by the lanes testing its triangles
+    __shared__ float4 s_ray[2][T];           // each lane's ray, read by the lanes testing its triangles
 #endif
 #if RTB_SLOTMASK
     __shared__ NodeLuts s_luts;
@@ -100,13 +103,13 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
 #else
     const NodeLuts* s_oct_perm = nullptr;
 #endif
-    uint2 lstack[LSTACK];
+    uint2 lstack[WalkT<T, SS>::L];
     const int lane = threadIdx.x & 31;
     const int wbase = threadIdx.x & ~31;
     int ray = -1;
     bool exhausted = false;
     Ray r;
-    Walk w;
+    WalkT<T, SS> w;
     float thit = 0.f, hu = 0.f, hv = 0.f;
     int hprim = -1;
     int prim_base = 0;
@@ -116,7 +119,7 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
         // ---- refill idle lanes ----
         const bool need = ray < 0 && !exhausted;
         const unsigned want = __ballot_sync(FULL_MASK, need);
-        RTB_STAT(10, __popc(want));
+        RTB_STAT(15, __popc(want));
         if (want) {
             const int leader = __ffs(want) - 1;
             int base = 0;
@@ -176,13 +179,20 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
 #else
         constexpr uint32_t tmask2 = 0;
 #endif
+#if RTB_THREE_SETS
+        uint32_t tri_base3 = 0, tmask3 = 0;  // and a third (RTB_THREE_SETS)
+#define RTB_LAST_SET tmask3
+#else
+        constexpr uint32_t tmask3 = 0;
+#define RTB_LAST_SET tmask2
+#endif
         bool overflow = false;
 #pragma unroll 1
         for (int it = 0; it < NITERS; it++) {
 #if RTB_STATS
             {
 #if RTB_TWO_SETS
-                const bool visit = ray >= 0 && tmask2 == 0 && !overflow && (w.ng.y & 0xFFu);
+                const bool visit = ray >= 0 && RTB_LAST_SET == 0 && !overflow && (w.ng.y & 0xFFu);
 #else
                 const bool visit = ray >= 0 && tmask == 0 && !overflow && (w.ng.y & 0xFFu);
 #endif
@@ -192,7 +202,12 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
             }
 #endif
 #if RTB_TWO_SETS
-            if (ray >= 0 && tmask2 == 0 && !overflow && (w.ng.y & 0xFFu)) {
+#if RTB_VISIT_VOTE
+            // later visits only while some lane can still take one
+            if (it > 0 && !__any_sync(FULL_MASK, ray >= 0 && RTB_LAST_SET == 0 && !overflow && (w.ng.y & 0xFFu)))
+                break;
+#endif
+            if (ray >= 0 && RTB_LAST_SET == 0 && !overflow && (w.ng.y & 0xFFu)) {
 #else
             if (ray >= 0 && tmask == 0 && !overflow && (w.ng.y & 0xFFu)) {
 #endif
@@ -211,10 +226,20 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
                 if (tmask == 0) {
                     tri_base = vb;
                     tmask = vm;
+#if RTB_THREE_SETS
+                } else if (tmask2 == 0) {
+                    tri_base2 = vb;
+                    tmask2 = vm;
+                } else {
+                    tri_base3 = vb;
+                    tmask3 = vm;
+                }
+#else
                 } else {
                     tri_base2 = vb;
                     tmask2 = vm;
                 }
+#endif
 #else
                 visit_node(nodes + (size_t)ni * 5, r, thit, nmask, tri_base, tmask, w.ng, s_oct_perm);
 #endif
@@ -241,7 +266,7 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
             }
         }
         // ---- triangle phase: pooled over the warp ----
-        const int cnt = __popc(tmask) + __popc(tmask2);
+        const int cnt = __popc(tmask) + __popc(tmask2) + __popc(tmask3);
         int incl = cnt, total = 0;
         // RTB_TRI_VOTE: one warp vote skips the scan when no lane holds triangles
         if (!RTB_TRI_VOTE || __any_sync(FULL_MASK, tmask != 0)) {
@@ -287,11 +312,25 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB_ANY : TRACE_MINB)
                 const uint32_t om2 = __shfl_sync(FULL_MASK, tmask2, o);
                 const uint32_t ob2 = __shfl_sync(FULL_MASK, tri_base2, o);
                 const int c1 = __popc(om);
+#if RTB_THREE_SETS
+                const uint32_t om3 = __shfl_sync(FULL_MASK, tmask3, o);
+                const uint32_t ob3 = __shfl_sync(FULL_MASK, tri_base3, o);
+                const int c12 = c1 + __popc(om2);
+                const int k = k0 < c1 ? k0 : (k0 < c12 ? k0 - c1 : k0 - c12);
+                if (k0 >= c12) {
+                    om = om3;
+                    ob = ob3;
+                } else if (k0 >= c1) {
+                    om = om2;
+                    ob = ob2;
+                }
+#else
                 const int k = k0 < c1 ? k0 : k0 - c1;
                 if (k0 >= c1) {
                     om = om2;
                     ob = ob2;
                 }
+#endif
 #else
                 const int k = k0;
                 const uint32_t om = __shfl_sync(FULL_MASK, tmask, o);
@@ -434,28 +473,59 @@ int launch_trace_blas(const Bvh8Device& b, const RtRay* rays, int n, RtHit* hits
     return RT_CUDA(cudaGetLastError()) ? RT_OK : RT_ERR_CUDA;
 }
 
-// Many scenes in one persistent launch: ctas_per_sm (1..TRACE_MINB) sets the
-// worker count, node_iters (1 or 2) the node visits per iteration.
+// Many scenes in one persistent launch, in the shape the batched form's
+// autotuner chose: persistent worker warps per SM, node visits per
+// iteration, threads per CTA and shared stack entries per thread.  The
+// instantiated shapes are the tuner's candidates: (block, shared stack) in
+// {(128, 8), (64, 8), (256, 8), (128, 4), (128, 12)}, node visits 2 or 4
+// (3 also at (128, 8)); other values fall back to the nearest (128, 8) one.
+template <bool ANY, int NI, int T, int SS>
+static void launch_batch(int warps_per_sm, const uint4* nodes, const float4* tris, const RtRay* rays, int n,
+                         RtHit* hits, uint8_t* occ, int* work, int* status, const int* ray_off, const int* tri_off,
+                         int nscenes, cudaStream_t s) {
+    const int max_ctas = (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE_T / T;
+    const int ctas = std::max(1, std::min(warps_per_sm * 32 / T, max_ctas));
+    k_trace_blas<ANY, false, MODE_BATCH, NI, T, SS><<<ctas * num_sms(), T, 0, s>>>(
+        nodes, tris, rays, n, hits, occ, nullptr, work, status, ray_off, tri_off, nscenes, nullptr);
+}
+
+template <bool ANY, int NI>
+static void launch_batch_shape(const BatchShape& sh, const uint4* nodes, const float4* tris, const RtRay* rays, int n,
+                               RtHit* hits, uint8_t* occ, int* work, int* status, const int* ray_off,
+                               const int* tri_off, int nscenes, cudaStream_t s) {
+#define RTB_BATCH_ARGS sh.warps_per_sm, nodes, tris, rays, n, hits, occ, work, status, ray_off, tri_off, nscenes, s
+    if (sh.block == 64 && sh.shared_stack == 8) launch_batch<ANY, NI, 64, 8>(RTB_BATCH_ARGS);
+    else if (sh.block == 256 && sh.shared_stack == 8) launch_batch<ANY, NI, 256, 8>(RTB_BATCH_ARGS);
+    else if (sh.block == 128 && sh.shared_stack == 4) launch_batch<ANY, NI, 128, 4>(RTB_BATCH_ARGS);
+    else if (sh.block == 128 && sh.shared_stack == 12) launch_batch<ANY, NI, 128, 12>(RTB_BATCH_ARGS);
+    else launch_batch<ANY, NI, 128, 8>(RTB_BATCH_ARGS);
+#undef RTB_BATCH_ARGS
+}
+
 int launch_trace_multi(const Bvh8Device& b, const RtRay* rays, int n, const int* ray_off, const int* tri_off,
-                       int nscenes, RtHit* hits, uint8_t* occ, int* work, int* status, int ctas_per_sm,
-                       int node_iters, cudaStream_t s) {
+                       int nscenes, RtHit* hits, uint8_t* occ, int* work, int* status, const BatchShape& sh,
+                       cudaStream_t s) {
     const uint4* nodes = reinterpret_cast<const uint4*>(b.nodes.p);
     const float4* tris = reinterpret_cast<const float4*>(b.tris.p);
-    const int g = std::max(1, std::min(ctas_per_sm, occ ? TRACE_MINB_ANY : TRACE_MINB)) * num_sms();
+    const bool base_shape = sh.block == 128 && sh.shared_stack == 8;
     if (occ) {
-        if (node_iters == 1)
-            k_trace_blas<true, false, MODE_BATCH, 1><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
-                                                                    status, ray_off, tri_off, nscenes, nullptr);
+        if (sh.node_iters == 3 && base_shape)
+            launch_batch<true, 3, 128, 8>(sh.warps_per_sm, nodes, tris, rays, n, hits, occ, work, status, ray_off,
+                                          tri_off, nscenes, s);
+        else if (sh.node_iters <= 2)
+            launch_batch_shape<true, 2>(sh, nodes, tris, rays, n, hits, occ, work, status, ray_off, tri_off, nscenes, s);
         else
-            k_trace_blas<true, false, MODE_BATCH, 2><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
-                                                                    status, ray_off, tri_off, nscenes, nullptr);
+            launch_batch_shape<true, 4>(sh, nodes, tris, rays, n, hits, occ, work, status, ray_off, tri_off, nscenes, s);
     } else {
-        if (node_iters == 1)
-            k_trace_blas<false, false, MODE_BATCH, 1><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
-                                                                     status, ray_off, tri_off, nscenes, nullptr);
+        if (sh.node_iters == 3 && base_shape)
+            launch_batch<false, 3, 128, 8>(sh.warps_per_sm, nodes, tris, rays, n, hits, occ, work, status, ray_off,
+                                           tri_off, nscenes, s);
+        else if (sh.node_iters <= 2)
+            launch_batch_shape<false, 2>(sh, nodes, tris, rays, n, hits, occ, work, status, ray_off, tri_off, nscenes,
+                                         s);
         else
-            k_trace_blas<false, false, MODE_BATCH, 2><<<g, TRACE_T, 0, s>>>(nodes, tris, rays, n, hits, occ, nullptr, work,
-                                                                     status, ray_off, tri_off, nscenes, nullptr);
+            launch_batch_shape<false, 4>(sh, nodes, tris, rays, n, hits, occ, work, status, ray_off, tri_off, nscenes,
+                                         s);
     }
     return RT_CUDA(cudaGetLastError()) ? RT_OK : RT_ERR_CUDA;
 }
@@ -465,11 +535,11 @@ int launch_trace_wave(const uint4* nodes, const float4* tris, const WaveSeg* seg
                       int* work, int* status, int ctas_per_sm, cudaStream_t s) {
     const int g = std::max(1, std::min(ctas_per_sm, any ? TRACE_MINB_ANY : TRACE_MINB)) * num_sms();
     if (any)
-        k_trace_blas<true, false, MODE_WAVE, 2><<<g, TRACE_T, 0, s>>>(nodes, tris, nullptr, n, nullptr, nullptr,
+        k_trace_blas<true, false, MODE_WAVE, RTB_NODE_ITERS><<<g, TRACE_T, 0, s>>>(nodes, tris, nullptr, n, nullptr, nullptr,
                                                                      nullptr, work, status, nullptr, nullptr, nseg,
                                                                      segs);
     else
-        k_trace_blas<false, false, MODE_WAVE, 2><<<g, TRACE_T, 0, s>>>(nodes, tris, nullptr, n, nullptr, nullptr,
+        k_trace_blas<false, false, MODE_WAVE, RTB_NODE_ITERS><<<g, TRACE_T, 0, s>>>(nodes, tris, nullptr, n, nullptr, nullptr,
                                                                       nullptr, work, status, nullptr, nullptr, nseg,
                                                                       segs);
     return RT_CUDA(cudaGetLastError()) ? RT_OK : RT_ERR_CUDA;

@@ -8,8 +8,9 @@ namespace rtb {
 constexpr unsigned FULL_MASK = 0xFFFFFFFFu;
 // Build-time knobs of the traversal kernels; the defaults are the measured
 // best on B200 for 2M incoherent rays (64 registers -> 32 warps per SM; two
-// node visits per lane between pooled triangle phases; 3-input min/max; the
-// owner's ray read from shared memory in the triangle phase, +1.4 %).
+// pending triangle sets and four node visits per lane between pooled
+// triangle phases; 3-input min/max; the owner's ray read from shared memory
+// in the triangle phase, +1.4 %).
 // Measured and rejected: L1 prefetch of the next node (-10%), branchless
 // child masks (-2%), folding the bias of an older 2^23 + byte decode into
 // the offsets (0%),
@@ -18,9 +19,11 @@ constexpr unsigned FULL_MASK = 0xFFFFFFFFu;
 #ifndef RTB_TRACE_MINB
 #define RTB_TRACE_MINB 8
 #endif
-// any hit keeps less state: 9 CTAs per SM (56 registers) measured +1.9 %
+// any-hit CTAs per SM: with two pending triangle sets and four node
+// visits, 8 (64 registers, no spills) measured +4.6 % over 9 (56 registers,
+// a few bytes spilled); 9 had been +1.9 % over 8 with one set and 2 visits
 #ifndef RTB_TRACE_MINB_ANY
-#define RTB_TRACE_MINB_ANY 9
+#define RTB_TRACE_MINB_ANY 8
 #endif
 #ifndef RTB_SSTACK
 #define RTB_SSTACK 8
@@ -31,8 +34,12 @@ constexpr unsigned FULL_MASK = 0xFFFFFFFFu;
 #ifndef RTB_BRANCHLESS
 #define RTB_BRANCHLESS 0
 #endif
+// node visits per lane between pooled triangle phases (with two pending
+// triangle sets, RTB_TWO_SETS): 4 measured best on 2M incoherent rays
+// (closest hit +9.5 %, any hit +6.7 % over 2 visits and one set; 3: +8.9 /
+// +4.1 %; 6: +3.5 / +0.7 %)
 #ifndef RTB_NODE_ITERS
-#define RTB_NODE_ITERS 2
+#define RTB_NODE_ITERS 4
 #endif
 #ifndef RTB_MAX3
 #define RTB_MAX3 1
@@ -189,9 +196,20 @@ __device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t k) {
 #define RTB_SLOTMASK 0
 #endif
 // RTB_TWO_SETS: a lane keeps up to two pending triangle sets, so a node
-// visit that finds leaves does not stop the lane's second visit.
+// visit that finds leaves does not stop the lane's next visit (measured
+// +3 % closest and any hit at 2 visits, and what makes more visits pay).
 #ifndef RTB_TWO_SETS
-#define RTB_TWO_SETS 0
+#define RTB_TWO_SETS 1
+#endif
+// RTB_THREE_SETS (with RTB_TWO_SETS): a third pending set.
+#ifndef RTB_THREE_SETS
+#define RTB_THREE_SETS 0
+#endif
+// RTB_VISIT_VOTE (with RTB_TWO_SETS): the node visits after the first stop
+// as soon as no lane of the warp can take one (both sets pending or no node
+// left), so RTB_NODE_ITERS can be a generous cap.
+#ifndef RTB_VISIT_VOTE
+#define RTB_VISIT_VOTE 0
 #endif
 constexpr int OCT_PERM_BYTES = 8 * 256;
 // Lookup tables of the node test in shared memory (RTB_SLOTMASK).
@@ -232,23 +250,30 @@ __device__ __forceinline__ uint32_t bit_mask(uint32_t start, uint32_t width) {
 }
 
 // Stack of node groups: x = child base, y = hit mask (8 bits, near-to-far
-// order) | inner mask << 8 | flags << 16.
-struct Walk {
+// order) | inner mask << 8 | flags << 16.  The top SS entries sit in shared
+// memory (one column per thread of a T-thread CTA), the rest of the
+// RTB_STACK_TOTAL entries in local memory.
+template <int T, int SS>
+struct WalkT {
+    // shared entries used: SS, or fewer when the whole stack is smaller
+    static constexpr int S = SS < RTB_STACK_TOTAL ? SS : RTB_STACK_TOTAL - 1;
+    static constexpr int L = RTB_STACK_TOTAL - S;
     uint2 ng;
     int sp;
     __device__ __forceinline__ void start() { sp = 0; }
-    __device__ __forceinline__ bool push(uint2 e, uint2 (*ss)[TRACE_T], uint2* ls) {
-        if (sp < SSTACK) ss[sp][threadIdx.x] = e;
-        else if (sp < SSTACK + LSTACK) ls[sp - SSTACK] = e;
+    __device__ __forceinline__ bool push(uint2 e, uint2 (*ss)[T], uint2* ls) {
+        if (sp < S) ss[sp][threadIdx.x] = e;
+        else if (sp < S + L) ls[sp - S] = e;
         else return false;
         sp++;
         return true;
     }
-    __device__ __forceinline__ uint2 pop(uint2 (*ss)[TRACE_T], uint2* ls) {
+    __device__ __forceinline__ uint2 pop(uint2 (*ss)[T], uint2* ls) {
         sp--;
-        return sp < SSTACK ? ss[sp][threadIdx.x] : ls[sp - SSTACK];
+        return sp < S ? ss[sp][threadIdx.x] : ls[sp - S];
     }
 };
+using Walk = WalkT<TRACE_T, SSTACK>;
 
 // Byte k of w as an exact float.  Written as a plain shift, mask and
 // conversion, which measured +3 % (closest hit) and +5 % (any hit) over
@@ -303,6 +328,7 @@ __device__ __forceinline__ void prefetch_next(const uint4* nodes, uint2 ng, uint
 // Fetches one 8-wide node and tests its eight child boxes against the ray
 // segment [tmin, thit].  Outputs the node group of hit inner children
 // (`ng`), and the triangle base + 32-bit mask of hit leaf triangles.
+template <int SLOT = RTB_SLOTMASK>
 __device__ __forceinline__ void visit_node(const uint4* __restrict__ np, const Ray& r, float thit,
                                            uint32_t& inner_hits, uint32_t& tri_base, uint32_t& tmask, uint2& ng,
                                            const NodeLuts* __restrict__ luts = nullptr) {
@@ -340,9 +366,7 @@ __device__ __forceinline__ void visit_node(const uint4* __restrict__ np, const R
     const uint32_t qny0 = ny ? w3.z : w3.x, qny1 = ny ? w3.w : w3.y, qfy0 = ny ? w3.x : w3.z, qfy1 = ny ? w3.y : w3.w;
     const uint32_t qnz0 = nz ? w4.z : w4.x, qnz1 = nz ? w4.w : w4.y, qfz0 = nz ? w4.x : w4.z, qfz1 = nz ? w4.y : w4.w;
     uint32_t nh = 0, th = 0;
-#if RTB_SLOTMASK
-    uint32_t hm = 0;  // hit children in slot order
-#endif
+    uint32_t hm = 0;  // SLOT != 0: hit children in slot order
 #pragma unroll
     for (int s = 0; s < 8; s++) {
         const int sh = (s & 3) * 8;
@@ -358,22 +382,23 @@ __device__ __forceinline__ void visit_node(const uint4* __restrict__ np, const R
         const float tn = max3f(tnx, tny, fmaxf(tnz, r.tmin));
         const float tf = min3f(tfx, tfy, fminf(tfz, thit));
         const bool hit = tn <= fmaf(fabsf(tf), 0x1p-21f, tf);
-#if RTB_SLOTMASK == 1
-        // leaf run from the meta byte (count << 5 | offset); inner slots (meta
-        // 0xFF) are excluded by the inner bit, empty slots have count 0
-        const uint32_t mw = s < 4 ? w1.z : w1.w;
-        const uint32_t run = bit_mask_wrap(mw >> sh, (mw >> (sh + 5)) & 7u);
-        if (hit) hm |= 1u << s;
-        if (hit && !((imask >> s) & 1u)) th |= run;
-        continue;
-#elif RTB_SLOTMASK == 2
-        const uint32_t mw = s < 4 ? w1.z : w1.w;
-        if (hit) {
-            hm |= 1u << s;
-            th |= luts->meta_run[(mw >> sh) & 0xFFu];
+        if (SLOT == 1) {
+            // leaf run from the meta byte (count << 5 | offset); inner slots
+            // (meta 0xFF) are excluded by the inner bit, empty slots have count 0
+            const uint32_t mw = s < 4 ? w1.z : w1.w;
+            const uint32_t run = bit_mask_wrap(mw >> sh, (mw >> (sh + 5)) & 7u);
+            if (hit) hm |= 1u << s;
+            if (hit && !((imask >> s) & 1u)) th |= run;
+            continue;
         }
-        continue;
-#endif
+        if (SLOT == 2) {
+            const uint32_t mw = s < 4 ? w1.z : w1.w;
+            if (hit) {
+                hm |= 1u << s;
+                th |= luts->meta_run[(mw >> sh) & 0xFFu];
+            }
+            continue;
+        }
         const uint32_t meta = ((s < 4 ? w1.z : w1.w) >> sh) & 0xFFu;
 #if RTB_BRANCHLESS
         const uint32_t inner = (imask >> s) & 1u;
@@ -390,9 +415,7 @@ __device__ __forceinline__ void visit_node(const uint4* __restrict__ np, const R
         }
 #endif
     }
-#if RTB_SLOTMASK
-    nh = luts->oct_perm[(r.oct << 8) | (hm & imask)];
-#endif
+    if (SLOT) nh = luts->oct_perm[(r.oct << 8) | (hm & imask)];
     inner_hits = nh;
     tri_base = w1.y;
     tmask = th;

@@ -74,6 +74,10 @@ class RtPTStats(C.Structure):
                 ("light_area", C.c_double)]
 
 
+class RtBatchTuning(C.Structure):
+    _fields_ = [("warps_per_sm", C.c_int), ("node_iters", C.c_int), ("block", C.c_int), ("shared_stack", C.c_int)]
+
+
 class RtGeometry(C.Structure):
     _fields_ = [("d_vertices", C.c_void_p), ("vertex_stride", C.c_uint64), ("vertex_format", C.c_int),
                 ("max_vertex", C.c_int), ("d_indices", C.c_void_p), ("index_type", C.c_int),
@@ -138,6 +142,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "cudaBVH_generateRays": (i32, [vp, vp, vp, i32, C.POINTER(RtRayGen), vp, vp, vp, vp]),
         "rtRays_regroup": (i32, [vp, i32, vp, i32, i32, vp, vp, vp]),
         "rtPT_setRegroup": (i32, [vp, i32, i32]),
+        "rtPT_setQueueCapacity": (i32, [vp, C.c_int64]),
+        "rtPT_autotune": (i32, [vp, C.POINTER(RtCamera), C.POINTER(RtPTParams), vp, vp, C.POINTER(C.c_int64)]),
         "rtDebug_failAllocations": (i32, [i32]),
         "rtProbe_readBandwidth": (i32, [C.c_uint64, i32, C.POINTER(f32)]),
         "cudaBVH_validate": (i32, [vp]),
@@ -175,6 +181,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "rtBatch_traceGraph": (i32, [vp, vp, vp, i32, vp, i32, vp]),
         "rtBatch_autotune": (i32, [vp, vp, vp, i32, vp, vp, C.POINTER(i32), C.POINTER(i32)]),
         "rtBatch_setTuning": (i32, [vp, i32, i32]),
+        "rtBatch_setTuningEx": (i32, [vp, C.POINTER(RtBatchTuning)]),
+        "rtBatch_getTuning": (i32, [vp, C.POINTER(RtBatchTuning)]),
         "rtBatch_getInfo": (i32, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(f32)]),
         "cudaBVH_buildGeometries": (vp, [C.POINTER(RtGeometry), i32, vp]),
         "cudaBVH_refit": (i32, [vp, vp, vp]),
@@ -504,6 +512,19 @@ class PathTracer:
         p = RtPTParams(w, h, spp, max_bounces, rr_start, seed)
         _check(load().rtPT_render(self.h, C.byref(cam), C.byref(p), _ptr(d_rgb), _stream(stream)), "rtPT_render")
 
+    def set_queue_capacity(self, paths: int):
+        """rtPT_setQueueCapacity: paths per slice (0 = the whole frame)."""
+        _check(load().rtPT_setQueueCapacity(self.h, paths), "rtPT_setQueueCapacity")
+
+    def autotune(self, cam, w: int, h: int, spp: int, max_bounces: int = 4, rr_start: int = 2, seed: int = 1,
+                 d_rgb=None, stream=None) -> int:
+        """rtPT_autotune: the fastest queue capacity for this frame (0 = whole frame)."""
+        prm = RtPTParams(w, h, spp, max_bounces, rr_start, seed)
+        out = C.c_int64()
+        _check(load().rtPT_autotune(self.h, C.byref(cam), C.byref(prm), _ptr(d_rgb), _stream(stream), C.byref(out)),
+               "rtPT_autotune")
+        return int(out.value)
+
     def set_regroup(self, key_bits: int, kind: int = RT_REGROUP_OCTANT_MORTON):
         """rtPT_setRegroup: regroup bounce rays before each extension trace (0 = off)."""
         _check(load().rtPT_setRegroup(self.h, kind, key_bits), "rtPT_setRegroup")
@@ -568,6 +589,16 @@ class Batch:
 
     def set_tuning(self, ctas, iters):
         _check(load().rtBatch_setTuning(self.h, ctas, iters), "rtBatch_setTuning")
+
+    def tuning(self) -> dict:
+        """rtBatch_getTuning: the launch shape in use."""
+        t = RtBatchTuning()
+        _check(load().rtBatch_getTuning(self.h, C.byref(t)), "rtBatch_getTuning")
+        return {f: getattr(t, f) for f, _ in RtBatchTuning._fields_}
+
+    def set_tuning_ex(self, warps_per_sm: int, node_iters: int, block: int, shared_stack: int):
+        t = RtBatchTuning(warps_per_sm, node_iters, block, shared_stack)
+        _check(load().rtBatch_setTuningEx(self.h, C.byref(t)), "rtBatch_setTuningEx")
 
     def close(self):
         if getattr(self, "h", None):
