@@ -62,6 +62,33 @@ def max_over_ranks(x: float, ws: int, device="cuda") -> float:
     return float(t.item())
 
 
+def init_dist(ws: int):
+    """One process per GPU: the NCCL process group (a short timeout, so ranks
+    waiting on a lost peer end with an error)."""
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+
+def finish_dist(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def gather_over_ranks(a, ws: int) -> np.ndarray:
+    """Every rank's 1-D array concatenated in rank order (all ranks call it,
+    same order)."""
+    if ws == 1:
+        return np.asarray(a)
+    import torch.distributed as dist
+    parts = [None] * ws
+    dist.all_gather_object(parts, np.asarray(a))
+    return np.concatenate(parts)
+
+
 def whole_job_mrays(rays_per_rank: int, ws: int, t_ms_max: float) -> float:
     """Weak scaling: every rank traces its own batch of rays_per_rank; the
     job takes as long as the slowest rank."""
@@ -548,10 +575,7 @@ def run_ours(args):
     import torch
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    init_dist(ws)
     from rtb200 import lib
     lib.load()
     tris = make_workload()
@@ -690,9 +714,7 @@ def run_ours(args):
         del d_dif, d_sha, d_hits, d_occ, h_rays, h_hits
         torch.cuda.empty_cache()
         out["served"] = served_legs(rates=(SERVED_RATE, 2 * SERVED_RATE, 4 * SERVED_RATE))
-    if ws > 1:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+    finish_dist(ws)
     if rank == 0:
         print(json.dumps(out), flush=True)
     return 0
@@ -765,13 +787,24 @@ def run_batched(args):
     multi-scene trace replayed from a CUDA graph with autotuned launch
     shape.  Plain: 256 cudaBVH_build + cudaBVH_traceClosest calls.  Build
     phases are timed by the host clock (the builders synchronise), trace
-    phases by CUDA events on the stream; L2 flushed between steps."""
+    phases by CUDA events on the stream; L2 flushed between steps.
+    On N GPUs the scenes split into contiguous blocks balanced by work
+    (rtb200.shard.scene_blocks, weight = triangles + rays / 20: the build
+    dominates), each rank builds and traces its own block, and value = all
+    ranks' rays / the slowest rank's step (strong scaling: the 256-scene job
+    is fixed)."""
     import torch
-    from rtb200 import lib, scenes
+    from rtb200 import lib, scenes, shard
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
+    init_dist(ws)
     t0 = time.time()
-    tris, rays, off = scenes.batched_workload()
+    ntri_all, nray_all = scenes.batched_sizes()
+    bounds = shard.scene_blocks(ntri_all + nray_all // 20, ws)
+    mine = range(bounds[rank], bounds[rank + 1])
+    if len(mine) == 0:
+        raise SystemExit(f"rank {rank}: no scenes left for this rank ({len(ntri_all)} scenes, {ws} ranks)")
+    tris, rays, off = scenes.batched_workload(scenes=mine)
     ntri = np.array([t.shape[0] for t in tris])
     tri_off = np.concatenate([[0], np.cumsum(ntri)]).astype(np.int32)
     # the triangles sit in pinned host memory, read by both arms (pageable
@@ -845,19 +878,30 @@ def run_batched(args):
             trace_plain.append(e0.elapsed_time(e1))
         del bv
     same = bool(torch.equal(d_ref, d_hits))
+    # every rank's own phases; the job's step is the slowest rank's
     bo, to = float(np.mean(build_ours)), float(np.mean(trace_ours))
     bp, tp = float(np.mean(build_plain)), float(np.mean(trace_plain))
-    out = {"metric": "Mrays/s batched build+trace (256 scenes)", "value": round(nr / (bo + to) / 1e3, 1),
-           "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(bo + to, 3),
-           "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": f"batched_256: 256 scenes of 1K-500K triangles ({int(ntri.sum())} total), "
-                                  f"{nr} rays (4K-2M per scene, half primary, half diffuse), closest hit",
-                      "l2": "flushed between steps", "host_tris": "pinned, shared by both arms"},
+    step_ours = max_over_ranks(bo + to, ws)
+    step_plain = max_over_ranks(bp + tp, ws)
+    same = max_over_ranks(0.0 if same else 1.0, ws) == 0.0
+    nr_all = int(nray_all.sum())
+    finish_dist(ws)
+    if rank != 0:
+        return 0 if same else 1
+    out = {"metric": "Mrays/s batched build+trace (256 scenes)", "value": round(nr_all / step_ours / 1e3, 1),
+           "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(step_ours, 3), "higher_is_better": True, "scaling": "strong", "dtype": "f32",
+           "data": "synthetic",
+           "config": {"workload": f"batched_256: 256 scenes of 1K-500K triangles ({int(ntri_all.sum())} total), "
+                                  f"{nr_all} rays (4K-2M per scene, half primary, half diffuse), closest hit",
+                      "l2": "flushed between steps", "host_tris": "pinned, shared by both arms",
+                      "parallelism": (f"scene blocks x{ws} (rtb200.shard.scene_blocks; rank 0: scenes "
+                                      f"{bounds[0]}-{bounds[1] - 1}), no collective" if ws > 1 else "one GPU")},
            "ours": {"build_ms": round(bo, 2), "trace_ms": round(to, 3), "trace_mrays_s": round(nr / to / 1e3, 1),
                     "device_build_ms": round(info["build_ms"], 2), "tuning": shape,
                     "launches": "one build pipeline for all scenes, one graph-captured trace launch"},
            "plain": {"build_ms": round(bp, 2), "trace_ms": round(tp, 3), "trace_mrays_s": round(nr / tp / 1e3, 1),
-                     "value": round(nr / (bp + tp) / 1e3, 1), "steps": psteps,
+                     "value": round(nr_all / step_plain / 1e3, 1), "steps": psteps,
                      "launches": "256 cudaBVH_build + 256 cudaBVH_traceClosest"},
            "hits_equal_plain": same}
     print(json.dumps(out), flush=True)
@@ -868,7 +912,7 @@ SERVED_RATE = 2000.0  # requests/s of the served configuration
 SERVED_NREQ = 256
 
 
-def served_legs(rates=(SERVED_RATE,), modes=("host", "device")):
+def served_legs(rates=(SERVED_RATE,), modes=("host", "device"), world=1, rank=0):
     """Served form against the plain per-call path on Poisson request traces.
 
     16 resident scenes (30M triangles, 200K-5M each); for each arrival rate a
@@ -881,18 +925,37 @@ def served_legs(rates=(SERVED_RATE,), modes=("host", "device")):
     cudaBVH_traceClosest / cudaBVH_traceAny and a synchronize), one call at a
     time in arrival order (layer/cuda_bvh_backend.cu:1379-1497 is the
     reference's per-call path).  Latency = results ready - scheduled
-    arrival; aggregate = all rays / (last completion - first arrival).  Both
-    arms' results are compared byte for byte on the GPU."""
+    arrival; aggregate = all rays / (last completion - trace start).  Both
+    arms' results are compared byte for byte on the GPU.
+    On `world` GPUs (one process each, this one `rank`) the 16 scenes split
+    into contiguous blocks balanced by the rays their requests ask for
+    (rtb200.shard.scene_blocks); each rank holds only its scenes and serves
+    the requests against them at their arrival times; latencies are gathered
+    over ranks and the aggregate divides all rays by the slowest rank's span.
+    The returned dict is complete on rank 0."""
     import torch
-    from rtb200 import lib, scenes
+    from rtb200 import lib, scenes, shard
+    _, scene0, nray0, _, _ = scenes.served_trace(SERVED_NREQ, rate=SERVED_RATE)
+    bounds = shard.scene_blocks(np.bincount(scene0, weights=nray0, minlength=16).astype(np.int64), world)
+    mine = range(bounds[rank], bounds[rank + 1])
+    if len(mine) == 0:
+        raise SystemExit(f"rank {rank}: no served scene left for this rank (16 scenes, {world} ranks)")
     t0 = time.time()
-    tris = scenes.served_scenes()
+    tris = scenes.served_scenes(only=mine)
     pool_c, pool_a = scenes.served_ray_pools()
     log(f"served workload: {sum(t.shape[0] for t in tris)} tris in {time.time() - t0:.1f}s")
     t0 = time.time()
-    bvhs = [lib.BVH(t) for t in tris]
+    bvhs = {g: lib.BVH(t) for g, t in zip(mine, tris)}
     torch.cuda.synchronize()
-    log(f"16 BVH builds: {time.time() - t0:.2f}s")
+    log(f"{len(bvhs)} BVH builds: {time.time() - t0:.2f}s")
+
+    def gather(a):
+        return gather_over_ranks(a, world)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
     L = lib.load()
     ic_h = torch.empty(pool_c.nbytes, dtype=torch.uint8, pin_memory=True)
     ia_h = torch.empty(pool_a.nbytes, dtype=torch.uint8, pin_memory=True)
@@ -900,8 +963,7 @@ def served_legs(rates=(SERVED_RATE,), modes=("host", "device")):
     ia_h.numpy()[:] = pool_a.view(np.uint8)
     ins = {"host": (ic_h, ia_h), "device": (ic_h.cuda(), ia_h.cuda())}
     srv = lib.Server(hbm_budget_bytes=120 << 30, pool_bytes=16 << 30)
-    for b in bvhs:
-        srv.add_scene(b)
+    sid = {g: srv.add_scene(b) for g, b in bvhs.items()}
     out = {"config": {"workload": "served_16x30m: 16 resident scenes (30,000,000 triangles, 200K-5M each), "
                                   f"{SERVED_NREQ} Poisson requests per trace, rays log-uniform 1K-8M (random "
                                   "incoherent rays), 70% closest / 30% any hit",
@@ -909,6 +971,9 @@ def served_legs(rates=(SERVED_RATE,), modes=("host", "device")):
            "rates": {}}
     for rate in rates:
         arrival, scene, nray, anyh, start = scenes.served_trace(SERVED_NREQ, rate=rate, pool=pool_c.shape[0])
+        sel = shard.requests_for_rank(scene, bounds, rank)  # this rank's requests, in arrival order
+        if sel.size == 0:
+            raise SystemExit(f"rank {rank}: no request of the trace falls on scenes {mine.start}-{mine.stop - 1}")
         esz = np.where(anyh, 1, 16)
         # each request's result slot starts on a 16-byte boundary (hit records
         # are written as 16-byte vectors by the device paths)
@@ -933,21 +998,23 @@ def served_legs(rates=(SERVED_RATE,), modes=("host", "device")):
 
             # ---- served arm
             for i in range(4):  # warm-up: largest requests of each kind
-                k = int(np.argmax(nray * (anyh == bool(i & 1))))
-                srv.wait(srv.submit(int(scene[k]), bool(anyh[k]), rays_ptr(k), int(nray[k]), out_ptr(k), device=dev))
+                k = int(sel[np.argmax(nray[sel] * (anyh[sel] == bool(i & 1)))])
+                srv.wait(srv.submit(sid[int(scene[k])], bool(anyh[k]), rays_ptr(k), int(nray[k]), out_ptr(k),
+                                    device=dev))
             w0 = srv.stats()["waves"]
-            tickets, lag = [0] * SERVED_NREQ, np.zeros(SERVED_NREQ)
+            tickets, lag = [0] * len(sel), np.zeros(len(sel))
 
             def submitter():
                 T0 = time.perf_counter()
-                for i in range(SERVED_NREQ):
+                for j, i in enumerate(sel):
                     ta = T0 + arrival[i]
                     while time.perf_counter() < ta:
                         pass
-                    tickets[i] = srv.submit(int(scene[i]), bool(anyh[i]), rays_ptr(i), int(nray[i]), out_ptr(i),
-                                            device=dev)
-                    lag[i] = time.perf_counter() - ta
+                    tickets[j] = srv.submit(sid[int(scene[i])], bool(anyh[i]), rays_ptr(i), int(nray[i]),
+                                            out_ptr(i), device=dev)
+                    lag[j] = time.perf_counter() - ta
 
+            barrier()
             th = threading.Thread(target=submitter)
             th.start()
             th.join()
@@ -955,7 +1022,9 @@ def served_legs(rates=(SERVED_RATE,), modes=("host", "device")):
             bad_status = sum(1 for f in infos if f["status"] != 0)
             st = srv.stats()
             lat_s = np.array([(f["done_us"] - f["submit_us"]) / 1e3 for f in infos]) + lag * 1e3
-            first = infos[0]["submit_us"] - lag[0] * 1e6
+            # the trace's start on the server clock: the first request's
+            # scheduled arrival less its offset in the trace
+            first = infos[0]["submit_us"] - (lag[0] + arrival[sel[0]]) * 1e6
             span_s = (max(f["done_us"] for f in infos) - first) / 1e3
             snap = outb.cuda() if not dev else outb.clone()  # served results, kept on the GPU
             # ---- plain arm: the per-call path, one call at a time
@@ -966,47 +1035,56 @@ def served_legs(rates=(SERVED_RATE,), modes=("host", "device")):
 
             def call(i):
                 f = fa if anyh[i] else fc
-                args_ = (bvhs[scene[i]].h, rays_ptr(i), int(nray[i]), out_ptr(i)) + ((None,) if dev else ())
+                args_ = (bvhs[int(scene[i])].h, rays_ptr(i), int(nray[i]), out_ptr(i)) + ((None,) if dev else ())
                 rc = f(*args_)
                 if dev:
                     torch.cuda.synchronize()
                 if rc != 0:
                     raise RuntimeError(lib.last_error())
 
-            for sc in range(len(bvhs)):  # warm-up: each scene's staging sized by its largest request
+            for sc in bvhs:  # warm-up: each scene's staging sized by its largest request
                 for kind in (False, True):
                     m = np.nonzero((scene == sc) & (anyh == kind))[0]
                     if m.size:
                         call(int(m[np.argmax(nray[m])]))
             outb.zero_()
             torch.cuda.synchronize()
-            lat_p = np.zeros(SERVED_NREQ)
+            lat_p = np.zeros(len(sel))
+            barrier()
             T0 = time.perf_counter()
-            for i in range(SERVED_NREQ):
+            for j, i in enumerate(sel):
                 ta = T0 + arrival[i]
                 while time.perf_counter() < ta:
                     pass
                 call(i)
-                lat_p[i] = (time.perf_counter() - ta) * 1e3
+                lat_p[j] = (time.perf_counter() - ta) * 1e3
             span_p = (time.perf_counter() - T0) * 1e3
             same = bool(torch.equal(snap, outb.cuda() if not dev else outb))
             del snap
+            # the job: every rank's latencies, the slowest rank's span
+            lat_s, lat_p, lag_all = gather(lat_s), gather(lat_p), gather(lag)
+            span_s, span_p = float(gather([span_s]).max()), float(gather([span_p]).max())
+            same = bool(gather([same and bad_status == 0]).all())
+            waves = int(gather([st["waves"] - w0]).sum())
             srv_m, pl_m = total / span_s / 1e3, total / span_p / 1e3
             pc = lambda a, q: round(float(np.percentile(a, q)), 3)
             row[mode] = {
                 "served": {"p50_ms": pc(lat_s, 50), "p99_ms": pc(lat_s, 99), "mrays_s": round(srv_m, 1),
-                           "span_ms": round(span_s, 2), "waves": st["waves"] - w0,
+                           "span_ms": round(span_s, 2), "waves": waves,
                            "peak_pool_gb": round(st["peak_pool_used"] / 2 ** 30, 3),
-                           "max_submit_lag_ms": round(float(lag.max() * 1e3), 3)},
+                           "max_submit_lag_ms": round(float(lag_all.max() * 1e3), 3)},
                 "plain": {"p50_ms": pc(lat_p, 50), "p99_ms": pc(lat_p, 99), "mrays_s": round(pl_m, 1),
                           "span_ms": round(span_p, 2)},
                 "p99_served_over_plain": round(float(np.percentile(lat_s, 99) / np.percentile(lat_p, 99)), 3),
                 "mrays_served_over_plain": round(srv_m / pl_m, 3),
-                "results_equal_plain": same and bad_status == 0}
+                "results_equal_plain": same}
             log(f"served rate {rate:.0f}/s {mode}: {json.dumps(row[mode])}")
             del outb
         out["rates"][f"{rate:.0f}"] = row
-    out["config"]["resident_gb"] = round(srv.stats()["resident_bytes"] / 2 ** 30, 3)
+    out["config"]["resident_gb"] = round(float(gather([srv.stats()["resident_bytes"]]).sum()) / 2 ** 30, 3)
+    if world > 1:
+        out["config"]["parallelism"] = (f"scene blocks x{world} (rtb200.shard.scene_blocks over the requested "
+                                        f"rays; boundaries {bounds}), no collective on the data path")
     srv.close()
     out["results_equal_plain"] = all(r[m]["results_equal_plain"] for r in out["rates"].values() for m in modes)
     return out
@@ -1019,10 +1097,14 @@ def run_served(args):
     import torch
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
-    res = served_legs(rates=(SERVED_RATE, 2 * SERVED_RATE, 4 * SERVED_RATE))
+    init_dist(ws)
+    res = served_legs(rates=(SERVED_RATE, 2 * SERVED_RATE, 4 * SERVED_RATE), world=ws, rank=rank)
+    finish_dist(ws)
+    if rank != 0:
+        return 0 if res["results_equal_plain"] else 1
     base = res["rates"][f"{SERVED_RATE:.0f}"]
     out = {"metric": "p99 trace latency served vs plain (ms), 256-request Poisson trace, host buffers",
-           "value": base["host"]["served"]["p99_ms"], "unit": "ms", "n_gpus": 1, "steps": 1, "warmup": 4,
+           "value": base["host"]["served"]["p99_ms"], "unit": "ms", "n_gpus": ws, "steps": 1, "warmup": 4,
            "higher_is_better": False, "dtype": "f32", "data": "synthetic", "config": res["config"],
            "served": res, "results_equal_plain": res["results_equal_plain"]}
     print(json.dumps(out), flush=True)

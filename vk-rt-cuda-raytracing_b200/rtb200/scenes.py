@@ -351,21 +351,32 @@ PT_CAM_TARGET = (0.0, 0.0, 0.0)
 
 
 # ---------------------------------------------------------- batched scenes --
-def batched_workload(nscenes: int = 256, tri_lo: int = 1000, tri_hi: int = 500_000, ray_lo: int = 4096,
-                     ray_hi: int = 2_000_000, seed: int = 7):
-    """Batched workload of 256 scenes: scene i = scene_meshes(seed=i, n_i) with
-    n_i log-uniform in [tri_lo, tri_hi]; its ray batch has r_i log-uniform in
-    [ray_lo, ray_hi] rays, half primary and half diffuse (scene_rays).
-    Returns (list of (n_i, 9) float32, rays concatenated, ray offsets)."""
+def batched_sizes(nscenes: int = 256, tri_lo: int = 1000, tri_hi: int = 500_000, ray_lo: int = 4096,
+                  ray_hi: int = 2_000_000, seed: int = 7):
+    """Triangle and ray counts of the batched workload's scenes (n_i and
+    r_i of batched_workload), without making the scenes."""
     u = uniforms(seed, S_BATCH, nscenes, 4).astype(np.float64)
     ntris = np.round(log_uniform(u[:, 0], tri_lo, tri_hi)).astype(int)
     nrays = np.round(log_uniform(u[:, 1], ray_lo, ray_hi)).astype(int)
+    return ntris, nrays
+
+
+def batched_workload(nscenes: int = 256, tri_lo: int = 1000, tri_hi: int = 500_000, ray_lo: int = 4096,
+                     ray_hi: int = 2_000_000, seed: int = 7, scenes=None):
+    """Batched workload of 256 scenes: scene i = scene_meshes(seed=i, n_i) with
+    n_i log-uniform in [tri_lo, tri_hi]; its ray batch has r_i log-uniform in
+    [ray_lo, ray_hi] rays, half primary and half diffuse (scene_rays).
+    `scenes` (a range of scene ids, default all) makes only those scenes, the
+    same as in the full workload.  Returns (list of (n_i, 9) float32, rays
+    concatenated, ray offsets)."""
+    ntris, nrays = batched_sizes(nscenes, tri_lo, tri_hi, ray_lo, ray_hi, seed)
+    ids = range(nscenes) if scenes is None else scenes
     def one(i):
         t = scene_meshes(i, int(ntris[i]))
         return t, scene_rays(t, int(nrays[i]), seed=i)
 
     with concurrent.futures.ThreadPoolExecutor(min(16, os.cpu_count() or 1)) as ex:
-        res = list(ex.map(one, range(nscenes)))
+        res = list(ex.map(one, ids))
     tris, rays = [r[0] for r in res], [r[1] for r in res]
     off = np.concatenate([[0], np.cumsum([r.shape[0] for r in rays])]).astype(np.int32)
     return tris, np.concatenate(rays), off
@@ -411,17 +422,18 @@ def scene_rays(tris: np.ndarray, n: int, seed: int) -> np.ndarray:
 
 # ----------------------------------------------------------- served trace --
 def served_scenes(nscenes: int = 16, total: int = 30_000_000, lo: int = 200_000, hi: int = 5_000_000,
-                  seed: int = 11):
+                  seed: int = 11, only=None):
     """Resident scenes of the served workload: sizes log-uniform in [lo, hi],
     rescaled so they sum to `total` (each kept within [lo, hi]); scene i =
-    scene_meshes(seed=1000 + i, n_i), all in the same 100^3 box."""
+    scene_meshes(seed=1000 + i, n_i), all in the same 100^3 box.  `only` (a
+    range of scene ids, default all) makes just those scenes."""
     u = uniforms(seed, S_SERVE, nscenes, 4)[:, 0].astype(np.float64)
     w = log_uniform(u, lo, hi)
     n = np.clip(np.round(w * total / w.sum()), lo, hi).astype(int)
     n[-1] += total - n.sum()
     n = np.clip(n, lo, hi)
     with concurrent.futures.ThreadPoolExecutor(min(16, os.cpu_count() or 1)) as ex:
-        return list(ex.map(lambda i: scene_meshes(1000 + i, int(n[i])), range(nscenes)))
+        return list(ex.map(lambda i: scene_meshes(1000 + i, int(n[i])), range(nscenes) if only is None else only))
 
 
 def served_trace(nreq: int, rate: float = 2000.0, nscenes: int = 16, ray_lo: int = 1000, ray_hi: int = 8_000_000,
