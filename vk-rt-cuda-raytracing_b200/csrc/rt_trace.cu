@@ -20,7 +20,10 @@
 //                   triangle once for its barycentrics.
 // The traversal stack holds (child base, hit mask, inner mask) groups: the
 // top SSTACK entries live in shared memory, the rest in local memory;
-// overflow is reported through the status word, never dropped.
+// overflow is reported through the status word, never dropped.  In the
+// batch's tail (ray pool exhausted), lanes without a ray help the busy
+// lanes of their warp: each takes the bottom group of a busy lane's shared
+// stack and walks it for that lane's ray (RTB_HELPERS).
 //
 // Box test robustness: t = q * (s/d) + (p - o)/d is evaluated with an
 // absolute slack of 2^-22 |(p - o)/d| folded into the near/far offsets and
@@ -51,6 +54,31 @@
 #endif
 #ifndef RTB_DUP_TRI
 #define RTB_DUP_TRI 0
+#endif
+// RTB_HELPERS: once the ray pool is exhausted, a lane left without a ray
+// takes the oldest node group a busy lane of its warp keeps in shared
+// memory and walks that subtree for the busy lane's ray (its triangles go
+// to the ray's owner slot in the pooled phase, which keeps the closest hit
+// exact: every triangle is still tested once and the minimum of the
+// (t, primitive) keys does not depend on the order).  The owner writes the
+// result once its own walk and all its helpers are done.  Not in the
+// work-counting kernels, whose per-ray counts follow one walk order.
+// 0: off; 1: closest hit only; 2: closest and any hit.  2 measured +1.8 %
+// closest and +1.3 % any hit on 2M incoherent rays (warp iterations -4.8 %,
+// lanes holding a ray at an iteration's start 28.6 -> 29.8 of 32) and
+// steadier run to run.  Measured and left out: a victim with nothing
+// stacked giving the far half of its current group (+1.1 / -0.6 %), and a
+// warp vote that skips the owner-slot shuffle while no lane helps (+0.5 /
+// -0.3 %: its register spills).
+#ifndef RTB_HELPERS
+#define RTB_HELPERS 2
+#endif
+// launch modes with helpers (bit 1 << MODE_SINGLE / MODE_BATCH / MODE_WAVE):
+// single scene only.  In the batch and wave modes the extra state spills
+// (10-12 bytes) and the tail is a small part of their long launches: the
+// 256-scene batched trace measured -4.5 % and the served waves -2 to -3 %.
+#ifndef RTB_HELPERS_MODES
+#define RTB_HELPERS_MODES 1
 #endif
 
 namespace rtb {
@@ -96,6 +124,13 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
 #if RTB_RAY_SMEM
     __shared__ float4 s_ray[2][T];           // each lane's ray, read by the lanes testing its triangles
 #endif
+    constexpr bool HELP =
+        !COUNT && (ANY ? RTB_HELPERS >= 2 : RTB_HELPERS >= 1) && ((RTB_HELPERS_MODES >> MODE) & 1);
+    static_assert(!HELP || RTB_RAY_SMEM, "helper lanes read the owner's ray from shared memory");
+    // helpers per owner lane (low 16 bits) | HELP_OVF when a helper's stack overflowed
+    constexpr int HELP_OVF = 1 << 16;
+    __shared__ int s_help[HELP ? T : 1];
+    if (HELP) s_help[threadIdx.x] = 0;
 #if RTB_SLOTMASK
     __shared__ NodeLuts s_luts;
     init_node_luts(&s_luts);
@@ -106,6 +141,8 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
     uint2 lstack[WalkT<T, SS>::L];
     const int lane = threadIdx.x & 31;
     const int wbase = threadIdx.x & ~31;
+    // ray >= 0: this lane's own ray; -1: none; HELP: -2 - l when this lane
+    // walks a subtree for the ray of lane l of its warp
     int ray = -1;
     bool exhausted = false;
     Ray r;
@@ -117,7 +154,7 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
     uint32_t cn = 0, ct = 0;
     for (;;) {
         // ---- refill idle lanes ----
-        const bool need = ray < 0 && !exhausted;
+        const bool need = ray == -1 && !exhausted;
         const unsigned want = __ballot_sync(FULL_MASK, need);
         RTB_STAT(15, __popc(want));
         if (want) {
@@ -169,7 +206,39 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
                 }
             }
         }
-        if (__all_sync(FULL_MASK, ray < 0)) break;
+        if (HELP) {
+            // ---- tail: idle lanes take the oldest stacked group of a busy lane ----
+            const bool idle = ray == -1 && exhausted;
+            const unsigned idles = __ballot_sync(FULL_MASK, idle);
+            const bool can = idles && ray != -1 && w.sp > w.sb && w.sb < WalkT<T, SS>::S;
+            const unsigned vict = idles ? __ballot_sync(FULL_MASK, can) : 0u;
+            if (vict) {
+                const int nst = min(__popc(idles), __popc(vict));
+                const int irank = __popc(idles & ((1u << lane) - 1));
+                const bool thief = idle && irank < nst;
+                const bool given = can && __popc(vict & ((1u << lane) - 1)) < nst;
+                const int v = thief ? (int)nth_set_bit(vict, (uint32_t)irank) : lane;
+                // the victim's part: its bottom stacked group (from its own shared column)
+                uint2 give = make_uint2(0u, 0u);
+                if (given) {
+                    give = sstack[w.sb][threadIdx.x];
+                    w.sb++;
+                }
+                const uint32_t gx = __shfl_sync(FULL_MASK, give.x, v), gy = __shfl_sync(FULL_MASK, give.y, v);
+                const int vslot = __shfl_sync(FULL_MASK, ray >= 0 ? lane : -2 - ray, v);
+                const float vthit = __shfl_sync(FULL_MASK, thit, v);
+                if (thief) {
+                    ray = -2 - vslot;
+                    r = make_ray(s_ray[0][wbase + vslot], s_ray[1][wbase + vslot]);
+                    thit = vthit;
+                    hprim = -1;
+                    w.start();
+                    w.ng = make_uint2(gx, gy);
+                    atomicAdd(&s_help[wbase + vslot], 1);
+                }
+            }
+        }
+        if (__all_sync(FULL_MASK, ray == -1)) break;
         RTB_STAT(0, 1);
         RTB_STAT(1, __popc(__ballot_sync(FULL_MASK, ray >= 0)));
         // ---- node phase ----
@@ -207,9 +276,9 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
             if (it > 0 && !__any_sync(FULL_MASK, ray >= 0 && RTB_LAST_SET == 0 && !overflow && (w.ng.y & 0xFFu)))
                 break;
 #endif
-            if (ray >= 0 && RTB_LAST_SET == 0 && !overflow && (w.ng.y & 0xFFu)) {
+            if (ray != -1 && RTB_LAST_SET == 0 && !overflow && (w.ng.y & 0xFFu)) {
 #else
-            if (ray >= 0 && tmask == 0 && !overflow && (w.ng.y & 0xFFu)) {
+            if (ray != -1 && tmask == 0 && !overflow && (w.ng.y & 0xFFu)) {
 #endif
                 uint32_t hitsm = w.ng.y & 0xFFu;
                 const uint32_t imask = (w.ng.y >> 8) & 0xFFu;
@@ -257,9 +326,9 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
 #endif
                 prefetch_next(nodes, w.ng, r.oct);
 #if RTB_TWO_SETS
-                if (NITERS > 1 && (w.ng.y & 0xFFu) == 0 && w.sp > 0) {
+                if (NITERS > 1 && (w.ng.y & 0xFFu) == 0 && w.sp > w.sb) {
 #else
-                if (NITERS > 1 && tmask == 0 && (w.ng.y & 0xFFu) == 0 && w.sp > 0) {
+                if (NITERS > 1 && tmask == 0 && (w.ng.y & 0xFFu) == 0 && w.sp > w.sb) {
 #endif
                     w.ng = w.pop(sstack, lstack);
                 }
@@ -295,6 +364,7 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
                 s_rec[threadIdx.x] = 0;
             }
             __syncwarp();
+            const int kslot = HELP && ray < -1 ? -2 - ray : lane;  // whose ray this lane's triangles belong to
             for (int base = 0; base < total; base += 32) {
                 const int g = base + lane;
                 // owner = first lane whose inclusive count exceeds g
@@ -306,6 +376,7 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
                 }
                 o = min(o, 31);
                 const int k0 = g - __shfl_sync(FULL_MASK, excl, o);
+                const int ko = HELP ? __shfl_sync(FULL_MASK, kslot, o) : o;  // the triangle's ray slot
 #if RTB_TWO_SETS
                 uint32_t om = __shfl_sync(FULL_MASK, tmask, o);
                 uint32_t ob = __shfl_sync(FULL_MASK, tri_base, o);
@@ -337,7 +408,7 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
                 const uint32_t ob = __shfl_sync(FULL_MASK, tri_base, o);
 #endif
 #if RTB_RAY_SMEM
-                const float4 ro = s_ray[0][wbase + o], rd = s_ray[1][wbase + o];
+                const float4 ro = s_ray[0][wbase + ko], rd = s_ray[1][wbase + ko];
                 const float ox = ro.x, oy = ro.y, oz = ro.z, tmn = ro.w;
                 const float dx = rd.x, dy = rd.y, dz = rd.z, tmx = rd.w;
 #else
@@ -355,24 +426,26 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
                     const float4 A = ld_tri(tp), B = ld_tri(tp + 1), Cc = ld_tri(tp + 2);
                     float t;
                     if (intersect_tri(ox, oy, oz, dx, dy, dz, A, B, Cc, t, u, v) && t > tmn && t < tmx) {
-                        if (ANY) s_rec[wbase + o] = 1;
+                        if (ANY) s_rec[wbase + ko] = 1;
                         else key = ((unsigned long long)f2ord(t) << 32) | (uint32_t)__float_as_int(A.w);
                     }
                 }
                 if (!ANY) {
-                    if (key != ~0ull) atomicMin(&s_key[wbase + o], key);
+                    if (key != ~0ull) atomicMin(&s_key[wbase + ko], key);
                     __syncwarp();
                     // the unique winner (keys are distinct per ray) publishes its barycentrics
-                    if (key != ~0ull && s_key[wbase + o] == key) {
-                        s_rec[wbase + o] = 1;
-                        s_uv[wbase + o] = make_float2(u, v);
+                    if (key != ~0ull && s_key[wbase + ko] == key) {
+                        s_rec[wbase + ko] = 1;
+                        s_uv[wbase + ko] = make_float2(u, v);
                     }
                     __syncwarp();
                 }
             }
             __syncwarp();
             if (ANY) {
-                found_any = s_rec[threadIdx.x] != 0;
+                found_any = s_rec[HELP && ray < -1 ? wbase - 2 - ray : threadIdx.x] != 0;
+            } else if (HELP && ray < -1) {
+                thit = ord2f((uint32_t)(s_key[wbase - 2 - ray] >> 32));  // the owner's best so far culls
             } else if (s_rec[threadIdx.x] >= 0) {
                 // a new closest hit for this lane
                 const unsigned long long key = s_key[threadIdx.x];
@@ -384,17 +457,49 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
             }
         }
         // ---- advance / finish ----
-        if (ray >= 0) {
+        bool owner_done = false;
+        if (ray != -1) {
             bool done = overflow || (ANY && found_any);
             if (!done && (w.ng.y & 0xFFu) == 0) {
-                if (w.sp == 0) {
+                if (w.sp == w.sb) {
                     done = true;
                 } else {
                     w.ng = w.pop(sstack, lstack);
                     prefetch_next(nodes, w.ng, r.oct);
                 }
             }
-            if (done) {
+            if (HELP && ray < -1) {
+                if (done) {  // subtree walked (or the ray already occluded): leave the owner
+                    if (overflow) atomicOr(&s_help[wbase - 2 - ray], HELP_OVF);
+                    atomicSub(&s_help[wbase - 2 - ray], 1);
+                    ray = -1;
+                }
+            } else {
+                owner_done = done;
+            }
+        }
+        if (HELP) {
+            __syncwarp();  // helpers' departures are visible to their owners
+            if (owner_done) {
+                const int hs = s_help[threadIdx.x];
+                if (hs & (HELP_OVF - 1)) {
+                    // own walk over, helpers still out: keep what decided it and wait
+                    if (overflow) atomicOr(&s_help[threadIdx.x], HELP_OVF);
+                    if (ANY && found_any) hprim = 0;  // any hit: found (hprim is otherwise unused)
+                    w.ng.y &= ~0xFFu;
+                    w.sp = w.sb;
+                    owner_done = false;
+                } else {
+                    overflow = overflow || (hs & HELP_OVF);
+                    if (ANY) found_any = found_any || hprim >= 0;
+                    s_help[threadIdx.x] = 0;
+                }
+            }
+        } else {
+            owner_done = ray >= 0 && owner_done;
+        }
+        if (owner_done) {
+            {
                 if (overflow) {
                     atomicOr(status, RT_STATUS_STACK);
                     hprim = -1;

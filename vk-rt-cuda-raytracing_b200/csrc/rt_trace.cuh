@@ -260,7 +260,8 @@ struct WalkT {
     static constexpr int L = RTB_STACK_TOTAL - S;
     uint2 ng;
     int sp;
-    __device__ __forceinline__ void start() { sp = 0; }
+    int sb;  // entries below sb were handed to helper lanes (RTB_HELPERS); 0 otherwise
+    __device__ __forceinline__ void start() { sp = 0; sb = 0; }
     __device__ __forceinline__ bool push(uint2 e, uint2 (*ss)[T], uint2* ls) {
         if (sp < S) ss[sp][threadIdx.x] = e;
         else if (sp < S + L) ls[sp - S] = e;
