@@ -575,11 +575,13 @@ void trace_two_level_one(const uint32_t* tlas, int tn, const int* tord, const fl
 //   4-7, hi 0-3, hi 4-7), [12..15] y, [16..19] z.
 // Triangle record, 12 floats: v0 and the primitive id (int bits), e1, 0,
 //   e2, 0.
-// One round of the walk: up to `niters` node visits (none once a visited
-// node gave triangles; a visited node with nothing hit pops the next
-// group), then every triangle of the hit leaves is tested and the least
-// (t, primitive) key kept, then the next group is popped if the current
-// one is spent.  Box test: t = q * (s / d) + (p - o) / d with an absolute
+// One round of the walk: up to `niters` node visits, then every triangle of
+// the hit leaves is tested and the least (t, primitive) key kept, then the
+// next group is popped if the current one is spent.  With `sets` = 1 a
+// visit that gave triangles ends the round's visits, and a visited node
+// with nothing hit pops the next group; with `sets` = 2 (the kernel's two
+// pending triangle sets) the visits go on until a second visit has given
+// triangles, and a spent group pops the next one after every visit.  Box test: t = q * (s / d) + (p - o) / d with an absolute
 // slack of 2^-22 |(p - o) / d| on the offsets and 2^-21 |t_far| on the
 // comparison; 1/d of a component with |d| <= 2^-64 uses +-2^-64.
 struct Walk8Out {
@@ -644,7 +646,7 @@ void visit8(const uint32_t* W, const float o[3], const float inv[3], uint32_t oc
 }
 
 void walk8_one(const uint32_t* nodes, int nnodes, const float* recs, int nrecs, const OrcRay& ray, bool any,
-               int niters, Walk8Out& out) {
+               int niters, int sets, Walk8Out& out) {
     const float* o = ray.org;
     const float* d = ray.dir;
     float inv[3];
@@ -660,9 +662,9 @@ void walk8_one(const uint32_t* nodes, int nnodes, const float* recs, int nrecs, 
     uint32_t ngx = 0, ngy = (1u << oct) | (1u << 8);  // the root as slot 0 of a one-child group
     out.bad = false;
     for (;;) {
-        uint32_t tri_base = 0, tmask = 0;
+        uint32_t tri_base = 0, tmask = 0, tri_base2 = 0, tmask2 = 0;
         for (int it = 0; it < niters; it++) {
-            if (tmask != 0 || overflow || (ngy & 0xFFu) == 0) continue;
+            if ((sets == 2 ? tmask2 : tmask) != 0 || overflow || (ngy & 0xFFu) == 0) continue;
             uint32_t hitsm = ngy & 0xFFu;
             const uint32_t imask = (ngy >> 8) & 0xFFu;
             const uint32_t k = (uint32_t)__builtin_ctz(hitsm);
@@ -683,20 +685,29 @@ void walk8_one(const uint32_t* nodes, int nnodes, const float* recs, int nrecs, 
                 out.bad = true;
                 return;
             }
-            visit8(nodes + (size_t)ni * 20, o, inv, oct, ray.tmin, thit, tri_base, tmask, ngx, ngy);
-            if (niters > 1 && tmask == 0 && (ngy & 0xFFu) == 0 && sp > 0) {
+            uint32_t vb, vm;
+            visit8(nodes + (size_t)ni * 20, o, inv, oct, ray.tmin, thit, vb, vm, ngx, ngy);
+            if (tmask == 0) {
+                tri_base = vb;
+                tmask = vm;
+            } else {
+                tri_base2 = vb;
+                tmask2 = vm;
+            }
+            if (niters > 1 && (sets == 2 || tmask == 0) && (ngy & 0xFFu) == 0 && sp > 0) {
                 sp--;
                 ngx = stx[sp];
                 ngy = sty[sp];
             }
         }
-        ct += (uint32_t)__builtin_popcount(tmask);
-        if (tmask) {
+        ct += (uint32_t)__builtin_popcount(tmask) + (uint32_t)__builtin_popcount(tmask2);
+        if (tmask | tmask2) {
             uint64_t best = ((uint64_t)ord_of(thit) << 32) | (uint32_t)(hprim >= 0 ? hprim : -1);
             float bu = 0.f, bv = 0.f;
             bool improved = false;
-            for (uint32_t m = tmask; m; m &= m - 1) {
-                const uint32_t rec = tri_base + (uint32_t)__builtin_ctz(m);
+            for (uint64_t m = (uint64_t)tmask | ((uint64_t)tmask2 << 32); m; m &= m - 1) {
+                const int bit = __builtin_ctzll(m);
+                const uint32_t rec = (bit < 32 ? tri_base : tri_base2) + (uint32_t)(bit & 31);
                 if (rec >= (uint32_t)nrecs) {
                     out.bad = true;
                     return;
@@ -956,16 +967,19 @@ int orc_fix_skips(uint32_t* dfs, int n) {
     return changed;
 }
 
-// 8-wide walk over the engine's own nodes (walk8_one).  hits (closest hit)
-// or occluded (any hit) may be null; counts: node visits and triangle tests
-// per ray (2 x u32).  Returns how many rays' walks left the arrays (0 for a
-// valid tree; those rays get counts 0xFFFFFFFF).
+// 8-wide walk over the engine's own nodes (walk8_one): `niters` node visits
+// per round and `sets` (1 or 2) pending triangle sets per ray.  hits
+// (closest hit) or occluded (any hit) may be null; counts: node visits and
+// triangle tests per ray (2 x u32).  Returns how many rays' walks left the
+// arrays (0 for a valid tree; those rays get counts 0xFFFFFFFF), or -1 for
+// a bad niters / sets.
 int orc_walk_bvh8(const uint32_t* nodes, int nnodes, const float* recs, int nrecs, const OrcRay* rays, int nrays,
-                  int any, int niters, OrcHit* hits, uint8_t* occluded, uint32_t* counts, int nthreads) {
+                  int any, int niters, int sets, OrcHit* hits, uint8_t* occluded, uint32_t* counts, int nthreads) {
+    if (sets < 1 || sets > 2 || niters < 1) return -1;
     std::atomic<int> bad(0);
     parallel_for(nrays, nthreads, 256, [&](int i) {
         Walk8Out w;
-        walk8_one(nodes, nnodes, recs, nrecs, rays[i], any != 0, niters, w);
+        walk8_one(nodes, nnodes, recs, nrecs, rays[i], any != 0, niters, sets, w);
         if (w.bad) {
             bad.fetch_add(1);
             w = Walk8Out{INFINITY, 0.f, 0.f, -1, 0, 0xFFFFFFFFu, 0xFFFFFFFFu, true};

@@ -66,7 +66,7 @@ void orc_trace_any_dfs(const uint32_t* dfs, int nnodes, const float* packed,
  * node visits per round of the walk (the kernel's RTB_NODE_ITERS).  Returns
  * the number of rays whose walk left the arrays (0 for a valid tree). */
 int orc_walk_bvh8(const uint32_t* nodes, int nnodes, const float* recs, int nrecs, const OrcRay* rays,
-                  int nrays, int any, int niters, OrcHit* hits, uint8_t* occluded, uint32_t* counts,
+                  int nrays, int any, int niters, int sets, OrcHit* hits, uint8_t* occluded, uint32_t* counts,
                   int nthreads);
 void orc_brute_closest(const float* tris9, int ntris, const OrcRay* rays, int nrays,
                        OrcHit* hits, int nthreads);

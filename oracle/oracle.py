@@ -61,7 +61,7 @@ def lib() -> C.CDLL:
         L.orc_f2h_rn.argtypes = [C.c_float]
         L.orc_pt_pixels.argtypes = [vp, vp, vp, vp, i32, vp, i32, vp]
         L.orc_walk_bvh8.restype = i32
-        L.orc_walk_bvh8.argtypes = [vp, i32, vp, i32, vp, i32, i32, i32, vp, vp, vp, i32]
+        L.orc_walk_bvh8.argtypes = [vp, i32, vp, i32, vp, i32, i32, i32, i32, vp, vp, vp, i32]
         f32 = C.c_float
         L.orc_generate_rays.restype = i32
         L.orc_generate_rays.argtypes = [vp, i32, vp, vp, i32, i32, i32, C.c_uint32, f32, f32, f32, vp, f32, vp, vp,
@@ -120,11 +120,17 @@ def trace_closest_dfs(dfs, packed, rays, nthreads=0, stats=False):
     return (hits, st) if stats else hits
 
 
-def walk_bvh8(nodes, recs, rays, any_hit=False, niters=2, nthreads=0):
+# the release kernel's walk shape: node visits per round, pending triangle sets
+KERNEL_NITERS, KERNEL_SETS = 4, 2
+
+
+def walk_bvh8(nodes, recs, rays, any_hit=False, niters=KERNEL_NITERS, sets=KERNEL_SETS, nthreads=0):
     """The engine's 8-wide walk restated on the CPU (orc_walk_bvh8).  nodes:
     (N, 20) u32 as laid out on the device; recs: (M, 12) f32 triangle
-    records.  Returns (hits or occlusion flags, counts (n, 2) u32 of node
-    visits and triangle tests per ray); raises if a walk leaves the arrays."""
+    records; niters node visits per round and `sets` (1 or 2) pending
+    triangle sets per ray (the kernel's RTB_NODE_ITERS / RTB_TWO_SETS).
+    Returns (hits or occlusion flags, counts (n, 2) u32 of node visits and
+    triangle tests per ray); raises if a walk leaves the arrays."""
     rays = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
     nodes = np.ascontiguousarray(nodes, dtype=np.uint32).reshape(-1, 20)
     recs = np.ascontiguousarray(recs, dtype=np.float32).reshape(-1, 12)
@@ -132,8 +138,10 @@ def walk_bvh8(nodes, recs, rays, any_hit=False, niters=2, nthreads=0):
     counts = np.zeros((n, 2), dtype=np.uint32)
     out = np.zeros(n, dtype=np.uint8) if any_hit else np.zeros(n, dtype=HIT_DTYPE)
     bad = lib().orc_walk_bvh8(_p(nodes), nodes.shape[0], _p(recs), recs.shape[0], _p(rays), n, int(any_hit),
-                              niters, None if any_hit else _p(out), _p(out) if any_hit else None, _p(counts),
-                              nthreads)
+                              niters, sets, None if any_hit else _p(out), _p(out) if any_hit else None,
+                              _p(counts), nthreads)
+    if bad < 0:
+        raise ValueError("walk_bvh8: niters must be >= 1 and sets 1 or 2")
     if bad:
         raise ValueError(f"walk_bvh8: {bad} walks left the node or record arrays")
     return out, counts

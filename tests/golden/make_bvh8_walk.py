@@ -7,10 +7,12 @@ turns into algorithmic bytes per ray):
   bvh8_walk_3k_diffuse.npz   3,000 triangles in ~75 meshes of 20-60 packed in
                              a 10-unit box, 1,536 diffuse rays leaving their
                              surfaces (incoherent; over half hit, deeper walks).
-tests/test_oracle_bvh8.py replays the walks over the same nodes with the
-oracle on the CPU and must reproduce every value exactly.
+Each fixture also records the kernel's walk shape (node visits per round,
+pending triangle sets).  tests/test_oracle_bvh8.py replays the walks over
+the same nodes with the oracle at that shape on the CPU and must reproduce
+every value exactly.
 
-    python tests/golden/make_bvh8_walk.py      # needs the built library and a GPU
+    python tests/golden/make_bvh8_walk.py [OUTDIR]   # needs the built library and a GPU
 """
 import os
 import sys
@@ -27,6 +29,9 @@ from rtb200 import lib, scenes  # noqa: E402
 from rtb200.scenes import HIT_DTYPE, RAY_DTYPE  # noqa: E402
 
 NODE_BYTES, REC_BYTES = 80, 48
+# the release kernel's walk shape (RTB_NODE_ITERS, RTB_TWO_SETS + 1)
+NITERS, SETS = 4, 2
+OUT = HERE
 
 
 def d2h(ptr: int, nbytes: int) -> np.ndarray:
@@ -68,7 +73,7 @@ def fixture(name: str, tris: np.ndarray, rays: np.ndarray):
     shadow["tmax"] = np.where(hit, hits["t"] * cut, np.float32(np.inf)).astype(np.float32)
     cnt_a, occ = run(bvh, shadow, True)
     bvh.close()
-    np.savez_compressed(os.path.join(HERE, name), nodes=nodes, recs=recs,
+    np.savez_compressed(os.path.join(OUT, name), niters=np.int32(NITERS), sets=np.int32(SETS), nodes=nodes, recs=recs,
                         rays=rays.view(np.float32).reshape(-1, 8), hits=hits.view(np.float32).reshape(-1, 4),
                         counts_closest=cnt_c, shadow=shadow.view(np.float32).reshape(-1, 8), occ=occ,
                         counts_any=cnt_a)
@@ -78,6 +83,10 @@ def fixture(name: str, tris: np.ndarray, rays: np.ndarray):
 
 
 def main():
+    global OUT
+    if len(sys.argv) > 1:
+        OUT = sys.argv[1]
+        os.makedirs(OUT, exist_ok=True)
     torch.cuda.set_device(0)
     tris = scenes.scene_meshes(11, 2000)
     fixture("bvh8_walk_2k.npz", tris, scenes.scene_rays(tris, 1024, seed=5))

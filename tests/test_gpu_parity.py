@@ -368,6 +368,14 @@ def test_tlas_set_transforms_equals_a_fresh_build(cuda):
         moved.close()
 
 
+def _d2h(ptr, nbytes):
+    from cuda.bindings import runtime as cudart
+    out = np.empty(nbytes, np.uint8)
+    (err,) = cudart.cudaMemcpy(out.ctypes.data, ptr, nbytes, cudart.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+    assert err == cudart.cudaError_t.cudaSuccess, err
+    return out
+
+
 def test_counters_match_closest_results(cuda, small_scene):
     import torch
     bvh = lib.BVH(small_scene)
@@ -378,6 +386,37 @@ def test_counters_match_closest_results(cuda, small_scene):
     torch.cuda.synchronize()
     c = d_cnt.cpu().numpy().reshape(-1, 2)
     assert c[:, 0].min() >= 1 and c[:, 1].mean() > 0
+
+
+@pytest.mark.parametrize("any_hit", [False, True])
+def test_work_counts_equal_the_oracle_walk(cuda, any_hit):
+    """The kernel's per-ray node visits and triangle tests (the counts bench.py
+    turns into algorithmic bytes) equal the oracle's restated 8-wide walk at
+    the kernel's walk shape (node visits per round, pending triangle sets),
+    ray for ray, on the library's own nodes, for incoherent diffuse rays."""
+    import torch
+    tris = scenes.scene_meshes(13, 20000, box=30.0, lo=200, hi=2000)
+    bvh = lib.BVH(tris)
+    try:
+        rays = scenes.scene_rays(tris, 8192, seed=8)[4096:]
+        pn, n_nodes, pt, n_recs = bvh.layout()
+        nodes = _d2h(pn, n_nodes * 80).view(np.uint32).reshape(n_nodes, 20)
+        recs = _d2h(pt, n_recs * 48).view(np.float32).reshape(n_recs, 12)
+        n = rays.shape[0]
+        d_rays = _dev(torch, rays)
+        d_cnt = torch.zeros(n * 2, dtype=torch.int32, device="cuda")
+        bvh.counters(d_rays, n, d_cnt, any_hit=any_hit)
+        torch.cuda.synchronize()
+        got = d_cnt.cpu().numpy().view(np.uint32).reshape(n, 2)
+        out, ref = O.walk_bvh8(nodes, recs, rays, any_hit=any_hit)
+        assert np.array_equal(got, ref), f"{int((got != ref).any(1).sum())} of {n} rays differ"
+        if any_hit:
+            assert np.array_equal(gpu_any(bvh, rays), out)
+        else:
+            assert_hits_equal(gpu_closest(bvh, rays), out, "8-wide walk")
+        assert got[:, 0].mean() > 4 and got[:, 1].mean() > 2  # deep, incoherent walks
+    finally:
+        bvh.close()
 
 
 def test_path_tracer_vs_fp64_oracle(cuda):

@@ -140,12 +140,15 @@ def test_walk_reproduces_the_kernel(path):
     g = np.load(path)
     rays = np.ascontiguousarray(g["rays"]).view(RAY_DTYPE).reshape(-1)
     shadow = np.ascontiguousarray(g["shadow"]).view(RAY_DTYPE).reshape(-1)
-    hits, cnt = O.walk_bvh8(g["nodes"], g["recs"], rays)
+    # the walk shape of the kernel that wrote the fixture
+    shape = dict(niters=int(g["niters"]), sets=int(g["sets"]))
+    assert (shape["niters"], shape["sets"]) == (O.KERNEL_NITERS, O.KERNEL_SETS), "fixture of another kernel"
+    hits, cnt = O.walk_bvh8(g["nodes"], g["recs"], rays, **shape)
     ref = np.ascontiguousarray(g["hits"]).view(HIT_DTYPE).reshape(-1)
     assert (ref["prim"] >= 0).any()
     assert np.array_equal(hits.view(np.uint8), ref.view(np.uint8))  # t, primitive, u, v bit for bit
     assert np.array_equal(cnt, g["counts_closest"])  # node visits and triangle tests, every ray
-    occ, cnt_any = O.walk_bvh8(g["nodes"], g["recs"], shadow, any_hit=True)
+    occ, cnt_any = O.walk_bvh8(g["nodes"], g["recs"], shadow, any_hit=True, **shape)
     assert 0 < occ.sum() < occ.size
     assert np.array_equal(occ, g["occ"])
     assert np.array_equal(cnt_any, g["counts_any"])
