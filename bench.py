@@ -855,6 +855,20 @@ def run_batched(args):
             b.close()
     info = b.info()
     b.close()
+    # --- A/B of the build: the same kernels driven level by level from the
+    # host (rtBatch_buildEx with RT_BATCH_BUILD_HOST_LOOP; same tree)
+    build_loop, dev_loop = [], []
+    for k in range(1 + max(1, min(args.steps, 3))):
+        flush.zero_()
+        torch.cuda.synchronize()
+        h0 = time.perf_counter()
+        bl = lib.Batch(all_tris=allt, tri_offsets=tri_off, host_loop=True)
+        torch.cuda.synchronize()
+        h1 = time.perf_counter()
+        if k >= 1:
+            build_loop.append((h1 - h0) * 1e3)
+            dev_loop.append(bl.info()["build_ms"])
+        bl.close()
     # --- plain per-scene calls on the same data
     build_plain, trace_plain = [], []
     psteps = max(1, min(args.steps, 3))
@@ -899,7 +913,10 @@ def run_batched(args):
                                       f"{bounds[0]}-{bounds[1] - 1}), no collective" if ws > 1 else "one GPU")},
            "ours": {"build_ms": round(bo, 2), "trace_ms": round(to, 3), "trace_mrays_s": round(nr / to / 1e3, 1),
                     "device_build_ms": round(info["build_ms"], 2), "tuning": shape,
-                    "launches": "one build pipeline for all scenes, one graph-captured trace launch"},
+                    "launches": "the whole build as one CUDA graph launch (level loops as conditional WHILE "
+                                "nodes), one graph-captured trace launch",
+                    "build_host_loop_ms": round(float(np.mean(build_loop)), 2),
+                    "device_build_host_loop_ms": round(float(np.mean(dev_loop)), 2)},
            "plain": {"build_ms": round(bp, 2), "trace_ms": round(tp, 3), "trace_mrays_s": round(nr / tp / 1e3, 1),
                      "value": round(nr_all / step_plain / 1e3, 1), "steps": psteps,
                      "launches": "256 cudaBVH_build + 256 cudaBVH_traceClosest"},

@@ -248,13 +248,21 @@ int cudaTLAS_getInverseTransforms(CudaTLAS_t tlas, float* out, int numInstances)
 
 /* ---------------- batched scenes ----------------
  * Many independent scenes built in one multi-scene SAH build (every build
- * stage is one launch for all scenes) and traced by one persistent
- * work-stealing launch.  Triangles of scene i are tri_offsets[i] ..
+ * stage is one launch for all scenes, all of it one CUDA graph) and traced
+ * by one persistent work-stealing launch.  Triangles of scene i are tri_offsets[i] ..
  * tri_offsets[i+1]-1 of h_tris; rays of scene i are d_ray_offsets[i] ..
  * d_ray_offsets[i+1]-1 (device array, num_scenes+1 entries).  Reported
  * primitive ids are relative to their scene. */
 typedef struct RtBatchHandle* RtBatch_t;
 RtBatch_t rtBatch_build(const CudaTri* h_tris, const int* tri_offsets, int num_scenes, void* stream);
+/* rtBatch_build runs the whole build (SAH levels, small and warp subtrees,
+ * 8-wide collapse) as ONE CUDA graph launch: both level loops are
+ * conditional WHILE nodes whose counts stay on the device.  flags
+ * RT_BATCH_BUILD_HOST_LOOP instead drives the same kernels from the host,
+ * level by level (the single-scene builder's loop).  Both give the same
+ * tree, byte for byte. */
+#define RT_BATCH_BUILD_HOST_LOOP 1
+RtBatch_t rtBatch_buildEx(const CudaTri* h_tris, const int* tri_offsets, int num_scenes, int flags, void* stream);
 void rtBatch_destroy(RtBatch_t batch);
 int rtBatch_traceClosest(RtBatch_t batch, const RtRay* d_rays, const int* d_ray_offsets, int n, RtHit* d_hits,
                          void* stream);
@@ -287,6 +295,11 @@ int rtBatch_setTuning(RtBatch_t batch, int ctas_per_sm, int node_iters);
 int rtBatch_setTuningEx(RtBatch_t batch, const RtBatchTuning* tuning);
 int rtBatch_getTuning(RtBatch_t batch, RtBatchTuning* out);
 int rtBatch_getInfo(RtBatch_t batch, int* num_scenes, int* num_nodes, float* build_ms);
+/* Device arrays of the batch's 8-wide layout (scene i's root is node i;
+ * triangle records carry scene-relative primitive ids), borrowed, valid
+ * until destroy. */
+int rtBatch_getDeviceLayout(RtBatch_t batch, const void** d_nodes, int* num_nodes, const void** d_tris,
+                            int* num_tris);
 
 /* ---------------- wavefront path tracer ----------------
  * Lambertian scene over a TLAS: per-instance albedo and emission; emission

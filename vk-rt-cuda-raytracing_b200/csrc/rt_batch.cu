@@ -30,6 +30,7 @@ struct RtBatchHandle {
     DevBuf<int> work, status;  // work[0]: plain launches, work[1]: graph launches
     RtBatchTuning tune{TRACE_MINB * TRACE_T / 32, RTB_NODE_ITERS, TRACE_T, SSTACK};
     float build_ms = 0.f;
+    bool graph_build = true;  // built by the graph-driven builder (else the host-driven level loop)
     // captured graph and the arguments it was captured with
     cudaGraphExec_t gexec = nullptr;
     cudaStream_t cap_stream = nullptr;
@@ -103,9 +104,10 @@ int check_trace_args(RtBatchHandle* b, const RtRay* rays, const int* off, int n,
 
 extern "C" {
 
-RtBatch_t rtBatch_build(const CudaTri* h_tris, const int* tri_offsets, int num_scenes, void* stream) {
+RtBatch_t rtBatch_buildEx(const CudaTri* h_tris, const int* tri_offsets, int num_scenes, int flags, void* stream) {
     clear_error();
-    if (!h_tris || !tri_offsets || num_scenes <= 0 || tri_offsets[0] != 0) {
+    if (!h_tris || !tri_offsets || num_scenes <= 0 || tri_offsets[0] != 0 ||
+        (flags & ~(RT_BATCH_BUILD_HOST_LOOP)) != 0) {
         set_error("rtBatch_build: invalid argument");
         return nullptr;
     }
@@ -140,7 +142,11 @@ RtBatch_t rtBatch_build(const CudaTri* h_tris, const int* tri_offsets, int num_s
         launch_tri_bounds(tris9.p, n, lo.p, hi.p, s);
         BuildConfig cfg = default_build_config();
         cfg.transient = true;
-        ok = build_bvh2(lo.p, hi.p, n, cfg, bvh2, s, &b->tri_off) && collapse_bvh8(bvh2, tris9.p, b->bvh8, s);
+        b->graph_build = !(flags & RT_BATCH_BUILD_HOST_LOOP);
+        if (b->graph_build)
+            ok = build_bvh8_graph(lo.p, hi.p, tris9.p, n, cfg, b->tri_off, b->bvh8, s, nullptr);
+        else
+            ok = build_bvh2(lo.p, hi.p, n, cfg, bvh2, s, &b->tri_off) && collapse_bvh8(bvh2, tris9.p, b->bvh8, s);
         cudaEventRecord(e1, s);
         ok = ok && RT_CUDA(cudaEventSynchronize(e1));
         if (ok) cudaEventElapsedTime(&b->build_ms, e0, e1);
@@ -154,6 +160,10 @@ RtBatch_t rtBatch_build(const CudaTri* h_tris, const int* tri_offsets, int num_s
         return nullptr;
     }
     return b;
+}
+
+RtBatch_t rtBatch_build(const CudaTri* h_tris, const int* tri_offsets, int num_scenes, void* stream) {
+    return rtBatch_buildEx(h_tris, tri_offsets, num_scenes, 0, stream);
 }
 
 void rtBatch_destroy(RtBatch_t b) {
@@ -302,6 +312,18 @@ int rtBatch_getTuning(RtBatch_t b, RtBatchTuning* out) {
         return RT_ERR_INVALID;
     }
     *out = b->tune;
+    return RT_OK;
+}
+
+int rtBatch_getDeviceLayout(RtBatch_t b, const void** d_nodes, int* num_nodes, const void** d_tris, int* num_tris) {
+    if (!b) {
+        set_error("rtBatch_getDeviceLayout: invalid argument");
+        return RT_ERR_INVALID;
+    }
+    if (d_nodes) *d_nodes = b->bvh8.nodes.p;
+    if (num_nodes) *num_nodes = b->bvh8.num_nodes;
+    if (d_tris) *d_tris = b->bvh8.tris.p;
+    if (num_tris) *num_tris = b->bvh8.num_leaf_items;
     return RT_OK;
 }
 

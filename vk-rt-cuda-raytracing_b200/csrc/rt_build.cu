@@ -119,6 +119,114 @@ bool scan_exclusive(const int* d_in, int* d_out, int n, int* d_total, cudaStream
     return RT_CUDA(cudaGetLastError());
 }
 
+// The same exclusive scan with its element count read on the device (d_n;
+// null: all `cap` elements) and caller-provided scratch (scan_scratch_ints),
+// so it can be enqueued into a graph whose counts the host never sees.
+// Tiles past the count write a zero tile sum, so the next level's scan over
+// all tiles stays exact.
+__device__ __forceinline__ int scan_count(const int* d_n, int cap) { return d_n ? min(max(*d_n, 0), cap) : cap; }
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_tiles_n(const int* __restrict__ in, int* __restrict__ out, int cap,
+                                                         const int* __restrict__ d_n, int* __restrict__ tile_sums) {
+    __shared__ int ws[SCAN_T / 32];
+    const int n = scan_count(d_n, cap);
+    if (blockIdx.x * SCAN_TILE >= n) {  // block-uniform
+        if (threadIdx.x == 0 && tile_sums) tile_sums[blockIdx.x] = 0;
+        return;
+    }
+    const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_IPT;
+    int v[SCAN_IPT];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_IPT; k++) {
+        v[k] = base + k < n ? in[base + k] : 0;
+        sum += v[k];
+    }
+    int total;
+    int run = block_exclusive_scan<SCAN_T>(sum, ws, total);
+#pragma unroll
+    for (int k = 0; k < SCAN_IPT; k++) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == 0 && tile_sums) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void k_scan_add_n(int* __restrict__ out, int cap, const int* __restrict__ d_n,
+                             const int* __restrict__ tile_off) {
+    const int n = scan_count(d_n, cap);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] += tile_off[i / SCAN_TILE];
+}
+
+__global__ void k_scan_total_n(const int* __restrict__ in, const int* __restrict__ out, int cap,
+                               const int* __restrict__ d_n, int* __restrict__ total) {
+    const int n = scan_count(d_n, cap);
+    *total = n > 0 ? out[n - 1] + in[n - 1] : 0;
+}
+
+size_t scan_scratch_ints(int cap) {
+    size_t total = 1;
+    for (int m = cap; m > SCAN_TILE;) {
+        const int tiles = (m + SCAN_TILE - 1) / SCAN_TILE;
+        total += 2 * (size_t)tiles;
+        m = tiles;
+    }
+    return total;
+}
+
+bool scan_exclusive_dev(const int* d_in, int* d_out, int cap, const int* d_n, int* d_total, int* scratch,
+                        cudaStream_t s) {
+    if (cap > 0) {
+        const int tiles = (cap + SCAN_TILE - 1) / SCAN_TILE;
+        if (tiles == 1) {
+            k_scan_tiles_n<<<1, SCAN_T, 0, s>>>(d_in, d_out, cap, d_n, nullptr);
+        } else {
+            int* sums = scratch;
+            int* offs = scratch + tiles;
+            k_scan_tiles_n<<<tiles, SCAN_T, 0, s>>>(d_in, d_out, cap, d_n, sums);
+            if (!scan_exclusive_dev(sums, offs, tiles, nullptr, nullptr, scratch + 2 * tiles, s)) return false;
+            k_scan_add_n<<<std::min((cap + 255) / 256, num_sms() * 16), 256, 0, s>>>(d_out, cap, d_n, offs);
+        }
+    }
+    if (d_total) k_scan_total_n<<<1, 1, 0, s>>>(d_in, d_out, cap > 0 ? cap : 0, cap > 0 ? d_n : nullptr, d_total);
+    return RT_CUDA(cudaGetLastError());
+}
+
+// Creates a conditional handle on the graph being captured on cs (value 0
+// at every launch until a kernel sets it).
+bool capture_conditional_handle(cudaStream_t cs, cudaGraphConditionalHandle* h) {
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    if (!RT_CUDA(cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, nullptr, nullptr))) return false;
+    if (st != cudaStreamCaptureStatusActive || !g) {
+        set_error("graph build: stream is not capturing");
+        return false;
+    }
+    return RT_CUDA(cudaGraphConditionalHandleCreate(h, g, 0, cudaGraphCondAssignDefault));
+}
+
+// Appends a WHILE node on handle h at the capture position of cs; its body
+// graph (empty, to be captured) is returned in *body.
+bool capture_while(cudaStream_t cs, cudaGraphConditionalHandle h, cudaGraph_t* body) {
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    if (!RT_CUDA(cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd))) return false;
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (!RT_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p)) ||
+        !RT_CUDA(cudaStreamUpdateCaptureDependencies(cs, &node, 1, cudaStreamSetCaptureDependencies)))
+        return false;
+    *body = p.conditional.phGraph_out[0];
+    return true;
+}
+
 // -------------------------------------------------------- prim bounds --
 __global__ void k_tri_bounds(const float* __restrict__ t9, int n, float4* __restrict__ lo,
                              float4* __restrict__ hi) {
@@ -662,16 +770,15 @@ __device__ void block_minmax6(float (&v)[6], float* sh) {
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(SMALL_T) k_build_small(const Task* __restrict__ small, const int* __restrict__ res_off,
-                                                         int res_base, int* __restrict__ perm,
-                                                         const float4* __restrict__ plo, const float4* __restrict__ phi,
-                                                         Node2* __restrict__ nodes, int max_leaf, int max_sah_depth,
-                                                         int small_task, int warp_task, WTask* __restrict__ wq,
-                                                         int wq_cap, int* __restrict__ wq_count,
-                                                         int* __restrict__ status) {
+__device__ __forceinline__ void build_small_task(int task, const Task* __restrict__ small,
+                                                 const int* __restrict__ res_off, int res_base, int* __restrict__ perm,
+                                                 const float4* __restrict__ plo, const float4* __restrict__ phi,
+                                                 Node2* __restrict__ nodes, int max_leaf, int max_sah_depth,
+                                                 int small_task, int warp_task, WTask* __restrict__ wq, int wq_cap,
+                                                 int* __restrict__ wq_count, int* __restrict__ status) {
     extern __shared__ float4 smem4[];
     float* sm = reinterpret_cast<float*>(smem4);
-    const Task tk = small[blockIdx.x];
+    const Task tk = small[task];
     const int n = tk.count;
     float* blo = sm;                                  // [3][small_task]
     float* bhi = blo + 3 * small_task;                // [3][small_task]
@@ -701,7 +808,7 @@ __global__ void __launch_bounds__(SMALL_T) k_build_small(const Task* __restrict_
         SubTask r;
         r.node = tk.node; r.lstart = 0; r.count = n; r.depth = tk.depth;
         stack[0] = r;
-        next_node = res_base + res_off[blockIdx.x];
+        next_node = res_base + res_off[task];
     }
     __syncthreads();
     while (true) {
@@ -913,6 +1020,43 @@ __global__ void __launch_bounds__(SMALL_T) k_build_small(const Task* __restrict_
         __syncthreads();
     }
     for (int i = threadIdx.x; i < n; i += SMALL_T) perm[tk.start + i] = gidx[pa[i]];
+}
+
+// One CTA per small task.
+__global__ void __launch_bounds__(SMALL_T) k_build_small(const Task* __restrict__ small, const int* __restrict__ res_off,
+                                                         int res_base, int* __restrict__ perm,
+                                                         const float4* __restrict__ plo, const float4* __restrict__ phi,
+                                                         Node2* __restrict__ nodes, int max_leaf, int max_sah_depth,
+                                                         int small_task, int warp_task, WTask* __restrict__ wq,
+                                                         int wq_cap, int* __restrict__ wq_count,
+                                                         int* __restrict__ status) {
+    build_small_task(blockIdx.x, small, res_off, res_base, perm, plo, phi, nodes, max_leaf, max_sah_depth, small_task,
+                     warp_task, wq, wq_cap, wq_count, status);
+}
+
+// Persistent CTAs take small tasks from a work counter until the device's
+// task count (*d_S) is reached; the node ids still come from each task's
+// reserved range, so the tree does not depend on which CTA took a task.
+__global__ void __launch_bounds__(SMALL_T) k_build_small_loop(const Task* __restrict__ small, const int* __restrict__ d_S,
+                                                              int* __restrict__ work, const int* __restrict__ res_off,
+                                                              const int* __restrict__ d_res_base, int* __restrict__ perm,
+                                                              const float4* __restrict__ plo,
+                                                              const float4* __restrict__ phi,
+                                                              Node2* __restrict__ nodes, int max_leaf,
+                                                              int max_sah_depth, int small_task, int warp_task,
+                                                              WTask* __restrict__ wq, int wq_cap,
+                                                              int* __restrict__ wq_count, int* __restrict__ status) {
+    __shared__ int s_task;
+    const int S = *d_S, res_base = *d_res_base;
+    for (;;) {
+        __syncthreads();  // the previous task is done with shared memory
+        if (threadIdx.x == 0) s_task = atomicAdd(work, 1);
+        __syncthreads();
+        const int t = s_task;
+        if (t >= S) break;
+        build_small_task(t, small, res_off, res_base, perm, plo, phi, nodes, max_leaf, max_sah_depth, small_task,
+                         warp_task, wq, wq_cap, wq_count, status);
+    }
 }
 
 // One warp finishes a subtree of at most 32 primitives with an exact SAH
@@ -1391,6 +1535,315 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
         return false;
     }
     out.num_nodes = node_count;
+    return true;
+}
+
+
+// ------------------------------------------------- graph-driven build --
+// The whole build -- per-scene roots, the level loop of large tasks, the
+// small and warp tiers, and the 8-wide collapse -- enqueued as ONE CUDA
+// graph whose two level loops are conditional WHILE nodes: no count ever
+// travels to the host, grids are sized for upper bounds (threads past the
+// device's counts exit, as in the host-driven loop), and the result is the
+// same tree, node for node.
+struct BuildCtl {
+    int T;         // this level's large-task count
+    int node;      // next free binary node id
+    int small;     // small tasks so far
+    int tot[2];    // scan totals: large and small kids of the level
+    int C;         // chunks of the level
+    int levels;    // levels run
+    int log_T;     // (k_level_end's per-level log slot, unused here)
+    int reserved;  // node ids reserved by the small tasks
+    int wq_count;  // warp-task queue length
+    int work;      // small-task work counter
+    int status;    // as the host-driven build; 16: more than kMaxLevels levels
+};
+
+__global__ void k_acc_init(uint32_t* __restrict__ acc, int S) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 12 * S; i += gridDim.x * blockDim.x) {
+        const int k = i % 12;
+        acc[i] = ((k >= 3 && k < 6) || k >= 9) ? 0u : 0xFFFFFFFFu;
+    }
+}
+
+// One CTA: every segment's root node and task, in segment order (leaf
+// roots finish here; the others go to the large or small task list), the
+// counters, and the loop condition.
+constexpr int ROOTS_T = 256;
+__global__ void __launch_bounds__(ROOTS_T) k_roots(const uint32_t* __restrict__ acc, const int* __restrict__ seg, int S,
+                                                   int max_leaf, int small_task, Node2* __restrict__ nodes,
+                                                   Task* __restrict__ large, Task* __restrict__ small,
+                                                   BuildCtl* __restrict__ ctl, cudaGraphConditionalHandle cond) {
+    __shared__ int ws[ROOTS_T / 32];
+    int nl = 0, ns = 0;
+    for (int base = 0; base < S; base += ROOTS_T) {
+        const int i = base + threadIdx.x;
+        Task t = {};
+        Node2 r = {};
+        int is_l = 0, is_s = 0;
+        if (i < S) {
+            const uint32_t* a = acc + (size_t)i * 12;
+            t.node = i;
+            t.start = seg[i];
+            t.count = seg[i + 1] - seg[i];
+            t.depth = 0;
+            for (int k = 0; k < 3; k++) {
+                r.lo[k] = ord2f(a[k]);
+                r.hi[k] = ord2f(a[3 + k]);
+                t.clo[k] = ord2f(a[6 + k]);
+                t.chi[k] = ord2f(a[9 + k]);
+            }
+            if (t.count <= max_leaf) {
+                r.a = t.start;
+                r.b = -t.count;
+            } else if (t.count <= small_task) {
+                is_s = 1;
+            } else {
+                is_l = 1;
+            }
+            nodes[i] = r;
+        }
+        int tl, ts;
+        const int ol = block_exclusive_scan<ROOTS_T>(is_l, ws, tl);
+        const int os = block_exclusive_scan<ROOTS_T>(is_s, ws, ts);
+        if (is_l) large[nl + ol] = t;
+        if (is_s) small[ns + os] = t;
+        nl += tl;
+        ns += ts;
+    }
+    if (threadIdx.x == 0) {
+        BuildCtl c = {};
+        c.T = nl;
+        c.node = S;
+        c.small = ns;
+        *ctl = c;
+        cudaGraphSetConditional(cond, nl > 0 ? 1u : 0u);
+    }
+}
+
+// After k_level_end: the next level's tasks become the current ones (the
+// loop's kernels keep fixed buffer arguments), and the loop goes on while
+// tasks remain, nothing overflowed and the level bound holds.
+__global__ void k_level_next(const Task* __restrict__ nxt, Task* __restrict__ cur, BuildCtl* __restrict__ ctl,
+                             cudaGraphConditionalHandle cond) {
+    const int T = ctl->T;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < T; i += gridDim.x * blockDim.x) cur[i] = nxt[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const int lv = ++ctl->levels;
+        if (T > 0 && lv >= kMaxLevels) ctl->status |= 16;
+        cudaGraphSetConditional(cond, (T > 0 && lv < kMaxLevels && !(ctl->status & 8)) ? 1u : 0u);
+    }
+}
+
+// Node ids each small task reserves (2 count - 2), zero past the count.
+__global__ void k_reserve_n(const Task* __restrict__ small, const int* __restrict__ d_S, int cap,
+                            int* __restrict__ need) {
+    const int S = *d_S;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x)
+        need[i] = i < S ? 2 * small[i].count - 2 : 0;
+}
+
+__global__ void k_build_result(const BuildCtl* __restrict__ ctl, int* __restrict__ out) {
+    out[0] = ctl->node + ctl->reserved;
+    out[1] = ctl->status;
+    out[2] = ctl->levels;
+    out[3] = ctl->small;
+}
+
+bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tris9, int n, const BuildConfig& cfg,
+                      const std::vector<int>& seg, Bvh8Device& out, cudaStream_t s, GraphBuildInfo* info) {
+    if (n <= 0 || !d_tris9) {
+        set_error("graph build: empty input");
+        return false;
+    }
+    if (cfg.max_leaf < 1 || cfg.max_leaf > 4 || cfg.small_task < WARP_TASK || cfg.small_task > 32 * SMALL_T) {
+        set_error("graph build: bad configuration");
+        return false;
+    }
+    const int S = (int)seg.size() - 1;
+    if (S < 1 || seg.front() != 0 || seg.back() != n) {
+        set_error("graph build: bad segment table");
+        return false;
+    }
+    int maxcnt = 0;
+    for (int i = 0; i < S; i++) {
+        if (seg[i + 1] <= seg[i]) {
+            set_error("graph build: segment %d is empty", i);
+            return false;
+        }
+        maxcnt = std::max(maxcnt, seg[i + 1] - seg[i]);
+    }
+    // upper bounds the graph's grids and buffers are sized for
+    const int maxT = n / (cfg.small_task + 1) + 2;     // large tasks per level
+    const int Cb = n / CHUNK + maxT + 1;               // chunks per level
+    const int maxChunks = Cb + 1;
+    const int Kb = 2 * maxT;                           // kids per level
+    const int maxSmall = n / (cfg.max_leaf + 1) + 2;   // small tasks in all
+    const int slots = 2 * n + 2;                       // binary node ids
+    const int warp_task = std::min(cfg.warp_task, WARP_TASK);
+    const int wq_cap = warp_task > 0 ? n / (cfg.max_leaf + 1) + 2 : 0;
+    const int scan_cap = std::max(std::max(maxT, Cb), std::max(Kb, maxSmall));
+    const size_t cbytes = collapse_graph_scratch_bytes(n, S, slots, true);
+    TmpBuf<Node2> nodes;
+    TmpBuf<int> perm, tmp, dseg, ccount, coff, cleft, cleftoff, flags, need, off, scan, result;
+    TmpBuf<uint32_t> acc, gbins, kcb;
+    TmpBuf<Task> tasks_a, tasks_b, kids, small;
+    TmpBuf<Split> splits;
+    TmpBuf<uint8_t> side;
+    TmpBuf<Chunk> chunks;
+    TmpBuf<WTask> wq;
+    TmpBuf<BuildCtl> ctl;
+    TmpBuf<char> cscratch;
+    if (!nodes.alloc(slots, s) || !perm.alloc(n, s) || !tmp.alloc(n, s) || !dseg.alloc(S + 1, s) ||
+        !acc.alloc((size_t)12 * S, s) || !tasks_a.alloc(maxT, s) || !tasks_b.alloc(maxT, s) || !kids.alloc(Kb, s) ||
+        !small.alloc(maxSmall, s) || !splits.alloc(maxT, s) || !gbins.alloc((size_t)maxT * TASK_BIN_WORDS, s) ||
+        !flags.alloc((size_t)4 * Kb, s) || !kcb.alloc((size_t)12 * maxT, s) || !side.alloc(n, s) ||
+        !chunks.alloc(maxChunks, s) || !ccount.alloc(maxT, s) || !coff.alloc(maxT, s) || !cleft.alloc(maxChunks, s) ||
+        !cleftoff.alloc(maxChunks, s) || !need.alloc(maxSmall, s) || !off.alloc(maxSmall, s) ||
+        (wq_cap > 0 && !wq.alloc(wq_cap, s)) || !ctl.alloc(1, s) || !scan.alloc(scan_scratch_ints(scan_cap), s) ||
+        !result.alloc(8, s) || !cscratch.alloc(cbytes, s))
+        return false;
+    if (!out.nodes.alloc((size_t)n + S) || !out.tris.alloc(n)) return false;
+    if (!RT_CUDA(cudaMemcpyAsync(dseg.p, seg.data(), sizeof(int) * (S + 1), cudaMemcpyHostToDevice, s))) return false;
+    const size_t smem = (size_t)cfg.small_task * (6 * 4 + 4 + 2 + 2) + 16 + 3 * kBins * 7 * 4;
+    if (!RT_CUDA(cudaFuncSetAttribute(k_build_small_loop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+        return false;
+    int small_per_sm = 0, warp_per_sm = 0;
+    if (!RT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&small_per_sm, k_build_small_loop, SMALL_T, smem)) ||
+        !RT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&warp_per_sm, k_build_warp, WB_T, 0)))
+        return false;
+    const int small_grid = num_sms() * std::max(1, small_per_sm);
+    const int warp_grid = num_sms() * std::max(1, warp_per_sm);
+
+    // capture on two private streams; nothing runs until the launch on s
+    cudaStream_t cs = nullptr, bs = nullptr;
+    if (!RT_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) ||
+        !RT_CUDA(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking))) {
+        if (cs) cudaStreamDestroy(cs);
+        return false;
+    }
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool ok = RT_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed));
+    bool capturing = ok;
+    BuildCtl* c = ctl.p;
+    Task* cur = tasks_a.p;
+    Task* nxt = tasks_b.p;
+    int* is_large = flags.p;
+    int* is_small = flags.p + Kb;
+    int* large_off = flags.p + 2 * Kb;
+    int* small_off = flags.p + 3 * Kb;
+    if (ok) {
+        cudaMemsetAsync(nodes.p, 0, sizeof(Node2) * (size_t)slots, cs);
+        k_iota<<<(n + 255) / 256, 256, 0, cs>>>(perm.p, n);
+        k_acc_init<<<std::max(1, std::min((12 * S + 255) / 256, 1024)), 256, 0, cs>>>(acc.p, S);
+        k_seg_bounds<<<dim3(std::min((maxcnt + 2047) / 2048, 64), S), 256, 0, cs>>>(d_lo, d_hi, dseg.p, acc.p);
+        cudaGraphConditionalHandle lv_cond;
+        cudaGraph_t body;
+        ok = capture_conditional_handle(cs, &lv_cond);
+        if (ok) {
+            k_roots<<<1, ROOTS_T, 0, cs>>>(acc.p, dseg.p, S, cfg.max_leaf, cfg.small_task, nodes.p, cur, small.p, c,
+                                           lv_cond);
+            ok = capture_while(cs, lv_cond, &body) &&
+                 RT_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        }
+        if (ok) {
+            // one level of large tasks (the host-driven loop's sequence)
+            k_chunk_counts<<<(maxT + 255) / 256, 256, 0, bs>>>(cur, &c->T, maxT, ccount.p);
+            bool lok = scan_exclusive_dev(ccount.p, coff.p, maxT, nullptr, &c->C, scan.p, bs);
+            k_fill_chunks<<<maxT, 128, 0, bs>>>(cur, &c->T, coff.p, chunks.p);
+            k_clear_bins<<<std::min(maxT * 8, 4096), 256, 0, bs>>>(gbins.p, &c->T);
+            k_bin_large<<<Cb, CHUNK_T, 0, bs>>>(chunks.p, cur, perm.p, d_lo, d_hi, gbins.p, &c->C);
+            k_split_large<<<(maxT + 3) / 4, 128, 0, bs>>>(cur, &c->T, gbins.p, splits.p, kids.p, kcb.p, nodes.p,
+                                                          &c->node, cfg.max_leaf, cfg.max_sah_depth);
+            k_count_left<<<Cb, CHUNK_T, 0, bs>>>(chunks.p, cur, splits.p, perm.p, d_lo, d_hi, cleft.p, kcb.p, &c->C,
+                                                 side.p);
+            lok = lok && scan_exclusive_dev(cleft.p, cleftoff.p, Cb, nullptr, nullptr, scan.p, bs);
+            k_scatter<<<Cb, CHUNK_T, 0, bs>>>(chunks.p, cur, splits.p, perm.p, side.p, cleftoff.p, tmp.p, &c->C);
+            k_copy_back<<<Cb, 256, 0, bs>>>(chunks.p, tmp.p, perm.p, &c->C);
+            k_classify_flags<<<(Kb + 255) / 256, 256, 0, bs>>>(kids.p, &c->T, Kb, cfg.max_leaf, cfg.small_task,
+                                                               is_large, is_small);
+            lok = lok && scan_exclusive_dev(is_large, large_off, Kb, nullptr, &c->tot[0], scan.p, bs) &&
+                  scan_exclusive_dev(is_small, small_off, Kb, nullptr, &c->tot[1], scan.p, bs);
+            k_compact_kids<<<(Kb + 255) / 256, 256, 0, bs>>>(kids.p, &c->T, is_large, large_off, is_small, small_off,
+                                                             nxt, maxT, small.p, maxSmall, &c->small, kcb.p,
+                                                             &c->status);
+            k_level_end<<<1, 1, 0, bs>>>(&c->T, &c->node, &c->small, c->tot, maxT, maxSmall, &c->log_T, &c->status);
+            k_level_next<<<std::min((maxT + 255) / 256, 1024), 256, 0, bs>>>(nxt, cur, c, lv_cond);
+            lok = lok && RT_CUDA(cudaGetLastError());
+            cudaGraph_t done = nullptr;
+            ok = RT_CUDA(cudaStreamEndCapture(bs, &done)) && lok;
+        }
+        if (ok) {
+            // small tasks (one CTA each, persistent) and warp subtrees
+            k_reserve_n<<<std::min((maxSmall + 255) / 256, num_sms() * 16), 256, 0, cs>>>(small.p, &c->small,
+                                                                                          maxSmall, need.p);
+            ok = scan_exclusive_dev(need.p, off.p, maxSmall, &c->small, &c->reserved, scan.p, cs);
+            k_build_small_loop<<<small_grid, SMALL_T, smem, cs>>>(small.p, &c->small, &c->work, off.p, &c->node,
+                                                                  perm.p, d_lo, d_hi, nodes.p, cfg.max_leaf,
+                                                                  cfg.max_sah_depth, cfg.small_task, warp_task, wq.p,
+                                                                  wq_cap, &c->wq_count, &c->status);
+            if (warp_task > 0)
+                k_build_warp<<<warp_grid, WB_T, 0, cs>>>(wq.p, &c->wq_count, wq_cap, perm.p, d_lo, d_hi, nodes.p,
+                                                         cfg.max_leaf, cfg.max_sah_depth);
+            k_build_result<<<1, 1, 0, cs>>>(c, result.p);
+            ok = ok && RT_CUDA(cudaGetLastError());
+        }
+        ok = ok && enqueue_collapse_graph(nodes.p, perm.p, n, S, slots, d_tris9, out.nodes.p, out.tris.p, nullptr,
+                                          cscratch.p, cbytes, result.p + 4, cs, bs);
+        cudaGraph_t g = nullptr;
+        const bool ended = RT_CUDA(cudaStreamEndCapture(cs, &g));
+        capturing = false;
+        graph = g;
+        ok = ok && ended && graph;
+    }
+    if (capturing) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(cs, &g);
+        if (g) cudaGraphDestroy(g);
+    }
+    int h[8] = {};
+    if (ok) {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        ok = RT_CUDA(cudaGraphInstantiate(&exec, graph, 0)) && RT_CUDA(cudaEventRecord(e0, s)) &&
+             RT_CUDA(cudaGraphLaunch(exec, s)) && RT_CUDA(cudaEventRecord(e1, s)) &&
+             RT_CUDA(cudaMemcpyAsync(h, result.p, sizeof(h), cudaMemcpyDeviceToHost, s)) &&
+             RT_CUDA(cudaStreamSynchronize(s));
+        if (ok && info) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            info->graph_ms = ms;
+        }
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(bs);
+    cudaStreamDestroy(cs);
+    if (!ok) return false;
+    if (h[1]) {
+        set_error("graph build: %s", (h[1] & 16) ? "more levels than the bound"
+                                     : (h[1] & 8) ? "task list overflow"
+                                     : (h[1] & 2) ? "subtree queue overflow"
+                                                  : "subtree stack overflow");
+        return false;
+    }
+    if (h[7]) {
+        set_error("collapse: %s", (h[7] & 1) ? "capacity exceeded" : "more levels than the bound");
+        return false;
+    }
+    out.num_nodes = h[4];
+    out.num_leaf_items = h[5];
+    out.depth = h[6];
+    if (info) {
+        info->bvh2_nodes = h[0];
+        info->levels = h[2];
+        info->small_tasks = h[3];
+    }
     return true;
 }
 

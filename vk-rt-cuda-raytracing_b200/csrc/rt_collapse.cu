@@ -19,6 +19,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -135,11 +136,9 @@ __global__ void k_dp(const Node2* __restrict__ nodes, int slots, const int* __re
     }
 }
 
-__global__ void k_gather_dp(const Node2* __restrict__ nodes, const DPNode* __restrict__ dp,
-                            const int* __restrict__ level, int L, Gather* __restrict__ out,
-                            int* __restrict__ n_inner, int* __restrict__ n_items) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= L) return;
+__device__ void gather_dp_one(int i, const Node2* __restrict__ nodes, const DPNode* __restrict__ dp,
+                              const int* __restrict__ level, Gather* __restrict__ out, int* __restrict__ n_inner,
+                              int* __restrict__ n_items) {
     const int b2 = level[i];
     const Node2 me = nodes[b2];
     int kid[8];
@@ -208,10 +207,8 @@ __global__ void k_gather_dp(const Node2* __restrict__ nodes, const DPNode* __res
     n_items[i] = nt;
 }
 
-__global__ void k_gather(const Node2* __restrict__ nodes, const int* __restrict__ level, int L,
-                         Gather* __restrict__ out, int* __restrict__ n_inner, int* __restrict__ n_items) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= L) return;
+__device__ void gather_greedy_one(int i, const Node2* __restrict__ nodes, const int* __restrict__ level,
+                                  Gather* __restrict__ out, int* __restrict__ n_inner, int* __restrict__ n_items) {
     const int b2 = level[i];
     const Node2 me = nodes[b2];
     int kid[8];
@@ -279,6 +276,40 @@ __global__ void k_gather(const Node2* __restrict__ nodes, const int* __restrict_
     n_items[i] = nt;
 }
 
+// The collapse's level loop keeps its state on the device, so a level can
+// be enqueued without the host knowing its width (the graph-driven build
+// runs the loop under a conditional node; the host-driven loop reads the
+// totals only to decide when to stop).
+// More 8-wide levels than any tree the builder makes (its binary depth is
+// bounded); the graph-driven loop stops there with status 2.
+constexpr int kMaxCollapseLevels = 1024;
+struct CollapseLevel {
+    int L;           // binary nodes turned into 8-wide nodes at this level
+    int level_base;  // first 8-wide node of this level
+    int items;       // leaf items (triangle records / instance slots) written so far
+    int depth;       // levels done
+    int status;      // 1: node or item capacity exceeded; 2: too many levels
+    int pad[3];
+};
+
+// The DP tables are used unless the bottom-up pass gave up (too deep).
+__device__ __forceinline__ const DPNode* dp_in_use(const DPNode* dp, const int* dp_status) {
+    return dp && dp_status && *dp_status == 0 ? dp : nullptr;
+}
+
+// One thread per binary node of the level (grid-stride over lv->L).
+__global__ void k_gather_lv(const Node2* __restrict__ nodes, const DPNode* __restrict__ dp,
+                            const int* __restrict__ dp_status, const int* __restrict__ level,
+                            const CollapseLevel* __restrict__ lv, Gather* __restrict__ out,
+                            int* __restrict__ n_inner, int* __restrict__ n_items) {
+    const int L = lv->L;
+    const DPNode* d = dp_in_use(dp, dp_status);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x) {
+        if (d) gather_dp_one(i, nodes, d, level, out, n_inner, n_items);
+        else gather_greedy_one(i, nodes, level, out, n_inner, n_items);
+    }
+}
+
 // smallest e with 255 * 2^e >= ext (ext > 0), from the exact double value
 __device__ __forceinline__ int grid_exponent(double ext) {
     int k;
@@ -289,14 +320,11 @@ __device__ __forceinline__ int grid_exponent(double ext) {
     return e;
 }
 
-__global__ void k_emit(const Node2* __restrict__ nodes, const int* __restrict__ level, int L,
-                       const Gather* __restrict__ gat, const int* __restrict__ inner_off,
-                       const int* __restrict__ item_off, int child_base0, int item_base0,
-                       const int* __restrict__ perm, const float* __restrict__ tris9,
-                       Bvh8Node* __restrict__ out_nodes, int out_base, TriRec* __restrict__ out_tris,
-                       int* __restrict__ out_ids, int* __restrict__ next_level, const DPNode* __restrict__ dp) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= L) return;
+__device__ void emit_one(int i, const Node2* __restrict__ nodes, const Gather* __restrict__ gat,
+                         const int* __restrict__ inner_off, const int* __restrict__ item_off, int child_base0,
+                         int item_base0, const int* __restrict__ perm, const float* __restrict__ tris9,
+                         Bvh8Node* __restrict__ out_nodes, int out_base, TriRec* __restrict__ out_tris,
+                         int* __restrict__ out_ids, int* __restrict__ next_level, const DPNode* __restrict__ dp) {
     const Gather g = gat[i];
     const int child_base = child_base0 + inner_off[i];
     const int tri_base = item_base0 + item_off[i];
@@ -387,6 +415,99 @@ __global__ void k_emit(const Node2* __restrict__ nodes, const int* __restrict__ 
     out_nodes[out_base + i] = nd;
 }
 
+// One thread per binary node of the level (grid-stride over lv->L): this
+// level's 8-wide nodes go to lv->level_base + i, their inner children to
+// the next level's list, their leaves' records after lv->items.
+// Writes nothing when the level's totals (tot: inner children, leaf items)
+// would pass the capacities; k_collapse_advance then reports it.
+__global__ void k_emit_lv(const Node2* __restrict__ nodes, const CollapseLevel* __restrict__ lv,
+                          const Gather* __restrict__ gat, const int* __restrict__ inner_off,
+                          const int* __restrict__ item_off, const int* __restrict__ tot, int max_nodes, int max_items,
+                          const int* __restrict__ perm, const float* __restrict__ tris9,
+                          Bvh8Node* __restrict__ out_nodes, TriRec* __restrict__ out_tris, int* __restrict__ out_ids,
+                          int* __restrict__ next_level, const DPNode* __restrict__ dp,
+                          const int* __restrict__ dp_status) {
+    const int L = lv->L, base = lv->level_base, items = lv->items;
+    if (base + L + tot[0] > max_nodes || items + tot[1] > max_items) return;
+    const DPNode* d = dp_in_use(dp, dp_status);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x)
+        emit_one(i, nodes, gat, inner_off, item_off, base + L, items, perm, tris9, out_nodes, base, out_tris, out_ids,
+                 next_level, d);
+}
+
+// Level 0: the roots (binary nodes 0 .. R-1 -> 8-wide nodes 0 .. R-1).
+template <bool COND>
+__global__ void k_collapse_init(CollapseLevel* __restrict__ lv, int* __restrict__ level, int R,
+                                cudaGraphConditionalHandle cond) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) level[i] = i;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        CollapseLevel z = {};
+        z.L = R;
+        *lv = z;
+        if (COND) cudaGraphSetConditional(cond, R > 0 ? 1u : 0u);
+    }
+}
+
+// End of a level: tot = {inner children, leaf items} of the level.  Checks
+// the capacities, advances the level record, and (graph-driven) continues
+// the loop while the next level has nodes and nothing overflowed.
+template <bool COND>
+__global__ void k_collapse_advance(CollapseLevel* __restrict__ lv, const int* __restrict__ tot, int max_nodes,
+                                   int max_items, cudaGraphConditionalHandle cond) {
+    CollapseLevel v = *lv;
+    const int child_base = v.level_base + v.L;
+    if (child_base + tot[0] > max_nodes || v.items + tot[1] > max_items) v.status |= 1;
+    if (v.depth + 1 >= kMaxCollapseLevels && tot[0] > 0) v.status |= 2;  // bounds the graph's loop
+    v.level_base = child_base;
+    v.items += tot[1];
+    v.L = v.status ? 0 : tot[0];
+    v.depth++;
+    *lv = v;
+    if (COND) cudaGraphSetConditional(cond, v.L > 0 ? 1u : 0u);
+}
+
+// Next level's node list becomes the current one (graph-driven loop, whose
+// kernels keep fixed buffer arguments).
+__global__ void k_copy_level(const int* __restrict__ src, int* __restrict__ dst, const CollapseLevel* __restrict__ lv) {
+    const int L = lv->L;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x) dst[i] = src[i];
+}
+
+// The level record's totals for the host: {nodes, leaf items, depth, status}.
+__global__ void k_collapse_result(const CollapseLevel* __restrict__ lv, int* __restrict__ out) {
+    out[0] = lv->level_base;
+    out[1] = lv->items;
+    out[2] = lv->depth;
+    out[3] = lv->status;
+}
+
+namespace {
+// SAH-optimal collapse for triangle BLASes unless RTB200_COLLAPSE=greedy
+// (TLAS leaves stay single instances: greedy); its cost constants.
+int collapse_mode() {
+    static const int mode = [] {
+        const char* e = getenv("RTB200_COLLAPSE");
+        return e && !strcmp(e, "greedy") ? 0 : 1;
+    }();
+    return mode;
+}
+float dp_c_prim() {
+    static const float c = [] {
+        const char* e = getenv("RTB200_DP_CPRIM");
+        return e ? (float)atof(e) : 0.5f;
+    }();
+    return c;
+}
+int dp_p_max() {
+    static const int p = [] {
+        const char* e = getenv("RTB200_DP_PMAX");
+        const int v = e ? atoi(e) : 4;
+        return v < 1 ? 1 : (v > 4 ? 4 : v);
+    }();
+    return p;
+}
+}  // namespace
+
 bool collapse_bvh8(const Bvh2Device& b2, const float* d_tris9, Bvh8Device& out, cudaStream_t s) {
     const int n = b2.num_prims;
     const int R = b2.num_roots;
@@ -401,61 +522,31 @@ bool collapse_bvh8(const Bvh2Device& b2, const float* d_tris9, Bvh8Device& out, 
     }
     TmpBuf<int> lvl_a, lvl_b, n_inner, n_items, inner_off, item_off, tot;
     TmpBuf<Gather> gat;
+    TmpBuf<CollapseLevel> lv;
     if (!lvl_a.alloc(max_nodes, s) || !lvl_b.alloc(max_nodes, s) || !n_inner.alloc(max_nodes, s) ||
         !n_items.alloc(max_nodes, s) || !inner_off.alloc(max_nodes, s) || !item_off.alloc(max_nodes, s) ||
-        !gat.alloc(max_nodes, s) || !tot.alloc(2, s))
+        !gat.alloc(max_nodes, s) || !tot.alloc(2, s) || !lv.alloc(1, s))
         return false;
-    {
-        // level 0: the roots, binary nodes 0 .. R-1 -> 8-wide nodes 0 .. R-1
-        std::vector<int> roots(R);
-        for (int i = 0; i < R; i++) roots[i] = i;
-        if (!RT_CUDA(cudaMemcpyAsync(lvl_a.p, roots.data(), R * sizeof(int), cudaMemcpyHostToDevice, s)) ||
-            !RT_CUDA(cudaStreamSynchronize(s)))
-            return false;
-    }
-    // SAH-optimal collapse for triangle BLASes unless RTB200_COLLAPSE=greedy
-    // (TLAS leaves stay single instances: greedy)
-    static const int mode = [] {
-        const char* e = getenv("RTB200_COLLAPSE");
-        return e && !strcmp(e, "greedy") ? 0 : 1;
-    }();
     TmpBuf<DPNode> dp;
-    if (d_tris9 && mode == 1) {
-        static const float c_prim = [] {
-            const char* e = getenv("RTB200_DP_CPRIM");
-            return e ? (float)atof(e) : 0.5f;
-        }();
-        static const int p_max = [] {
-            const char* e = getenv("RTB200_DP_PMAX");
-            const int v = e ? atoi(e) : 4;
-            return v < 1 ? 1 : (v > 4 ? 4 : v);
-        }();
+    TmpBuf<int> parent, arrive, st;  // st: 1 when the bottom-up pass gave up (greedy collapse instead)
+    if (d_tris9 && collapse_mode() == 1) {
         const int slots = b2.num_nodes;
-        TmpBuf<int> parent, arrive, st;
-        if (!dp.alloc(slots, s) || !parent.alloc(slots, s) || !arrive.alloc(slots, s) || !st.alloc(1, s))
-            return false;
-        int h_st = 0;
+        if (!dp.alloc(slots, s) || !parent.alloc(slots, s) || !arrive.alloc(slots, s) || !st.alloc(1, s)) return false;
         if (!RT_CUDA(cudaMemsetAsync(parent.p, 0xFF, sizeof(int) * (size_t)slots, s)) ||
             !RT_CUDA(cudaMemsetAsync(arrive.p, 0, sizeof(int) * (size_t)slots, s)) ||
             !RT_CUDA(cudaMemsetAsync(st.p, 0, sizeof(int), s)))
             return false;
         k_dp_parents<<<(slots + 255) / 256, 256, 0, s>>>(b2.nodes.p, slots, parent.p);
-        k_dp<<<(slots + 255) / 256, 256, 0, s>>>(b2.nodes.p, slots, parent.p, arrive.p, dp.p, 1.0f, c_prim, p_max,
-                                                 st.p);
-        if (!RT_CUDA(cudaGetLastError()) ||
-            !RT_CUDA(cudaMemcpyAsync(&h_st, st.p, sizeof(int), cudaMemcpyDeviceToHost, s)) ||
-            !RT_CUDA(cudaStreamSynchronize(s)))
-            return false;
-        if (h_st) dp.release();  // too deep: greedy collapse
+        k_dp<<<(slots + 255) / 256, 256, 0, s>>>(b2.nodes.p, slots, parent.p, arrive.p, dp.p, 1.0f, dp_c_prim(),
+                                                 dp_p_max(), st.p);
     }
-    int L = R, level_base = 0, items = 0, depth = 0;
     int* cur = lvl_a.p;
     int* nxt = lvl_b.p;
+    k_collapse_init<false><<<(R + 255) / 256, 256, 0, s>>>(lv.p, cur, R, 0);
+    int L = R, level_base = 0, items = 0, depth = 0;
     while (L > 0) {
-        if (dp.p)
-            k_gather_dp<<<(L + 127) / 128, 128, 0, s>>>(b2.nodes.p, dp.p, cur, L, gat.p, n_inner.p, n_items.p);
-        else
-            k_gather<<<(L + 127) / 128, 128, 0, s>>>(b2.nodes.p, cur, L, gat.p, n_inner.p, n_items.p);
+        const int grid = (L + 127) / 128;
+        k_gather_lv<<<grid, 128, 0, s>>>(b2.nodes.p, dp.p, st.p, cur, lv.p, gat.p, n_inner.p, n_items.p);
         if (!scan_exclusive(n_inner.p, inner_off.p, L, tot.p, s)) return false;
         if (!scan_exclusive(n_items.p, item_off.p, L, tot.p + 1, s)) return false;
         int h[2];
@@ -466,9 +557,9 @@ bool collapse_bvh8(const Bvh2Device& b2, const float* d_tris9, Bvh8Device& out, 
             set_error("collapse: capacity exceeded");
             return false;
         }
-        k_emit<<<(L + 127) / 128, 128, 0, s>>>(b2.nodes.p, cur, L, gat.p, inner_off.p, item_off.p, child_base, items,
-                                               b2.perm.p, d_tris9, out.nodes.p, level_base, out.tris.p,
-                                               out.leaf_ids.p, nxt, dp.p);
+        k_emit_lv<<<grid, 128, 0, s>>>(b2.nodes.p, lv.p, gat.p, inner_off.p, item_off.p, tot.p, max_nodes, n,
+                                       b2.perm.p, d_tris9, out.nodes.p, out.tris.p, out.leaf_ids.p, nxt, dp.p, st.p);
+        k_collapse_advance<false><<<1, 1, 0, s>>>(lv.p, tot.p, max_nodes, n, 0);
         level_base = child_base;
         items += h[1];
         L = h[0];
@@ -478,6 +569,83 @@ bool collapse_bvh8(const Bvh2Device& b2, const float* d_tris9, Bvh8Device& out, 
     out.num_nodes = level_base;
     out.num_leaf_items = items;
     out.depth = depth;
+    return RT_CUDA(cudaGetLastError());
+}
+
+size_t collapse_graph_scratch_bytes(int n, int R, int slots, bool dp) {
+    const size_t max_nodes = (size_t)n + R;
+    size_t b = max_nodes * (6 * sizeof(int) + sizeof(Gather)) + 2 * sizeof(int) + sizeof(CollapseLevel) +
+               2 * scan_scratch_ints((int)max_nodes) * sizeof(int) + 16 * 256;
+    if (dp) b += (size_t)slots * (sizeof(DPNode) + 2 * sizeof(int)) + sizeof(int);
+    return b;
+}
+
+bool enqueue_collapse_graph(const Node2* nodes2, const int* perm, int n, int R, int slots, const float* d_tris9,
+                            Bvh8Node* out_nodes, TriRec* out_tris, int* out_ids, char* scratch, size_t scratch_bytes,
+                            int* d_result, cudaStream_t cs, cudaStream_t bs) {
+    const int max_nodes = n + R;
+    const bool use_dp = d_tris9 && collapse_mode() == 1;
+    if (collapse_graph_scratch_bytes(n, R, slots, use_dp) > scratch_bytes) {
+        set_error("collapse: graph scratch too small");
+        return false;
+    }
+    char* q = scratch;
+    auto take = [&q](size_t bytes) {
+        char* r = q;
+        q += (bytes + 255) & ~size_t(255);
+        return r;
+    };
+    const size_t scan_ints = scan_scratch_ints(max_nodes);
+    int* lvl_a = reinterpret_cast<int*>(take(sizeof(int) * (size_t)max_nodes));
+    int* lvl_b = reinterpret_cast<int*>(take(sizeof(int) * (size_t)max_nodes));
+    int* n_inner = reinterpret_cast<int*>(take(sizeof(int) * (size_t)max_nodes));
+    int* n_items = reinterpret_cast<int*>(take(sizeof(int) * (size_t)max_nodes));
+    int* inner_off = reinterpret_cast<int*>(take(sizeof(int) * (size_t)max_nodes));
+    int* item_off = reinterpret_cast<int*>(take(sizeof(int) * (size_t)max_nodes));
+    Gather* gat = reinterpret_cast<Gather*>(take(sizeof(Gather) * (size_t)max_nodes));
+    int* tot = reinterpret_cast<int*>(take(2 * sizeof(int)));
+    CollapseLevel* lv = reinterpret_cast<CollapseLevel*>(take(sizeof(CollapseLevel)));
+    int* scan_a = reinterpret_cast<int*>(take(sizeof(int) * scan_ints));
+    int* scan_b = reinterpret_cast<int*>(take(sizeof(int) * scan_ints));
+    DPNode* dp = nullptr;
+    int *parent = nullptr, *arrive = nullptr, *st = nullptr;
+    if (use_dp) {
+        dp = reinterpret_cast<DPNode*>(take(sizeof(DPNode) * (size_t)slots));
+        parent = reinterpret_cast<int*>(take(sizeof(int) * (size_t)slots));
+        arrive = reinterpret_cast<int*>(take(sizeof(int) * (size_t)slots));
+        st = reinterpret_cast<int*>(take(sizeof(int)));
+        if (!RT_CUDA(cudaMemsetAsync(parent, 0xFF, sizeof(int) * (size_t)slots, cs)) ||
+            !RT_CUDA(cudaMemsetAsync(arrive, 0, sizeof(int) * (size_t)slots, cs)) ||
+            !RT_CUDA(cudaMemsetAsync(st, 0, sizeof(int), cs)))
+            return false;
+        k_dp_parents<<<(slots + 255) / 256, 256, 0, cs>>>(nodes2, slots, parent);
+        k_dp<<<(slots + 255) / 256, 256, 0, cs>>>(nodes2, slots, parent, arrive, dp, 1.0f, dp_c_prim(), dp_p_max(),
+                                                  st);
+    }
+    cudaGraphConditionalHandle cond;
+    cudaGraph_t body;
+    if (!capture_conditional_handle(cs, &cond)) return false;
+    k_collapse_init<true><<<(R + 255) / 256, 256, 0, cs>>>(lv, lvl_a, R, cond);
+    if (!capture_while(cs, cond, &body)) return false;
+    if (!RT_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed)))
+        return false;
+    // grid-stride kernels: a level is at most max_nodes wide
+    const int grid = std::max(1, std::min((max_nodes + 127) / 128, num_sms() * 16));
+    k_gather_lv<<<grid, 128, 0, bs>>>(nodes2, dp, st, lvl_a, lv, gat, n_inner, n_items);
+    bool ok = scan_exclusive_dev(n_inner, inner_off, max_nodes, &lv->L, tot, scan_a, bs) &&
+              scan_exclusive_dev(n_items, item_off, max_nodes, &lv->L, tot + 1, scan_b, bs);
+    if (ok) {
+        k_emit_lv<<<grid, 128, 0, bs>>>(nodes2, lv, gat, inner_off, item_off, tot, max_nodes, n, perm, d_tris9,
+                                        out_nodes, out_tris, out_ids, lvl_b, dp, st);
+        k_collapse_advance<true><<<1, 1, 0, bs>>>(lv, tot, max_nodes, n, cond);
+        k_copy_level<<<grid, 128, 0, bs>>>(lvl_b, lvl_a, lv);
+        ok = RT_CUDA(cudaGetLastError());
+    }
+    cudaGraph_t done = nullptr;
+    const bool ended = RT_CUDA(cudaStreamEndCapture(bs, &done));
+    if (!ok || !ended) return false;
+    // results for the host: nodes, leaf items, depth, status
+    k_collapse_result<<<1, 1, 0, cs>>>(lv, d_result);
     return RT_CUDA(cudaGetLastError());
 }
 

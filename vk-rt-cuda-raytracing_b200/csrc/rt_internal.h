@@ -212,6 +212,44 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
 // d_tris9 is null and leaf_ids receives primitive (instance) indices.
 bool collapse_bvh8(const Bvh2Device& b2, const float* d_tris9, Bvh8Device& out, cudaStream_t s);
 
+// The whole BLAS build (SAH levels, small and warp tiers, 8-wide collapse)
+// as one CUDA graph launched on s: both level loops are conditional WHILE
+// nodes driven by counts that stay on the device, so the host neither
+// waits between levels nor sizes any launch from a device count.  Same
+// tree as build_bvh2 + collapse_bvh8 (segments: scenes built together;
+// scene i's root is 8-wide node i).  Returns false with the error set.
+struct GraphBuildInfo {
+    float graph_ms = 0.f;  // the graph launch, CUDA events on s
+    int bvh2_nodes = 0;    // binary node ids used
+    int levels = 0;        // large-task levels
+    int small_tasks = 0;
+};
+bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tris9, int n, const BuildConfig& cfg,
+                      const std::vector<int>& segments, Bvh8Device& out, cudaStream_t s, GraphBuildInfo* info);
+
+// Capture helpers for the graph-driven build: a conditional handle on the
+// graph being captured on cs, and a WHILE node on it at the capture
+// position (its empty body graph returned for capture on another stream).
+bool capture_conditional_handle(cudaStream_t cs, cudaGraphConditionalHandle* h);
+bool capture_while(cudaStream_t cs, cudaGraphConditionalHandle h, cudaGraph_t* body);
+
+// Exclusive scan whose element count is read on the device (d_n; null: all
+// `cap` elements), with caller scratch of scan_scratch_ints(cap) ints; no
+// allocation, so it can be captured.
+size_t scan_scratch_ints(int cap);
+bool scan_exclusive_dev(const int* d_in, int* d_out, int cap, const int* d_n, int* d_total, int* scratch,
+                        cudaStream_t s);
+
+// The collapse enqueued on a capturing stream cs (its level loop a WHILE
+// node whose body is captured on bs), over a binary tree of at most `slots`
+// node ids (unused ids zeroed) with R roots; scratch of at least
+// collapse_graph_scratch_bytes; d_result receives {nodes, leaf items,
+// depth, status (1: capacity exceeded)}.
+size_t collapse_graph_scratch_bytes(int n, int R, int slots, bool dp);
+bool enqueue_collapse_graph(const Node2* nodes2, const int* perm, int n, int R, int slots, const float* d_tris9,
+                            Bvh8Node* out_nodes, TriRec* out_tris, int* out_ids, char* scratch, size_t scratch_bytes,
+                            int* d_result, cudaStream_t cs, cudaStream_t bs);
+
 // Primitive boxes.
 void launch_tri_bounds(const float* d_tris9, int n, float4* d_lo, float4* d_hi, cudaStream_t s);
 

@@ -40,6 +40,7 @@ class RtRayGen(C.Structure):
 
 
 RT_GEN_DIFFUSE, RT_GEN_SHADOW = 0, 1
+RT_BATCH_BUILD_HOST_LOOP = 1  # rtBatch_buildEx: host-driven level loop
 RT_REGROUP_MORTON, RT_REGROUP_OCTANT_MORTON = 0, 1
 
 
@@ -175,6 +176,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "cudaTLAS_setTransforms": (i32, [vp, vp, i32]),
         "cudaTLAS_getStatus": (i32, [vp, vp]),
         "rtBatch_build": (vp, [vp, vp, i32, vp]),
+        "rtBatch_buildEx": (vp, [vp, vp, i32, i32, vp]),
         "rtBatch_destroy": (None, [vp]),
         "rtBatch_traceClosest": (i32, [vp, vp, vp, i32, vp, vp]),
         "rtBatch_traceAny": (i32, [vp, vp, vp, i32, vp, vp]),
@@ -184,6 +186,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "rtBatch_setTuningEx": (i32, [vp, C.POINTER(RtBatchTuning)]),
         "rtBatch_getTuning": (i32, [vp, C.POINTER(RtBatchTuning)]),
         "rtBatch_getInfo": (i32, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(f32)]),
+        "rtBatch_getDeviceLayout": (i32, [vp, C.POINTER(vp), C.POINTER(i32), C.POINTER(vp), C.POINTER(i32)]),
         "cudaBVH_buildGeometries": (vp, [C.POINTER(RtGeometry), i32, vp]),
         "cudaBVH_refit": (i32, [vp, vp, vp]),
         "cudaBVH_refitGeometries": (i32, [vp, C.POINTER(RtGeometry), i32, vp]),
@@ -549,9 +552,10 @@ class PathTracer:
 class Batch:
     """rtBatch_*: many scenes built and traced together."""
 
-    def __init__(self, scenes_tris=None, stream=None, *, all_tris=None, tri_offsets=None):
+    def __init__(self, scenes_tris=None, stream=None, *, all_tris=None, tri_offsets=None, host_loop=False):
         """scenes_tris: list of (n_i, 9) arrays; or all_tris (sum n_i, 9) with
-        tri_offsets (num_scenes + 1) already concatenated."""
+        tri_offsets (num_scenes + 1) already concatenated.  host_loop: build
+        with the host-driven level loop instead of the one-graph build."""
         L = load()
         if all_tris is None:
             tris = [np.ascontiguousarray(t, np.float32).reshape(-1, 9) for t in scenes_tris]
@@ -559,7 +563,8 @@ class Batch:
             all_tris = np.concatenate(tris)
         self.tri_off = np.ascontiguousarray(tri_offsets, np.int32)
         allt = np.ascontiguousarray(all_tris, np.float32).reshape(-1, 9)
-        self.h = L.rtBatch_build(allt.ctypes.data, self.tri_off.ctypes.data, len(self.tri_off) - 1, _stream(stream))
+        self.h = L.rtBatch_buildEx(allt.ctypes.data, self.tri_off.ctypes.data, len(self.tri_off) - 1,
+                                   RT_BATCH_BUILD_HOST_LOOP if host_loop else 0, _stream(stream))
         if not self.h:
             raise RtError(f"rtBatch_build failed: {last_error()}")
         self.num_scenes = len(self.tri_off) - 1
@@ -568,6 +573,14 @@ class Batch:
         a, b, c = C.c_int(), C.c_int(), C.c_float()
         _check(load().rtBatch_getInfo(self.h, C.byref(a), C.byref(b), C.byref(c)), "rtBatch_getInfo")
         return {"num_scenes": a.value, "num_nodes": b.value, "build_ms": c.value}
+
+    def layout(self):
+        """(nodes pointer, node count, triangle-record pointer, record count) on the device."""
+        n_nodes, n_tris = C.c_int(), C.c_int()
+        pn, pt = C.c_void_p(), C.c_void_p()
+        _check(load().rtBatch_getDeviceLayout(self.h, C.byref(pn), C.byref(n_nodes), C.byref(pt), C.byref(n_tris)),
+               "rtBatch_getDeviceLayout")
+        return pn.value, n_nodes.value, pt.value, n_tris.value
 
     def closest(self, d_rays, d_off, n, d_hits, stream=None):
         _check(load().rtBatch_traceClosest(self.h, _ptr(d_rays), _ptr(d_off), n, _ptr(d_hits), _stream(stream)),
