@@ -73,6 +73,16 @@
 #ifndef RTB_HELPERS
 #define RTB_HELPERS 2
 #endif
+// RTB_MID_REFILL: a lane whose ray has finished its traversal (no group,
+// nothing stacked) takes the next ray at its next node visit instead of
+// waiting for the iteration's end; the finished ray is parked in the lane's
+// second shared-memory slot (its best key, barycentrics and output index)
+// until the triangle phase has tested its pending triangles, then written.
+// Pending triangle sets carry their ray's slot in the top bit of the
+// record base.  Single-scene launches only, not the work-counting kernels.
+#ifndef RTB_MID_REFILL
+#define RTB_MID_REFILL 0
+#endif
 // launch modes with helpers (bit 1 << MODE_SINGLE / MODE_BATCH / MODE_WAVE):
 // single scene only.  In the batch and wave modes the extra state spills
 // (10-12 bytes) and the tail is a small part of their long launches: the
@@ -117,16 +127,23 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
                  int n, RtHit* __restrict__ hits, uint8_t* __restrict__ occ, uint32_t* __restrict__ counts,
                  int* __restrict__ work, int* __restrict__ status, const int* __restrict__ ray_off,
                  const int* __restrict__ tri_off, int nscenes, const WaveSeg* __restrict__ segs) {
+    // ray slots per lane: the current ray, and with mid-iteration refill a
+    // parked (finished) one; slot index = tag * T + thread
+    constexpr bool MID = RTB_MID_REFILL && !COUNT && MODE == MODE_SINGLE;
+    constexpr int NSL = MID ? 2 : 1;
     __shared__ uint2 sstack[SS][T];
-    __shared__ unsigned long long s_key[T];  // owner's best (ordered t, prim)
-    __shared__ int s_rec[T];                 // set when a worker improved it (any hit: found)
-    __shared__ float2 s_uv[T];               // barycentrics of the improved best
+    __shared__ unsigned long long s_key[NSL * T];  // a slot's best (ordered t, prim)
+    __shared__ int s_rec[NSL * T];                 // set when a worker improved it (any hit: found)
+    __shared__ float2 s_uv[NSL * T];               // barycentrics of the improved best
 #if RTB_RAY_SMEM
-    __shared__ float4 s_ray[2][T];           // each lane's ray, read by the lanes testing its triangles
+    __shared__ float4 s_ray[NSL][2][T];            // each slot's ray, read by the lanes testing its triangles
 #endif
+    __shared__ int s_prev[MID ? T : 1];            // output index of the lane's parked ray, -1: none
+    if (MID) s_prev[threadIdx.x] = -1;
     constexpr bool HELP =
         !COUNT && (ANY ? RTB_HELPERS >= 2 : RTB_HELPERS >= 1) && ((RTB_HELPERS_MODES >> MODE) & 1);
     static_assert(!HELP || RTB_RAY_SMEM, "helper lanes read the owner's ray from shared memory");
+    static_assert(!MID || (RTB_RAY_SMEM && RTB_TWO_SETS), "parked rays are read from shared memory by set tag");
     // helpers per owner lane (low 16 bits) | HELP_OVF when a helper's stack overflowed
     constexpr int HELP_OVF = 1 << 16;
     __shared__ int s_help[HELP ? T : 1];
@@ -152,6 +169,7 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
     int prim_base = 0;
     int wseg = 0;
     uint32_t cn = 0, ct = 0;
+    uint32_t tag = 0;  // slot of this lane's current ray (always 0 without MID)
     for (;;) {
         // ---- refill idle lanes ----
         const bool need = ray == -1 && !exhausted;
@@ -196,8 +214,8 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
                     hu = hv = 0.f;
                     w.start();
 #if RTB_RAY_SMEM
-                    s_ray[0][threadIdx.x] = make_float4(r.ox, r.oy, r.oz, r.tmin);
-                    s_ray[1][threadIdx.x] = make_float4(r.dx, r.dy, r.dz, r.tmax);
+                    s_ray[tag][0][threadIdx.x] = make_float4(r.ox, r.oy, r.oz, r.tmin);
+                    s_ray[tag][1][threadIdx.x] = make_float4(r.dx, r.dy, r.dz, r.tmax);
 #endif
                     w.ng = make_uint2(root, (1u << r.oct) | (1u << 8));
                     cn = ct = 0;
@@ -227,9 +245,11 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
                 const uint32_t gx = __shfl_sync(FULL_MASK, give.x, v), gy = __shfl_sync(FULL_MASK, give.y, v);
                 const int vslot = __shfl_sync(FULL_MASK, ray >= 0 ? lane : -2 - ray, v);
                 const float vthit = __shfl_sync(FULL_MASK, thit, v);
+                const uint32_t vtag = MID ? __shfl_sync(FULL_MASK, tag, v) : 0u;
                 if (thief) {
                     ray = -2 - vslot;
-                    r = make_ray(s_ray[0][wbase + vslot], s_ray[1][wbase + vslot]);
+                    if (MID) tag = vtag;  // the owner's slot
+                    r = make_ray(s_ray[vtag][0][wbase + vslot], s_ray[vtag][1][wbase + vslot]);
                     thit = vthit;
                     hprim = -1;
                     w.start();
@@ -270,6 +290,45 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
                 RTB_STAT(3 + 2 * it, __popc(act));  //           lanes
             }
 #endif
+            if (MID && it > 0) {
+                // lanes whose own ray has finished its traversal take the next ray
+                const bool fin = ray >= 0 && !exhausted && !overflow && RTB_LAST_SET == 0 &&
+                                 (w.ng.y & 0xFFu) == 0 && w.sp == w.sb && s_prev[threadIdx.x] < 0;
+                const unsigned fwant = __ballot_sync(FULL_MASK, fin);
+                if (fwant) {
+                    const int leader = __ffs(fwant) - 1;
+                    int base = 0;
+                    if (lane == leader) base = atomicAdd(work, __popc(fwant));
+                    base = __shfl_sync(FULL_MASK, base, leader);
+                    if (fin) {
+                        const int ri = base + __popc(fwant & ((1u << lane) - 1));
+                        if (ri < n) {
+                            // park the finished ray: its best so far stays in its slot
+                            const int ps = (int)tag * T + threadIdx.x;
+                            if (ANY) {
+                                s_rec[ps] = 0;
+                            } else {
+                                s_key[ps] = ((unsigned long long)f2ord(thit) << 32) |
+                                            (uint32_t)(hprim >= 0 ? hprim : -1);
+                                s_uv[ps] = make_float2(hu, hv);
+                            }
+                            s_prev[threadIdx.x] = ray;
+                            tag ^= 1u;
+                            ray = ri;
+                            r = load_ray(rays, ri);
+                            thit = r.tmax;
+                            hprim = -1;
+                            hu = hv = 0.f;
+                            w.start();
+                            s_ray[tag][0][threadIdx.x] = make_float4(r.ox, r.oy, r.oz, r.tmin);
+                            s_ray[tag][1][threadIdx.x] = make_float4(r.dx, r.dy, r.dz, r.tmax);
+                            w.ng = make_uint2(0u, (1u << r.oct) | (1u << 8));
+                        } else {
+                            exhausted = true;
+                        }
+                    }
+                }
+            }
 #if RTB_TWO_SETS
 #if RTB_VISIT_VOTE
             // later visits only while some lane can still take one
@@ -292,6 +351,7 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
 #if RTB_TWO_SETS
                 uint32_t vb, vm;
                 visit_node(nodes + (size_t)ni * 5, r, thit, nmask, vb, vm, w.ng, s_oct_perm);
+                if (MID) vb |= tag << 31;  // the set's ray slot
                 if (tmask == 0) {
                     tri_base = vb;
                     tmask = vm;
@@ -357,11 +417,12 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
         if (total) {
             const int excl = incl - cnt;
             if (COUNT) ct += cnt;
+            const int cur_slot = (int)tag * T + threadIdx.x;
             if (!ANY) {
-                s_key[threadIdx.x] = ((unsigned long long)f2ord(thit) << 32) | (uint32_t)(hprim >= 0 ? hprim : -1);
-                s_rec[threadIdx.x] = -1;
+                s_key[cur_slot] = ((unsigned long long)f2ord(thit) << 32) | (uint32_t)(hprim >= 0 ? hprim : -1);
+                s_rec[cur_slot] = -1;
             } else {
-                s_rec[threadIdx.x] = 0;
+                s_rec[cur_slot] = 0;
             }
             __syncwarp();
             const int kslot = HELP && ray < -1 ? -2 - ray : lane;  // whose ray this lane's triangles belong to
@@ -405,10 +466,14 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
 #else
                 const int k = k0;
                 const uint32_t om = __shfl_sync(FULL_MASK, tmask, o);
-                const uint32_t ob = __shfl_sync(FULL_MASK, tri_base, o);
+                uint32_t ob = __shfl_sync(FULL_MASK, tri_base, o);
 #endif
+                // the set's ray slot (MID: top bit of the record base)
+                const uint32_t otag = MID ? ob >> 31 : 0u;
+                if (MID) ob &= 0x7FFFFFFFu;
+                const int kidx = (int)otag * T + wbase + ko;
 #if RTB_RAY_SMEM
-                const float4 ro = s_ray[0][wbase + ko], rd = s_ray[1][wbase + ko];
+                const float4 ro = s_ray[otag][0][wbase + ko], rd = s_ray[otag][1][wbase + ko];
                 const float ox = ro.x, oy = ro.y, oz = ro.z, tmn = ro.w;
                 const float dx = rd.x, dy = rd.y, dz = rd.z, tmx = rd.w;
 #else
@@ -426,34 +491,58 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
                     const float4 A = ld_tri(tp), B = ld_tri(tp + 1), Cc = ld_tri(tp + 2);
                     float t;
                     if (intersect_tri(ox, oy, oz, dx, dy, dz, A, B, Cc, t, u, v) && t > tmn && t < tmx) {
-                        if (ANY) s_rec[wbase + ko] = 1;
+                        if (ANY) s_rec[kidx] = 1;
                         else key = ((unsigned long long)f2ord(t) << 32) | (uint32_t)__float_as_int(A.w);
                     }
                 }
                 if (!ANY) {
-                    if (key != ~0ull) atomicMin(&s_key[wbase + ko], key);
+                    if (key != ~0ull) atomicMin(&s_key[kidx], key);
                     __syncwarp();
                     // the unique winner (keys are distinct per ray) publishes its barycentrics
-                    if (key != ~0ull && s_key[wbase + ko] == key) {
-                        s_rec[wbase + ko] = 1;
-                        s_uv[wbase + ko] = make_float2(u, v);
+                    if (key != ~0ull && s_key[kidx] == key) {
+                        s_rec[kidx] = 1;
+                        s_uv[kidx] = make_float2(u, v);
                     }
                     __syncwarp();
                 }
             }
             __syncwarp();
+            const int tb = (int)tag * T;
             if (ANY) {
-                found_any = s_rec[HELP && ray < -1 ? wbase - 2 - ray : threadIdx.x] != 0;
+                found_any = s_rec[tb + (HELP && ray < -1 ? wbase - 2 - ray : (int)threadIdx.x)] != 0;
             } else if (HELP && ray < -1) {
-                thit = ord2f((uint32_t)(s_key[wbase - 2 - ray] >> 32));  // the owner's best so far culls
-            } else if (s_rec[threadIdx.x] >= 0) {
+                thit = ord2f((uint32_t)(s_key[tb + wbase - 2 - ray] >> 32));  // the owner's best so far culls
+            } else if (s_rec[tb + threadIdx.x] >= 0) {
                 // a new closest hit for this lane
-                const unsigned long long key = s_key[threadIdx.x];
-                const float2 uv = s_uv[threadIdx.x];
+                const unsigned long long key = s_key[tb + threadIdx.x];
+                const float2 uv = s_uv[tb + threadIdx.x];
                 thit = ord2f((uint32_t)(key >> 32));
                 hprim = (int)(uint32_t)key;
                 hu = uv.x;
                 hv = uv.y;
+            }
+        }
+        if (MID) {
+            // the parked ray's triangles are tested: its slot holds the result
+            const int pr = s_prev[threadIdx.x];
+            if (pr >= 0) {
+                const int ps = (int)(tag ^ 1u) * T + threadIdx.x;
+                if (ANY) {
+                    occ[pr] = s_rec[ps] != 0 ? 1 : 0;
+                } else {
+                    const unsigned long long key = s_key[ps];
+                    const float2 uv = s_uv[ps];
+                    const int pp = (int)(uint32_t)key;
+                    const float4 hv4 = make_float4(pp >= 0 ? ord2f((uint32_t)(key >> 32)) : __int_as_float(0x7f800000),
+                                                   __int_as_float(pp >= 0 ? pp : -1), pp >= 0 ? uv.x : 0.f,
+                                                   pp >= 0 ? uv.y : 0.f);
+#if RTB_RAY_CS
+                    __stcs(reinterpret_cast<float4*>(hits) + pr, hv4);
+#else
+                    reinterpret_cast<float4*>(hits)[pr] = hv4;
+#endif
+                }
+                s_prev[threadIdx.x] = -1;
             }
         }
         // ---- advance / finish ----
