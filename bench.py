@@ -15,7 +15,11 @@ step).  Multi-GPU: one process per GPU, each holds a replica of the scene and
 traces its own ray batch (weak scaling, no collective on the data path);
 time = max over ranks.  `--impl reference` times the reference's CPU path
 (its own builder, compiled from its sources, plus the restated traversal)
-on the host cores.
+on the host cores.  At N=1 the default run also reports, as extra keys,
+config 0 (primary rays) beside the rebuilt reference kernels, the served
+form against the plain per-call path at three arrival rates, the wavefront
+path tracer with its FP64 oracle check, and the 256-scene batched form
+against 256 plain calls.
 """
 import argparse
 import json
@@ -714,21 +718,36 @@ def run_ours(args):
         del d_dif, d_sha, d_hits, d_occ, h_rays, h_hits
         torch.cuda.empty_cache()
         out["served"] = served_legs(rates=(SERVED_RATE, 2 * SERVED_RATE, 4 * SERVED_RATE))
+    # the two other forms of the path, timed in the same run (three timed
+    # steps each): the wavefront path tracer with its FP64 oracle check, and
+    # the 256-scene batched build + trace against 256 plain calls
+    forms = not args.no_served and not args.no_forms
+    if ws > 1 and forms:
+        out["pathtrace"] = out["batched"] = "reported by the N=1 run"
+    if rank == 0 and ws == 1 and forms:
+        torch.cuda.empty_cache()
+        pt = pathtrace_leg(args, 3, 3, oracle=not args.no_baselines)
+        out["pathtrace"] = {k: pt[k] for k in ("metric", "value", "unit", "ms_per_step", "steps", "config",
+                                               "rays_per_frame", "fp64_oracle", "cpu_baseline") if k in pt}
+        torch.cuda.empty_cache()
+        bt, same = batched_leg(args, 3, 3)
+        out["batched"] = {k: bt[k] for k in ("metric", "value", "unit", "ms_per_step", "steps", "config", "ours",
+                                             "plain", "hits_equal_plain")}
+        if not same:
+            raise SystemExit("batched: hits differ from the plain per-scene calls")
     finish_dist(ws)
     if rank == 0:
         print(json.dumps(out), flush=True)
     return 0
 
 
-def run_pathtrace(args):
+def pathtrace_leg(args, steps, warmup, oracle=True):
     """Path-tracer workload: wavefront path tracer, 1920x1080, 8 spp, <= 4 bounces,
     RR from bounce 2, TLAS of 64 instances over 16 BLASes (5M triangles).
     value = (extension + shadow rays) / frame time; radiance checked against
-    the FP64 oracle on a random pixel subset."""
+    the FP64 oracle on a random pixel subset.  Returns the result line."""
     import torch
     from rtb200 import lib, scenes
-    ws, rank, local = dist_env()
-    torch.cuda.set_device(local)
     t0 = time.time()
     blases, xf, bidx, alb, emi = scenes.instanced_scene(2, 5_000_000, nblas=16, ninst=64, world=100.0,
                                                         emissive_frac=0.05)
@@ -743,14 +762,13 @@ def run_pathtrace(args):
     d_rgb = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
-    ms = time_steps(torch, lambda: pt.render(cam, W, H, spp, 4, 2, 1, d_rgb, stream=stream), args.steps, args.warmup,
-                    flush)
+    ms = time_steps(torch, lambda: pt.render(cam, W, H, spp, 4, 2, 1, d_rgb, stream=stream), steps, warmup, flush)
     st = pt.stats()
     rays = st["extension_rays"] + st["shadow_rays"]
     t_frame = sum(ms) / len(ms)
     img = d_rgb.cpu().numpy().reshape(-1, 3).astype(np.float64)
     out = {"metric": "Mrays/s wavefront path tracer (extension + shadow rays)", "value": round(rays / t_frame / 1e3, 1),
-           "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_frame, 3),
+           "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": warmup, "ms_per_step": round(t_frame, 3),
            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
            "config": {"workload": "pathtrace_tlas_5m: 1920x1080, 8 spp, <=4 bounces, RR from bounce 2, 64 instances "
                                   "over 16 BLASes (5,000,000 triangles), Lambertian, 5% emissive",
@@ -759,7 +777,7 @@ def run_pathtrace(args):
                                   "extension trace (rtPT_setRegroup)") if args.pt_regroup else "off"},
            "rays_per_frame": {"extension": st["extension_rays"], "shadow": st["shadow_rays"]},
            "light_triangles": st["light_tris"], "mean_radiance": float(img.mean())}
-    if not args.no_baselines:
+    if oracle:
         from oracle import oracle as O
         t0 = time.time()
         orc = O.OraclePT(blases, xf, bidx, tl.inverse(), alb, emi)
@@ -775,11 +793,22 @@ def run_pathtrace(args):
         out["cpu_baseline"] = {"value": round(float(counts.sum()) / cpu_s / 1e6, 3), "unit": UNIT,
                                "cores": os.cpu_count() or 1, "kind": "port",
                                "sample": f"{px.size} pixels x {spp} spp through the FP64 oracle path tracer"}
-    print(json.dumps(out), flush=True)
+    pt.close()
+    tl.close()
+    for b in bvhs:
+        b.close()
+    return out
+
+
+def run_pathtrace(args):
+    import torch
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    print(json.dumps(pathtrace_leg(args, args.steps, args.warmup, oracle=not args.no_baselines)), flush=True)
     return 0
 
 
-def run_batched(args):
+def batched_leg(args, steps, warmup, ws=1, rank=0):
     """Batched form: 256 independent scenes (1K-500K triangles, log-uniform,
     seeds 0-255), each with its own 4K-2M ray batch (half primary, half
     diffuse).  One step = build every scene and trace every ray, closest
@@ -792,12 +821,10 @@ def run_batched(args):
     (rtb200.shard.scene_blocks, weight = triangles + rays / 20: the build
     dominates), each rank builds and traces its own block, and value = all
     ranks' rays / the slowest rank's step (strong scaling: the 256-scene job
-    is fixed)."""
+    is fixed).  The process group (N > 1) is set up by the caller; returns
+    (result line, complete on rank 0; hits equal the plain calls)."""
     import torch
     from rtb200 import lib, scenes, shard
-    ws, rank, local = dist_env()
-    torch.cuda.set_device(local)
-    init_dist(ws)
     t0 = time.time()
     ntri_all, nray_all = scenes.batched_sizes()
     bounds = shard.scene_blocks(ntri_all + nray_all // 20, ws)
@@ -835,7 +862,7 @@ def run_batched(args):
     torch.cuda.synchronize()
     b.close()
     build_ours, trace_ours = [], []
-    for k in range(args.warmup + args.steps):
+    for k in range(warmup + steps):
         flush.zero_()
         torch.cuda.synchronize()
         h0 = time.perf_counter()
@@ -848,17 +875,17 @@ def run_batched(args):
         b.graph(d_rays, d_off, nr, d_hits, stream=stream)
         e1.record(stream)
         torch.cuda.synchronize()
-        if k >= args.warmup:
+        if k >= warmup:
             build_ours.append((h1 - h0) * 1e3)
             trace_ours.append(e0.elapsed_time(e1))
-        if k + 1 < args.warmup + args.steps:
+        if k + 1 < warmup + steps:
             b.close()
     info = b.info()
     b.close()
     # --- A/B of the build: the same kernels driven level by level from the
     # host (rtBatch_buildEx with RT_BATCH_BUILD_HOST_LOOP; same tree)
     build_loop, dev_loop = [], []
-    for k in range(1 + max(1, min(args.steps, 3))):
+    for k in range(1 + max(1, min(steps, 3))):
         flush.zero_()
         torch.cuda.synchronize()
         h0 = time.perf_counter()
@@ -871,7 +898,7 @@ def run_batched(args):
         bl.close()
     # --- plain per-scene calls on the same data
     build_plain, trace_plain = [], []
-    psteps = max(1, min(args.steps, 3))
+    psteps = max(1, min(steps, 3))
     for k in range(1 + psteps):
         flush.zero_()
         torch.cuda.synchronize()
@@ -899,11 +926,10 @@ def run_batched(args):
     step_plain = max_over_ranks(bp + tp, ws)
     same = max_over_ranks(0.0 if same else 1.0, ws) == 0.0
     nr_all = int(nray_all.sum())
-    finish_dist(ws)
     if rank != 0:
-        return 0 if same else 1
+        return None, same
     out = {"metric": "Mrays/s batched build+trace (256 scenes)", "value": round(nr_all / step_ours / 1e3, 1),
-           "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+           "unit": UNIT, "n_gpus": ws, "steps": steps, "warmup": warmup,
            "ms_per_step": round(step_ours, 3), "higher_is_better": True, "scaling": "strong", "dtype": "f32",
            "data": "synthetic",
            "config": {"workload": f"batched_256: 256 scenes of 1K-500K triangles ({int(ntri_all.sum())} total), "
@@ -921,7 +947,19 @@ def run_batched(args):
                      "value": round(nr_all / step_plain / 1e3, 1), "steps": psteps,
                      "launches": "256 cudaBVH_build + 256 cudaBVH_traceClosest"},
            "hits_equal_plain": same}
-    print(json.dumps(out), flush=True)
+    del d_rays, d_off, d_hits, d_ref, flush, pinned
+    return out, same
+
+
+def run_batched(args):
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    init_dist(ws)
+    out, same = batched_leg(args, args.steps, args.warmup, ws, rank)
+    finish_dist(ws)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
     return 0 if same else 1
 
 
@@ -1135,7 +1173,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-baselines", action="store_true", help="skip the reference-kernel and CPU legs")
-    ap.add_argument("--no-served", action="store_true", help="skip the served-vs-plain legs of the default run")
+    ap.add_argument("--no-served", action="store_true",
+                    help="skip the served-vs-plain legs (and the path-tracer and batched legs) of the default run")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the path-tracer and batched legs of the default run")
     ap.add_argument("--pt-regroup", type=int, default=0, choices=[0, 16, 32],
                     help="pathtrace: regroup bounce rays by a 16- or 32-bit octant+Morton key before each extension")
     ap.add_argument("--workload", choices=["incoherent", "pathtrace", "batched", "served"], default="incoherent",

@@ -141,7 +141,16 @@ bool build_into(CudaBVHHandle* h, cudaStream_t s) {
     cudaEventRecord(e0, s);
     launch_tri_bounds(h->tris9.p, n, lo.p, hi.p, s);
     const BuildConfig cfg = default_config();
-    bool ok = build_bvh2(lo.p, hi.p, n, cfg, h->bvh2, s) && collapse_bvh8(h->bvh2, h->tris9.p, h->bvh8, s);
+    // one CUDA graph launch with device-side level loops (the host-driven
+    // loop's times swing with the host thread's scheduling: 7.7 ms to 45 ms
+    // for the same 2M-triangle build); RTB200_BUILD=host keeps that loop
+    static const bool host_loop = [] {
+        const char* e = getenv("RTB200_BUILD");
+        return e && !strcmp(e, "host");
+    }();
+    bool ok = host_loop ? build_bvh2(lo.p, hi.p, n, cfg, h->bvh2, s) && collapse_bvh8(h->bvh2, h->tris9.p, h->bvh8, s)
+                        : build_bvh8_graph(lo.p, hi.p, h->tris9.p, n, cfg, std::vector<int>{0, n}, h->bvh8, s, nullptr,
+                                           &h->bvh2);
     cudaEventRecord(e1, s);
     if (ok) ok = RT_CUDA(cudaEventSynchronize(e1));
     float ms = 0.f;

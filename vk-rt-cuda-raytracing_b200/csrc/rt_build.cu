@@ -1652,7 +1652,8 @@ __global__ void k_build_result(const BuildCtl* __restrict__ ctl, int* __restrict
 }
 
 bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tris9, int n, const BuildConfig& cfg,
-                      const std::vector<int>& seg, Bvh8Device& out, cudaStream_t s, GraphBuildInfo* info) {
+                      const std::vector<int>& seg, Bvh8Device& out, cudaStream_t s, GraphBuildInfo* info,
+                      Bvh2Device* keep) {
     if (n <= 0 || !d_tris9) {
         set_error("graph build: empty input");
         return false;
@@ -1685,8 +1686,8 @@ bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tri
     const int wq_cap = warp_task > 0 ? n / (cfg.max_leaf + 1) + 2 : 0;
     const int scan_cap = std::max(std::max(maxT, Cb), std::max(Kb, maxSmall));
     const size_t cbytes = collapse_graph_scratch_bytes(n, S, slots, true);
-    TmpBuf<Node2> nodes;
-    TmpBuf<int> perm, tmp, dseg, ccount, coff, cleft, cleftoff, flags, need, off, scan, result;
+    TmpBuf<Node2> tnodes;
+    TmpBuf<int> tperm, tmp, dseg, ccount, coff, cleft, cleftoff, flags, need, off, scan, result;
     TmpBuf<uint32_t> acc, gbins, kcb;
     TmpBuf<Task> tasks_a, tasks_b, kids, small;
     TmpBuf<Split> splits;
@@ -1695,7 +1696,12 @@ bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tri
     TmpBuf<WTask> wq;
     TmpBuf<BuildCtl> ctl;
     TmpBuf<char> cscratch;
-    if (!nodes.alloc(slots, s) || !perm.alloc(n, s) || !tmp.alloc(n, s) || !dseg.alloc(S + 1, s) ||
+    // the binary tree: scratch, or the caller's (kept for exports and refits)
+    if (keep ? (!keep->nodes.alloc(slots) || !keep->perm.alloc(n)) : (!tnodes.alloc(slots, s) || !tperm.alloc(n, s)))
+        return false;
+    Node2* d_nodes = keep ? keep->nodes.p : tnodes.p;
+    int* d_perm = keep ? keep->perm.p : tperm.p;
+    if (!tmp.alloc(n, s) || !dseg.alloc(S + 1, s) ||
         !acc.alloc((size_t)12 * S, s) || !tasks_a.alloc(maxT, s) || !tasks_b.alloc(maxT, s) || !kids.alloc(Kb, s) ||
         !small.alloc(maxSmall, s) || !splits.alloc(maxT, s) || !gbins.alloc((size_t)maxT * TASK_BIN_WORDS, s) ||
         !flags.alloc((size_t)4 * Kb, s) || !kcb.alloc((size_t)12 * maxT, s) || !side.alloc(n, s) ||
@@ -1735,15 +1741,15 @@ bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tri
     int* large_off = flags.p + 2 * Kb;
     int* small_off = flags.p + 3 * Kb;
     if (ok) {
-        cudaMemsetAsync(nodes.p, 0, sizeof(Node2) * (size_t)slots, cs);
-        k_iota<<<(n + 255) / 256, 256, 0, cs>>>(perm.p, n);
+        cudaMemsetAsync(d_nodes, 0, sizeof(Node2) * (size_t)slots, cs);
+        k_iota<<<(n + 255) / 256, 256, 0, cs>>>(d_perm, n);
         k_acc_init<<<std::max(1, std::min((12 * S + 255) / 256, 1024)), 256, 0, cs>>>(acc.p, S);
         k_seg_bounds<<<dim3(std::min((maxcnt + 2047) / 2048, 64), S), 256, 0, cs>>>(d_lo, d_hi, dseg.p, acc.p);
         cudaGraphConditionalHandle lv_cond;
         cudaGraph_t body;
         ok = capture_conditional_handle(cs, &lv_cond);
         if (ok) {
-            k_roots<<<1, ROOTS_T, 0, cs>>>(acc.p, dseg.p, S, cfg.max_leaf, cfg.small_task, nodes.p, cur, small.p, c,
+            k_roots<<<1, ROOTS_T, 0, cs>>>(acc.p, dseg.p, S, cfg.max_leaf, cfg.small_task, d_nodes, cur, small.p, c,
                                            lv_cond);
             ok = capture_while(cs, lv_cond, &body) &&
                  RT_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
@@ -1754,14 +1760,14 @@ bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tri
             bool lok = scan_exclusive_dev(ccount.p, coff.p, maxT, nullptr, &c->C, scan.p, bs);
             k_fill_chunks<<<maxT, 128, 0, bs>>>(cur, &c->T, coff.p, chunks.p);
             k_clear_bins<<<std::min(maxT * 8, 4096), 256, 0, bs>>>(gbins.p, &c->T);
-            k_bin_large<<<Cb, CHUNK_T, 0, bs>>>(chunks.p, cur, perm.p, d_lo, d_hi, gbins.p, &c->C);
-            k_split_large<<<(maxT + 3) / 4, 128, 0, bs>>>(cur, &c->T, gbins.p, splits.p, kids.p, kcb.p, nodes.p,
+            k_bin_large<<<Cb, CHUNK_T, 0, bs>>>(chunks.p, cur, d_perm, d_lo, d_hi, gbins.p, &c->C);
+            k_split_large<<<(maxT + 3) / 4, 128, 0, bs>>>(cur, &c->T, gbins.p, splits.p, kids.p, kcb.p, d_nodes,
                                                           &c->node, cfg.max_leaf, cfg.max_sah_depth);
-            k_count_left<<<Cb, CHUNK_T, 0, bs>>>(chunks.p, cur, splits.p, perm.p, d_lo, d_hi, cleft.p, kcb.p, &c->C,
+            k_count_left<<<Cb, CHUNK_T, 0, bs>>>(chunks.p, cur, splits.p, d_perm, d_lo, d_hi, cleft.p, kcb.p, &c->C,
                                                  side.p);
             lok = lok && scan_exclusive_dev(cleft.p, cleftoff.p, Cb, nullptr, nullptr, scan.p, bs);
-            k_scatter<<<Cb, CHUNK_T, 0, bs>>>(chunks.p, cur, splits.p, perm.p, side.p, cleftoff.p, tmp.p, &c->C);
-            k_copy_back<<<Cb, 256, 0, bs>>>(chunks.p, tmp.p, perm.p, &c->C);
+            k_scatter<<<Cb, CHUNK_T, 0, bs>>>(chunks.p, cur, splits.p, d_perm, side.p, cleftoff.p, tmp.p, &c->C);
+            k_copy_back<<<Cb, 256, 0, bs>>>(chunks.p, tmp.p, d_perm, &c->C);
             k_classify_flags<<<(Kb + 255) / 256, 256, 0, bs>>>(kids.p, &c->T, Kb, cfg.max_leaf, cfg.small_task,
                                                                is_large, is_small);
             lok = lok && scan_exclusive_dev(is_large, large_off, Kb, nullptr, &c->tot[0], scan.p, bs) &&
@@ -1781,16 +1787,16 @@ bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tri
                                                                                           maxSmall, need.p);
             ok = scan_exclusive_dev(need.p, off.p, maxSmall, &c->small, &c->reserved, scan.p, cs);
             k_build_small_loop<<<small_grid, SMALL_T, smem, cs>>>(small.p, &c->small, &c->work, off.p, &c->node,
-                                                                  perm.p, d_lo, d_hi, nodes.p, cfg.max_leaf,
+                                                                  d_perm, d_lo, d_hi, d_nodes, cfg.max_leaf,
                                                                   cfg.max_sah_depth, cfg.small_task, warp_task, wq.p,
                                                                   wq_cap, &c->wq_count, &c->status);
             if (warp_task > 0)
-                k_build_warp<<<warp_grid, WB_T, 0, cs>>>(wq.p, &c->wq_count, wq_cap, perm.p, d_lo, d_hi, nodes.p,
+                k_build_warp<<<warp_grid, WB_T, 0, cs>>>(wq.p, &c->wq_count, wq_cap, d_perm, d_lo, d_hi, d_nodes,
                                                          cfg.max_leaf, cfg.max_sah_depth);
             k_build_result<<<1, 1, 0, cs>>>(c, result.p);
             ok = ok && RT_CUDA(cudaGetLastError());
         }
-        ok = ok && enqueue_collapse_graph(nodes.p, perm.p, n, S, slots, d_tris9, out.nodes.p, out.tris.p, nullptr,
+        ok = ok && enqueue_collapse_graph(d_nodes, d_perm, n, S, slots, d_tris9, out.nodes.p, out.tris.p, nullptr,
                                           cscratch.p, cbytes, result.p + 4, cs, bs);
         cudaGraph_t g = nullptr;
         const bool ended = RT_CUDA(cudaStreamEndCapture(cs, &g));
@@ -1839,6 +1845,11 @@ bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tri
     out.num_nodes = h[4];
     out.num_leaf_items = h[5];
     out.depth = h[6];
+    if (keep) {
+        keep->num_nodes = h[0];
+        keep->num_prims = n;
+        keep->num_roots = S;
+    }
     if (info) {
         info->bvh2_nodes = h[0];
         info->levels = h[2];

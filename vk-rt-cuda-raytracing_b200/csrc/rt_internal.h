@@ -224,8 +224,11 @@ struct GraphBuildInfo {
     int levels = 0;        // large-task levels
     int small_tasks = 0;
 };
+// keep (optional): receives the binary tree and permutation (owned buffers)
+// for callers that export or refit it; without it they are scratch.
 bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tris9, int n, const BuildConfig& cfg,
-                      const std::vector<int>& segments, Bvh8Device& out, cudaStream_t s, GraphBuildInfo* info);
+                      const std::vector<int>& segments, Bvh8Device& out, cudaStream_t s, GraphBuildInfo* info,
+                      Bvh2Device* keep = nullptr);
 
 // Capture helpers for the graph-driven build: a conditional handle on the
 // graph being captured on cs, and a WHILE node on it at the capture
