@@ -146,7 +146,7 @@ bool build_into(CudaBVHHandle* h, cudaStream_t s) {
     // for the same 2M-triangle build); RTB200_BUILD=host keeps that loop
     static const bool host_loop = [] {
         const char* e = getenv("RTB200_BUILD");
-        return e && !strcmp(e, "host");
+        return (e && !strcmp(e, "host")) || !graph_build_supported();
     }();
     bool ok = host_loop ? build_bvh2(lo.p, hi.p, n, cfg, h->bvh2, s) && collapse_bvh8(h->bvh2, h->tris9.p, h->bvh8, s)
                         : build_bvh8_graph(lo.p, hi.p, h->tris9.p, n, cfg, std::vector<int>{0, n}, h->bvh8, s, nullptr,

@@ -142,7 +142,7 @@ RtBatch_t rtBatch_buildEx(const CudaTri* h_tris, const int* tri_offsets, int num
         launch_tri_bounds(tris9.p, n, lo.p, hi.p, s);
         BuildConfig cfg = default_build_config();
         cfg.transient = true;
-        b->graph_build = !(flags & RT_BATCH_BUILD_HOST_LOOP);
+        b->graph_build = !(flags & RT_BATCH_BUILD_HOST_LOOP) && graph_build_supported();
         if (b->graph_build)
             ok = build_bvh8_graph(lo.p, hi.p, tris9.p, n, cfg, b->tri_off, b->bvh8, s, nullptr);
         else

@@ -1651,6 +1651,19 @@ __global__ void k_build_result(const BuildCtl* __restrict__ ctl, int* __restrict
     out[3] = ctl->small;
 }
 
+bool graph_build_supported() {
+    // conditional WHILE nodes and capture into a node's body graph: CUDA 12.4
+    static const bool ok = [] {
+        int v = 0;
+        if (cudaDriverGetVersion(&v) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return v >= 12040;
+    }();
+    return ok;
+}
+
 bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tris9, int n, const BuildConfig& cfg,
                       const std::vector<int>& seg, Bvh8Device& out, cudaStream_t s, GraphBuildInfo* info,
                       Bvh2Device* keep) {

@@ -224,6 +224,9 @@ struct GraphBuildInfo {
     int levels = 0;        // large-task levels
     int small_tasks = 0;
 };
+// Whether the driver runs graphs with conditional nodes (else callers use
+// the host-driven loop).
+bool graph_build_supported();
 // keep (optional): receives the binary tree and permutation (owned buffers)
 // for callers that export or refit it; without it they are scratch.
 bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tris9, int n, const BuildConfig& cfg,
