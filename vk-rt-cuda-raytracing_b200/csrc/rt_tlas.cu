@@ -72,6 +72,21 @@ __device__ __forceinline__ InstView load_inst(const float4* __restrict__ inst, i
 #ifndef RTB_TLAS_SLOTMASK
 #define RTB_TLAS_SLOTMASK 2
 #endif
+// RTB_TLAS_SMEM: a lane entering an instance also writes its instance-space
+// ray and its instance (triangle array, id base, index) to shared memory,
+// where the lanes testing its triangles read them (three 16-byte loads)
+// instead of gathering them with thirteen shuffles per pooled round.
+#ifndef RTB_TLAS_SMEM
+#define RTB_TLAS_SMEM 1
+#endif
+// RTB_TLAS_TWO_SETS (with RTB_TLAS_SMEM): a lane keeps two pending sets of
+// leaf triangles, each with its own instance (ray, triangle array, id base)
+// written to shared memory when the set is recorded, so a step that finds
+// leaves does not end the lane's steps and the second set may come from
+// another instance.
+#ifndef RTB_TLAS_TWO_SETS
+#define RTB_TLAS_TWO_SETS 0
+#endif
 template <bool ANY>
 __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
     k_trace_tlas(const uint4* __restrict__ tnodes, const int* __restrict__ leaf_ids, const float4* __restrict__ inst,
@@ -82,6 +97,12 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
     __shared__ unsigned long long s_key[TRACE_T];
     __shared__ int s_rec[TRACE_T];
     __shared__ int4 s_res[TRACE_T];  // u, v bits, instance, primitive of the improved best
+#if RTB_TLAS_SMEM
+    constexpr int NSET = RTB_TLAS_TWO_SETS ? 2 : 1;
+    __shared__ float4 s_ray[NSET][2][TRACE_T];  // per pending set: instance-space ray (o, world tmin), (d, world tmax)
+    __shared__ uint4 s_inst[NSET][TRACE_T];     // per pending set: triangle array (lo, hi), id base, instance index
+#endif
+    static_assert(!RTB_TLAS_TWO_SETS || RTB_TLAS_SMEM, "two pending sets keep their instances in shared memory");
 #if RTB_TLAS_SLOTMASK
     __shared__ NodeLuts s_luts;
     init_node_luts(&s_luts);
@@ -134,10 +155,17 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
         if (__all_sync(FULL_MASK, ray < 0)) break;
         // ---- node phase ----
         uint32_t tri_base = 0, tmask = 0;
+#if RTB_TLAS_TWO_SETS
+        uint32_t tri_base2 = 0, tmask2 = 0;  // a second set while the first waits
+#define RTB_TLAS_LAST tmask2
+#else
+        constexpr uint32_t tmask2 = 0;
+#define RTB_TLAS_LAST tmask
+#endif
         bool overflow = false;
 #pragma unroll 1
         for (int it = 0; it < RTB_TLAS_ITERS; it++) {
-            if (ray < 0 || tmask || overflow) break;
+            if (ray < 0 || RTB_TLAS_LAST || overflow) break;
             if (w.ng.y & G_INST) {
                 // enter the next instance of an instance group
                 uint32_t m = w.ng.y & 0xFFu;
@@ -157,6 +185,13 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
                 btris = iv.tris;
                 cur_base = iv.base;
                 in_blas = true;
+#if RTB_TLAS_SMEM && !RTB_TLAS_TWO_SETS
+                s_ray[0][0][threadIdx.x] = make_float4(cr.ox, cr.oy, cr.oz, wr.tmin);
+                s_ray[0][1][threadIdx.x] = make_float4(cr.dx, cr.dy, cr.dz, wr.tmax);
+                s_inst[0][threadIdx.x] = make_uint4((uint32_t)(unsigned long long)btris,
+                                                    (uint32_t)((unsigned long long)btris >> 32), cur_base,
+                                                    (uint32_t)cur_inst);
+#endif
                 w.ng = make_uint2(0u, (1u << cr.oct) | (1u << 8));
                 continue;
             }
@@ -186,10 +221,28 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
                     w.ng = make_uint2(tb, (tm & 0xFFu) | G_INST | G_TOP);
                 }
             } else {
+#if RTB_TLAS_TWO_SETS
+                if (tm) {
+                    const int set = tmask ? 1 : 0;
+                    if (set) {
+                        tri_base2 = tb;
+                        tmask2 = tm;
+                    } else {
+                        tri_base = tb;
+                        tmask = tm;
+                    }
+                    s_ray[set][0][threadIdx.x] = make_float4(cr.ox, cr.oy, cr.oz, wr.tmin);
+                    s_ray[set][1][threadIdx.x] = make_float4(cr.dx, cr.dy, cr.dz, wr.tmax);
+                    s_inst[set][threadIdx.x] = make_uint4((uint32_t)(unsigned long long)btris,
+                                                          (uint32_t)((unsigned long long)btris >> 32), cur_base,
+                                                          (uint32_t)cur_inst);
+                }
+#else
                 tri_base = tb;
                 tmask = tm;
+#endif
             }
-            if ((w.ng.y & 0xFFu) == 0 && !(w.ng.y & G_INST) && !tmask && w.sp > 0) {
+            if ((w.ng.y & 0xFFu) == 0 && !(w.ng.y & G_INST) && (RTB_TLAS_TWO_SETS || !tmask) && w.sp > 0) {
                 w.ng = w.pop(sstack, lstack);
                 if (in_blas && (w.ng.y & G_TOP)) {
                     in_blas = false;
@@ -197,8 +250,9 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
                 }
             }
         }
+#undef RTB_TLAS_LAST
         // ---- triangle phase: pooled over the warp ----
-        const int cnt = __popc(tmask);
+        const int cnt = __popc(tmask) + __popc(tmask2);
         int incl = cnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -212,7 +266,9 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
             if (!ANY) s_key[threadIdx.x] = ((unsigned long long)f2ord(thit) << 32) | hid;
             s_rec[threadIdx.x] = ANY ? 0 : -1;
             __syncwarp();
+#if !RTB_TLAS_SMEM
             const unsigned long long tp64 = (unsigned long long)btris;
+#endif
             for (int b = 0; b < total; b += 32) {
                 const int g = b + lane;
                 int o = 0;
@@ -222,9 +278,32 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
                     if (v <= g) o += s;
                 }
                 o = min(o, 31);
-                const int k = g - __shfl_sync(FULL_MASK, excl, o);
-                const uint32_t om = __shfl_sync(FULL_MASK, tmask, o);
-                const uint32_t ob = __shfl_sync(FULL_MASK, tri_base, o);
+                const int k0 = g - __shfl_sync(FULL_MASK, excl, o);
+                uint32_t om = __shfl_sync(FULL_MASK, tmask, o);
+                uint32_t ob = __shfl_sync(FULL_MASK, tri_base, o);
+#if RTB_TLAS_TWO_SETS
+                const uint32_t om2 = __shfl_sync(FULL_MASK, tmask2, o);
+                const uint32_t ob2 = __shfl_sync(FULL_MASK, tri_base2, o);
+                const int c1 = __popc(om);
+                const int set = k0 >= c1 ? 1 : 0;
+                const int k = set ? k0 - c1 : k0;
+                if (set) {
+                    om = om2;
+                    ob = ob2;
+                }
+#else
+                constexpr int set = 0;
+                const int k = k0;
+#endif
+#if RTB_TLAS_SMEM
+                const uint4 oi = s_inst[set][wbase + o];
+                const unsigned long long optr = ((unsigned long long)oi.y << 32) | oi.x;
+                const uint32_t obase = oi.z;
+                const int oinst = (int)oi.w;
+                const float4 ro = s_ray[set][0][wbase + o], rd = s_ray[set][1][wbase + o];
+                const float ox = ro.x, oy = ro.y, oz = ro.z, tmn = ro.w;
+                const float dx = rd.x, dy = rd.y, dz = rd.z, tmx = rd.w;
+#else
                 const unsigned long long optr = __shfl_sync(FULL_MASK, tp64, o);
                 const uint32_t obase = __shfl_sync(FULL_MASK, cur_base, o);
                 const int oinst = __shfl_sync(FULL_MASK, cur_inst, o);
@@ -233,6 +312,7 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
                 const float dx = __shfl_sync(FULL_MASK, cr.dx, o), dy = __shfl_sync(FULL_MASK, cr.dy, o),
                             dz = __shfl_sync(FULL_MASK, cr.dz, o);
                 const float tmn = __shfl_sync(FULL_MASK, wr.tmin, o), tmx = __shfl_sync(FULL_MASK, wr.tmax, o);
+#endif
                 unsigned long long key = ~0ull;
                 float u = 0.f, v = 0.f;
                 int prim = 0;
