@@ -111,6 +111,50 @@ def test_injected_allocation_failures_fail_cleanly(cuda):
     assert np.array_equal(got["t"].view(np.uint32), want["t"].view(np.uint32))
 
 
+def test_every_build_allocation_failure_is_clean(cuda):
+    """A build whose k-th device allocation fails, for every k up to the
+    first that no build reaches: the one-graph build (single scene and
+    batched) and the host-driven loop return the error, leave no stream
+    capturing, and the next build is byte-identical to one that never
+    failed."""
+    L = lib.load()
+    tris = scenes.scene_meshes(21, 40_000, box=30.0, lo=500, hi=4000)
+    parts = [tris[:15_000], tris[15_000:15_003], tris[15_003:]]
+    rays = np.ascontiguousarray(scenes.random_rays(24, 20_000, box=40.0))
+    ref = lib.BVH(tris)
+    want = ref.closest_host(rays)
+    ref.close()
+
+    def sweep(make):
+        failed = 0
+        for k in range(200):
+            L.rtDebug_failAllocations(k)
+            try:
+                obj = make()
+            except lib.RtError as e:
+                assert "injected" in str(e) or "injected" in lib.last_error()
+                failed += 1
+                continue
+            finally:
+                L.rtDebug_failAllocations(-1)
+            obj.close()
+            return failed
+        raise AssertionError("every build failed")
+
+    try:
+        assert sweep(lambda: lib.BVH(tris)) >= 3
+        assert sweep(lambda: lib.Batch(parts)) >= 3
+        assert sweep(lambda: lib.Batch(parts, host_loop=True)) >= 3
+    finally:
+        L.rtDebug_failAllocations(-1)
+    bvh = lib.BVH(tris)
+    try:
+        got = bvh.closest_host(rays)
+        assert np.array_equal(got.view(np.uint8), want.view(np.uint8))
+    finally:
+        bvh.close()
+
+
 def test_server_wait_times_out_then_completes(cuda):
     import torch
     bvh = lib.BVH(scenes.scene_meshes(7, 300_000))
