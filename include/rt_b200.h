@@ -251,8 +251,9 @@ int cudaTLAS_getInverseTransforms(CudaTLAS_t tlas, float* out, int numInstances)
  * stage is one launch for all scenes, all of it one CUDA graph) and traced
  * by one persistent work-stealing launch.  Triangles of scene i are tri_offsets[i] ..
  * tri_offsets[i+1]-1 of h_tris; rays of scene i are d_ray_offsets[i] ..
- * d_ray_offsets[i+1]-1 (device array, num_scenes+1 entries).  Reported
- * primitive ids are relative to their scene. */
+ * d_ray_offsets[i+1]-1 (device array, num_scenes+1 entries), at most
+ * 65,535 scenes per batch.  Reported primitive ids are relative to their
+ * scene. */
 typedef struct RtBatchHandle* RtBatch_t;
 RtBatch_t rtBatch_build(const CudaTri* h_tris, const int* tri_offsets, int num_scenes, void* stream);
 /* rtBatch_build runs the whole build (SAH levels, small and warp subtrees,

@@ -258,7 +258,9 @@ __device__ __forceinline__ float bin_scale(float cmin, float cmax) {
 }
 
 // Per-segment box and centroid box (12 ordered uints per segment); grid.y
-// is the segment, grid.x strides over its primitives.
+// is the segment (so at most kMaxSegments of them), grid.x strides over its
+// primitives.
+constexpr int kMaxSegments = 65535;
 __global__ void k_seg_bounds(const float4* __restrict__ lo, const float4* __restrict__ hi,
                              const int* __restrict__ seg_off, uint32_t* __restrict__ acc) {
     const int sgi = blockIdx.y;
@@ -1330,6 +1332,10 @@ bool build_bvh2(const float4* d_lo, const float4* d_hi, int n, const BuildConfig
         set_error("build: bad segment table");
         return false;
     }
+    if (S > kMaxSegments) {
+        set_error("build: %d scenes, at most %d per build", S, kMaxSegments);
+        return false;
+    }
     for (int i = 0; i < S; i++)
         if (seg[i + 1] <= seg[i]) {
             set_error("build: segment %d is empty", i);
@@ -1678,6 +1684,10 @@ bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tri
     const int S = (int)seg.size() - 1;
     if (S < 1 || seg.front() != 0 || seg.back() != n) {
         set_error("graph build: bad segment table");
+        return false;
+    }
+    if (S > kMaxSegments) {
+        set_error("graph build: %d scenes, at most %d per build", S, kMaxSegments);
         return false;
     }
     int maxcnt = 0;
