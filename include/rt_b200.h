@@ -119,6 +119,17 @@ int cudaBVH_getStatus(CudaBVH_t bvh, void* stream);
 int cudaBVH_traceClosestHost(CudaBVH_t bvh, const RtRay* h_rays, int n, RtHit* h_hits);
 int cudaBVH_traceAnyHost(CudaBVH_t bvh, const RtRay* h_rays, int n, uint8_t* h_occluded);
 
+/* The same host-buffer traces over several replicas of one scene, one
+ * handle per GPU (each built with its device current): the n rays split into
+ * `count` contiguous blocks, as even as possible in handle order, and each
+ * block runs through its handle's host pipeline on its own device from its
+ * own host thread, so the GPUs' copy engines and SMs work at once.  Returns
+ * when every result is in host memory; the first failing block's code, with
+ * the replica's index in rtGetLastError().  At most 64 handles.  No
+ * counterpart in the reference (one device per process there). */
+int cudaBVH_traceClosestHostMulti(const CudaBVH_t* bvhs, int count, const RtRay* h_rays, int n, RtHit* h_hits);
+int cudaBVH_traceAnyHostMulti(const CudaBVH_t* bvhs, int count, const RtRay* h_rays, int n, uint8_t* h_occluded);
+
 /* Closest hit of up to 65,536 host rays without allocating any memory.
  * No counterpart in the reference.  For callers that must not allocate while
  * they trace: a Vulkan layer tracing on the application's render thread (a

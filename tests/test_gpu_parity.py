@@ -376,6 +376,37 @@ def _d2h(ptr, nbytes):
     return out
 
 
+def test_host_traces_over_replicas_equal_one_handle(cuda):
+    """cudaBVH_traceClosestHostMulti / AnyHostMulti: a host batch split over
+    replicas (here several handles on the one GPU of this box, each with its
+    own host thread and pipeline) gives the single handle's results byte for
+    byte, for batches longer and shorter than the replica count; bad
+    arguments are rejected."""
+    import ctypes as C
+    tris = scenes.scene_meshes(31, 30_000, box=30.0, lo=300, hi=3000)
+    rays = scenes.scene_rays(tris, 60_001, seed=9)
+    reps = [lib.BVH(tris) for _ in range(3)]
+    try:
+        want = reps[0].closest_host(rays)
+        want_occ = reps[0].any_host(rays)
+        assert (want["prim"] >= 0).mean() > 0.2
+        for k in (1, 2, 3):
+            got = lib.trace_host_multi(reps[:k], rays)
+            assert np.array_equal(got.view(np.uint8), want.view(np.uint8)), f"{k} replicas"
+            assert np.array_equal(lib.trace_host_multi(reps[:k], rays, any_hit=True), want_occ)
+        few = np.ascontiguousarray(rays[:2])
+        assert np.array_equal(lib.trace_host_multi(reps, few).view(np.uint8), want[:2].view(np.uint8))
+        assert lib.trace_host_multi(reps, rays[:0]).shape == (0,)
+        L = lib.load()
+        hs = (C.c_void_p * 2)(reps[0].h, None)
+        out = np.zeros(4, HIT_DTYPE)
+        assert L.cudaBVH_traceClosestHostMulti(hs, 2, few.ctypes.data, 2, out.ctypes.data) == -1  # RT_ERR_INVALID
+        assert L.cudaBVH_traceClosestHostMulti(hs, 0, few.ctypes.data, 2, out.ctypes.data) == -1  # RT_ERR_INVALID
+    finally:
+        for b in reps:
+            b.close()
+
+
 def test_counters_match_closest_results(cuda, small_scene):
     import torch
     bvh = lib.BVH(small_scene)

@@ -194,6 +194,10 @@ CudaBVHHandle* new_handle(int n) {
         return nullptr;
     }
     h->num_tris = n;
+    if (cudaGetDevice(&h->device) != cudaSuccess) {
+        cudaGetLastError();
+        h->device = 0;
+    }
     return h;
 }
 
@@ -722,7 +726,62 @@ int trace_host(CudaBVHHandle* h, const RtRay* rays, int n, void* out, bool any) 
     return check_status(h);
 }
 
+constexpr int kMaxReplicas = 64;  // handles per multi-replica call
+
+// One host-buffer batch over several replicas (one handle per device): the
+// rays split into contiguous blocks, as even as possible in handle order,
+// each traced by its handle's host pipeline on its own device from its own
+// host thread; returns when every block's results are in host memory.  The
+// first failing block's code and message are returned.
+int trace_host_multi(const CudaBVH_t* bvhs, int count, const RtRay* rays, int n, void* out, bool any,
+                     const char* who) {
+    if (!bvhs || count < 1 || count > kMaxReplicas || n < 0 || (n > 0 && (!rays || !out))) {
+        set_error("%s: invalid argument", who);
+        return RT_ERR_INVALID;
+    }
+    for (int i = 0; i < count; i++)
+        if (!bvhs[i]) {
+            set_error("%s: handle %d is null", who, i);
+            return RT_ERR_INVALID;
+        }
+    if (n == 0) return RT_OK;
+    const size_t es = any ? 1 : sizeof(RtHit);
+    std::vector<int> rc(count, RT_OK);
+    std::vector<std::string> msg(count);
+    std::vector<std::thread> th;
+    th.reserve(count);
+    const int q = n / count, r = n % count;
+    for (int i = 0; i < count; i++) {
+        const int first = i * q + std::min(i, r), cnt = q + (i < r ? 1 : 0);
+        if (cnt == 0) continue;
+        th.emplace_back([&, i, first, cnt] {
+            CudaBVHHandle* h = bvhs[i];
+            if (!RT_CUDA(cudaSetDevice(h->device))) {
+                rc[i] = RT_ERR_CUDA;
+            } else {
+                rc[i] = trace_host(h, rays + first, cnt, (char*)out + (size_t)first * es, any);
+            }
+            if (rc[i] != RT_OK) msg[i] = rtGetLastError();
+        });
+    }
+    for (std::thread& t : th) t.join();
+    for (int i = 0; i < count; i++)
+        if (rc[i] != RT_OK) {
+            set_error("%s: replica %d: %s", who, i, msg[i].c_str());
+            return rc[i];
+        }
+    return RT_OK;
+}
+
 }  // namespace
+
+int cudaBVH_traceClosestHostMulti(const CudaBVH_t* bvhs, int count, const RtRay* rays, int n, RtHit* hits) {
+    return trace_host_multi(bvhs, count, rays, n, hits, false, "cudaBVH_traceClosestHostMulti");
+}
+
+int cudaBVH_traceAnyHostMulti(const CudaBVH_t* bvhs, int count, const RtRay* rays, int n, uint8_t* occ) {
+    return trace_host_multi(bvhs, count, rays, n, occ, true, "cudaBVH_traceAnyHostMulti");
+}
 
 int cudaBVH_traceClosestHost(CudaBVH_t h, const RtRay* rays, int n, RtHit* hits) {
     if (!h || n < 0 || (n > 0 && (!rays || !hits))) {

@@ -288,6 +288,7 @@ struct HostPipe {
 // ---- the handle behind CudaBVH_t ----
 struct CudaBVHHandle {
     int num_tris = 0;
+    int device = 0;               // the CUDA device current when the handle was created
     float bmin[3], bmax[3], center[3], extent = 0.f;
     rtb::DevBuf<float> tris9;     // input triangles (device copy)
     rtb::Bvh2Device bvh2;

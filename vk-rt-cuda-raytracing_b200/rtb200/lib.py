@@ -137,6 +137,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "cudaBVH_traceAny": (i32, [vp, vp, i32, vp, vp]),
         "cudaBVH_traceClosestHost": (i32, [vp, vp, i32, vp]),
         "cudaBVH_traceAnyHost": (i32, [vp, vp, i32, vp]),
+        "cudaBVH_traceClosestHostMulti": (i32, [vp, i32, vp, i32, vp]),
+        "cudaBVH_traceAnyHostMulti": (i32, [vp, i32, vp, i32, vp]),
         "cudaBVH_traceCounters": (i32, [vp, vp, i32, i32, vp, vp]),
         "cudaBVH_traceClosestHostNoAlloc": (i32, [vp, vp, i32, vp, vp]),
         "cudaBVH_getStatus": (i32, [vp, vp]),
@@ -428,6 +430,22 @@ def tlas_fast(aabbs: np.ndarray):
     libc.free(C.cast(pn, C.c_void_p))
     libc.free(C.cast(po, C.c_void_p))
     return nodes, ordered
+
+
+def trace_host_multi(bvhs, rays: np.ndarray, any_hit: bool = False) -> np.ndarray:
+    """cudaBVH_traceClosestHostMulti / cudaBVH_traceAnyHostMulti: one host
+    batch split over replicas of a scene (one BVH per GPU)."""
+    rays = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
+    hs = (C.c_void_p * len(bvhs))(*[b.h for b in bvhs])
+    if any_hit:
+        out = np.zeros(rays.shape[0], dtype=np.uint8)
+        _check(load().cudaBVH_traceAnyHostMulti(hs, len(bvhs), rays.ctypes.data, rays.shape[0], out.ctypes.data),
+               "cudaBVH_traceAnyHostMulti")
+    else:
+        out = np.zeros(rays.shape[0], dtype=HIT_DTYPE)
+        _check(load().cudaBVH_traceClosestHostMulti(hs, len(bvhs), rays.ctypes.data, rays.shape[0],
+                                                    out.ctypes.data), "cudaBVH_traceClosestHostMulti")
+    return out
 
 
 class TLAS:
