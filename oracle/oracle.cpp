@@ -277,7 +277,9 @@ inline void unpack(const float* p, float v0[3], float e1[3], float e2[3], int& p
     prim = (int)p[9];
 }
 
-// Conservative slab test, evaluated in double with a relative slack, so the
+// Conservative slab test, evaluated in double with a relative slack and a
+// per-axis slack of 2^-20 of the box and origin coordinates times |1/d| (a
+// grazing ray's accepted fp32 hit can lie that far outside the box), so the
 // oracle never culls a box that holds an accepted fp32 hit.  Culling only
 // affects speed; the hit set is defined by the triangle test alone.
 struct DRay { double o[3], inv[3]; bool zero[3]; };
@@ -300,8 +302,12 @@ inline bool box_hit(const DRay& r, const float* bmin, const float* bmax, double 
             continue;
         }
         double t1 = (lo - r.o[a]) * r.inv[a], t2 = (hi - r.o[a]) * r.inv[a];
-        tn = std::max(tn, std::min(t1, t2));
-        tf = std::min(tf, std::max(t1, t2));
+        // per-axis slack for a ray nearly parallel to the slab: the fp32
+        // triangle test's hit point may lie a few float roundings of the
+        // coordinates outside the box, which 1/d turns into a large t
+        const double ea = ldexp((fabs(lo) + fabs(hi) + 2.0 * fabs(r.o[a])) * fabs(r.inv[a]), -20);
+        tn = std::max(tn, std::min(t1, t2) - ea);
+        tf = std::min(tf, std::max(t1, t2) + ea);
     }
     double sl = 1e-5 * std::max(fabs(tn), fabs(tf)) + 1e-9;
     if (!(tn <= tf + sl)) return false;

@@ -305,6 +305,104 @@ def test_tlas_two_level_vs_oracle(cuda):
         L.cudaTLAS_destroy(tl)
 
 
+def _oracle_two_level(blas_tris, xf, bidx, inv, rays):
+    """The oracle's two-level walk (restated builder per BLAS, LBVH over
+    padded world boxes): closest hits, instance ids and occlusion flags."""
+    obs = [O.OracleBVH(t, 32, 4) for t in blas_tris]
+    node_off = np.cumsum([0] + [o.dfs.size // 8 for o in obs]).astype(np.int32)
+    tri_off = np.cumsum([0] + [o.packed.size // 12 for o in obs]).astype(np.int32)
+    bdfs = np.concatenate([o.dfs for o in obs])
+    bpk = np.concatenate([o.packed for o in obs])
+    ninst = len(bidx)
+    wb = []
+    for k in range(ninst):
+        v = blas_tris[bidx[k]].reshape(-1, 3).astype(np.float64) @ xf[k][:, :3].T.astype(np.float64) + xf[k][:, 3]
+        pad = 1e-4 * (np.abs(v).max() + 1)
+        wb.append(np.concatenate([v.min(0) - pad, v.max(0) + pad]))
+    tnodes, tord = O.tlas_fast(np.array(wb, np.float32))
+    tnodes = O.fix_skips(tnodes)
+    iblas = np.ascontiguousarray(bidx, np.int32)
+    inv = np.ascontiguousarray(inv, np.float32)
+    hits = np.zeros(rays.shape[0], HIT_DTYPE)
+    inst_ref = np.zeros(rays.shape[0], np.int32)
+    occ_ref = np.zeros(rays.shape[0], np.uint8)
+    Lo = O.lib()
+    args = (tnodes.ctypes.data, tnodes.size // 8, tord.ctypes.data, inv.ctypes.data, iblas.ctypes.data, ninst,
+            bdfs.ctypes.data, node_off.ctypes.data, bpk.ctypes.data, tri_off.ctypes.data, rays.ctypes.data,
+            rays.shape[0])
+    Lo.orc_trace_closest_two_level(*args, hits.ctypes.data, inst_ref.ctypes.data, 0)
+    Lo.orc_trace_any_two_level(*args, occ_ref.ctypes.data, 0)
+    return hits, inst_ref, occ_ref
+
+
+def test_tlas_rotated_floored_instances_vs_oracle(cuda):
+    """Two-level traversal on the path tracer's kind of scene -- BLASes of
+    mesh clusters over a two-triangle floor, rotated and scaled instances
+    whose boxes overlap -- against the oracle's two-level walk: camera
+    rays, bounce rays from their hits, and rays grazing the instances'
+    floor planes and box faces, where any culling that is not conservative
+    (the instance world boxes, the object-space box tested after entering
+    an instance) shows up as a changed hit."""
+    import torch
+    blas_tris, xf, bidx, _, _ = scenes.instanced_scene(3, 240_000, nblas=8, ninst=48, world=100.0)
+    tl = lib.TLAS([lib.BVH(t) for t in blas_tris], xf, bidx)
+    try:
+        rng = np.random.default_rng(4)
+        cam = scenes.pinhole_rays(480, 270, scenes.PT_CAM_EYE, scenes.PT_CAM_TARGET, vfov_deg=50.0)
+        parts = [cam]
+        d_cam = _dev(torch, cam)
+        d_h = torch.empty(cam.shape[0] * 16, dtype=torch.uint8, device="cuda")
+        tl.closest(d_cam, cam.shape[0], d_h)
+        torch.cuda.synchronize()
+        h = d_h.cpu().numpy().view(HIT_DTYPE)
+        hit = h["prim"] >= 0
+        # bounce rays: uniform directions on the side of the incoming ray
+        o = cam["org"][hit] + cam["dir"][hit] * h["t"][hit][:, None]
+        dn = rng.normal(size=(int(hit.sum()), 3)).astype(np.float32)
+        dn /= np.linalg.norm(dn, axis=1, keepdims=True)
+        dn = np.where((dn * cam["dir"][hit]).sum(1, keepdims=True) > 0, -dn, dn)
+        bnc = np.zeros(dn.shape[0], RAY_DTYPE)
+        bnc["org"], bnc["dir"], bnc["tmin"], bnc["tmax"] = o + dn * np.float32(1e-3), dn, 1e-3, 1e30
+        parts.append(bnc)
+        # grazing rays: in each instance's floor plane (and the planes of its
+        # object box faces), aimed across the instance with a tiny tilt
+        for k in range(len(bidx)):
+            v = blas_tris[bidx[k]].reshape(-1, 3).astype(np.float64)
+            lo, hi = v.min(0), v.max(0)
+            M = xf[k].astype(np.float64)
+            m = 400
+            q = rng.uniform(lo, hi, (m, 3))
+            ax = rng.integers(0, 3, m)
+            face = np.where(rng.random(m) < 0.5, lo[ax], hi[ax])
+            q[np.arange(m), ax] = face
+            q[: m // 4, 1] = v[:6, 1].min()  # the floor's plane
+            dl = rng.normal(size=(m, 3))
+            dl[np.arange(m), ax] *= 1e-4
+            dl[: m // 4, 1] *= 1e-4
+            dl /= np.linalg.norm(dl, axis=1, keepdims=True)
+            wq, wd = q @ M[:, :3].T + M[:, 3], dl @ M[:, :3].T
+            wd /= np.linalg.norm(wd, axis=1, keepdims=True)
+            g = np.zeros(m, RAY_DTYPE)
+            g["org"], g["dir"], g["tmin"], g["tmax"] = wq - wd * 50.0, wd, 0.0, 1e30
+            parts.append(g)
+        rays = np.ascontiguousarray(np.concatenate(parts))
+        ref, inst_ref, occ_ref = _oracle_two_level(blas_tris, xf, bidx, tl.inverse(), rays)
+        n = rays.shape[0]
+        d_rays = _dev(torch, rays)
+        d_hits = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
+        d_inst = torch.empty(n, dtype=torch.int32, device="cuda")
+        d_occ = torch.empty(n, dtype=torch.uint8, device="cuda")
+        tl.closest(d_rays, n, d_hits, d_inst)
+        tl.any(d_rays, n, d_occ)
+        torch.cuda.synchronize()
+        assert_hits_equal(d_hits.cpu().numpy().view(HIT_DTYPE), ref, "floored instances")
+        assert np.array_equal(d_inst.cpu().numpy(), inst_ref)
+        assert np.array_equal(d_occ.cpu().numpy(), occ_ref)
+        assert (ref["prim"] >= 0).mean() > 0.3
+    finally:
+        tl.close()
+
+
 def test_tlas_set_transforms_equals_a_fresh_build(cuda):
     """cudaTLAS_setTransforms moves every instance and changes BLAS choices in
     place: traces afterwards are byte-identical to those of a TLAS built with

@@ -3,8 +3,9 @@
 // and the instance records of layer/VkLayer_CudaRT.cpp:4517-4558, done on
 // the compressed 8-wide layout).
 //
-// Build: world box of every instance = the 8 transformed corners of its
-// BLAS root box, padded outward by a relative 2^-16 of the coordinate
+// Build: world box of every instance = the bounds of its BLAS's vertices
+// under its transform (evaluated on the GPU in double precision, rounded
+// outward to float), padded outward by a relative 2^-16 of the coordinate
 // magnitudes (covers the rounding of the object-space ray transform), then
 // the same GPU SAH builder with one instance per leaf.
 // Trace: one stack for both levels.  Entering an instance transforms the
@@ -23,21 +24,24 @@ namespace rtb {
 
 constexpr uint32_t G_TOP = 1u << 16;   // group belongs to the top level
 constexpr uint32_t G_INST = 1u << 17;  // group is a mask of instance leaves
-constexpr int INST_F4 = 5;             // float4 words per instance record
+constexpr int INST_F4 = 6;             // float4 words per instance record
 
-// Instance record (5 x float4): inverse 3x4 rows, BLAS node and triangle
-// pointers, and the instance's base in the global (instance, primitive)
-// numbering used for tie breaks.
+// Instance record (6 x float4): inverse 3x4 rows, BLAS node and triangle
+// pointers, the instance's base in the global (instance, primitive)
+// numbering used for tie breaks, and the object-space bounds of the BLAS's
+// vertices (base, lo.xyz), (hi.xyz, 0).
 struct InstView {
     float m[12];
     const uint4* nodes;
     const float4* tris;
     uint32_t base;
+    float lo[3], hi[3];
 };
 
 __device__ __forceinline__ InstView load_inst(const float4* __restrict__ inst, int i) {
     const float4* ip = inst + (size_t)i * INST_F4;
-    const float4 r0 = __ldg(ip), r1 = __ldg(ip + 1), r2 = __ldg(ip + 2), pp = __ldg(ip + 3), bb = __ldg(ip + 4);
+    const float4 r0 = __ldg(ip), r1 = __ldg(ip + 1), r2 = __ldg(ip + 2), pp = __ldg(ip + 3), bb = __ldg(ip + 4),
+                 bh = __ldg(ip + 5);
     InstView v;
     v.m[0] = r0.x; v.m[1] = r0.y; v.m[2] = r0.z; v.m[3] = r0.w;
     v.m[4] = r1.x; v.m[5] = r1.y; v.m[6] = r1.z; v.m[7] = r1.w;
@@ -45,7 +49,29 @@ __device__ __forceinline__ InstView load_inst(const float4* __restrict__ inst, i
     v.nodes = reinterpret_cast<const uint4*>(((unsigned long long)__float_as_uint(pp.y) << 32) | __float_as_uint(pp.x));
     v.tris = reinterpret_cast<const float4*>(((unsigned long long)__float_as_uint(pp.w) << 32) | __float_as_uint(pp.z));
     v.base = __float_as_uint(bb.x);
+    v.lo[0] = bb.y; v.lo[1] = bb.z; v.lo[2] = bb.w;
+    v.hi[0] = bh.x; v.hi[1] = bh.y; v.hi[2] = bh.z;
     return v;
+}
+
+// Whether the object-space ray can meet the box within [tmin, thit]: the
+// slab distances (p - o) / d carry a relative slack of 2^-22 and the far
+// distance one of 2^-21, which bound the roundings of the subtraction, the
+// product and the guarded reciprocal, so a box holding an accepted hit is
+// never culled (the node test's argument, with the planes given directly).
+__device__ __forceinline__ bool box_reached(const Ray& r, const float (&lo)[3], const float (&hi)[3], float tmin,
+                                           float thit) {
+    const float ax = (lo[0] - r.ox) * r.ix, bx = (hi[0] - r.ox) * r.ix;
+    const float ay = (lo[1] - r.oy) * r.iy, by = (hi[1] - r.oy) * r.iy;
+    const float az = (lo[2] - r.oz) * r.iz, bz = (hi[2] - r.oz) * r.iz;
+    const float nx = fminf(ax, bx), fx = fmaxf(ax, bx);
+    const float ny = fminf(ay, by), fy = fmaxf(ay, by);
+    const float nz = fminf(az, bz), fz = fmaxf(az, bz);
+    const float tn = max3f(fmaf(-fabsf(nx), 0x1p-22f, nx), fmaf(-fabsf(ny), 0x1p-22f, ny),
+                           fmaxf(fmaf(-fabsf(nz), 0x1p-22f, nz), tmin));
+    const float tf = min3f(fmaf(fabsf(fx), 0x1p-22f, fx), fmaf(fabsf(fy), 0x1p-22f, fy),
+                           fminf(fmaf(fabsf(fz), 0x1p-22f, fz), thit));
+    return tn <= fmaf(fabsf(tf), 0x1p-21f, tf);
 }
 
 // Two-level closest/any hit.  Same iteration structure as the single-level
@@ -87,6 +113,26 @@ __device__ __forceinline__ InstView load_inst(const float4* __restrict__ inst, i
 #ifndef RTB_TLAS_TWO_SETS
 #define RTB_TLAS_TWO_SETS 0
 #endif
+// RTB_TLAS_STATS (analysis builds only; the release kernel is unchanged):
+// event counters in g_tlas_stats, read by rtTlasStats_read: [0] warp
+// iterations, [1] lanes holding a ray at an iteration's start, [2] instance
+// entries, [3] top-level node visits, [4] bottom-level node visits,
+// [5] triangle tests, [6] 32-lane triangle rounds, [7] rays finished,
+// [8] instances skipped by their object-space box.
+#ifndef RTB_TLAS_STATS
+#define RTB_TLAS_STATS 0
+#endif
+// RTB_TLAS_ROOTBOX: after transforming the ray into an instance, test the
+// object-space bounds of its BLAS (an oriented box in world space, tighter
+// than the instance's world-axis box for a rotated instance) before
+// visiting the BLAS's root node.
+#ifndef RTB_TLAS_ROOTBOX
+#define RTB_TLAS_ROOTBOX 1
+#endif
+#if RTB_TLAS_STATS
+__device__ unsigned long long g_tlas_stats[9];
+#endif
+
 template <bool ANY>
 __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
     k_trace_tlas(const uint4* __restrict__ tnodes, const int* __restrict__ leaf_ids, const float4* __restrict__ inst,
@@ -126,6 +172,9 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
     float thit = 0.f, hu = 0.f, hv = 0.f;
     int hprim = -1, hinst = -1;
     uint32_t hid = 0xFFFFFFFFu;
+#if RTB_TLAS_STATS
+    unsigned long long st_entry = 0, st_top = 0, st_bot = 0, st_done = 0, st_skip = 0;
+#endif
     for (;;) {
         const bool need = ray < 0 && !exhausted;
         const unsigned want = __ballot_sync(FULL_MASK, need);
@@ -153,6 +202,15 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
             }
         }
         if (__all_sync(FULL_MASK, ray < 0)) break;
+#if RTB_TLAS_STATS
+        {
+            const unsigned hold = __ballot_sync(FULL_MASK, ray >= 0);
+            if (lane == 0) {
+                atomicAdd(&g_tlas_stats[0], 1ull);
+                atomicAdd(&g_tlas_stats[1], (unsigned long long)__popc(hold));
+            }
+        }
+#endif
         // ---- node phase ----
         uint32_t tri_base = 0, tmask = 0;
 #if RTB_TLAS_TWO_SETS
@@ -171,16 +229,37 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
                 uint32_t m = w.ng.y & 0xFFu;
                 const int j = __ffs(m) - 1;
                 m &= m - 1;
+                const int next_inst = leaf_ids[w.ng.x + j];
+                const InstView iv = load_inst(inst, next_inst);
+                float ox, oy, oz, dx, dy, dz;
+                xform_point(iv.m, wr.ox, wr.oy, wr.oz, ox, oy, oz);
+                xform_dir(iv.m, wr.dx, wr.dy, wr.dz, dx, dy, dz);
+                const Ray tr = make_ray(make_float4(ox, oy, oz, wr.tmin), make_float4(dx, dy, dz, wr.tmax));
+#if RTB_TLAS_ROOTBOX
+                if (!box_reached(tr, iv.lo, iv.hi, wr.tmin, thit)) {
+                    // the instance's own box is missed: its root node is not visited;
+                    // the group's other instances (or the next stacked group) come next
+#if RTB_TLAS_STATS
+                    st_skip++;
+#endif
+                    if (m) {
+                        w.ng.y = (w.ng.y & ~0xFFu) | m;
+                    } else {
+                        w.ng.y = 0;
+                        if (w.sp > 0) w.ng = w.pop(sstack, lstack);  // at the top level: the world ray stays
+                    }
+                    continue;
+                }
+#endif
                 if (m && !w.push(make_uint2(w.ng.x, m | G_INST | G_TOP), sstack, lstack)) {
                     overflow = true;
                     break;
                 }
-                cur_inst = leaf_ids[w.ng.x + j];
-                const InstView iv = load_inst(inst, cur_inst);
-                float ox, oy, oz, dx, dy, dz;
-                xform_point(iv.m, wr.ox, wr.oy, wr.oz, ox, oy, oz);
-                xform_dir(iv.m, wr.dx, wr.dy, wr.dz, dx, dy, dz);
-                cr = make_ray(make_float4(ox, oy, oz, wr.tmin), make_float4(dx, dy, dz, wr.tmax));
+                cur_inst = next_inst;
+#if RTB_TLAS_STATS
+                st_entry++;
+#endif
+                cr = tr;
                 bnodes = iv.nodes;
                 btris = iv.tris;
                 cur_base = iv.base;
@@ -208,6 +287,10 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
                 break;
             }
             uint32_t nh, tb, tm;
+#if RTB_TLAS_STATS
+            if (top) st_top++;
+            else st_bot++;
+#endif
             visit_node<RTB_TLAS_SLOTMASK>((top ? tnodes : bnodes) + (size_t)ni * 5, cr, thit, nh, tb, tm, w.ng,
                                           s_oct_perm);
             if (top) {
@@ -260,6 +343,12 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
             if (lane >= o) incl += y;
         }
         const int total = __shfl_sync(FULL_MASK, incl, 31);
+#if RTB_TLAS_STATS
+        if (lane == 0 && total) {
+            atomicAdd(&g_tlas_stats[5], (unsigned long long)total);
+            atomicAdd(&g_tlas_stats[6], (unsigned long long)((total + 31) / 32));
+        }
+#endif
         bool found_any = false;
         if (total) {
             const int excl = incl - cnt;
@@ -379,11 +468,34 @@ __global__ void __launch_bounds__(TRACE_T, ANY ? TRACE_MINB : RTB_TLAS_MINB)
                                     hprim >= 0 ? hu : 0.f, hprim >= 0 ? hv : 0.f);
                     if (inst_out) inst_out[ray] = hprim >= 0 ? hinst : -1;
                 }
+#if RTB_TLAS_STATS
+                st_done++;
+#endif
                 ray = -1;
             }
         }
     }
+#if RTB_TLAS_STATS
+    atomicAdd(&g_tlas_stats[2], st_entry);
+    atomicAdd(&g_tlas_stats[3], st_top);
+    atomicAdd(&g_tlas_stats[4], st_bot);
+    atomicAdd(&g_tlas_stats[7], st_done);
+    atomicAdd(&g_tlas_stats[8], st_skip);
+#endif
 }
+
+#if RTB_TLAS_STATS
+extern "C" int rtTlasStats_read(unsigned long long* out9, int reset) {
+    if (cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpyFromSymbol(out9, g_tlas_stats, sizeof(unsigned long long) * 9) != cudaSuccess)
+        return -1;
+    if (reset) {
+        static const unsigned long long zero[9] = {};
+        if (cudaMemcpyToSymbol(g_tlas_stats, zero, sizeof(zero)) != cudaSuccess) return -1;
+    }
+    return 0;
+}
+#endif
 
 template <class K>
 static int grid_for(K kernel) {
@@ -436,18 +548,145 @@ static bool invert34(const float* m, double* inv) {
     return true;
 }
 
+// World bounds of the instances' geometry: the BLAS's vertices under the
+// instance's transform, one CTA row per instance (grid.y), sums of exact
+// float products in double, min / max rounded outward to float and folded
+// into ordered-uint atomics (6 per instance: lo xyz, hi xyz).  Tighter than
+// the transformed corners of the BLAS's root box, which for a rotated
+// instance bound a box around a box: fewer rays enter an instance they then
+// miss (the path tracer's scene: 72 % of the surface area of the corner
+// boxes), and hits do not change (the boxes still hold every triangle).
+struct InstBoundsJob {
+    const float* tris9;  // the BLAS's input triangles, 9 floats each
+    int ntris;
+    float m[12];         // object -> world, row-major 3x4
+};
+
+__global__ void k_instance_bounds(const InstBoundsJob* __restrict__ jobs, uint32_t* __restrict__ out) {
+    const InstBoundsJob j = jobs[blockIdx.y];
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    float olo[3] = {INFINITY, INFINITY, INFINITY}, ohi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    const int nv = j.ntris * 3;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x) {
+        const float* v = j.tris9 + (size_t)i * 3;
+        const double x = v[0], y = v[1], z = v[2];
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            olo[r] = fminf(olo[r], v[r]);
+            ohi[r] = fmaxf(ohi[r], v[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            const double w = (double)j.m[r * 4] * x + (double)j.m[r * 4 + 1] * y + (double)j.m[r * 4 + 2] * z +
+                             (double)j.m[r * 4 + 3];
+            lo[r] = fmin(lo[r], w);
+            hi[r] = fmax(hi[r], w);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        for (int o = 16; o; o >>= 1) {
+            lo[r] = fmin(lo[r], __shfl_xor_sync(FULL_MASK, lo[r], o));
+            hi[r] = fmax(hi[r], __shfl_xor_sync(FULL_MASK, hi[r], o));
+            olo[r] = fminf(olo[r], __shfl_xor_sync(FULL_MASK, olo[r], o));
+            ohi[r] = fmaxf(ohi[r], __shfl_xor_sync(FULL_MASK, ohi[r], o));
+        }
+    }
+    if ((threadIdx.x & 31) == 0 && nv > 0) {
+        uint32_t* o12 = out + (size_t)blockIdx.y * 12;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            atomicMin(&o12[r], f2ord(__double2float_rd(lo[r])));
+            atomicMax(&o12[3 + r], f2ord(__double2float_ru(hi[r])));
+            atomicMin(&o12[6 + r], f2ord(olo[r]));
+            atomicMax(&o12[9 + r], f2ord(ohi[r]));
+        }
+    }
+}
+
+// The instances' world bounds (see k_instance_bounds), padded outward by
+// 2^-16 of the box's coordinate magnitude plus its extents, as float4 lo/hi.
+static bool instance_bounds(const std::vector<CudaBVH_t>& blas, const RtInstance* inst, int ni,
+                            std::vector<float4>& lo, std::vector<float4>& hi, std::vector<float>& obj6) {
+    std::vector<InstBoundsJob> jobs(ni);
+    int maxtris = 0;
+    for (int k = 0; k < ni; k++) {
+        const CudaBVHHandle* b = blas[inst[k].blas];
+        if (!b->tris9.p || b->num_tris <= 0) {
+            set_error("TLAS: BLAS %d holds no triangles", inst[k].blas);
+            return false;
+        }
+        jobs[k].tris9 = b->tris9.p;
+        jobs[k].ntris = b->num_tris;
+        memcpy(jobs[k].m, inst[k].xform, sizeof(jobs[k].m));
+        maxtris = std::max(maxtris, b->num_tris);
+    }
+    std::vector<uint32_t> h((size_t)ni * 12);
+    for (int k = 0; k < ni; k++)
+        for (int r = 0; r < 12; r++) h[(size_t)k * 12 + r] = (r < 3 || (r >= 6 && r < 9)) ? 0xFFFFFFFFu : 0u;
+    DevBuf<InstBoundsJob> d_jobs;
+    DevBuf<uint32_t> d_out;
+    if (!d_jobs.alloc(ni) || !d_out.alloc((size_t)ni * 12) ||
+        !RT_CUDA(cudaMemcpy(d_jobs.p, jobs.data(), sizeof(InstBoundsJob) * ni, cudaMemcpyHostToDevice)) ||
+        !RT_CUDA(cudaMemcpy(d_out.p, h.data(), sizeof(uint32_t) * h.size(), cudaMemcpyHostToDevice)))
+        return false;
+    const int gx = std::max(1, std::min((3 * maxtris + 255) / 256, 64));
+    if (ni > 65535) {
+        set_error("TLAS: %d instances, at most 65535", ni);
+        return false;
+    }
+    k_instance_bounds<<<dim3(gx, ni), 256>>>(d_jobs.p, d_out.p);
+    if (!RT_CUDA(cudaGetLastError()) ||
+        !RT_CUDA(cudaMemcpy(h.data(), d_out.p, sizeof(uint32_t) * h.size(), cudaMemcpyDeviceToHost)))
+        return false;
+    lo.resize(ni);
+    hi.resize(ni);
+    obj6.resize((size_t)ni * 6);
+    auto ordf = [](uint32_t u) {
+        const uint32_t v = (u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u;
+        float f;
+        memcpy(&f, &v, 4);
+        return (double)f;
+    };
+    for (int k = 0; k < ni; k++) {
+        double wl[3], wh[3], mag = 0.0;
+        double ol[3], oh[3], omag = 0.0;
+        for (int r = 0; r < 3; r++) {
+            wl[r] = ordf(h[(size_t)k * 12 + r]);
+            wh[r] = ordf(h[(size_t)k * 12 + 3 + r]);
+            mag = std::max(mag, std::max(fabs(wl[r]), fabs(wh[r])));
+            ol[r] = ordf(h[(size_t)k * 12 + 6 + r]);
+            oh[r] = ordf(h[(size_t)k * 12 + 9 + r]);
+            omag = std::max(omag, std::max(fabs(ol[r]), fabs(oh[r])));
+        }
+        // the object-space box gets the world box's relative pad: the kernels
+        // test v0 + fl(v1 - v0) and v0 + fl(v2 - v0), which can lie a rounding
+        // outside the input vertices' bounds, and the triangle test accepts
+        // rays grazing an edge within its own rounding
+        const double opad = ldexp(omag + (oh[0] - ol[0]) + (oh[1] - ol[1]) + (oh[2] - ol[2]), -16);
+        for (int r = 0; r < 3; r++) {
+            obj6[(size_t)k * 6 + r] = nextafterf((float)(ol[r] - opad), -INFINITY);
+            obj6[(size_t)k * 6 + 3 + r] = nextafterf((float)(oh[r] + opad), INFINITY);
+        }
+        const double pad = ldexp(mag + (wh[0] - wl[0]) + (wh[1] - wl[1]) + (wh[2] - wl[2]), -16);
+        lo[k] = make_float4(nextafterf((float)(wl[0] - pad), -INFINITY), nextafterf((float)(wl[1] - pad), -INFINITY),
+                            nextafterf((float)(wl[2] - pad), -INFINITY), 0.f);
+        hi[k] = make_float4(nextafterf((float)(wh[0] + pad), INFINITY), nextafterf((float)(wh[1] + pad), INFINITY),
+                            nextafterf((float)(wh[2] + pad), INFINITY), 0.f);
+    }
+    return true;
+}
+
 // Per instance: the inverse transform (12 floats), the record the kernels
 // read (inverse as 3 float4, BLAS node / record pointers, tie-break id
-// base) and the padded world box of its BLAS.  False, with the error set,
-// on a bad instance.
+// base) and the padded world box of its geometry.  False, with the error
+// set, on a bad instance.
 static bool instance_data(const std::vector<CudaBVH_t>& blas, const RtInstance* inst, int ni, const char* who,
                           std::vector<float>& h_inv, std::vector<float4>& rec, std::vector<float4>& lo,
                           std::vector<float4>& hi) {
     const int nb = (int)blas.size();
     h_inv.assign((size_t)ni * 12, 0.f);
     rec.assign((size_t)ni * INST_F4, make_float4(0.f, 0.f, 0.f, 0.f));
-    lo.resize(ni);
-    hi.resize(ni);
     unsigned long long id_base = 0;
     for (int k = 0; k < ni; k++) {
         const RtInstance& I = inst[k];
@@ -463,23 +702,6 @@ static bool instance_data(const std::vector<CudaBVH_t>& blas, const RtInstance* 
         float* fi = &h_inv[(size_t)k * 12];
         for (int j = 0; j < 12; j++) fi[j] = (float)inv[j];
         const CudaBVHHandle* b = blas[I.blas];
-        double wl[3] = {1e300, 1e300, 1e300}, wh[3] = {-1e300, -1e300, -1e300}, mag = 0.0;
-        for (int c = 0; c < 8; c++) {
-            const double p[3] = {(c & 1) ? b->bmax[0] : b->bmin[0], (c & 2) ? b->bmax[1] : b->bmin[1],
-                                 (c & 4) ? b->bmax[2] : b->bmin[2]};
-            for (int r = 0; r < 3; r++) {
-                const double v = I.xform[r * 4] * p[0] + I.xform[r * 4 + 1] * p[1] + I.xform[r * 4 + 2] * p[2] +
-                                 I.xform[r * 4 + 3];
-                wl[r] = std::min(wl[r], v);
-                wh[r] = std::max(wh[r], v);
-                mag = std::max(mag, fabs(v));
-            }
-        }
-        const double pad = ldexp(mag + (wh[0] - wl[0]) + (wh[1] - wl[1]) + (wh[2] - wl[2]), -16);
-        lo[k] = make_float4(nextafterf((float)(wl[0] - pad), -INFINITY), nextafterf((float)(wl[1] - pad), -INFINITY),
-                            nextafterf((float)(wl[2] - pad), -INFINITY), 0.f);
-        hi[k] = make_float4(nextafterf((float)(wh[0] + pad), INFINITY), nextafterf((float)(wh[1] + pad), INFINITY),
-                            nextafterf((float)(wh[2] + pad), INFINITY), 0.f);
         const unsigned long long np = (unsigned long long)b->bvh8.nodes.p, tp = (unsigned long long)b->bvh8.tris.p;
         rec[(size_t)k * INST_F4 + 0] = make_float4(fi[0], fi[1], fi[2], fi[3]);
         rec[(size_t)k * INST_F4 + 1] = make_float4(fi[4], fi[5], fi[6], fi[7]);
@@ -492,6 +714,16 @@ static bool instance_data(const std::vector<CudaBVH_t>& blas, const RtInstance* 
     if (id_base >= 0xFFFFFFFFull) {
         set_error("%s: %llu instance primitives exceed the 32-bit tie-break id", who, id_base);
         return false;
+    }
+    std::vector<float> obj6;
+    if (!instance_bounds(blas, inst, ni, lo, hi, obj6)) return false;
+    for (int k = 0; k < ni; k++) {
+        const float* o = &obj6[(size_t)k * 6];
+        float4& w4 = rec[(size_t)k * INST_F4 + 4];
+        w4.y = o[0];
+        w4.z = o[1];
+        w4.w = o[2];
+        rec[(size_t)k * INST_F4 + 5] = make_float4(o[3], o[4], o[5], 0.f);
     }
     return true;
 }
