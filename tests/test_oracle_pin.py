@@ -7,7 +7,8 @@
 * cudaBVH_buildTLASFast restatement == reference, same way.
 * The reference's stackless export leaves skip == -2 placeholders; the
   fixed export walks to the same result as brute force.
-* Traversal restatement == brute force Moller-Trumbore, bit for bit.
+* Traversal restatement == brute force Moller-Trumbore, bit for bit,
+  including the two-level walk on rays grazing rotated instances.
 * Philox4x32-10 == the Random123 known-answer vectors.
 """
 from pathlib import Path
@@ -17,6 +18,7 @@ import pytest
 
 from oracle import oracle as O
 from rtb200 import philox, scenes
+from rtb200.scenes import HIT_DTYPE, RAY_DTYPE
 
 GOLD = Path(__file__).resolve().parent / "golden"
 
@@ -123,3 +125,88 @@ def test_philox_known_answers():
 def test_fp16_round_to_nearest():
     for x in [0.0, 1.0, 1.0009765625, 65504.0, 65520.0, 1e30, -1e30, 3.14159, -2.71828, 6e-8, 1e-10]:
         assert O.f2h(x) == int(np.array([x], np.float32).astype(np.float16).view(np.uint16)[0])
+
+
+def _object_rays(inv12, rays):
+    """Rays in an instance's space, every step one float32 rounding in the
+    kernels' order (left-to-right sums, layer/rt_ir_exec.cu:81-91)."""
+    m = np.asarray(inv12, np.float32).reshape(3, 4)
+    o, d = rays["org"], rays["dir"]
+    out = np.zeros(rays.shape[0], RAY_DTYPE)
+    for r in range(3):
+        a = (m[r, 0] * o[:, 0]).astype(np.float32) + (m[r, 1] * o[:, 1]).astype(np.float32)
+        a = a.astype(np.float32) + (m[r, 2] * o[:, 2]).astype(np.float32)
+        out["org"][:, r] = (a.astype(np.float32) + m[r, 3]).astype(np.float32)
+        b = (m[r, 0] * d[:, 0]).astype(np.float32) + (m[r, 1] * d[:, 1]).astype(np.float32)
+        out["dir"][:, r] = (b.astype(np.float32) + (m[r, 2] * d[:, 2]).astype(np.float32)).astype(np.float32)
+    out["tmin"], out["tmax"] = rays["tmin"], rays["tmax"]
+    return out
+
+
+def test_two_level_walk_equals_brute_force_on_grazing_rays():
+    """The oracle's two-level walk (restated stackless walk per BLAS, LBVH
+    over padded world boxes) finds exactly the brute-force hits over every
+    instance for rays grazing rotated floors and box faces: its box test
+    widens each slab by 2^-20 of the coordinates times |1/d|, since the fp32
+    triangle test accepts a grazing ray's hit a little outside the box."""
+    blas, xf, bidx, _, _ = scenes.instanced_scene(5, 24_000, nblas=3, ninst=10, world=60.0)
+    ninst = len(bidx)
+    inv = np.zeros((ninst, 12), np.float32)
+    for k in range(ninst):
+        M = xf[k].astype(np.float64)
+        A = np.linalg.inv(M[:, :3])
+        inv[k] = np.concatenate([A, (-A @ M[:, 3])[:, None]], 1).astype(np.float32).ravel()
+    rng = np.random.default_rng(11)
+    parts = []
+    for k in range(ninst):
+        v = blas[bidx[k]].reshape(-1, 3).astype(np.float64)
+        lo, hi = v.min(0), v.max(0)
+        M = xf[k].astype(np.float64)
+        m = 300
+        q = rng.uniform(lo, hi, (m, 3))
+        ax = rng.integers(0, 3, m)
+        q[np.arange(m), ax] = np.where(rng.random(m) < 0.5, lo[ax], hi[ax])
+        q[: m // 3, 1] = v[:6, 1].min()  # the floor's plane
+        dl = rng.normal(size=(m, 3))
+        dl[np.arange(m), ax] *= 1e-4
+        dl[: m // 3, 1] *= 1e-4
+        dl /= np.linalg.norm(dl, axis=1, keepdims=True)
+        wq, wd = q @ M[:, :3].T + M[:, 3], dl @ M[:, :3].T
+        wd /= np.linalg.norm(wd, axis=1, keepdims=True)
+        g = np.zeros(m, RAY_DTYPE)
+        g["org"], g["dir"], g["tmin"], g["tmax"] = wq - wd * 30.0, wd, 0.0, 1e30
+        parts.append(g)
+    rays = np.ascontiguousarray(np.concatenate(parts))
+    # the oracle's walk
+    obs = [O.OracleBVH(t, 32, 4) for t in blas]
+    node_off = np.cumsum([0] + [o.dfs.size // 8 for o in obs]).astype(np.int32)
+    tri_off = np.cumsum([0] + [o.packed.size // 12 for o in obs]).astype(np.int32)
+    bdfs, bpk = np.concatenate([o.dfs for o in obs]), np.concatenate([o.packed for o in obs])
+    wb = []
+    for k in range(ninst):
+        w = blas[bidx[k]].reshape(-1, 3).astype(np.float64) @ xf[k][:, :3].T.astype(np.float64) + xf[k][:, 3]
+        pad = 1e-4 * (np.abs(w).max() + 1)
+        wb.append(np.concatenate([w.min(0) - pad, w.max(0) + pad]))
+    tnodes, tord = O.tlas_fast(np.array(wb, np.float32))
+    tnodes = O.fix_skips(tnodes)
+    iblas = np.ascontiguousarray(bidx, np.int32)
+    hits = np.zeros(rays.shape[0], HIT_DTYPE)
+    inst = np.zeros(rays.shape[0], np.int32)
+    O.lib().orc_trace_closest_two_level(tnodes.ctypes.data, tnodes.size // 8, tord.ctypes.data, inv.ctypes.data,
+                                        iblas.ctypes.data, ninst, bdfs.ctypes.data, node_off.ctypes.data,
+                                        bpk.ctypes.data, tri_off.ctypes.data, rays.ctypes.data, rays.shape[0],
+                                        hits.ctypes.data, inst.ctypes.data, 0)
+    # brute force over every instance: least t, then least (instance base + primitive)
+    base = np.cumsum([0] + [blas[b].shape[0] for b in bidx])
+    bt = np.full(rays.shape[0], np.inf, np.float32)
+    bid = np.full(rays.shape[0], np.iinfo(np.int64).max, np.int64)
+    binst = np.full(rays.shape[0], -1)
+    for k in range(ninst):
+        h = O.brute_closest(blas[bidx[k]], _object_rays(inv[k], rays))
+        gid = base[k] + h["prim"].astype(np.int64)
+        better = (h["prim"] >= 0) & ((h["t"] < bt) | ((h["t"] == bt) & (gid < bid)))
+        bt[better], bid[better], binst[better] = h["t"][better], gid[better], k
+    got_t = np.where(hits["prim"] >= 0, hits["t"], np.float32(np.inf)).astype(np.float32)
+    assert (binst >= 0).mean() > 0.2
+    assert np.array_equal(inst, binst)
+    assert np.array_equal(got_t.view(np.uint32), bt.view(np.uint32))
