@@ -142,6 +142,7 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
     if (MID) s_prev[threadIdx.x] = -1;
     constexpr bool HELP =
         !COUNT && (ANY ? RTB_HELPERS >= 2 : RTB_HELPERS >= 1) && ((RTB_HELPERS_MODES >> MODE) & 1);
+    constexpr bool PACK = (ANY ? RTB_PACK_ANY : RTB_PACK_CLOSEST) != 0;  // packed f32x2 plane distances
     static_assert(!HELP || RTB_RAY_SMEM, "helper lanes read the owner's ray from shared memory");
     static_assert(!MID || (RTB_RAY_SMEM && RTB_TWO_SETS), "parked rays are read from shared memory by set tag");
     // helpers per owner lane (low 16 bits) | HELP_OVF when a helper's stack overflowed
@@ -350,7 +351,7 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
                 uint32_t nmask;
 #if RTB_TWO_SETS
                 uint32_t vb, vm;
-                visit_node(nodes + (size_t)ni * 5, r, thit, nmask, vb, vm, w.ng, s_oct_perm);
+                visit_node<RTB_SLOTMASK, PACK>(nodes + (size_t)ni * 5, r, thit, nmask, vb, vm, w.ng, s_oct_perm);
                 if (MID) vb |= tag << 31;  // the set's ray slot
                 if (tmask == 0) {
                     tri_base = vb;
@@ -370,13 +371,13 @@ __global__ void __launch_bounds__(T, (ANY ? TRACE_MINB_ANY : TRACE_MINB) * TRACE
                 }
 #endif
 #else
-                visit_node(nodes + (size_t)ni * 5, r, thit, nmask, tri_base, tmask, w.ng, s_oct_perm);
+                visit_node<RTB_SLOTMASK, PACK>(nodes + (size_t)ni * 5, r, thit, nmask, tri_base, tmask, w.ng, s_oct_perm);
 #endif
 #if RTB_DUP_NODE
                 {
                     uint32_t nm2, tb2, tm2;
                     uint2 ng2;
-                    visit_node(nodes + (size_t)ni * 5, r, thit, nm2, tb2, tm2, ng2, s_oct_perm);
+                    visit_node<RTB_SLOTMASK, PACK>(nodes + (size_t)ni * 5, r, thit, nm2, tb2, tm2, ng2, s_oct_perm);
                     const uint32_t z = (uint32_t)(n >> 31);  // 0 for n >= 0, unknown at compile time
                     tmask |= tm2 & z;
                     tri_base |= tb2 & z;
