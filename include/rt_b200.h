@@ -159,7 +159,11 @@ typedef struct {
     int depth;              /* 8-wide levels */
     int max_leaf;
     int bins;
-    float build_ms;         /* device time of the build kernels */
+    float build_ms;         /* device time of the build kernels: the triangle
+                               boxes and the build's one graph launch (the
+                               host's graph capture and instantiation are not
+                               in it); with RTB200_BUILD=host, the span of the
+                               host-driven launches on the stream */
     float sah_cost;         /* SAH cost of the binary tree, normalised by root area */
     uint64_t node_bytes;    /* bytes of the 8-wide nodes */
     uint64_t tri_bytes;     /* bytes of the triangle records */
@@ -306,6 +310,7 @@ int rtBatch_autotune(RtBatch_t batch, const RtRay* d_rays, const int* d_ray_offs
 int rtBatch_setTuning(RtBatch_t batch, int ctas_per_sm, int node_iters);
 int rtBatch_setTuningEx(RtBatch_t batch, const RtBatchTuning* tuning);
 int rtBatch_getTuning(RtBatch_t batch, RtBatchTuning* out);
+/* build_ms: device time of the build kernels, as RtBuildStats.build_ms. */
 int rtBatch_getInfo(RtBatch_t batch, int* num_scenes, int* num_nodes, float* build_ms);
 /* Device arrays of the batch's 8-wide layout (scene i's root is node i;
  * triangle records carry scene-relative primitive ids), borrowed, valid

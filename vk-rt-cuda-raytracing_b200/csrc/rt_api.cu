@@ -135,11 +135,13 @@ bool build_into(CudaBVHHandle* h, cudaStream_t s) {
     const int n = h->num_tris;
     TmpBuf<float4> lo, hi;
     if (!lo.alloc(n, s) || !hi.alloc(n, s)) return false;
-    cudaEvent_t e0, e1;
+    cudaEvent_t e0, eb, e1;
     cudaEventCreate(&e0);
+    cudaEventCreate(&eb);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s);
     launch_tri_bounds(h->tris9.p, n, lo.p, hi.p, s);
+    cudaEventRecord(eb, s);
     const BuildConfig cfg = default_config();
     // one CUDA graph launch with device-side level loops (the host-driven
     // loop's times swing with the host thread's scheduling: 7.7 ms to 45 ms
@@ -148,14 +150,23 @@ bool build_into(CudaBVHHandle* h, cudaStream_t s) {
         const char* e = getenv("RTB200_BUILD");
         return (e && !strcmp(e, "host")) || !graph_build_supported();
     }();
+    GraphBuildInfo gi;
     bool ok = host_loop ? build_bvh2(lo.p, hi.p, n, cfg, h->bvh2, s) && collapse_bvh8(h->bvh2, h->tris9.p, h->bvh8, s)
-                        : build_bvh8_graph(lo.p, hi.p, h->tris9.p, n, cfg, std::vector<int>{0, n}, h->bvh8, s, nullptr,
+                        : build_bvh8_graph(lo.p, hi.p, h->tris9.p, n, cfg, std::vector<int>{0, n}, h->bvh8, s, &gi,
                                            &h->bvh2);
     cudaEventRecord(e1, s);
     if (ok) ok = RT_CUDA(cudaEventSynchronize(e1));
+    // device time of the build kernels: the triangle boxes and the graph
+    // launch (the host's capture and instantiation in between excluded); the
+    // host-driven loop's span on the stream
     float ms = 0.f;
-    if (ok) cudaEventElapsedTime(&ms, e0, e1);
+    if (ok && host_loop) cudaEventElapsedTime(&ms, e0, e1);
+    if (ok && !host_loop) {
+        cudaEventElapsedTime(&ms, e0, eb);
+        ms += gi.graph_ms;
+    }
     cudaEventDestroy(e0);
+    cudaEventDestroy(eb);
     cudaEventDestroy(e1);
     if (!ok) return false;
     Node2 root;

@@ -128,8 +128,9 @@ RtBatch_t rtBatch_buildEx(const CudaTri* h_tris, const int* tri_offsets, int num
     TmpBuf<float> tris9;
     TmpBuf<float4> lo, hi;
     Bvh2Device bvh2;
-    cudaEvent_t e0, e1;
+    cudaEvent_t e0, eb, e1;
     cudaEventCreate(&e0);
+    cudaEventCreate(&eb);
     cudaEventCreate(&e1);
     bool ok = tris9.alloc((size_t)n * 9, s) && b->d_tri_off.alloc(num_scenes + 1) && lo.alloc(n, s) && hi.alloc(n, s) &&
               b->work.alloc(2) && b->status.alloc(1) &&
@@ -140,18 +141,27 @@ RtBatch_t rtBatch_buildEx(const CudaTri* h_tris, const int* tri_offsets, int num
     if (ok) {
         cudaEventRecord(e0, s);
         launch_tri_bounds(tris9.p, n, lo.p, hi.p, s);
+        cudaEventRecord(eb, s);
         BuildConfig cfg = default_build_config();
         cfg.transient = true;
         b->graph_build = !(flags & RT_BATCH_BUILD_HOST_LOOP) && graph_build_supported();
+        GraphBuildInfo gi;
         if (b->graph_build)
-            ok = build_bvh8_graph(lo.p, hi.p, tris9.p, n, cfg, b->tri_off, b->bvh8, s, nullptr);
+            ok = build_bvh8_graph(lo.p, hi.p, tris9.p, n, cfg, b->tri_off, b->bvh8, s, &gi);
         else
             ok = build_bvh2(lo.p, hi.p, n, cfg, bvh2, s, &b->tri_off) && collapse_bvh8(bvh2, tris9.p, b->bvh8, s);
         cudaEventRecord(e1, s);
         ok = ok && RT_CUDA(cudaEventSynchronize(e1));
-        if (ok) cudaEventElapsedTime(&b->build_ms, e0, e1);
+        // device time: triangle boxes + the graph launch (capture and
+        // instantiation on the host excluded), or the host loop's span
+        if (ok && !b->graph_build) cudaEventElapsedTime(&b->build_ms, e0, e1);
+        if (ok && b->graph_build) {
+            cudaEventElapsedTime(&b->build_ms, e0, eb);
+            b->build_ms += gi.graph_ms;
+        }
     }
     cudaEventDestroy(e0);
+    cudaEventDestroy(eb);
     cudaEventDestroy(e1);
     if (ok && getenv("RTB200_VALIDATE") && atoi(getenv("RTB200_VALIDATE")))
         ok = validate_bvh8(b->bvh8, b->bvh8.num_leaf_items, n, num_scenes);
