@@ -264,19 +264,23 @@ int cudaTLAS_getInverseTransforms(CudaTLAS_t tlas, float* out, int numInstances)
 /* ---------------- batched scenes ----------------
  * Many independent scenes built in one multi-scene SAH build (every build
  * stage is one launch for all scenes, all of it one CUDA graph) and traced
- * by one persistent work-stealing launch.  Triangles of scene i are tri_offsets[i] ..
+ * by one persistent work-stealing launch.  A batch of 8M triangles or more
+ * is built as two groups of whole scenes, one graph launch each, so the
+ * first group builds while the second group's triangles are uploaded
+ * (page-locked input: both copies queued at once); the groups merge into
+ * the one layout below.  RTB200_BATCH_GROUPS=<g> sets the group count.  Triangles of scene i are tri_offsets[i] ..
  * tri_offsets[i+1]-1 of h_tris; rays of scene i are d_ray_offsets[i] ..
  * d_ray_offsets[i+1]-1 (device array, num_scenes+1 entries), at most
  * 65,535 scenes per batch.  Reported primitive ids are relative to their
  * scene. */
 typedef struct RtBatchHandle* RtBatch_t;
 RtBatch_t rtBatch_build(const CudaTri* h_tris, const int* tri_offsets, int num_scenes, void* stream);
-/* rtBatch_build runs the whole build (SAH levels, small and warp subtrees,
- * 8-wide collapse) as ONE CUDA graph launch: both level loops are
+/* rtBatch_build runs each group's whole build (SAH levels, small and warp
+ * subtrees, 8-wide collapse) as ONE CUDA graph launch: both level loops are
  * conditional WHILE nodes whose counts stay on the device.  flags
  * RT_BATCH_BUILD_HOST_LOOP instead drives the same kernels from the host,
- * level by level (the single-scene builder's loop).  Both give the same
- * tree, byte for byte. */
+ * level by level (the single-scene builder's loop), over the same groups.
+ * Both give the same layout, byte for byte. */
 #define RT_BATCH_BUILD_HOST_LOOP 1
 RtBatch_t rtBatch_buildEx(const CudaTri* h_tris, const int* tri_offsets, int num_scenes, int flags, void* stream);
 void rtBatch_destroy(RtBatch_t batch);
@@ -311,6 +315,8 @@ int rtBatch_setTuning(RtBatch_t batch, int ctas_per_sm, int node_iters);
 int rtBatch_setTuningEx(RtBatch_t batch, const RtBatchTuning* tuning);
 int rtBatch_getTuning(RtBatch_t batch, RtBatchTuning* out);
 /* build_ms: device time of the build kernels, as RtBuildStats.build_ms. */
+/* build_ms: device time of the build kernels (every group's triangle boxes
+ * and graph launch, and the merge), as RtBuildStats.build_ms. */
 int rtBatch_getInfo(RtBatch_t batch, int* num_scenes, int* num_nodes, float* build_ms);
 /* Device arrays of the batch's 8-wide layout (scene i's root is node i;
  * triangle records carry scene-relative primitive ids), borrowed, valid

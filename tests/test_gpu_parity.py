@@ -209,13 +209,11 @@ def test_exports_are_valid_bvhs(cuda, small_scene):
 
 
 def _d2h(ptr, nbytes):
-    import ctypes as C
-    import torch
-    torch.cuda.synchronize()
-    out = np.zeros(nbytes, np.uint8)
-    rt = C.CDLL("libcudart.so.12")
-    rt.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
-    assert rt.cudaMemcpy(out.ctypes.data, ptr, nbytes, 2) == 0
+    """Device bytes to a host array (a synchronous copy, after all queued work)."""
+    from cuda.bindings import runtime as cudart
+    out = np.empty(nbytes, np.uint8)
+    (err,) = cudart.cudaMemcpy(out.ctypes.data, ptr, nbytes, cudart.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+    assert err == cudart.cudaError_t.cudaSuccess, err
     return out
 
 
@@ -466,14 +464,6 @@ def test_tlas_set_transforms_equals_a_fresh_build(cuda):
         moved.close()
 
 
-def _d2h(ptr, nbytes):
-    from cuda.bindings import runtime as cudart
-    out = np.empty(nbytes, np.uint8)
-    (err,) = cudart.cudaMemcpy(out.ctypes.data, ptr, nbytes, cudart.cudaMemcpyKind.cudaMemcpyDeviceToHost)
-    assert err == cudart.cudaError_t.cudaSuccess, err
-    return out
-
-
 def test_host_traces_over_replicas_equal_one_handle(cuda):
     """cudaBVH_traceClosestHostMulti / AnyHostMulti: a host batch split over
     replicas (here several handles on the one GPU of this box, each with its
@@ -577,12 +567,16 @@ def test_path_tracer_vs_fp64_oracle(cuda):
     assert torch.equal(d_rgb, d2)
 
 
-def test_batched_graph_build_equals_host_loop_build(cuda):
+@pytest.mark.parametrize("groups", ["1", "3"])
+def test_batched_graph_build_equals_host_loop_build(cuda, monkeypatch, groups):
     """rtBatch_build's one-graph build (level loops as conditional WHILE
     nodes, counts kept on the device) writes the same 8-wide nodes and
     triangle records, byte for byte, as the host-driven level loop, on
     scenes of 1 to 60,000 triangles (leaf roots, small-task roots and deep
-    large-task levels)."""
+    large-task levels); also when both build the scenes in three groups and
+    merge them into one layout (structure checked in the build)."""
+    monkeypatch.setenv("RTB200_BATCH_GROUPS", groups)
+    monkeypatch.setenv("RTB200_VALIDATE", "1")
     sizes = [1, 2, 3, 700, 1024, 1025, 60000, 5000, 30000, 9]
     tris = [scenes.scene_meshes(300 + i, n, box=30.0, lo=min(n, 100), hi=max(min(n, 4000), 100), ground=False)
             if n > 3 else np.array([[0, 0, 0, 1, 0, 0, 0, 1, 0]] * n, np.float32) + np.float32(i)
@@ -601,11 +595,14 @@ def test_batched_graph_build_equals_host_loop_build(cuda):
     assert np.array_equal(gb, hb), "triangle records differ"
 
 
-def test_batched_scenes_equal_per_scene_calls(cuda):
+@pytest.mark.parametrize("groups", ["1", "4"])
+def test_batched_scenes_equal_per_scene_calls(cuda, monkeypatch, groups):
     """rtBatch_*: one multi-scene build and one persistent launch (plain and
     replayed from a CUDA graph) give exactly the per-scene results,
-    including a 1-triangle scene and scenes without rays."""
+    including a 1-triangle scene and scenes without rays; the same when the
+    scenes are built in four groups and merged."""
     import torch
+    monkeypatch.setenv("RTB200_BATCH_GROUPS", groups)
     sizes = [1, 3, 250, 5000, 20000, 777, 40000, 12]
     tris = [scenes.scene_meshes(100 + i, n, box=30.0, lo=min(n, 100), hi=max(min(n, 2000), 100), ground=False)
             if n > 2 else np.array([[0, 0, 0, 1, 0, 0, 0, 1, 0]] * n, np.float32) + np.float32(i)
@@ -651,6 +648,49 @@ def test_batched_scenes_equal_per_scene_calls(cuda):
         b.graph(d_rays, d_off, n, d_y)
         torch.cuda.synchronize()
         assert torch.equal(d_x, d_h) and torch.equal(d_y, d_h), shape
+
+
+def test_grouped_batch_build_pinned_and_pageable(cuda, monkeypatch):
+    """A batch built in two scene groups whose builds overlap the upload:
+    from page-locked input (every group's copy queued at once) and from
+    pageable input (each copy issued after the previous group's build was
+    launched) the layout is the same byte for byte, and its closest and any
+    hits equal those of one build over all scenes on every ray."""
+    import torch
+    sizes = [40000, 3, 25000, 1, 60000, 800, 15000, 5000]
+    tris = [scenes.scene_meshes(500 + i, k, box=30.0, lo=min(k, 100), hi=max(min(k, 4000), 100), ground=False)
+            if k > 3 else np.array([[0, 0, 0, 1, 0, 0, 0, 1, 0]] * k, np.float32) + np.float32(i)
+            for i, k in enumerate(sizes)]
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    pageable = np.concatenate(tris)
+    pin = torch.empty(pageable.nbytes, dtype=torch.uint8, pin_memory=True)
+    pinned = pin.numpy().view(np.float32).reshape(-1, 9)
+    pinned[:] = pageable
+    nr = [4000, 500, 3000, 100, 6000, 1000, 2000, 1500]
+    rays = np.concatenate([scenes.random_rays(600 + i, k, box=40.0) for i, k in enumerate(nr)])
+    roff = np.concatenate([[0], np.cumsum(nr)]).astype(np.int32)
+    d_rays, d_off, n = _dev(torch, rays), torch.from_numpy(roff).cuda(), rays.shape[0]
+    monkeypatch.setenv("RTB200_VALIDATE", "1")
+    layouts, hits, occ = [], [], []
+    for groups, src in (("2", pinned), ("2", pageable), ("1", pageable)):
+        monkeypatch.setenv("RTB200_BATCH_GROUPS", groups)
+        b = lib.Batch(all_tris=src, tri_offsets=off)
+        try:
+            pn, n_nodes, pt, n_recs = b.layout()
+            layouts.append((_d2h(pn, n_nodes * 80), _d2h(pt, n_recs * 48)))
+            d_h = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
+            d_o = torch.empty(n, dtype=torch.uint8, device="cuda")
+            b.closest(d_rays, d_off, n, d_h)
+            b.any(d_rays, d_off, n, d_o)
+            torch.cuda.synchronize()
+            hits.append(d_h.cpu().numpy())
+            occ.append(d_o.cpu().numpy())
+        finally:
+            b.close()
+    assert np.array_equal(layouts[0][0], layouts[1][0]) and np.array_equal(layouts[0][1], layouts[1][1])
+    assert layouts[0][0].size == layouts[2][0].size  # the same nodes, in another order
+    assert (hits[0].view(HIT_DTYPE)["prim"] >= 0).mean() > 0.05
+    assert np.array_equal(hits[0], hits[2]) and np.array_equal(occ[0], occ[2])
 
 
 def test_pipelined_host_calls_equal_device_calls(cuda):

@@ -78,7 +78,10 @@ cudaMemPool_t scratch_pool() {
             return nullptr;
         }
         const char* e = getenv("RTB200_POOL_KEEP_MB");
-        uint64_t keep = (uint64_t)(e ? std::max(0, atoi(e)) : 8192) << 20;
+        // at most what the builds used is ever kept; 32 GB holds the whole
+        // peak of a 22M-triangle batch built in two groups (about 8.5 GB),
+        // whose re-mapping above an 8 GB limit cost 3-4 ms per build
+        uint64_t keep = (uint64_t)(e ? std::max(0, atoi(e)) : 32768) << 20;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
         pools[dev] = pool;
     }

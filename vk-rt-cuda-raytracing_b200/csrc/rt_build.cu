@@ -1673,6 +1673,23 @@ bool graph_build_supported() {
 bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tris9, int n, const BuildConfig& cfg,
                       const std::vector<int>& seg, Bvh8Device& out, cudaStream_t s, GraphBuildInfo* info,
                       Bvh2Device* keep) {
+    GraphBuildJob job;
+    return launch_bvh8_graph(d_lo, d_hi, d_tris9, n, cfg, seg, out, s, job, keep) && finish_bvh8_graph(job, info);
+}
+
+// A build's segment table from absolute offsets already on the device.
+__global__ void k_seg_rebase(const int* __restrict__ src, int count, int base, int* __restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) dst[i] = src[i] - base;
+}
+
+bool launch_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tris9, int n, const BuildConfig& cfg,
+                       const std::vector<int>& seg, Bvh8Device& out, cudaStream_t s, GraphBuildJob& job,
+                       Bvh2Device* keep, const int* d_seg, int seg_base) {
+    if (job.launched) {
+        set_error("graph build: job already launched");
+        return false;
+    }
     if (n <= 0 || !d_tris9) {
         set_error("graph build: empty input");
         return false;
@@ -1710,7 +1727,8 @@ bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tri
     const int scan_cap = std::max(std::max(maxT, Cb), std::max(Kb, maxSmall));
     const size_t cbytes = collapse_graph_scratch_bytes(n, S, slots, true);
     TmpBuf<Node2> tnodes;
-    TmpBuf<int> tperm, tmp, dseg, ccount, coff, cleft, cleftoff, flags, need, off, scan, result;
+    TmpBuf<int> tperm, tmp, dseg, ccount, coff, cleft, cleftoff, flags, need, off, scan;
+    TmpBuf<int>& result = job.result;
     TmpBuf<uint32_t> acc, gbins, kcb;
     TmpBuf<Task> tasks_a, tasks_b, kids, small;
     TmpBuf<Split> splits;
@@ -1733,8 +1751,15 @@ bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tri
         (wq_cap > 0 && !wq.alloc(wq_cap, s)) || !ctl.alloc(1, s) || !scan.alloc(scan_scratch_ints(scan_cap), s) ||
         !result.alloc(8, s) || !cscratch.alloc(cbytes, s))
         return false;
-    if (!out.nodes.alloc((size_t)n + S) || !out.tris.alloc(n)) return false;
-    if (!RT_CUDA(cudaMemcpyAsync(dseg.p, seg.data(), sizeof(int) * (S + 1), cudaMemcpyHostToDevice, s))) return false;
+    // the output: a caller's buffers when large enough (pooled group
+    // outputs of a batch build), else allocated here
+    if (!out.nodes.ensure((size_t)n + S) || !out.tris.ensure(n)) return false;
+    if (d_seg) {
+        k_seg_rebase<<<(S + 1 + 255) / 256, 256, 0, s>>>(d_seg, S + 1, seg_base, dseg.p);
+        if (!RT_CUDA(cudaGetLastError())) return false;
+    } else if (!RT_CUDA(cudaMemcpyAsync(dseg.p, seg.data(), sizeof(int) * (S + 1), cudaMemcpyHostToDevice, s))) {
+        return false;
+    }
     const size_t smem = (size_t)cfg.small_task * (6 * 4 + 4 + 2 + 2) + 16 + 3 * kBins * 7 * 4;
     if (!RT_CUDA(cudaFuncSetAttribute(k_build_small_loop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
         return false;
@@ -1753,7 +1778,6 @@ bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tri
         return false;
     }
     cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
     bool ok = RT_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed));
     bool capturing = ok;
     BuildCtl* c = ctl.p;
@@ -1832,28 +1856,38 @@ bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tri
         cudaStreamEndCapture(cs, &g);
         if (g) cudaGraphDestroy(g);
     }
-    int h[8] = {};
-    if (ok) {
-        cudaEvent_t e0 = nullptr, e1 = nullptr;
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
-        ok = RT_CUDA(cudaGraphInstantiate(&exec, graph, 0)) && RT_CUDA(cudaEventRecord(e0, s)) &&
-             RT_CUDA(cudaGraphLaunch(exec, s)) && RT_CUDA(cudaEventRecord(e1, s)) &&
-             RT_CUDA(cudaMemcpyAsync(h, result.p, sizeof(h), cudaMemcpyDeviceToHost, s)) &&
-             RT_CUDA(cudaStreamSynchronize(s));
-        if (ok && info) {
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            info->graph_ms = ms;
-        }
-        if (e0) cudaEventDestroy(e0);
-        if (e1) cudaEventDestroy(e1);
-    }
-    if (exec) cudaGraphExecDestroy(exec);
+    if (ok)
+        ok = RT_CUDA(cudaEventCreate(&job.e0)) && RT_CUDA(cudaEventCreate(&job.e1)) &&
+             RT_CUDA(cudaGraphInstantiate(&job.exec, graph, 0)) && RT_CUDA(cudaEventRecord(job.e0, s)) &&
+             RT_CUDA(cudaGraphLaunch(job.exec, s)) && RT_CUDA(cudaEventRecord(job.e1, s));
     if (graph) cudaGraphDestroy(graph);
     cudaStreamDestroy(bs);
     cudaStreamDestroy(cs);
     if (!ok) return false;
+    job.s = s;
+    job.n = n;
+    job.S = S;
+    job.out = &out;
+    job.keep = keep;
+    job.launched = true;
+    return true;
+}
+
+bool finish_bvh8_graph(GraphBuildJob& job, GraphBuildInfo* info) {
+    if (!job.launched) {
+        set_error("graph build: nothing launched");
+        return false;
+    }
+    job.launched = false;
+    int h[8] = {};
+    if (!RT_CUDA(cudaMemcpyAsync(h, job.result.p, sizeof(h), cudaMemcpyDeviceToHost, job.s)) ||
+        !RT_CUDA(cudaStreamSynchronize(job.s)))
+        return false;
+    if (info) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, job.e0, job.e1);
+        info->graph_ms = ms;
+    }
     if (h[1]) {
         set_error("graph build: %s", (h[1] & 16) ? "more levels than the bound"
                                      : (h[1] & 8) ? "task list overflow"
@@ -1865,6 +1899,9 @@ bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tri
         set_error("collapse: %s", (h[7] & 1) ? "capacity exceeded" : "more levels than the bound");
         return false;
     }
+    Bvh8Device& out = *job.out;
+    Bvh2Device* keep = job.keep;
+    const int n = job.n, S = job.S;
     out.num_nodes = h[4];
     out.num_leaf_items = h[5];
     out.depth = h[6];

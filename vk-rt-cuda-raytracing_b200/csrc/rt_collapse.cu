@@ -514,11 +514,12 @@ bool collapse_bvh8(const Bvh2Device& b2, const float* d_tris9, Bvh8Device& out, 
     // upper bound on 8-wide nodes: every node has >= 2 children except a
     // root that is a single leaf, so nodes <= leaves + roots <= n + R
     const int max_nodes = n + R;
-    if (!out.nodes.alloc(max_nodes)) return false;
+    // the output: a caller's buffers when large enough, else allocated here
+    if (!out.nodes.ensure(max_nodes)) return false;
     if (d_tris9) {
-        if (!out.tris.alloc(n)) return false;
+        if (!out.tris.ensure(n)) return false;
     } else {
-        if (!out.leaf_ids.alloc(n)) return false;
+        if (!out.leaf_ids.ensure(n)) return false;
     }
     TmpBuf<int> lvl_a, lvl_b, n_inner, n_items, inner_off, item_off, tot;
     TmpBuf<Gather> gat;

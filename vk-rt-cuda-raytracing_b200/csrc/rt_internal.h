@@ -89,7 +89,7 @@ struct DevBuf {
 // with cudaMalloc/cudaFree maps and unmaps pages on every build, and every
 // cudaFree waits for the whole device, so the build's timeline fills with
 // idle gaps.  Scratch comes instead from one pool per device that keeps up to
-// `RTB200_POOL_KEEP_MB` (default 8192) MB of freed memory for the next
+// `RTB200_POOL_KEEP_MB` (default 32768) MB of freed memory for the next
 // build; allocation and release are ordered on the build's stream.
 cudaMemPool_t scratch_pool();
 
@@ -232,6 +232,37 @@ bool graph_build_supported();
 bool build_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tris9, int n, const BuildConfig& cfg,
                       const std::vector<int>& segments, Bvh8Device& out, cudaStream_t s, GraphBuildInfo* info,
                       Bvh2Device* keep = nullptr);
+// The same build in two halves, so a caller can capture and launch the next
+// build while this one runs: launch_bvh8_graph allocates, captures,
+// instantiates and launches on s without waiting (its scratch is released in
+// stream order after the graph); finish_bvh8_graph waits for s, reads the
+// device counts into `out` (and keep) and checks the build's status.
+struct GraphBuildJob {
+    TmpBuf<int> result;  // the device counts finish_bvh8_graph reads
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;  // around the graph launch
+    cudaGraphExec_t exec = nullptr;
+    int n = 0, S = 0;
+    Bvh8Device* out = nullptr;
+    Bvh2Device* keep = nullptr;
+    bool launched = false;
+    GraphBuildJob() = default;
+    GraphBuildJob(const GraphBuildJob&) = delete;
+    GraphBuildJob& operator=(const GraphBuildJob&) = delete;
+    ~GraphBuildJob() {
+        // an executable graph destroyed while in flight is freed when it completes
+        if (exec) cudaGraphExecDestroy(exec);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    }
+};
+// d_seg (optional): the segment table already on the device, as absolute
+// offsets less seg_base (so nothing is copied from pageable host memory,
+// which could wait for the work queued on s).
+bool launch_bvh8_graph(const float4* d_lo, const float4* d_hi, const float* d_tris9, int n, const BuildConfig& cfg,
+                       const std::vector<int>& segments, Bvh8Device& out, cudaStream_t s, GraphBuildJob& job,
+                       Bvh2Device* keep = nullptr, const int* d_seg = nullptr, int seg_base = 0);
+bool finish_bvh8_graph(GraphBuildJob& job, GraphBuildInfo* info);
 
 // Capture helpers for the graph-driven build: a conditional handle on the
 // graph being captured on cs, and a WHILE node on it at the capture
