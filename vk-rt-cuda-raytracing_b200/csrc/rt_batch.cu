@@ -193,8 +193,9 @@ RtBatch_t rtBatch_buildEx(const CudaTri* h_tris, const int* tri_offsets, int num
     // page-locked input: every group's copy is queued at once; otherwise a
     // group's copy is issued after the previous group's build is launched
     cudaPointerAttributes pa{};
-    const bool pinned = cudaPointerGetAttributes(&pa, h_tris) == cudaSuccess && pa.type == cudaMemoryTypeHost;
-    cudaGetLastError();
+    const cudaError_t pe = cudaPointerGetAttributes(&pa, h_tris);
+    if (pe != cudaSuccess) cudaGetLastError();  // clear only this query's own failure
+    const bool pinned = pe == cudaSuccess && pa.type == cudaMemoryTypeHost;
     // the input triangles and the binary trees are needed only while building:
     // pooled scratch, gone when the build returns
     TmpBuf<float> tris9;
