@@ -189,6 +189,14 @@ int cudaBVH_traceCounters(CudaBVH_t bvh, const RtRay* d_rays, int n, int any, ui
  * and the library stays usable.  Process-wide. */
 int rtDebug_failAllocations(int after);
 
+/* Inspection helper, no counterpart in the reference: the scene groups
+ * rtBatch_build would use for these offsets (RTB200_BATCH_GROUPS honoured).
+ * Writes the group count + 1 boundaries (scene indices, first 0, last
+ * num_scenes) to out_bounds, which holds max_groups + 1 entries, and returns
+ * the group count; RT_ERR_INVALID on bad arguments.  Host only: no device
+ * work. */
+int rtDebug_batchGroups(const int* tri_offsets, int num_scenes, int* out_bounds, int max_groups);
+
 /* Measurement helper, no counterpart in the reference: read bandwidth of
  * this GPU in GB/s, streaming a `bytes` buffer (allocated and freed by the
  * call) `reps` times in one launch with 16-byte loads cached in L2 only,

@@ -319,6 +319,25 @@ RtBatch_t rtBatch_buildEx(const CudaTri* h_tris, const int* tri_offsets, int num
     return b;
 }
 
+int rtDebug_batchGroups(const int* tri_offsets, int num_scenes, int* out_bounds, int max_groups) {
+    if (!tri_offsets || !out_bounds || num_scenes <= 0 || max_groups < 1 || tri_offsets[0] != 0) {
+        set_error("rtDebug_batchGroups: invalid argument");
+        return RT_ERR_INVALID;
+    }
+    for (int i = 0; i < num_scenes; i++)
+        if (tri_offsets[i + 1] <= tri_offsets[i]) {
+            set_error("rtDebug_batchGroups: scene %d has no triangles", i);
+            return RT_ERR_INVALID;
+        }
+    const std::vector<int> g = scene_groups(std::vector<int>(tri_offsets, tri_offsets + num_scenes + 1), num_scenes);
+    if ((int)g.size() - 1 > max_groups) {
+        set_error("rtDebug_batchGroups: %d groups, room for %d", (int)g.size() - 1, max_groups);
+        return RT_ERR_INVALID;
+    }
+    std::copy(g.begin(), g.end(), out_bounds);
+    return (int)g.size() - 1;
+}
+
 RtBatch_t rtBatch_build(const CudaTri* h_tris, const int* tri_offsets, int num_scenes, void* stream) {
     return rtBatch_buildEx(h_tris, tri_offsets, num_scenes, 0, stream);
 }

@@ -148,6 +148,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "rtPT_setQueueCapacity": (i32, [vp, C.c_int64]),
         "rtPT_autotune": (i32, [vp, C.POINTER(RtCamera), C.POINTER(RtPTParams), vp, vp, C.POINTER(C.c_int64)]),
         "rtDebug_failAllocations": (i32, [i32]),
+        "rtDebug_batchGroups": (i32, [vp, i32, vp, i32]),
         "rtProbe_readBandwidth": (i32, [C.c_uint64, i32, C.POINTER(f32)]),
         "cudaBVH_validate": (i32, [vp]),
         "cudaBVH_getBuildStats": (i32, [vp, C.POINTER(RtBuildStats)]),
@@ -223,6 +224,17 @@ def read_bandwidth_gbs(nbytes: int, reps: int = 20) -> float:
     v = C.c_float()
     _check(load().rtProbe_readBandwidth(nbytes, reps, C.byref(v)), "rtProbe_readBandwidth")
     return float(v.value)
+
+
+def batch_groups(tri_offsets) -> list[int]:
+    """Scene-group boundaries rtBatch_build would use for these triangle
+    offsets (rtDebug_batchGroups; host only)."""
+    off = np.ascontiguousarray(tri_offsets, np.int32)
+    out = np.zeros(9, np.int32)
+    g = load().rtDebug_batchGroups(off.ctypes.data, len(off) - 1, out.ctypes.data, 8)
+    if g < 0:
+        raise RtError(f"rtDebug_batchGroups: {last_error()}")
+    return out[:g + 1].tolist()
 
 
 def last_error() -> str:
