@@ -400,8 +400,9 @@ void rtPT_destroy(RtPathTracer_t pt);
 int rtPT_cameraBasis(const RtCamera* cam, int width, int height, float* out14);
 
 /* ---- Geometry from the application's buffers, refit, blobs ---------------
- * Survey "next" rows: the reference layer reads every BLAS's vertex and index
- * buffers back to the host and rebuilds a triangle soup there
+ * The callers on either side of the build: the reference layer reads every
+ * BLAS's vertex and index buffers back to the host and rebuilds a triangle
+ * soup there
  * (layer/VkLayer_CudaRT.cpp:2961-2981, 3087-3125); refit and a versioned BVH
  * blob have no counterpart in the reference. */
 #define RT_VERTEX_FLOAT3 0   /* 3 x fp32 per vertex (VK_FORMAT_R32G32B32_SFLOAT) */
